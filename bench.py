@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""QSketch insert/query throughput on B200 — one JSON line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config zipf|uniform]
+
+A step is one pass of the hot path over one batch of synthetic input: clear the sketch,
+insert the whole key stream, query the distinct keys.  The default workload is the
+Zipf-skewed stream (2^27 keys, Zipf s=1.1 over 2^24 ranks, 64 MB low table, 16 MB high
+pool, query the 2^24 distinct keys); `--config uniform` is the 2^24-key uniform case.
+For N > 1 (torchrun, one process per GPU) every rank runs its own sketch over its own
+seeded stream: the path has no data exchange, so this is weak scaling with no collective
+on the data path.  `--impl reference` times the CPU restatement of the reference path
+(oracle/, bucket-partitioned threads) on the host cores, rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "insert/query Gkeys/s on 1 B200; avg rel. error learned vs plain at equal bytes"
+SEED = 2654435769  # odd multiplier in the reference's seed range [1, 2^32-1]
+
+CONFIGS = {
+    "zipf": dict(workload="zipf1.1_2^27keys_2^24ranks_low64MB_high16MB_query2^24", kind=1, n_keys=1 << 27,
+                 n_ranks=1 << 24, s=1.1, n_low=2097143, n_high=1 << 17, n_query=1 << 24),
+    "uniform": dict(workload="uniform_2^24keys_nlow262139_high8MB_query2^24", kind=0, n_keys=1 << 24, n_ranks=0,
+                    s=0.0, n_low=262139, n_high=1 << 16, n_query=1 << 24),
+}
+INSERT_BYTES_PER_KEY = 68  # 4 B key + 32 B bucket sector read + 32 B write-back
+QUERY_BYTES_PER_KEY = 40   # 4 B key + 32 B bucket sector + 4 B result
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """Samples nvidia-smi during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = str(index)
+        self.p = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.p = None
+        return self
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9 or f[0] != self.index:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != gpus and world > 1:
+        raise SystemExit(f"--gpus {gpus} but WORLD_SIZE={world}")
+    return world, rank, local
+
+
+def run_ours(args, cfg):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import qsketch_b200 as qs
+    from qsketch_b200 import data
+
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    stream = torch.cuda.current_stream()
+    seed = 1000 + rank
+    perm_seed = 99 + 7919 * rank
+    if cfg["kind"] == 1:
+        keys, ranks = data.zipf_keys(cfg["n_keys"], cfg["n_ranks"], cfg["s"], seed=seed, perm_seed=perm_seed,
+                                     with_ranks=True)
+        queries = data.rank_keys(perm_seed, 0, cfg["n_query"])
+        exact = data.rank_histogram(ranks, cfg["n_ranks"])[:cfg["n_query"]].contiguous()
+        del ranks
+    else:
+        keys = data.uniform_keys(cfg["n_keys"], seed=seed)
+        queries = keys[:cfg["n_query"]]
+        exact = None
+    out = torch.empty(cfg["n_query"], dtype=torch.uint32, device="cuda")
+    sk = qs.Sketch_GPU_Sub_Warp_Level(cfg["n_low"], 8, cfg["n_high"], 32, hash_seed=SEED, mask_rng=1)
+    n_ins, n_q = cfg["n_keys"], cfg["n_query"]
+
+    def step(ev=None):
+        sk.clear()
+        if ev:
+            ev[0].record(stream)
+        sk.insert(keys)
+        if ev:
+            ev[1].record(stream)
+        sk.search(queries, counts=out)
+        if ev:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sk.sync()
+    prof0 = sk.profile()
+    launches0 = prof0["insert_launches"] + prof0["repair_launches"] + prof0["query_launches"]
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for i in range(args.steps):
+            step(evs[i])
+        t1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    total_ms = max_over_ranks(t0.elapsed_time(t1))
+    ins_ms = max_over_ranks(sum(e[0].elapsed_time(e[1]) for e in evs) / args.steps)
+    q_ms = max_over_ranks(sum(e[1].elapsed_time(e[2]) for e in evs) / args.steps)
+    sk.sync()
+    prof1 = sk.profile()
+    launches = prof1["insert_launches"] + prof1["repair_launches"] + prof1["query_launches"] - launches0
+    ms_per_step = total_ms / args.steps
+    value = world * (n_ins + n_q) / (ms_per_step * 1e6)
+
+    # accuracy of the plain sketch against exact counts
+    rel = ratio = None
+    if exact is not None:
+        rel, ratio = data.error_metrics(out, exact)
+
+    # one instrumented step: per-launch CUDA events inside the library, for the roofline
+    sk.set_profiling(True)
+    step()
+    torch.cuda.synchronize()
+    prof = sk.profile()
+    sk.set_profiling(False)
+    hbm, peak_kind = peaks()
+    kern = {"insert": (prof["insert_ms"], prof["insert_timed"], n_ins, INSERT_BYTES_PER_KEY),
+            "query": (prof["query_ms"], prof["query_timed"], n_q, QUERY_BYTES_PER_KEY)}
+    dom = max(kern, key=lambda k: kern[k][0])
+    ms_k, launches_k, units, bpu = kern[dom]
+    per_launch_units = units / max(1, launches_k)
+    avg_ms = ms_k / max(1, launches_k)
+    achieved = per_launch_units * bpu / (avg_ms * 1e-3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            tj = json.load(f)
+        k = tj.get(f"{args.config}:{dom}")
+        if k:
+            traffic = k["dram_bytes_per_unit"] * per_launch_units
+    atomic_peak = data.probe(0, max(64 << 20, cfg["n_low"] * 32), 1 << 26) if rank == 0 else None
+    ins_rate = per_launch_units / (avg_ms * 1e-3) if dom == "insert" else n_ins / (prof["insert_ms"] * 1e-3)
+
+    # end to end through the host-buffer C ABI calls: pinned keys in, counts out
+    hk = keys.cpu().pin_memory()
+    hq = queries.cpu().pin_memory()
+    ho = torch.empty(n_q, dtype=torch.uint32).pin_memory()
+    e2e_steps = max(1, min(args.steps, 5))
+    sk.clear()
+    sk.insert_host(hk)
+    sk.search_host(hq, ho)
+    torch.cuda.synchronize()
+    barrier()
+    w0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sk.clear()
+        sk.insert_host(hk)
+        sk.search_host(hq, ho)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks((time.perf_counter() - w0) * 1e3 / e2e_steps)
+    barrier()
+    assert torch.equal(ho.cuda(), out), "host-buffer query results differ from the device path"
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": "Gkeys/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic: seeded Zipf(s) ranks by rejection-inversion mapped to distinct u32 keys"
+                    if cfg["kind"] == 1 else "synthetic: seeded xorshift64* uniform u32 keys",
+            "config": {"workload": cfg["workload"], "n_keys": n_ins, "n_query": n_q, "n_low": cfg["n_low"],
+                       "n_high": cfg["n_high"], "hash_mask_ones": 3, "hash_mask_table_sz": 1021,
+                       "l2": "key stream of %d MB per step > 126 MB L2" % (n_ins * 4 >> 20),
+                       "parallelism": "independent sketch per GPU" if world > 1 else "single GPU"},
+            "insert_gkeys_per_s": round(world * n_ins / (ins_ms * 1e6), 4),
+            "query_gkeys_per_s": round(world * n_q / (q_ms * 1e6), 4),
+            "avg_rel_error": rel, "mean_est_over_exact": ratio,
+            "e2e": {"value": round(world * (n_ins + n_q) / (e2e_ms * 1e6), 4), "unit": "Gkeys/s",
+                    "h2d_bytes_per_step": (n_ins + n_q) * 4, "d2h_bytes_per_step": n_q * 4,
+                    "ms_per_step": round(e2e_ms, 3), "api": "qs_insert_host + qs_query_host"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "k_msws_insert" if dom == "insert" else "k_msws_query",
+                         "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_source": peak_kind,
+                         "bytes_per_unit": bpu, "units_per_launch": per_launch_units,
+                         "avg_launch_ms": round(avg_ms, 5)},
+            "atomic_roofline": {"kernel": "k_msws_insert", "achieved_gsectors": round(ins_rate / 1e9, 3),
+                                "peak_gsectors": round(atomic_peak / 1e9, 3) if atomic_peak else None,
+                                "frac": round(ins_rate / atomic_peak, 4) if atomic_peak else None,
+                                "probe": "random 32 B sectors, 3 red.add.u32 words per sector, sub-warp of 8"},
+            "kernel_ms_per_step": {"insert": round(prof["insert_ms"], 4), "repair": round(prof["repair_ms"], 4),
+                                   "query": round(prof["query_ms"], 4)},
+            "clocks": clk.summary(),
+        }
+        if args.cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(cfg, keys.cpu().numpy(), queries.cpu().numpy())
+        print(json.dumps(line), flush=True)
+    sk.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------
+def host_zipf_keys(n, n_ranks, s, seed):
+    """Bounded Zipf(s) over n_ranks by inverse CDF (numpy), ranks mapped by a seeded bijection."""
+    rng = np.random.default_rng(seed)
+    w = np.arange(1, n_ranks + 1, dtype=np.float64) ** (-s)
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    r = np.searchsorted(cdf, rng.random(n)).astype(np.uint32)
+    return r * np.uint32(2654435761) ^ np.uint32(0x5bd1e995), np.arange(n_ranks, dtype=np.uint32) * \
+        np.uint32(2654435761) ^ np.uint32(0x5bd1e995)
+
+
+def oracle_step(cfg, keys, queries, threads):
+    import oracle
+    masks = oracle.generate_hashmask(1)
+    s = oracle.Msws(cfg["n_low"], cfg["n_high"], SEED, masks)
+    t0 = time.perf_counter()
+    s.insert(keys, threads=threads)
+    t1 = time.perf_counter()
+    parts = np.array_split(queries, threads)
+    outs = [None] * threads
+
+    def q(i):
+        outs[i] = s.query(parts[i])
+
+    th = [threading.Thread(target=q, args=(i,)) for i in range(threads)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1
+
+
+def cpu_baseline(cfg, keys, queries):
+    threads = os.cpu_count() or 1
+    ni = min(keys.size, 1 << 25)
+    nq = min(queries.size, 1 << 22)
+    ti, tq = oracle_step(cfg, keys[:ni], queries[:nq], threads)
+    return {"value": round((ni + nq) / (ti + tq) / 1e9, 5), "unit": "Gkeys/s", "cores": threads, "kind": "port",
+            "sample": f"first {ni} keys inserted + {nq} queries of the same stream and sketch size "
+                      "(oracle/oracle.cpp, bucket-partitioned threads, array order per bucket)",
+            "insert_gkeys_per_s": round(ni / ti / 1e9, 5), "query_gkeys_per_s": round(nq / tq / 1e9, 5)}
+
+
+def run_reference(args, cfg):
+    world, rank, _ = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    ni = min(cfg["n_keys"], 1 << 24)
+    nq = min(cfg["n_query"], 1 << 21)
+    if cfg["kind"] == 1:
+        keys, distinct = host_zipf_keys(ni, cfg["n_ranks"], cfg["s"], 1000)
+        queries = distinct[:nq]
+    else:
+        keys = np.random.default_rng(1000).integers(0, 1 << 32, ni, dtype=np.uint64).astype(np.uint32)
+        queries = keys[:nq]
+    for _ in range(args.warmup):
+        oracle_step(cfg, keys, queries, threads)
+    tot = 0.0
+    for _ in range(args.steps):
+        ti, tq = oracle_step(cfg, keys, queries, threads)
+        tot += ti + tq
+    ms = tot * 1e3 / args.steps
+    v = (ni + nq) / (ms * 1e6)
+    sample = (f"per step: clear + insert {ni} keys + query {nq} keys of the {cfg['workload']} stream; "
+              "CPU restatement of the reference path (oracle/oracle.cpp), bucket-partitioned threads")
+    print(json.dumps({
+        "metric": METRIC, "value": round(v, 5), "unit": "Gkeys/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (numpy inverse-CDF Zipf / uniform)",
+        "config": {"workload": cfg["workload"], "n_low": cfg["n_low"], "n_high": cfg["n_high"]},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(v, 5), "unit": "Gkeys/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(v, 5), "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="zipf")
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, cfg)
+    else:
+        run_ours(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,225 @@
+/*
+ * qsketch_c.h — C ABI of the B200-native QSketch insert/query path.
+ *
+ * The reference exposes its sketches as the C++ abstract class
+ *   template<Key_T, Count_T> struct qsketch::Sketch {
+ *       virtual int insert(Key_T *keys, size_t n);
+ *       virtual int search(Key_T *keys, size_t n, Count_T *counts);
+ *       virtual void clear();  virtual ~Sketch(); }
+ * (reference include/sketch/sketch.h:5-28) with concrete constructors
+ *   Sketch_GPU_Sub_Warp_Level(n_low, m_low, n_high, m_high, seed_sz, n_hash_mask_table)
+ *     (include/sketch/device_sketch/device_sketch_v3.h:544-563)
+ *   Sketch_GPU_Thread(n, m, seed_sz)
+ *     (include/sketch/device_sketch/device_sketch_v0.h:121-131)
+ * Key_T = Count_T = unsigned int (reference src/main.cu:3-6).
+ *
+ * This header is the drop-in boundary: every entry point takes plain pointers and
+ * sizes, device pointers where the reference takes device pointers, and a CUDA stream
+ * passed as `void *` (0 = legacy default stream).  No C++ or torch types cross it.
+ * All calls are stream-ordered and asynchronous; device-side errors (pool exhaustion,
+ * bounded-wait timeouts) are latched in a per-sketch status word and reported by
+ * qs_sync() / qs_get_stats().  No call aborts the process.
+ */
+#ifndef QSKETCH_C_H
+#define QSKETCH_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QS_ABI_VERSION 1u
+
+/* Status codes.  The reference returns 0 from every call and ignores CUDA errors in
+ * release builds (include/qsketch.h:104-105); these replace that. */
+typedef enum qs_status {
+    QS_OK = 0,
+    QS_ERR_INVALID_ARG = 1, /* bad parameter, null handle, unsupported layout */
+    QS_ERR_OOM = 2,         /* device allocation failed */
+    QS_ERR_CUDA = 3,        /* CUDA runtime error (text via qs_last_error_string) */
+    QS_ERR_POOL_FULL = 4,   /* the high-level bucket pool ran out (latched) */
+    QS_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up (latched) */
+    QS_ERR_NO_DEVICE = 6,   /* no CUDA device / extension compiled for another arch */
+    QS_ERR_CAPACITY = 7     /* a call exceeds a documented size limit */
+} qs_status;
+
+/* Sketch families on the path. */
+typedef enum qs_kind {
+    QS_KIND_MSWS = 0,     /* lock-free multi-level sub-warp sketch ("Level"),
+                             reference Sketch_GPU_Sub_Warp_Level (device_sketch_v3.h:526) */
+    QS_KIND_PLAIN_CM = 1  /* plain count-min ("thread sketch"),
+                             reference Sketch_GPU_Thread (device_sketch_v0.h:107) */
+} qs_kind;
+
+/* Flags. */
+#define QS_FLAG_COMPAT_V3 0x1u /* reproduce device_sketch_v3.h:187: the key that links a
+                                  bucket adds its high increments at index (bit % 8)
+                                  instead of at the bit's own counter */
+
+/* Creation parameters.  Zero-initialise and set what you need; qs_params_default()
+ * fills the reference defaults (lib/default.cu:39-54). */
+typedef struct qs_params {
+    uint32_t kind;              /* qs_kind */
+    uint32_t flags;             /* QS_FLAG_* */
+    /* MSWS: n_low low buckets of m_low u32 words (m_low must be 8: 32 B buckets with
+     * 28 packed 8-bit counters + the high-bucket index word), n_high high buckets of
+     * m_high u32 counters (m_high must be 32).
+     * PLAIN_CM: n_low counters per row, m_low rows (the reference's "m").
+     * n_low == 0 derives it from low_bytes with find_greatest_prime(). */
+    uint64_t n_low;
+    uint64_t low_bytes;
+    uint32_t m_low;
+    uint32_t m_high;
+    uint64_t n_high;
+    uint32_t seed_sz;            /* hash seeds per row; must be 1 (lib/default.cu:52) */
+    uint32_t hash_mask_table_sz; /* H, masks in the table (lib/default.cu:54: 1021) */
+    uint32_t hash_mask_ones;     /* counters per key in a low bucket, the "row count"
+                                    (lib/default.cu:53: 3); 1..28 */
+    uint32_t hash_seed;          /* MSWS multiplier; 0 = draw it like the reference
+                                    (device_sketch.h:290) from seed_rng */
+    uint32_t seed_rng;           /* seeds std::minstd_rand0 for hash-seed draws */
+    uint32_t mask_rng;           /* seeds std::minstd_rand0 for generate_hashmask */
+    const uint32_t *seeds;       /* optional host array of m_low (CM) or 1 (MSWS) seeds;
+                                    overrides hash_seed / seed_rng */
+    const uint8_t *mask_table;   /* optional host table of H*4 bytes (bits 0..27 only);
+                                    overrides mask_rng */
+    uint64_t max_batch;          /* keys per internal insert chunk (scratch sizing);
+                                    0 = 1<<22 */
+    int32_t device;              /* CUDA device ordinal; -1 = current */
+    uint32_t lanes_per_key;      /* sub-warp width for the insert kernel: 0 = autotune,
+                                    else 8 (one lane per bucket word) */
+    uint32_t aggregate;          /* 0 = autotune, 1 = off, 2 = warp, 3 = block
+                                    pre-aggregation of duplicate keys */
+} qs_params;
+
+typedef struct qs_sketch qs_sketch;
+
+/* Counters the device keeps per sketch (read after a sync). */
+typedef struct qs_stats {
+    uint32_t status_bits;     /* bit0 pool full, bit1 timeout */
+    uint32_t next_level_id;   /* bump allocator value (starts at 1025) */
+    uint64_t linked_buckets;  /* next_level_id - 1025, capped at the pool */
+    uint64_t dropped_keys;    /* keys dropped in saturated buckets (pool exhausted) */
+    uint64_t repaired_buckets;/* buckets that crossed the 8-bit threshold and were
+                                 replayed in stream order, cumulative */
+    uint64_t repaired_keys;   /* keys routed through the ordered replay, cumulative */
+    uint64_t inserted_keys;   /* keys accepted by qs_insert, cumulative */
+} qs_stats;
+
+/* Library / device queries. */
+uint32_t qs_abi_version(void);
+const char *qs_status_string(qs_status s);
+/* Text of the most recent error on this host thread ("" if none). */
+const char *qs_last_error_string(void);
+
+/* Fill the reference defaults: MSWS, m_low 8, m_high 32, n_high 1024, seed_sz 1,
+ * H 1021, ones 3 (lib/default.cu:39-54, src/main.cu:390-391). */
+void qs_params_default(qs_params *p);
+
+/* find_greatest_prime (reference lib/qsketch.cu:50-115): largest prime of the
+ * reference's table that is <= upper_bound, 0 if none. */
+uint64_t qs_find_greatest_prime(uint64_t upper_bound);
+
+/* Sketch_GPU::number_of_buckets (reference device_sketch.h:371-376):
+ * find_greatest_prime(((keys / factor) * ones) / m). */
+uint64_t qs_number_of_buckets(uint64_t insert_keys, uint64_t m, double factor,
+                              uint32_t hash_mask_ones);
+
+/* generate_hashmask (reference lib/hashmask.cu:32-83) on a std::minstd_rand0 seeded
+ * with `rng_seed`: n masks of ceil(m_bits/8) bytes, each with `ones` distinct bits in
+ * [0, m_bits - padding).  out must hold n*ceil(m_bits/8) bytes. */
+qs_status qs_generate_hashmask(uint32_t rng_seed, size_t n, size_t m_bits, size_t ones,
+                               size_t padding, uint8_t *out);
+
+/* The reference's seed draw (device_sketch.h:290 → include/tool/tool.h:206-220):
+ * `count` values of uniform_int_distribution<uint>(1, UINT_MAX) on a
+ * std::minstd_rand0 seeded with rng_seed. */
+qs_status qs_draw_seeds(uint32_t rng_seed, size_t count, uint32_t *out);
+
+/* Construct / destroy.  Replaces the constructors cited above and ~Sketch_GPU
+ * (device_sketch.h:387-394).  The handle owns all device memory. */
+qs_status qs_create(const qs_params *params, qs_sketch **out);
+qs_status qs_destroy(qs_sketch *sk);
+
+/* Sketch::insert (sketch.h:7, device_sketch_v3.h:570-599, device_sketch_v0.h:140-161).
+ * d_keys: device pointer to n uint32 keys (any 4-byte alignment).  Results are exactly
+ * those of inserting the keys one by one in array order (the sequential semantics of
+ * device_sketch_v3.h:88-191), whatever the GPU schedule. */
+qs_status qs_insert(qs_sketch *sk, const uint32_t *d_keys, size_t n, void *stream);
+
+/* Sketch::search (sketch.h:8, device_sketch_v3.h:600-632, device_sketch_v0.h:162-189).
+ * Writes n uint32 estimates to d_counts (device pointer). */
+qs_status qs_query(qs_sketch *sk, const uint32_t *d_keys, size_t n, uint32_t *d_counts,
+                   void *stream);
+
+/* Host-buffer variants: keys / counts in host memory (pinned or pageable).  The copies
+ * run chunked and overlapped with the kernels on internal streams; the call returns
+ * when the results are in h_counts (query) or the keys are consumed (insert). */
+qs_status qs_insert_host(qs_sketch *sk, const uint32_t *h_keys, size_t n);
+qs_status qs_query_host(qs_sketch *sk, const uint32_t *h_keys, size_t n, uint32_t *h_counts);
+
+/* Sketch::clear (sketch.h:14, device_sketch.h:378-381, 115-124): zero the tables and
+ * reset the bump allocator to 1025. */
+qs_status qs_clear(qs_sketch *sk, void *stream);
+
+/* Synchronise the sketch's work on `stream` and return the latched device status
+ * (QS_ERR_POOL_FULL / QS_ERR_TIMEOUT) or QS_OK. */
+qs_status qs_sync(qs_sketch *sk, void *stream);
+qs_status qs_get_stats(qs_sketch *sk, qs_stats *out);
+/* Launch accounting.  Counters are cumulative; times cover the launches issued while
+ * profiling was on, measured with CUDA events recorded around each launch on the stream
+ * it ran on, and are reset by each qs_get_profile call. */
+typedef struct qs_profile {
+    double insert_ms;          /* pass-1 insert kernels (MSWS) / insert kernels (CM) */
+    double repair_ms;          /* ordered-repair kernels (MSWS) */
+    double query_ms;           /* query kernels */
+    uint64_t insert_timed, repair_timed, query_timed;
+    uint64_t insert_launches, repair_launches, query_launches;
+} qs_profile;
+qs_status qs_set_profiling(qs_sketch *sk, int enable);
+qs_status qs_get_profile(qs_sketch *sk, qs_profile *out);
+
+/* Clear the latched device status bits. */
+qs_status qs_reset_status(qs_sketch *sk);
+
+/* Sizes of the device tables in u32 words (low, high) and the seeds in use. */
+qs_status qs_get_info(qs_sketch *sk, uint64_t *n_low, uint64_t *n_high, uint32_t *m_low,
+                      uint32_t *seeds_out /* m_low for CM, 1 for MSWS; may be null */,
+                      uint8_t *mask_table_out /* H*4 bytes; may be null */);
+
+/* Copy the device tables to host buffers (debug / oracle comparison):
+ * low: n_low*m_low words (MSWS: word 7 of each bucket is the high index),
+ * high: n_high*m_high words (null to skip). */
+qs_status qs_get_tables(qs_sketch *sk, uint32_t *h_low, uint32_t *h_high);
+
+/* Synthetic key streams (bench / tests), written to device memory on `stream`.
+ * kind 0: uniform u32 from a seeded xorshift64 stream;
+ * kind 1: Zipf(s) over n_ranks ranks (rejection-inversion, Hoermann & Derflinger
+ *         1996), rank r mapped to a distinct key by a seeded bijection of u32;
+ * d_ranks (may be null) receives the 0-based rank of each key (kind 1 only). */
+qs_status qs_gen_keys(uint32_t kind, uint64_t seed, uint64_t n_ranks, double s,
+                      uint64_t perm_seed, uint32_t *d_keys, uint32_t *d_ranks, size_t n,
+                      void *stream);
+/* The key that qs_gen_keys(kind 1) maps rank r to, for r in [first, first+n). */
+qs_status qs_gen_rank_keys(uint64_t perm_seed, uint64_t first, uint32_t *d_keys, size_t n,
+                           void *stream);
+/* d_hist[r] += occurrences of rank r in d_ranks[0..n) (exact counts for error metrics). */
+qs_status qs_rank_histogram(const uint32_t *d_ranks, size_t n, uint32_t *d_hist,
+                            uint64_t n_ranks, void *stream);
+/* Mean relative error |est-exact|/exact and mean est/exact over n keys (exact > 0),
+ * reduced on the device; results written to host doubles. */
+qs_status qs_error_metrics(const uint32_t *d_est, const uint32_t *d_exact, size_t n,
+                           double *mean_rel_err, double *mean_ratio, void *stream);
+
+/* Roofline probes: time `kind` (0 random sub-warp sector red with 3 words per sector,
+ * 1 random 32 B sector load, 2 streaming read) over a device buffer of `bytes`,
+ * returning operations per second (sectors/s or bytes/s for kind 2). */
+qs_status qs_probe(uint32_t kind, uint64_t bytes, uint64_t ops, double *ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QSKETCH_C_H */

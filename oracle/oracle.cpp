@@ -1,0 +1,251 @@
+// oracle.cpp — TEST INFRASTRUCTURE ONLY.  CPU restatement of the reference QSketch
+// insert/query semantics, used by tests/, __graft_entry__.smoke() and bench.py's
+// cpu_baseline leg as the checker.  Nothing in the product (qsketch_b200/, include/)
+// links or calls this file.
+//
+// Sequential semantics restated from the reference (bu-hpc/QSketch):
+//   hash          include/sketch/device_sketch/device_hash_function.h:6-18
+//                 hv = key * seed (mod 2^32), seed_sz = 1 (lib/default.cu:52)
+//   bucket/mask   include/sketch/device_sketch/device_sketch_v3.h:39-45
+//                 bucket = hv % n_low, mask = table[hv % H]
+//   insert        device_sketch_v3.h:88-191 (calculation_s2_insert), 54-85
+//                 (insert_high, atomic_malloc); low→high switch when a selected 8-bit
+//                 counter exceeds 128 (:160); ids start at NEXT_LEVEL_ID_START+1 = 1025
+//                 (device_sketch.h:107-111), high bucket at (id-1024)*32 (:119,:185)
+//   query         device_sketch_v3.h:311-408 (calculation_s2_search): min over the
+//                 selected low bytes + (linked ? min over the selected high counters : 0)
+//   plain CM      device_sketch_v0.h:45-54 (insert), :90-100 (query)
+//   masks         lib/hashmask.cu:32-83 (generate_hashmask) on std::default_random_engine
+//                 (= std::minstd_rand0 in libstdc++), reseeded here with an integer
+//   seed draw     device_sketch.h:290 → include/tool/tool.h:206-220
+//   primes        lib/qsketch.cu:50-115 (find_greatest_prime)
+//   exact counts  include/sketch/host_sketch/host_sketch.h:20-39 (Unordered_Map)
+//   error metric  include/analyze/analyze.h:15-41 (Percentage_Functor, average)
+//
+// Decisions where the reference is racy or unbounded (identical in the GPU path):
+//   * the high pool is bounded: a link needs (id - 1024) < n_high; when it is full the
+//     bucket becomes SATURATED (word 7 = 2): its keys are dropped and counted, its query
+//     is the frozen low minimum.  Which buckets saturate depends on the global order of
+//     allocation, so results under exhaustion are only compared through the status.
+//   * compat_v3 = 1 reproduces device_sketch_v3.h:187 (the linking key's high increments
+//     land on index bit % 8); compat_v3 = 0 uses the bit's own index, as the later
+//     device_sketch_v32.h:175 and the paper's Algorithm 4 do.
+#include <algorithm>
+#include <atomic>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+namespace {
+constexpr uint32_t START = 1024;   // lib/default.cu:45
+constexpr uint32_t LIMIT = 128;    // device_sketch_v3.h:160
+constexpr uint32_t SATURATED = 2;  // reserved value (< START), see header comment
+constexpr int W = 8;               // words per low bucket
+constexpr int HW = 32;             // counters per high bucket
+
+inline uint32_t low_byte(const uint32_t* w, int i) { return (w[i >> 2] >> (8 * (i & 3))) & 0xffu; }
+}  // namespace
+
+extern "C" {
+
+// lib/qsketch.cu:50-115 — the same table of primes near 2^k and 1.5*2^k.
+uint64_t or_find_greatest_prime(uint64_t upper_bound) {
+    static const uint64_t ps[] = {
+        402653171, 268435399, 201326557, 134217689, 100663291, 67108859, 50331599, 33554393,
+        25165813,  16777213,  12582893,  8388593,   6291449,   4194301,  3145721,  2097143,
+        1572853,   1048573,   786431,    524287,    393209,    262139,   196597,   131071,
+        98299,     65521,     49139,     32749,     24571,     16381,    12281,    8191,
+        6143,      4093,      3067,      2039,      1531,      1021,     761,      509,
+        383,       251,       191,       127,       89,        61,       47,       31,
+        23,        13,        11,        7,         5,         3,        2};
+    for (uint64_t p : ps)
+        if (p <= upper_bound) return p;
+    return 0;
+}
+
+// lib/hashmask.cu:32-83 with an integer-seeded engine.  Returns 0 on success.
+int or_generate_hashmask(uint32_t rng_seed, size_t n, size_t m_bits, size_t ones, size_t padding,
+                         uint8_t* out) {
+    if (m_bits <= padding || ones > m_bits - padding) return -1;
+    const size_t mask_bytes = (m_bits + 7) / 8;
+    std::memset(out, 0, n * mask_bytes);
+    std::minstd_rand0 eng(rng_seed);
+    std::uniform_int_distribution<uint32_t> dis(0, (uint32_t)(m_bits - padding - 1));
+    for (size_t i = 0; i < n; ++i) {
+        size_t j = 0;
+        while (j < ones) {
+            uint32_t id = dis(eng);
+            uint8_t* m = out + i * mask_bytes;
+            uint8_t b = (uint8_t)(1u << (id % 8));
+            if ((m[id / 8] & b) == 0) {  // lib/hashmask.cu:5-20 (set)
+                m[id / 8] |= b;
+                ++j;
+            }
+        }
+    }
+    return 0;
+}
+
+// include/tool/tool.h:206-220 with min = 1, max = UINT_MAX.
+void or_draw_seeds(uint32_t rng_seed, size_t count, uint32_t* out) {
+    std::minstd_rand0 eng(rng_seed);
+    std::uniform_int_distribution<uint32_t> dis(1u, 0xffffffffu);
+    for (size_t i = 0; i < count; ++i) out[i] = dis(eng);
+}
+
+// ---------------------------------------------------------------------------------------
+// MSWS state.  low: n_low*8 words, high: n_high*32 words, masks: H 32-bit mask words.
+typedef struct or_msws {
+    uint32_t* low;
+    uint64_t n_low;
+    uint32_t* high;
+    uint64_t n_high;
+    const uint32_t* masks;
+    uint32_t n_masks;
+    uint32_t seed;
+    uint32_t next_id;
+    int32_t compat_v3;
+    uint32_t pool_full;
+    uint32_t pad;
+    uint64_t dropped;
+} or_msws;
+
+static inline void msws_insert_one(or_msws* s, uint32_t key, std::atomic<uint32_t>* shared_next) {
+    const uint32_t hv = key * s->seed;
+    const uint64_t b = hv % s->n_low;
+    const uint32_t mask = s->masks[hv % s->n_masks];
+    uint32_t* w = s->low + b * W;
+    uint32_t ptr = w[7];
+    if (ptr == SATURATED) { ++s->dropped; return; }
+    if (ptr > START) {  // device_sketch_v3.h:111-129
+        uint32_t* h = s->high + (uint64_t)(ptr - START) * HW;
+        for (uint32_t m = mask; m; m &= m - 1) h[__builtin_ctz(m)] += 1;
+        return;
+    }
+    bool over = false;  // device_sketch_v3.h:132-161
+    for (uint32_t m = mask; m; m &= m - 1)
+        if (low_byte(w, __builtin_ctz(m)) > LIMIT) over = true;
+    if (!over) {  // :163-170
+        for (uint32_t m = mask; m; m &= m - 1) {
+            int i = __builtin_ctz(m);
+            w[i >> 2] += 1u << (8 * (i & 3));
+        }
+        return;
+    }
+    // :172-190 — allocate (atomic_malloc :69-85) and insert into the new high bucket
+    uint32_t id;
+    if (shared_next) {
+        id = shared_next->fetch_add(1);
+        if ((uint64_t)(id - START) >= s->n_high) { w[7] = SATURATED; s->pool_full = 1; ++s->dropped; return; }
+    } else {
+        if ((uint64_t)(s->next_id - START) >= s->n_high) { w[7] = SATURATED; s->pool_full = 1; ++s->dropped; return; }
+        id = s->next_id++;
+    }
+    w[7] = id;
+    uint32_t* h = s->high + (uint64_t)(id - START) * HW;
+    for (uint32_t m = mask; m; m &= m - 1) {
+        int i = __builtin_ctz(m);
+        h[s->compat_v3 ? (i % 8) : i] += 1;
+    }
+}
+
+void or_msws_insert(or_msws* s, const uint32_t* keys, uint64_t n) {
+    for (uint64_t i = 0; i < n; ++i) msws_insert_one(s, keys[i], nullptr);
+}
+
+// Bucket-partitioned parallel insert: thread t applies, in stream order, the keys whose
+// bucket satisfies b % T == t.  Per-bucket order is the stream order, so the result equals
+// the sequential one (high ids differ; query results do not unless the pool runs out).
+void or_msws_insert_mt(or_msws* s, const uint32_t* keys, uint64_t n, int threads) {
+    if (threads <= 1) { or_msws_insert(s, keys, n); return; }
+    std::atomic<uint32_t> next(s->next_id);
+    std::vector<or_msws> local(threads, *s);
+    std::vector<std::thread> th;
+    for (int t = 0; t < threads; ++t) {
+        th.emplace_back([&, t] {
+            or_msws* ls = &local[t];
+            ls->dropped = 0;
+            ls->pool_full = 0;
+            for (uint64_t i = 0; i < n; ++i) {
+                const uint32_t hv = keys[i] * s->seed;
+                if ((hv % s->n_low) % (uint64_t)threads != (uint64_t)t) continue;
+                msws_insert_one(ls, keys[i], &next);
+            }
+        });
+    }
+    for (auto& x : th) x.join();
+    uint32_t nid = next.load();
+    uint64_t cap = START + s->n_high;
+    s->next_id = nid > cap ? (uint32_t)cap : nid;
+    for (auto& ls : local) { s->dropped += ls.dropped; s->pool_full |= ls.pool_full; }
+}
+
+void or_msws_query(const or_msws* s, const uint32_t* keys, uint64_t n, uint32_t* out) {
+    for (uint64_t k = 0; k < n; ++k) {
+        const uint32_t hv = keys[k] * s->seed;
+        const uint64_t b = hv % s->n_low;
+        const uint32_t mask = s->masks[hv % s->n_masks];
+        const uint32_t* w = s->low + b * W;
+        uint32_t lo = 0xffffffffu, hi = 0xffffffffu;
+        for (uint32_t m = mask; m; m &= m - 1) lo = std::min(lo, low_byte(w, __builtin_ctz(m)));
+        const uint32_t ptr = w[7];
+        if (ptr > START) {
+            const uint32_t* h = s->high + (uint64_t)(ptr - START) * HW;
+            for (uint32_t m = mask; m; m &= m - 1) hi = std::min(hi, h[__builtin_ctz(m)]);
+        } else {
+            hi = 0;
+        }
+        out[k] = lo + hi;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Plain count-min (device_sketch_v0.h): rows m, n counters per row, seeds[m].
+void or_cm_insert(uint32_t* table, uint64_t n, uint32_t m, const uint32_t* seeds, const uint32_t* keys,
+                  uint64_t nk) {
+    for (uint64_t i = 0; i < nk; ++i)
+        for (uint32_t j = 0; j < m; ++j) table[j * n + (uint32_t)(keys[i] * seeds[j]) % n] += 1;
+}
+
+void or_cm_query(const uint32_t* table, uint64_t n, uint32_t m, const uint32_t* seeds, const uint32_t* keys,
+                 uint64_t nk, uint32_t* out) {
+    for (uint64_t i = 0; i < nk; ++i) {
+        uint32_t c = 0xffffffffu;
+        for (uint32_t j = 0; j < m; ++j) c = std::min(c, table[j * n + (uint32_t)(keys[i] * seeds[j]) % n]);
+        out[i] = c;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Exact counter (host_sketch.h:20-39): counts of `queries` among `keys`.
+void or_exact_counts(const uint32_t* keys, uint64_t n, const uint32_t* queries, uint64_t nq, uint32_t* out) {
+    std::unordered_map<uint32_t, uint32_t> um;
+    um.reserve(nq * 2 + 16);
+    for (uint64_t i = 0; i < nq; ++i) um.emplace(queries[i], 0u);
+    for (uint64_t i = 0; i < n; ++i) {
+        auto it = um.find(keys[i]);
+        if (it != um.end()) ++it->second;
+    }
+    for (uint64_t i = 0; i < nq; ++i) out[i] = um[queries[i]];
+}
+
+// Mean |est-exact|/exact and mean est/exact over entries with exact > 0
+// (analyze.h:15-41 reports mean(est/exact)*100).
+void or_error_metrics(const uint32_t* est, const uint32_t* exact, uint64_t n, double* mean_rel, double* mean_ratio) {
+    double r = 0, q = 0;
+    uint64_t c = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (!exact[i]) continue;
+        double e = est[i], a = exact[i];
+        r += (e > a ? e - a : a - e) / a;
+        q += e / a;
+        ++c;
+    }
+    *mean_rel = c ? r / c : 0.0;
+    *mean_ratio = c ? q / c : 0.0;
+}
+
+}  // extern "C"

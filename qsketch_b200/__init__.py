@@ -1,0 +1,11 @@
+"""B200-native (sm_100a) QSketch insert/query path behind a C ABI (include/qsketch_c.h).
+
+The sketch kernels live in libqsketch.so; this package is the Python mirror of the
+reference's host interface (qsketch::Sketch, Sketch_GPU_Sub_Warp_Level, Sketch_GPU_Thread).
+"""
+from ._lib import LIB_PATH, QsError, check, lib  # noqa: F401  (raises ImportError if unbuilt)
+from .sketch import (Sketch, Sketch_GPU_Sub_Warp_Level, Sketch_GPU_Thread, draw_seeds,  # noqa: F401
+                     find_greatest_prime, generate_hashmask, number_of_buckets)
+
+__all__ = ["Sketch", "Sketch_GPU_Sub_Warp_Level", "Sketch_GPU_Thread", "find_greatest_prime",
+           "number_of_buckets", "generate_hashmask", "draw_seeds", "QsError", "LIB_PATH"]

@@ -1,0 +1,663 @@
+// qs_api.cu — the C ABI (include/qsketch_c.h): sketch construction, host-side table
+// preparation (seeds, hash masks, prime sizing) and the stream-ordered launch sequence.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/qsketch_c.h"
+#include "qs_kernels.h"
+
+using namespace qsb;
+
+namespace {
+
+thread_local std::string g_err;
+
+qs_status fail(qs_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+qs_status cuda_fail(cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return fail(QS_ERR_OOM, "%s: %s", what, cudaGetErrorString(e));
+    }
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorNoKernelImageForDevice)
+        return fail(QS_ERR_NO_DEVICE, "%s: %s", what, cudaGetErrorString(e));
+    return fail(QS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(expr, what)                                     \
+    do {                                                   \
+        cudaError_t _e = (expr);                           \
+        if (_e != cudaSuccess) return cuda_fail(_e, what); \
+    } while (0)
+#define CKB(expr, what)                                          \
+    do {                                                         \
+        cudaError_t _e = (expr);                                 \
+        if (_e != cudaSuccess) return bail(cuda_fail(_e, what)); \
+    } while (0)
+
+// lib/qsketch.cu:50-115
+const uint64_t kPrimes[] = {402653171, 268435399, 201326557, 134217689, 100663291, 67108859, 50331599, 33554393,
+                            25165813,  16777213,  12582893,  8388593,   6291449,   4194301,  3145721,  2097143,
+                            1572853,   1048573,   786431,    524287,    393209,    262139,   196597,   131071,
+                            98299,     65521,     49139,     32749,     24571,     16381,    12281,    8191,
+                            6143,      4093,      3067,      2039,      1531,      1021,     761,      509,
+                            383,       251,       191,       127,       89,        61,       47,       31,
+                            23,        13,        11,        7,         5,         3,        2};
+
+}  // namespace
+
+struct qs_sketch {
+    qs_params p{};
+    int device = 0;
+    uint32_t kind = 0;
+    uint64_t max_batch = 0;
+    int agg = 1;
+    std::vector<uint32_t> seeds;
+    std::vector<uint32_t> masks;  // mask words
+    std::vector<void*> allocs;
+    MswsDev D{};
+    MswsLaunch L{};
+    CmDev C{};
+    int cm_grid = 0;
+    // host-buffer pipeline
+    cudaStream_t io[2] = {nullptr, nullptr};
+    cudaEvent_t done = nullptr;
+    uint32_t* stage_keys[2] = {nullptr, nullptr};
+    uint32_t* stage_out[2] = {nullptr, nullptr};
+    uint64_t stage_n = 0;
+    std::mutex mu;
+    // launch accounting and optional per-launch event timing (qs_set_profiling)
+    uint64_t launches[3] = {0, 0, 0};  // insert pass, repair, query
+    bool prof = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[3];
+    size_t ev_used[3] = {0, 0, 0};
+
+    cudaError_t prof_begin(int k, cudaStream_t st) {
+        ++launches[k];
+        if (!prof) return cudaSuccess;
+        if (ev_used[k] == ev[k].size()) {
+            cudaEvent_t a, b;
+            cudaError_t e = cudaEventCreate(&a);
+            if (e == cudaSuccess) e = cudaEventCreate(&b);
+            if (e != cudaSuccess) return e;
+            ev[k].push_back({a, b});
+        }
+        return cudaEventRecord(ev[k][ev_used[k]].first, st);
+    }
+    cudaError_t prof_end(int k, cudaStream_t st) {
+        if (!prof) return cudaSuccess;
+        return cudaEventRecord(ev[k][ev_used[k]++].second, st);
+    }
+
+    template <class T>
+    cudaError_t alloc(T** ptr, size_t count) {
+        void* v = nullptr;
+        const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+        cudaError_t e = cudaMalloc(&v, bytes);
+        if (e != cudaSuccess) return e;
+        allocs.push_back(v);
+        e = cudaMemset(v, 0, bytes);
+        *ptr = static_cast<T*>(v);
+        return e;
+    }
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// generate_hashmask (lib/hashmask.cu:32-83): per mask, draw uniform_int_distribution(0,
+// m_bits - padding - 1) until `ones` distinct bits are set (lib/hashmask.cu:5-20).
+void gen_hashmask(uint32_t rng_seed, size_t n, size_t m_bits, size_t ones, size_t padding, uint8_t* out) {
+    const size_t mb = (m_bits + 7) / 8;
+    std::memset(out, 0, n * mb);
+    std::minstd_rand0 eng(rng_seed);  // std::default_random_engine of libstdc++
+    std::uniform_int_distribution<uint32_t> dis(0, (uint32_t)(m_bits - padding - 1));
+    for (size_t i = 0; i < n; ++i) {
+        uint8_t* m = out + i * mb;
+        size_t j = 0;
+        while (j < ones) {
+            const uint32_t id = dis(eng);
+            const uint8_t bit = (uint8_t)(1u << (id % 8));
+            if (!(m[id / 8] & bit)) {
+                m[id / 8] |= bit;
+                ++j;
+            }
+        }
+    }
+}
+
+// CPU_Tools::random(.., 1, UINT_MAX) (include/tool/tool.h:206-220).
+void draw_seeds(uint32_t rng_seed, size_t count, uint32_t* out) {
+    std::minstd_rand0 eng(rng_seed);
+    std::uniform_int_distribution<uint32_t> dis(1u, std::numeric_limits<uint32_t>::max());
+    for (size_t i = 0; i < count; ++i) out[i] = dis(eng);
+}
+
+qs_status check_status_word(qs_sketch* sk) {
+    Ctl c;
+    if (sk->kind != QS_KIND_MSWS) return QS_OK;
+    cudaError_t e = cudaMemcpy(&c, sk->D.ctl, sizeof c, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "read status");
+    if (c.status & ST_TIMEOUT) return fail(QS_ERR_TIMEOUT, "a bounded device wait timed out");
+    if (c.status & ST_CAPACITY) return fail(QS_ERR_CAPACITY, "flagged-bucket list overflow");
+    if (c.status & ST_POOL_FULL)
+        return fail(QS_ERR_POOL_FULL, "high-level bucket pool exhausted (%llu keys dropped)",
+                    (unsigned long long)c.dropped);
+    return QS_OK;
+}
+
+qs_status ctl_reset(qs_sketch* sk, cudaStream_t st) {
+    static const Ctl init = [] {
+        Ctl c;
+        std::memset(&c, 0, sizeof c);
+        c.next_id = FIRST_ID;
+        return c;
+    }();
+    CK(cudaMemcpyAsync(sk->D.ctl, &init, sizeof init, cudaMemcpyHostToDevice, st), "reset control block");
+    return QS_OK;
+}
+
+qs_status setup_io(qs_sketch* sk) {
+    if (sk->io[0]) return QS_OK;
+    sk->stage_n = std::min<uint64_t>(sk->max_batch, 1ull << 22);
+    for (int i = 0; i < 2; ++i) {
+        CK(cudaStreamCreateWithFlags(&sk->io[i], cudaStreamNonBlocking), "io stream");
+        CK(sk->alloc(&sk->stage_keys[i], sk->stage_n), "staging keys");
+        CK(sk->alloc(&sk->stage_out[i], sk->stage_n), "staging counts");
+    }
+    CK(cudaEventCreateWithFlags(&sk->done, cudaEventDisableTiming), "io event");
+    return QS_OK;
+}
+
+qs_status insert_device(qs_sketch* sk, const uint32_t* d_keys, size_t n, cudaStream_t st) {
+    if (sk->kind == QS_KIND_MSWS) {
+        for (size_t off = 0; off < n; off += sk->max_batch) {
+            const uint64_t c = std::min<uint64_t>(sk->max_batch, n - off);
+            CK(sk->prof_begin(0, st), "profile");
+            CK(msws_insert_pass(d_keys + off, c, sk->D, sk->L, sk->agg, st), "msws insert");
+            CK(sk->prof_end(0, st), "profile");
+            CK(sk->prof_begin(1, st), "profile");
+            CK(msws_repair(d_keys + off, c, sk->D, sk->L, st), "msws repair");
+            CK(sk->prof_end(1, st), "profile");
+        }
+    } else {
+        CK(sk->prof_begin(0, st), "profile");
+        CK(cm_insert(d_keys, n, sk->C, sk->agg, sk->cm_grid, st), "cm insert");
+        CK(sk->prof_end(0, st), "profile");
+    }
+    return QS_OK;
+}
+
+qs_status query_device(qs_sketch* sk, const uint32_t* d_keys, size_t n, uint32_t* d_out, cudaStream_t st) {
+    CK(sk->prof_begin(2, st), "profile");
+    if (sk->kind == QS_KIND_MSWS)
+        CK(msws_query(d_keys, n, d_out, sk->D, sk->L, st), "msws query");
+    else
+        CK(cm_query(d_keys, n, d_out, sk->C, sk->cm_grid, st), "cm query");
+    CK(sk->prof_end(2, st), "profile");
+    return QS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t qs_abi_version(void) { return QS_ABI_VERSION; }
+
+const char* qs_status_string(qs_status s) {
+    switch (s) {
+        case QS_OK: return "ok";
+        case QS_ERR_INVALID_ARG: return "invalid argument";
+        case QS_ERR_OOM: return "out of device memory";
+        case QS_ERR_CUDA: return "CUDA error";
+        case QS_ERR_POOL_FULL: return "high-level pool exhausted";
+        case QS_ERR_TIMEOUT: return "device wait timed out";
+        case QS_ERR_NO_DEVICE: return "no usable CUDA device";
+        case QS_ERR_CAPACITY: return "size limit exceeded";
+    }
+    return "unknown status";
+}
+
+const char* qs_last_error_string(void) { return g_err.c_str(); }
+
+void qs_params_default(qs_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->kind = QS_KIND_MSWS;
+    p->m_low = 8;
+    p->m_high = 32;
+    p->n_high = 1024;            // src/main.cu:390-391
+    p->seed_sz = 1;              // lib/default.cu:52
+    p->hash_mask_table_sz = 1021;  // lib/default.cu:54
+    p->hash_mask_ones = 3;       // lib/default.cu:53
+    p->seed_rng = 1;
+    p->mask_rng = 1;
+    p->device = -1;
+}
+
+uint64_t qs_find_greatest_prime(uint64_t upper_bound) {
+    for (uint64_t x : kPrimes)
+        if (x <= upper_bound) return x;
+    return 0;
+}
+
+uint64_t qs_number_of_buckets(uint64_t insert_keys, uint64_t m, double factor, uint32_t ones) {
+    if (m == 0 || factor <= 0) return 0;
+    const uint64_t row = (uint64_t)(((double)(uint64_t)((double)insert_keys / factor)) * ones) / m;
+    return qs_find_greatest_prime(row);
+}
+
+qs_status qs_generate_hashmask(uint32_t rng_seed, size_t n, size_t m_bits, size_t ones, size_t padding, uint8_t* out) {
+    if (!out || m_bits == 0 || m_bits <= padding || ones == 0 || ones > m_bits - padding)
+        return fail(QS_ERR_INVALID_ARG, "generate_hashmask: bad sizes");
+    gen_hashmask(rng_seed, n, m_bits, ones, padding, out);
+    return QS_OK;
+}
+
+qs_status qs_draw_seeds(uint32_t rng_seed, size_t count, uint32_t* out) {
+    if (!out && count) return fail(QS_ERR_INVALID_ARG, "draw_seeds: null output");
+    draw_seeds(rng_seed, count, out);
+    return QS_OK;
+}
+
+qs_status qs_create(const qs_params* params, qs_sketch** out) {
+    if (!params || !out) return fail(QS_ERR_INVALID_ARG, "qs_create: null argument");
+    *out = nullptr;
+    const qs_params& p = *params;
+    if (p.kind != QS_KIND_MSWS && p.kind != QS_KIND_PLAIN_CM) return fail(QS_ERR_INVALID_ARG, "unknown kind %u", p.kind);
+    if (p.seed_sz != 1) return fail(QS_ERR_INVALID_ARG, "seed_sz must be 1 (lib/default.cu:52)");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return cuda_fail(e == cudaSuccess ? cudaErrorNoDevice : e, "cudaGetDeviceCount");
+    int dev = p.device;
+    if (dev < 0) cudaGetDevice(&dev);
+    if (dev >= ndev) return fail(QS_ERR_INVALID_ARG, "device %d out of range", dev);
+    int major = 0, minor = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+    if (major != 10 || minor != 0)
+        return fail(QS_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a only", dev, major, minor);
+    DeviceGuard guard(dev);
+
+    qs_sketch* sk = new qs_sketch();
+    sk->p = p;
+    sk->device = dev;
+    sk->kind = p.kind;
+    sk->max_batch = p.max_batch ? p.max_batch : (1ull << 22);
+    if (sk->max_batch > (1ull << 30)) {
+        delete sk;
+        return fail(QS_ERR_INVALID_ARG, "max_batch above 2^30");
+    }
+    sk->agg = (p.aggregate == 1) ? 0 : 1;
+    auto bail = [&](qs_status s) {
+        qs_destroy(sk);
+        return s;
+    };
+
+    if (p.kind == QS_KIND_MSWS) {
+        if (p.m_low != 8) return bail(fail(QS_ERR_INVALID_ARG, "m_low must be 8 (32 B low buckets)"));
+        if (p.m_high != 32) return bail(fail(QS_ERR_INVALID_ARG, "m_high must be 32"));
+        uint64_t n_low = p.n_low ? p.n_low : qs_find_greatest_prime(p.low_bytes / 32);
+        if (n_low == 0 || n_low > 0xffffffffull) return bail(fail(QS_ERR_INVALID_ARG, "n_low out of range"));
+        if (p.n_high < 2 || p.n_high > (1ull << 30)) return bail(fail(QS_ERR_INVALID_ARG, "n_high out of [2, 2^30]"));
+        const uint32_t H = p.hash_mask_table_sz;
+        if (H == 0 || H > 16384) return bail(fail(QS_ERR_INVALID_ARG, "hash_mask_table_sz out of [1, 16384]"));
+        if (p.lanes_per_key != 0 && p.lanes_per_key != 8)
+            return bail(fail(QS_ERR_INVALID_ARG, "lanes_per_key must be 0 or 8"));
+        std::vector<uint8_t> bytes((size_t)H * 4);
+        if (p.mask_table) {
+            std::memcpy(bytes.data(), p.mask_table, bytes.size());
+        } else {
+            if (p.hash_mask_ones == 0 || p.hash_mask_ones > (uint32_t)LOW_COUNTERS)
+                return bail(fail(QS_ERR_INVALID_ARG, "hash_mask_ones out of [1, 28]"));
+            gen_hashmask(p.mask_rng, H, 32, p.hash_mask_ones, 4, bytes.data());  // device_sketch_v3.h:559
+        }
+        sk->masks.resize(H);
+        for (uint32_t i = 0; i < H; ++i) {
+            uint32_t w = (uint32_t)bytes[4 * i] | ((uint32_t)bytes[4 * i + 1] << 8) | ((uint32_t)bytes[4 * i + 2] << 16) |
+                         ((uint32_t)bytes[4 * i + 3] << 24);
+            if (w == 0 || (w >> LOW_COUNTERS)) return bail(fail(QS_ERR_INVALID_ARG, "mask %u selects no counter or a bit above 27", i));
+            sk->masks[i] = w;
+        }
+        sk->seeds.resize(1);
+        if (p.seeds)
+            sk->seeds[0] = p.seeds[0];
+        else if (p.hash_seed)
+            sk->seeds[0] = p.hash_seed;
+        else
+            draw_seeds(p.seed_rng, 1, sk->seeds.data());
+
+        MswsDev& D = sk->D;
+        D.n_low = n_low;
+        D.n_high = p.n_high;
+        D.fm_low = make_fastmod((uint32_t)n_low);
+        D.fm_mask = make_fastmod(H);
+        D.seed = sk->seeds[0];
+        D.n_masks = H;
+        D.compat_v3 = (p.flags & QS_FLAG_COMPAT_V3) ? 1u : 0u;
+        const uint64_t B = sk->max_batch;
+        const uint64_t cap = std::min<uint64_t>(n_low, B);
+        D.flag_cap = (uint32_t)cap;
+        D.max_tiles = (uint32_t)((B + REPAIR_TILE - 1) / REPAIR_TILE);
+        D.long_cap = (uint32_t)(B / LONG_SEGMENT + 1);
+        uint32_t* masks_d = nullptr;
+        CKB(sk->alloc(&D.low, n_low * LOW_WORDS), "alloc low table");
+        CKB(sk->alloc(&D.high, p.n_high * HIGH_WORDS), "alloc high table");
+        CKB(sk->alloc(&masks_d, H), "alloc masks");
+        D.masks = masks_d;
+        CKB(sk->alloc(&D.ctl, 1), "alloc control");
+        CKB(sk->alloc(&D.flag_list, cap), "alloc flag list");
+        CKB(sk->alloc(&D.bitmap, (n_low + 31) / 32), "alloc bitmap");
+        CKB(sk->alloc(&D.tile_counts, D.max_tiles), "alloc tile counts");
+        CKB(sk->alloc(&D.rec[0], B), "alloc records");
+        CKB(sk->alloc(&D.rec[1], B), "alloc records");
+        CKB(sk->alloc(&D.hist, (uint64_t)256 * D.max_tiles), "alloc histograms");
+        CKB(sk->alloc(&D.seg_beg, cap), "alloc segments");
+        CKB(sk->alloc(&D.long_id, cap), "alloc segment classes");
+        CKB(sk->alloc(&D.totals, (uint64_t)D.long_cap * LOW_COUNTERS), "alloc totals");
+        CKB(cudaMemcpy(masks_d, sk->masks.data(), (size_t)H * 4, cudaMemcpyHostToDevice), "upload masks");
+        qs_status s = ctl_reset(sk, 0);
+        if (s != QS_OK) return bail(s);
+        CKB(cudaStreamSynchronize(0), "create sync");
+        e = msws_configure(dev, H, &sk->L);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "configure kernels"));
+    } else {
+        const uint32_t rows = p.m_low;
+        if (rows == 0 || rows > (uint32_t)MAX_CM_ROWS) return bail(fail(QS_ERR_INVALID_ARG, "cm rows out of [1, 16]"));
+        uint64_t n = p.n_low ? p.n_low : qs_find_greatest_prime(p.low_bytes / (4ull * rows));
+        if (n == 0 || n > 0xffffffffull) return bail(fail(QS_ERR_INVALID_ARG, "cm n out of range"));
+        sk->seeds.resize(rows);
+        if (p.seeds)
+            std::memcpy(sk->seeds.data(), p.seeds, rows * 4);
+        else
+            draw_seeds(p.seed_rng, rows, sk->seeds.data());  // ds.resize(_m, _ss), device_sketch_v0.h:130
+        CmDev& C = sk->C;
+        C.n = n;
+        C.fm = make_fastmod((uint32_t)n);
+        C.rows = rows;
+        for (uint32_t j = 0; j < rows; ++j) C.seeds[j] = sk->seeds[j];
+        CKB(sk->alloc(&C.table, n * rows), "alloc cm table");
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        sk->cm_grid = sms * 8;
+        CKB(cudaDeviceSynchronize(), "create sync");
+    }
+    *out = sk;
+    return QS_OK;
+}
+
+qs_status qs_destroy(qs_sketch* sk) {
+    if (!sk) return QS_OK;
+    {
+        DeviceGuard guard(sk->device);
+        for (int i = 0; i < 2; ++i)
+            if (sk->io[i]) {
+                cudaStreamSynchronize(sk->io[i]);
+                cudaStreamDestroy(sk->io[i]);
+            }
+        if (sk->done) cudaEventDestroy(sk->done);
+        for (auto& v : sk->ev)
+            for (auto& pr : v) {
+                cudaEventDestroy(pr.first);
+                cudaEventDestroy(pr.second);
+            }
+        cudaDeviceSynchronize();
+        for (void* v : sk->allocs) cudaFree(v);
+    }
+    delete sk;
+    return QS_OK;
+}
+
+qs_status qs_insert(qs_sketch* sk, const uint32_t* d_keys, size_t n, void* stream) {
+    if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
+    if (n == 0) return QS_OK;
+    if (!d_keys) return fail(QS_ERR_INVALID_ARG, "null keys");
+    if ((reinterpret_cast<uintptr_t>(d_keys) & 3u) != 0) return fail(QS_ERR_INVALID_ARG, "keys not 4-byte aligned");
+    DeviceGuard guard(sk->device);
+    return insert_device(sk, d_keys, n, static_cast<cudaStream_t>(stream));
+}
+
+qs_status qs_query(qs_sketch* sk, const uint32_t* d_keys, size_t n, uint32_t* d_counts, void* stream) {
+    if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
+    if (n == 0) return QS_OK;
+    if (!d_keys || !d_counts) return fail(QS_ERR_INVALID_ARG, "null keys or counts");
+    if (((reinterpret_cast<uintptr_t>(d_keys) | reinterpret_cast<uintptr_t>(d_counts)) & 3u) != 0)
+        return fail(QS_ERR_INVALID_ARG, "keys/counts not 4-byte aligned");
+    DeviceGuard guard(sk->device);
+    return query_device(sk, d_keys, n, d_counts, static_cast<cudaStream_t>(stream));
+}
+
+qs_status qs_insert_host(qs_sketch* sk, const uint32_t* h_keys, size_t n) {
+    if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
+    if (n == 0) return QS_OK;
+    if (!h_keys) return fail(QS_ERR_INVALID_ARG, "null keys");
+    DeviceGuard guard(sk->device);
+    std::lock_guard<std::mutex> lk(sk->mu);
+    qs_status s = setup_io(sk);
+    if (s != QS_OK) return s;
+    // Chunk c copies on io[c % 2] while chunk c-1 is inserted on io[(c-1) % 2]; the inserts
+    // stay in array order through the `done` event.
+    bool first = true;
+    uint64_t c = 0;
+    for (size_t off = 0; off < n; off += sk->stage_n, ++c) {
+        const int b = (int)(c & 1);
+        const uint64_t len = std::min<uint64_t>(sk->stage_n, n - off);
+        CK(cudaMemcpyAsync(sk->stage_keys[b], h_keys + off, len * 4, cudaMemcpyHostToDevice, sk->io[b]), "H2D keys");
+        if (!first) CK(cudaStreamWaitEvent(sk->io[b], sk->done, 0), "order inserts");
+        s = insert_device(sk, sk->stage_keys[b], len, sk->io[b]);
+        if (s != QS_OK) return s;
+        CK(cudaEventRecord(sk->done, sk->io[b]), "record insert");
+        first = false;
+    }
+    CK(cudaStreamSynchronize(sk->io[0]), "sync io");
+    CK(cudaStreamSynchronize(sk->io[1]), "sync io");
+    return QS_OK;
+}
+
+qs_status qs_query_host(qs_sketch* sk, const uint32_t* h_keys, size_t n, uint32_t* h_counts) {
+    if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
+    if (n == 0) return QS_OK;
+    if (!h_keys || !h_counts) return fail(QS_ERR_INVALID_ARG, "null keys or counts");
+    DeviceGuard guard(sk->device);
+    std::lock_guard<std::mutex> lk(sk->mu);
+    qs_status s = setup_io(sk);
+    if (s != QS_OK) return s;
+    uint64_t c = 0;
+    for (size_t off = 0; off < n; off += sk->stage_n, ++c) {
+        const int b = (int)(c & 1);
+        const uint64_t len = std::min<uint64_t>(sk->stage_n, n - off);
+        CK(cudaMemcpyAsync(sk->stage_keys[b], h_keys + off, len * 4, cudaMemcpyHostToDevice, sk->io[b]), "H2D keys");
+        s = query_device(sk, sk->stage_keys[b], len, sk->stage_out[b], sk->io[b]);
+        if (s != QS_OK) return s;
+        CK(cudaMemcpyAsync(h_counts + off, sk->stage_out[b], len * 4, cudaMemcpyDeviceToHost, sk->io[b]), "D2H counts");
+    }
+    CK(cudaStreamSynchronize(sk->io[0]), "sync io");
+    CK(cudaStreamSynchronize(sk->io[1]), "sync io");
+    return QS_OK;
+}
+
+qs_status qs_clear(qs_sketch* sk, void* stream) {
+    if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
+    DeviceGuard guard(sk->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (sk->kind == QS_KIND_MSWS) {
+        CK(cudaMemsetAsync(sk->D.low, 0, sk->D.n_low * LOW_WORDS * 4, st), "clear low");
+        CK(cudaMemsetAsync(sk->D.high, 0, sk->D.n_high * HIGH_WORDS * 4, st), "clear high");
+        CK(cudaMemsetAsync(sk->D.bitmap, 0, (sk->D.n_low + 31) / 32 * 4, st), "clear bitmap");
+        return ctl_reset(sk, st);
+    }
+    CK(cudaMemsetAsync(sk->C.table, 0, sk->C.n * sk->C.rows * 4, st), "clear table");
+    return QS_OK;
+}
+
+qs_status qs_sync(qs_sketch* sk, void* stream) {
+    if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
+    DeviceGuard guard(sk->device);
+    CK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "stream sync");
+    return check_status_word(sk);
+}
+
+qs_status qs_get_stats(qs_sketch* sk, qs_stats* out) {
+    if (!sk || !out) return fail(QS_ERR_INVALID_ARG, "null argument");
+    DeviceGuard guard(sk->device);
+    std::memset(out, 0, sizeof *out);
+    if (sk->kind != QS_KIND_MSWS) return QS_OK;
+    CK(cudaDeviceSynchronize(), "stats sync");
+    Ctl c;
+    CK(cudaMemcpy(&c, sk->D.ctl, sizeof c, cudaMemcpyDeviceToHost), "read stats");
+    out->status_bits = c.status;
+    const uint64_t cap = (uint64_t)START + sk->D.n_high;
+    out->next_level_id = (uint32_t)std::min<uint64_t>(c.next_id, cap);
+    out->linked_buckets = out->next_level_id - FIRST_ID;
+    out->dropped_keys = c.dropped;
+    out->repaired_buckets = c.repaired_buckets;
+    out->repaired_keys = c.repaired_keys;
+    return QS_OK;
+}
+
+qs_status qs_set_profiling(qs_sketch* sk, int enable) {
+    if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
+    DeviceGuard guard(sk->device);
+    CK(cudaDeviceSynchronize(), "profiling sync");
+    sk->prof = enable != 0;
+    for (int k = 0; k < 3; ++k) sk->ev_used[k] = 0;
+    return QS_OK;
+}
+
+qs_status qs_get_profile(qs_sketch* sk, qs_profile* out) {
+    if (!sk || !out) return fail(QS_ERR_INVALID_ARG, "null argument");
+    DeviceGuard guard(sk->device);
+    CK(cudaDeviceSynchronize(), "profile sync");
+    std::memset(out, 0, sizeof *out);
+    double ms[3] = {0, 0, 0};
+    for (int k = 0; k < 3; ++k)
+        for (size_t i = 0; i < sk->ev_used[k]; ++i) {
+            float t = 0;
+            CK(cudaEventElapsedTime(&t, sk->ev[k][i].first, sk->ev[k][i].second), "event time");
+            ms[k] += t;
+        }
+    out->insert_ms = ms[0];
+    out->repair_ms = ms[1];
+    out->query_ms = ms[2];
+    out->insert_timed = sk->ev_used[0];
+    out->repair_timed = sk->ev_used[1];
+    out->query_timed = sk->ev_used[2];
+    out->insert_launches = sk->launches[0];
+    out->repair_launches = sk->launches[1];
+    out->query_launches = sk->launches[2];
+    for (int k = 0; k < 3; ++k) sk->ev_used[k] = 0;
+    return QS_OK;
+}
+
+qs_status qs_reset_status(qs_sketch* sk) {
+    if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
+    if (sk->kind != QS_KIND_MSWS) return QS_OK;
+    DeviceGuard guard(sk->device);
+    CK(cudaDeviceSynchronize(), "sync");
+    CK(cudaMemset(&sk->D.ctl->status, 0, 4), "reset status");
+    return QS_OK;
+}
+
+qs_status qs_get_info(qs_sketch* sk, uint64_t* n_low, uint64_t* n_high, uint32_t* m_low, uint32_t* seeds_out,
+                      uint8_t* mask_table_out) {
+    if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
+    if (sk->kind == QS_KIND_MSWS) {
+        if (n_low) *n_low = sk->D.n_low;
+        if (n_high) *n_high = sk->D.n_high;
+        if (m_low) *m_low = LOW_WORDS;
+        if (mask_table_out) std::memcpy(mask_table_out, sk->masks.data(), sk->masks.size() * 4);
+    } else {
+        if (n_low) *n_low = sk->C.n;
+        if (n_high) *n_high = 0;
+        if (m_low) *m_low = sk->C.rows;
+    }
+    if (seeds_out) std::memcpy(seeds_out, sk->seeds.data(), sk->seeds.size() * 4);
+    return QS_OK;
+}
+
+qs_status qs_get_tables(qs_sketch* sk, uint32_t* h_low, uint32_t* h_high) {
+    if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
+    DeviceGuard guard(sk->device);
+    CK(cudaDeviceSynchronize(), "tables sync");
+    if (sk->kind == QS_KIND_MSWS) {
+        if (h_low) CK(cudaMemcpy(h_low, sk->D.low, sk->D.n_low * LOW_WORDS * 4, cudaMemcpyDeviceToHost), "copy low");
+        if (h_high) CK(cudaMemcpy(h_high, sk->D.high, sk->D.n_high * HIGH_WORDS * 4, cudaMemcpyDeviceToHost), "copy high");
+    } else if (h_low) {
+        CK(cudaMemcpy(h_low, sk->C.table, sk->C.n * sk->C.rows * 4, cudaMemcpyDeviceToHost), "copy table");
+    }
+    return QS_OK;
+}
+
+qs_status qs_gen_keys(uint32_t kind, uint64_t seed, uint64_t n_ranks, double s, uint64_t perm_seed, uint32_t* d_keys,
+                      uint32_t* d_ranks, size_t n, void* stream) {
+    if (kind > 1 || (!d_keys && n)) return fail(QS_ERR_INVALID_ARG, "gen_keys: bad arguments");
+    if (kind == 1 && (n_ranks == 0 || n_ranks > (1ull << 32) || s <= 0))
+        return fail(QS_ERR_INVALID_ARG, "gen_keys: zipf needs 0 < n_ranks <= 2^32, s > 0");
+    CK(gen_keys(kind, seed, n_ranks, s, perm_seed, d_keys, d_ranks, n, static_cast<cudaStream_t>(stream)), "gen_keys");
+    return QS_OK;
+}
+
+qs_status qs_gen_rank_keys(uint64_t perm_seed, uint64_t first, uint32_t* d_keys, size_t n, void* stream) {
+    if (!d_keys && n) return fail(QS_ERR_INVALID_ARG, "gen_rank_keys: null output");
+    CK(gen_rank_keys(perm_seed, first, d_keys, n, static_cast<cudaStream_t>(stream)), "gen_rank_keys");
+    return QS_OK;
+}
+
+qs_status qs_rank_histogram(const uint32_t* d_ranks, size_t n, uint32_t* d_hist, uint64_t n_ranks, void* stream) {
+    if ((!d_ranks || !d_hist) && n) return fail(QS_ERR_INVALID_ARG, "rank_histogram: null argument");
+    CK(rank_histogram(d_ranks, n, d_hist, n_ranks, static_cast<cudaStream_t>(stream)), "rank_histogram");
+    return QS_OK;
+}
+
+qs_status qs_error_metrics(const uint32_t* d_est, const uint32_t* d_exact, size_t n, double* mean_rel_err,
+                           double* mean_ratio, void* stream) {
+    if (!mean_rel_err || !mean_ratio) return fail(QS_ERR_INVALID_ARG, "error_metrics: null output");
+    double* acc = nullptr;
+    CK(cudaMalloc(&acc, 3 * sizeof(double)), "metrics scratch");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(acc, 0, 3 * sizeof(double), st);
+    if (e == cudaSuccess) e = error_metrics(d_est, d_exact, n, acc, st);
+    double h[3] = {0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, acc, sizeof h, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(acc);
+    if (e != cudaSuccess) return cuda_fail(e, "error_metrics");
+    *mean_rel_err = h[2] > 0 ? h[0] / h[2] : 0.0;
+    *mean_ratio = h[2] > 0 ? h[1] / h[2] : 0.0;
+    return QS_OK;
+}
+
+qs_status qs_probe(uint32_t kind, uint64_t bytes, uint64_t ops, double* ops_per_s) {
+    if (!ops_per_s) return fail(QS_ERR_INVALID_ARG, "probe: null output");
+    CK(probe(kind, bytes, ops, ops_per_s), "probe");
+    return QS_OK;
+}
+
+}  // extern "C"

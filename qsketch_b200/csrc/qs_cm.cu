@@ -1,0 +1,68 @@
+// qs_cm.cu — plain count-min ("thread sketch", Algorithm 1 of the paper), the in-GPU
+// baseline.  Reference: include/sketch/device_sketch/device_sketch_v0.h
+//   insert_kernel :13-55 (thread per key, m rows, atomicAdd), search_kernel :58-101 (min).
+// Row j hashes with its own seed: hv = key * seed[j], column hv % n (:48-52, :94-97).
+// Counter additions commute, so any schedule gives the sequential result.
+#include "qs_kernels.h"
+
+namespace qsb {
+
+constexpr int CM_THREADS = 256;
+
+template <int AGG>
+__global__ void __launch_bounds__(CM_THREADS) k_cm_insert(const uint32_t* __restrict__ keys, uint64_t n, CmDev D) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const uint64_t i = base + threadIdx.x;
+        const bool valid = i < n;
+        const uint32_t key = valid ? __ldcs(keys + i) : 0u;
+        uint32_t c = valid ? 1u : 0u;
+        if (AGG) {
+            const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
+            const uint32_t peers = __match_any_sync(0xffffffffu, key) & vmask;
+            c = (valid && lane == __ffs(peers) - 1) ? (uint32_t)__popc(peers) : 0u;
+        }
+        if (c) {
+            for (uint32_t j = 0; j < D.rows; ++j) {
+                const uint32_t col = fast_mod(D.fm, key * D.seeds[j]);
+                atomicAdd(D.table + (uint64_t)j * D.n + col, c);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(CM_THREADS) k_cm_query(const uint32_t* __restrict__ keys, uint64_t n,
+                                                         uint32_t* __restrict__ out, CmDev D) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t key = __ldcs(keys + i);
+        uint32_t c = 0xffffffffu;
+        for (uint32_t j = 0; j < D.rows; ++j) {
+            const uint32_t col = fast_mod(D.fm, key * D.seeds[j]);
+            c = min(c, __ldg(D.table + (uint64_t)j * D.n + col));
+        }
+        __stcs(out + i, c);
+    }
+}
+
+cudaError_t cm_insert(const uint32_t* d_keys, uint64_t n, const CmDev& D, int agg, int grid, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const uint64_t want = (n + CM_THREADS - 1) / CM_THREADS;
+    const int g = (int)std::min<uint64_t>((uint64_t)grid, std::max<uint64_t>(1, want));
+    if (agg)
+        k_cm_insert<1><<<g, CM_THREADS, 0, st>>>(d_keys, n, D);
+    else
+        k_cm_insert<0><<<g, CM_THREADS, 0, st>>>(d_keys, n, D);
+    return cudaGetLastError();
+}
+
+cudaError_t cm_query(const uint32_t* d_keys, uint64_t n, uint32_t* d_out, const CmDev& D, int grid, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const uint64_t want = (n + CM_THREADS - 1) / CM_THREADS;
+    const int g = (int)std::min<uint64_t>((uint64_t)grid, std::max<uint64_t>(1, want));
+    k_cm_query<<<g, CM_THREADS, 0, st>>>(d_keys, n, d_out, D);
+    return cudaGetLastError();
+}
+
+}  // namespace qsb

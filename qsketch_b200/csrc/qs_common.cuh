@@ -1,0 +1,116 @@
+// qs_common.cuh — constants, device layout and helpers shared by the sm_100a kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace qsb {
+
+// Reference constants (lib/default.cu:39-54, device_sketch_v3.h:160).
+constexpr uint32_t START = 1024;       // NEXT_LEVEL_ID_START: ids <= START are reserved
+constexpr uint32_t FIRST_ID = START + 1;  // Device_Hash_Table::resize sets 1025 (device_sketch.h:109)
+constexpr uint32_t LIMIT = 128;        // a selected 8-bit counter > LIMIT triggers the high level
+constexpr uint32_t CROSS = LIMIT + 2;  // a byte reaching 130 under all-adds means order matters
+constexpr uint32_t SATURATED = 2;      // word-7 value of a bucket whose link failed (pool full)
+constexpr uint32_t FLAG = 0x80000000u; // word-7 bit: bucket crossed during the current chunk
+constexpr int LOW_WORDS = 8;           // 32 B low bucket: 7 words of packed counters + index
+constexpr int LOW_COUNTERS = 28;       // generate_hashmask(..., 32, 3, 4): bits 0..27
+constexpr int HIGH_WORDS = 32;         // 128 B high bucket of u32 counters
+
+// Status bits latched in Ctl::status.
+constexpr uint32_t ST_POOL_FULL = 1u;
+constexpr uint32_t ST_TIMEOUT = 2u;
+constexpr uint32_t ST_CAPACITY = 4u;
+
+// Lemire-Kaser-Kurz direct remainder ("Faster Remainder by Direct Computation", 2019):
+// for d < 2^32 and M = ceil(2^64 / d), a % d == mulhi64(M * a mod 2^64, d) for all
+// 32-bit a.  Replaces the two run-time `%` of device_sketch_v3.h:42-44 per key.
+struct FastMod {
+    uint64_t M;
+    uint32_t d;
+    uint32_t pad;
+};
+
+inline FastMod make_fastmod(uint32_t d) {
+    FastMod f;
+    f.M = (d == 0) ? 0 : (~0ull / d + 1ull);  // d == 1 wraps to 0: a % 1 == 0 below too
+    f.d = d;
+    f.pad = 0;
+    return f;
+}
+
+__host__ __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
+__device__ __forceinline__ uint32_t fast_mod(const FastMod& f, uint32_t a) {
+    return (uint32_t)__umul64hi(f.M * (uint64_t)a, (uint64_t)f.d);
+}
+
+// Per-sketch device control block.
+struct Ctl {
+    uint32_t next_id;      // bump allocator (atomic_malloc, device_sketch_v3.h:69-85)
+    uint32_t status;       // latched ST_* bits
+    uint32_t n_flagged;    // buckets flagged in the current chunk
+    uint32_t n_records;    // records gathered for the ordered replay
+    uint32_t n_long;       // slots whose segment needed a grid-wide count
+    uint32_t bar_count;    // grid barrier
+    uint32_t bar_gen;
+    uint32_t pad0;
+    unsigned long long dropped;
+    unsigned long long repaired_buckets;
+    unsigned long long repaired_keys;
+    unsigned long long inserted;
+    uint32_t pad1[16];
+};
+
+// Everything a MSWS kernel needs, passed by value.
+struct MswsDev {
+    uint32_t* low;           // n_low * 8 words
+    uint32_t* high;          // n_high * 32 words
+    const uint32_t* masks;   // n_masks mask words (bit i selects counter i)
+    Ctl* ctl;
+    uint64_t n_low;
+    uint64_t n_high;
+    FastMod fm_low;
+    FastMod fm_mask;
+    uint32_t seed;
+    uint32_t n_masks;
+    uint32_t compat_v3;
+    uint32_t flag_cap;       // capacity of flag_list / per-slot arrays
+    // ordered-replay scratch
+    uint32_t* flag_list;     // slot -> bucket
+    uint32_t* bitmap;        // 1 bit per bucket, set while the bucket is flagged
+    uint32_t* tile_counts;   // per key tile of the chunk
+    uint2* rec[2];           // (slot, mask) records, ping-pong for the radix passes
+    uint32_t* hist;          // 256 * max record tiles
+    uint32_t* seg_beg;       // per slot: first record of its segment
+    uint32_t* long_id;       // per slot: index into totals or ~0u
+    uint32_t* totals;        // long slots * 28 counts
+    uint32_t long_cap;
+    uint32_t max_tiles;      // tiles of REPAIR_TILE elements in a chunk
+};
+
+struct CmDev {
+    uint32_t* table;  // rows * n
+    uint64_t n;
+    FastMod fm;
+    uint32_t rows;
+    uint32_t pad;
+    uint32_t seeds[16];
+};
+
+constexpr int REPAIR_TILE = 4096;   // elements per tile in the ordered-replay passes
+constexpr int REPAIR_THREADS = 512; // 16 warps x 256 elements
+constexpr int LONG_SEGMENT = 256;   // segments longer than this get grid-wide counting
+constexpr int MAX_CM_ROWS = 16;
+
+// Spread a 4-bit nibble to the low bit of each byte: b0->bit0, b1->bit8, b2->bit16, b3->bit24.
+__device__ __forceinline__ uint32_t expand_nibble(uint32_t nib) {
+    return (nib * 0x00204081u) & 0x01010101u;
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(r));
+    return r;
+}
+
+}  // namespace qsb

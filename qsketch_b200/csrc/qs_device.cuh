@@ -1,0 +1,145 @@
+// qs_device.cuh — PTX helpers (mbarrier, TMA bulk copy), bounded waits, block scans.
+#pragma once
+#include "qs_common.cuh"
+
+namespace qsb {
+
+// ---- bounded waits -------------------------------------------------------------------
+// Every spin in this library gives up after about a second and latches ST_TIMEOUT.
+constexpr uint32_t SPIN_LIMIT = 1u << 23;  // iterations of ~128 ns sleeps (~1 s)
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// TMA bulk copy global -> this CTA's shared memory (no tensor map, no multicast).
+// dst, src 16-byte aligned; bytes a multiple of 16.
+__device__ __forceinline__ void tma_bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase; false after SPIN_LIMIT tries.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (uint32_t it = 0; it < SPIN_LIMIT; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        __nanosleep(64);
+    }
+    return false;
+}
+
+// ---- grid barrier for cooperative launches (bounded) ---------------------------------
+// All blocks of the grid are co-resident (cudaLaunchCooperativeKernel).  Returns false
+// (and latches ST_TIMEOUT) if the other blocks do not arrive within the spin limit.
+__device__ __forceinline__ bool grid_barrier(Ctl* ctl) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile uint32_t* genp = &ctl->bar_gen;
+        const uint32_t gen = *genp;
+        __threadfence();
+        const uint32_t arrived = atomicAdd(&ctl->bar_count, 1u);
+        int ok = 1;
+        if (arrived == gridDim.x - 1) {
+            atomicExch(&ctl->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&ctl->bar_gen, 1u);
+        } else {
+            uint32_t it = 0;
+            while (*genp == gen) {
+                if (++it > SPIN_LIMIT) {
+                    ok = 0;
+                    atomicOr(&ctl->status, ST_TIMEOUT);
+                    break;
+                }
+                __nanosleep(128);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// ---- block-wide scans ------------------------------------------------------------------
+// Exclusive scan of one value per thread (blockDim.x <= 1024, multiple of 32).
+// Returns the exclusive prefix; *total receives the block sum (all threads).
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_total;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t t = lane < nw ? s_warp[lane] : 0u;
+        uint32_t u = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, u, o);
+            if (lane >= o) u += y;
+        }
+        if (lane < nw) s_warp[lane] = u - t;
+        if (lane == 31) s_total = u;
+    }
+    __syncthreads();
+    const uint32_t r = s_warp[wid] + x - v;
+    *total = s_total;
+    __syncthreads();
+    return r;
+}
+
+// Exclusive scan in place of a global array a[0..len) by one block; returns the total.
+__device__ __forceinline__ uint32_t block_scan_array(uint32_t* a, uint32_t len) {
+    const uint32_t per = (len + blockDim.x - 1) / blockDim.x;
+    const uint32_t beg = threadIdx.x * per;
+    const uint32_t end = min(len, beg + per);
+    uint32_t sum = 0;
+    for (uint32_t i = beg; i < end; ++i) sum += __ldcg(a + i);
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(sum, &total);
+    for (uint32_t i = beg; i < end; ++i) {
+        uint32_t t = __ldcg(a + i);
+        __stcg(a + i, run);
+        run += t;
+    }
+    return total;
+}
+
+}  // namespace qsb

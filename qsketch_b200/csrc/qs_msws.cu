@@ -1,0 +1,625 @@
+// qs_msws.cu — MSWS ("Level" QSketch) insert and query kernels for sm_100a.
+//
+// Reference path: include/sketch/device_sketch/device_sketch_v3.h
+//   insert_kernel :194-290, calculation_s2_insert :88-191, insert_high :54-65,
+//   atomic_malloc :69-85, search_kernel :411-521, calculation_s2_search :311-408.
+//
+// Exactness.  The reference applies keys concurrently, so once a bucket's 8-bit counter
+// passes 128 its result depends on the schedule.  Here a chunk of keys is applied in two
+// steps whose result equals the one-key-at-a-time order of the array:
+//   1. k_msws_insert: every key of an unlinked bucket adds its packed 8-bit increments
+//      with returning 32-bit atomics (a sub-warp of 8 lanes per key, lane w on word w, as
+//      in the reference).  A bucket's result is independent of order iff no selected
+//      counter ends the chunk above 129; a key whose atomic saw old + add >= 130 proves
+//      the opposite and flags the bucket (word 7 := FLAG | slot).  Keys of linked buckets
+//      add to the high bucket (commutative).
+//   2. k_msws_repair (only if something was flagged): gathers the flagged buckets' keys
+//      in array order (stable filter + stable LSD radix by slot), restores each bucket's
+//      pre-chunk words (u32 addition is a group: pre = final - sum of the packed adds),
+//      finds the first key that sees a selected counter > 128, links the bucket there and
+//      moves the increments of that key and all later ones to the new high bucket.
+#include "qs_device.cuh"
+#include "qs_kernels.h"
+
+namespace qsb {
+
+constexpr int INS_THREADS = 256;
+constexpr int INS_TILE = 2048;  // keys per TMA stage (8 KiB)
+constexpr int INS_STAGES = 3;
+
+// ---- pass 1 -------------------------------------------------------------------------------
+
+__device__ __forceinline__ void flag_bucket(const MswsDev& D, uint32_t b) {
+    uint32_t* w7 = D.low + (uint64_t)b * LOW_WORDS + 7;
+    const uint32_t old = atomicOr(w7, FLAG);
+    if (old & FLAG) return;
+    const uint32_t slot = atomicAdd(&D.ctl->n_flagged, 1u);
+    if (slot < D.flag_cap) {
+        D.flag_list[slot] = b;
+        atomicOr(D.bitmap + (b >> 5), 1u << (b & 31));
+        atomicExch(w7, FLAG | slot);
+    } else {
+        atomicOr(&D.ctl->status, ST_CAPACITY);
+    }
+}
+
+// Process up to 32 keys held one per lane (valid lanes: lane < cnt).
+template <int AGG>
+__device__ __forceinline__ void insert_group(const MswsDev& D, const uint32_t* s_masks, uint32_t key, int cnt) {
+    const int lane = threadIdx.x & 31;
+    const int sub = lane >> 3, w = lane & 7;
+    const bool valid = lane < cnt;
+    const uint32_t hv = key * D.seed;  // hash_mul_add, device_hash_function.h:6-18
+    const uint32_t b = fast_mod(D.fm_low, hv);
+    const uint32_t m = s_masks[fast_mod(D.fm_mask, hv)];
+    uint32_t c = valid ? 1u : 0u;
+    if (AGG) {  // merge equal keys of the warp: one leader carries the multiplicity
+        const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
+        const uint32_t peers = __match_any_sync(0xffffffffu, key) & vmask;
+        c = (valid && lane == __ffs(peers) - 1) ? (uint32_t)__popc(peers) : 0u;
+    }
+    const uint32_t w7 = c ? __ldcg(D.low + (uint64_t)b * LOW_WORDS + 7) : 0u;
+
+    // Issue the atomics of all 8 rounds (4 keys per round) before checking any result.
+    uint32_t olds[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int src = r * 4 + sub;
+        const uint32_t bb = __shfl_sync(0xffffffffu, b, src);
+        const uint32_t mm = __shfl_sync(0xffffffffu, m, src);
+        const uint32_t cc = __shfl_sync(0xffffffffu, c, src);
+        const uint32_t ww = __shfl_sync(0xffffffffu, w7, src);
+        olds[r] = 0;
+        if (cc == 0 || ww == SATURATED) continue;
+        if (ww > START && (uint64_t)(ww - START) < D.n_high) {
+            // linked bucket: insert_high (device_sketch_v3.h:111-129), lane w takes the
+            // w-th selected counter
+            uint32_t* hb = D.high + (uint64_t)(ww - START) * HIGH_WORDS;
+            const int pc = __popc(mm);
+            for (int k = w; k < pc; k += 8) atomicAdd(hb + __fns(mm, 0, k + 1), cc);
+        } else {
+            // packed low add (device_sketch_v3.h:131-170), lane w owns word w
+            const uint32_t nib = (w < 7) ? (mm >> (4 * w)) & 0xfu : 0u;
+            if (nib) olds[r] = atomicAdd(D.low + (uint64_t)bb * LOW_WORDS + w, expand_nibble(nib) * cc);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int src = r * 4 + sub;
+        const uint32_t bb = __shfl_sync(0xffffffffu, b, src);
+        const uint32_t mm = __shfl_sync(0xffffffffu, m, src);
+        const uint32_t cc = __shfl_sync(0xffffffffu, c, src);
+        const uint32_t ww = __shfl_sync(0xffffffffu, w7, src);
+        const bool lowp = cc != 0 && ww != SATURATED && !(ww > START && (uint64_t)(ww - START) < D.n_high);
+        const uint32_t nib = (w < 7) ? (mm >> (4 * w)) & 0xfu : 0u;
+        bool cross = false;
+        if (lowp && nib) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (((nib >> k) & 1u) && ((olds[r] >> (8 * k)) & 0xffu) + cc >= CROSS) cross = true;
+        }
+        const uint32_t bal = __ballot_sync(0xffffffffu, cross);
+        if (w == 0 && ((bal >> (sub * 8)) & 0xffu)) flag_bucket(D, bb);
+        if (w == 0 && cc != 0 && ww == SATURATED) atomicAdd(&D.ctl->dropped, (unsigned long long)cc);
+    }
+}
+
+template <int AGG>
+__global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* __restrict__ keys, uint64_t n,
+                                                             MswsDev D) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint32_t* s_keys = reinterpret_cast<uint32_t*>(smem);                      // STAGES * TILE
+    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_keys + INS_STAGES * INS_TILE);
+    uint32_t* s_masks = reinterpret_cast<uint32_t*>(s_bar + INS_STAGES);       // n_masks
+    __shared__ uint32_t s_extra[8];
+    __shared__ int s_ok;
+
+    const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
+    for (uint32_t i = tid; i < D.n_masks; i += blockDim.x) s_masks[i] = __ldg(D.masks + i);
+
+    // 16-byte aligned body for the TMA bulk copies; the <= 6 ragged keys go through CTA 0.
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(keys);
+    const uint64_t head = umin64(n, ((16u - (addr & 15u)) & 15u) >> 2);
+    const uint64_t body_n = ((n - head) >> 2) << 2;
+    const uint64_t tail = n - head - body_n;
+    const uint32_t* body = keys + head;
+
+    if (tid == 0) {
+        for (int s = 0; s < INS_STAGES; ++s) mbar_init(&s_bar[s], 1);
+        fence_mbar_init();
+    }
+    if (blockIdx.x == 0 && tid < (int)(head + tail))
+        s_extra[tid] = (tid < (int)head) ? keys[tid] : keys[head + body_n + (tid - head)];
+    __syncthreads();
+    if (blockIdx.x == 0 && wid == 0 && head + tail > 0) {
+        const uint32_t k = lane < (int)(head + tail) ? s_extra[lane] : 0u;
+        insert_group<AGG>(D, s_masks, k, (int)(head + tail));
+    }
+
+    const uint64_t ntiles = (body_n + INS_TILE - 1) / INS_TILE;
+    if (blockIdx.x >= ntiles) return;
+    const uint64_t my_tiles = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x;
+
+    auto issue = [&](uint64_t i) {
+        const int st = (int)(i % INS_STAGES);
+        const uint64_t g = blockIdx.x + i * gridDim.x;
+        const uint64_t start = g * INS_TILE;
+        const uint32_t cnt = (uint32_t)umin64(INS_TILE, body_n - start);
+        mbar_arrive_expect_tx(&s_bar[st], cnt * 4u);
+        tma_bulk_g2s(s_keys + st * INS_TILE, body + start, cnt * 4u, &s_bar[st]);
+    };
+    if (tid == 0)
+        for (uint64_t i = 0; i < umin64(INS_STAGES, my_tiles); ++i) issue(i);
+
+    for (uint64_t i = 0; i < my_tiles; ++i) {
+        const int st = (int)(i % INS_STAGES);
+        const uint32_t parity = (uint32_t)((i / INS_STAGES) & 1u);
+        if (tid == 0) s_ok = mbar_wait_bounded(&s_bar[st], parity) ? 1 : 0;
+        __syncthreads();
+        if (!s_ok) {
+            if (tid == 0) {
+                atomicOr(&D.ctl->status, ST_TIMEOUT);
+                // wait (bounded) for the copies still in flight before leaving
+                for (uint64_t j = i; j < umin64(i + INS_STAGES, my_tiles); ++j)
+                    mbar_wait_bounded(&s_bar[j % INS_STAGES], (uint32_t)((j / INS_STAGES) & 1u));
+            }
+            return;
+        }
+        for (uint32_t it = 0; it < 64 && !mbar_try_wait(&s_bar[st], parity); ++it) {
+        }
+        const uint64_t g = blockIdx.x + i * gridDim.x;
+        const int cnt = (int)umin64(INS_TILE, body_n - g * INS_TILE);
+        const uint32_t* tk = s_keys + st * INS_TILE;
+        // each warp takes 32-key groups round-robin
+        for (int base = wid * 32; base < cnt; base += INS_THREADS) {
+            const int c = min(32, cnt - base);
+            const uint32_t k = lane < c ? tk[base + lane] : 0u;
+            insert_group<AGG>(D, s_masks, k, c);
+        }
+        __syncthreads();
+        if (tid == 0 && i + INS_STAGES < my_tiles) {
+            fence_proxy_async_smem();
+            issue(i + INS_STAGES);
+        }
+    }
+}
+
+// ---- ordered replay ---------------------------------------------------------------------
+
+__device__ __forceinline__ bool is_flagged(const MswsDev& D, uint32_t b) {
+    return (__ldcg(D.bitmap + (b >> 5)) >> (b & 31)) & 1u;
+}
+
+__device__ __forceinline__ int radix_passes(uint32_t F) {
+    if (F <= 1) return 0;
+    const int bits = 32 - __clz(F - 1);
+    return (bits + 7) / 8;
+}
+
+// Stable per-warp ranking of 256 consecutive elements by an 8-bit digit, three steps:
+// count (per warp), offsets (per digit across warps), rank + scatter.
+struct RadixSmem {
+    uint32_t whist[REPAIR_THREADS / 32][256];
+};
+
+__global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* __restrict__ keys, uint64_t n,
+                                                                MswsDev D) {
+    __shared__ RadixSmem rs;
+    __shared__ uint32_t s_acc[2][LOW_COUNTERS];
+    __shared__ uint32_t s_acc_slot[2];
+    Ctl* ctl = D.ctl;
+    const uint32_t F = min(__ldcg(&ctl->n_flagged), D.flag_cap);
+    if (F == 0) return;
+
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    constexpr int NW = REPAIR_THREADS / 32;
+    constexpr int PER = REPAIR_TILE / REPAIR_THREADS;  // 8 elements per thread
+    const uint32_t ntk = (uint32_t)((n + REPAIR_TILE - 1) / REPAIR_TILE);
+
+    // Phase 1: count keys of flagged buckets per tile of the chunk.
+    for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
+        const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
+        uint32_t c = 0;
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const uint64_t i = base + j;
+            if (i < n) {
+                const uint32_t hv = __ldg(keys + i) * D.seed;
+                c += is_flagged(D, fast_mod(D.fm_low, hv)) ? 1u : 0u;
+            }
+        }
+        uint32_t total;
+        block_exclusive_scan(c, &total);
+        if (tid == 0) __stcg(D.tile_counts + t, total);
+    }
+    if (!grid_barrier(ctl)) return;
+    // Phase 2: exclusive scan of the tile counts.
+    if (blockIdx.x == 0) {
+        const uint32_t K = block_scan_array(D.tile_counts, ntk);
+        if (tid == 0) __stcg(&ctl->n_records, K);
+    }
+    if (!grid_barrier(ctl)) return;
+    const uint32_t K = __ldcg(&ctl->n_records);
+    // Phase 3: stable write of (slot, mask) records in array order.
+    for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
+        const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
+        uint32_t c = 0;
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const uint64_t i = base + j;
+            if (i < n) {
+                const uint32_t hv = __ldg(keys + i) * D.seed;
+                if (is_flagged(D, fast_mod(D.fm_low, hv))) ++c;
+            }
+        }
+        uint32_t total;
+        uint32_t pos = block_exclusive_scan(c, &total) + __ldcg(D.tile_counts + t);
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const uint64_t i = base + j;
+            if (i < n) {
+                const uint32_t hv = __ldg(keys + i) * D.seed;
+                const uint32_t b = fast_mod(D.fm_low, hv);
+                if (is_flagged(D, b)) {
+                    const uint32_t slot = __ldcg(D.low + (uint64_t)b * LOW_WORDS + 7) & ~FLAG;
+                    const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hv));
+                    __stcg(D.rec[0] + pos, make_uint2(slot, mask));
+                    ++pos;
+                }
+            }
+        }
+    }
+    if (!grid_barrier(ctl)) return;
+
+    // Phase 4: stable LSD radix sort of the records by slot, 8 bits per pass.
+    const int npass = radix_passes(F);
+    const uint32_t ntr = (K + REPAIR_TILE - 1) / REPAIR_TILE;
+    for (int p = 0; p < npass; ++p) {
+        const uint2* src = D.rec[p & 1];
+        uint2* dst = D.rec[(p + 1) & 1];
+        const int shift = 8 * p;
+        // 4a: per-tile digit histograms (digit-major: hist[d * ntr + t])
+        for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {
+            for (int d = tid; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
+            __syncthreads();
+            for (int r = 0; r < 256 / 32; ++r) {
+                const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
+                const bool v = i < K;
+                const uint32_t d = v ? (__ldcg(&src[i].x) >> shift) & 0xffu : 256u + lane;
+                const uint32_t peers = __match_any_sync(0xffffffffu, d);
+                if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
+                __syncwarp();
+            }
+            __syncthreads();
+            for (int d = tid; d < 256; d += REPAIR_THREADS) {
+                uint32_t s = 0;
+                for (int w = 0; w < NW; ++w) s += rs.whist[w][d];
+                __stcg(D.hist + (uint64_t)d * ntr + t, s);
+            }
+            __syncthreads();
+        }
+        if (!grid_barrier(ctl)) return;
+        if (blockIdx.x == 0) block_scan_array(D.hist, 256u * ntr);
+        if (!grid_barrier(ctl)) return;
+        // 4c: stable scatter
+        for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {
+            for (int d = tid; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
+            __syncthreads();
+            for (int r = 0; r < 256 / 32; ++r) {
+                const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
+                const bool v = i < K;
+                const uint32_t d = v ? (__ldcg(&src[i].x) >> shift) & 0xffu : 256u + lane;
+                const uint32_t peers = __match_any_sync(0xffffffffu, d);
+                if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
+                __syncwarp();
+            }
+            __syncthreads();
+            for (int d = tid; d < 256; d += REPAIR_THREADS) {
+                uint32_t run = __ldcg(D.hist + (uint64_t)d * ntr + t);
+                for (int w = 0; w < NW; ++w) {
+                    const uint32_t x = rs.whist[w][d];
+                    rs.whist[w][d] = run;
+                    run += x;
+                }
+            }
+            __syncthreads();
+            for (int r = 0; r < 256 / 32; ++r) {
+                const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
+                const bool v = i < K;
+                const uint2 rec = v ? __ldcg(&src[i]) : make_uint2(0, 0);
+                const uint32_t d = v ? (rec.x >> shift) & 0xffu : 256u + lane;
+                const uint32_t peers = __match_any_sync(0xffffffffu, d);
+                if (v) {
+                    const uint32_t rank = rs.whist[wid][d] + __popc(peers & lanemask_lt());
+                    __stcg(dst + rank, rec);
+                }
+                __syncwarp();
+                if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
+                __syncwarp();
+            }
+            __syncthreads();
+        }
+        if (!grid_barrier(ctl)) return;
+    }
+    const uint2* sorted = D.rec[npass & 1];
+
+    // Phase 5: segment starts per slot, then segment classes.
+    for (uint32_t i = blockIdx.x * REPAIR_THREADS + tid; i < K; i += gridDim.x * REPAIR_THREADS) {
+        const uint32_t s = __ldcg(&sorted[i].x);
+        if (i == 0 || __ldcg(&sorted[i - 1].x) != s) __stcg(D.seg_beg + s, i);
+    }
+    if (!grid_barrier(ctl)) return;
+    for (uint32_t s = blockIdx.x * REPAIR_THREADS + tid; s < F; s += gridDim.x * REPAIR_THREADS) {
+        const uint32_t beg = __ldcg(D.seg_beg + s);
+        const uint32_t end = (s + 1 < F) ? __ldcg(D.seg_beg + s + 1) : K;
+        uint32_t lid = ~0u;
+        if (end - beg > (uint32_t)LONG_SEGMENT) {
+            const uint32_t l = atomicAdd(&ctl->n_long, 1u);
+            if (l < D.long_cap) {
+                lid = l;
+                for (int i = 0; i < LOW_COUNTERS; ++i) __stcg(D.totals + (uint64_t)l * LOW_COUNTERS + i, 0u);
+            }
+        }
+        __stcg(D.long_id + s, lid);
+    }
+    if (!grid_barrier(ctl)) return;
+
+    // Phase 6: per-counter totals of long segments; each block a contiguous record range,
+    // the range's first and last slot accumulate in shared memory.
+    {
+        const uint32_t per = ((K + gridDim.x - 1) / gridDim.x + 31) & ~31u;
+        const uint32_t beg = min(K, blockIdx.x * per), end = min(K, beg + per);
+        if (tid < 2 * LOW_COUNTERS) (&s_acc[0][0])[tid] = 0;
+        if (tid == 0) {
+            s_acc_slot[0] = beg < end ? __ldcg(&sorted[beg].x) : ~0u;
+            s_acc_slot[1] = beg < end ? __ldcg(&sorted[end - 1].x) : ~0u;
+        }
+        __syncthreads();
+        for (uint32_t g = beg + wid * 32; g < end; g += REPAIR_THREADS) {
+            const uint32_t i = g + lane;
+            const bool v = i < end;
+            const uint2 rec = v ? __ldcg(&sorted[i]) : make_uint2(~0u, 0u);
+            const uint32_t lid = v ? __ldcg(D.long_id + rec.x) : ~0u;
+            const bool use = v && lid != ~0u;
+            const uint32_t peers = __match_any_sync(0xffffffffu, rec.x);
+            const bool leader = lane == __ffs(peers) - 1;
+            const int sl = rec.x == s_acc_slot[0] ? 0 : (rec.x == s_acc_slot[1] ? 1 : -1);
+            for (int c = 0; c < LOW_COUNTERS; ++c) {
+                const uint32_t bal = __ballot_sync(0xffffffffu, use && ((rec.y >> c) & 1u));
+                const uint32_t cnt = __popc(bal & peers);
+                if (use && leader && cnt) {
+                    if (sl >= 0)
+                        atomicAdd(&s_acc[sl][c], cnt);
+                    else
+                        atomicAdd(D.totals + (uint64_t)lid * LOW_COUNTERS + c, cnt);
+                }
+            }
+        }
+        __syncthreads();
+        if (tid < 2 * LOW_COUNTERS) {
+            const int sl = tid / LOW_COUNTERS, c = tid % LOW_COUNTERS;
+            const uint32_t s = s_acc_slot[sl];
+            const bool dup = (sl == 1 && s == s_acc_slot[0]);
+            const uint32_t v = s_acc[sl][c];
+            if (s != ~0u && !dup && v) {
+                const uint32_t lid = __ldcg(D.long_id + s);
+                if (lid != ~0u) atomicAdd(D.totals + (uint64_t)lid * LOW_COUNTERS + c, v);
+            }
+        }
+    }
+    if (!grid_barrier(ctl)) return;
+
+    // Phase 7: replay each flagged bucket in array order, one warp per slot.
+    const uint32_t lt = lanemask_lt();
+    for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) {
+        const uint32_t b = __ldcg(D.flag_list + s);
+        const uint32_t beg = __ldcg(D.seg_beg + s);
+        const uint32_t end = (s + 1 < F) ? __ldcg(D.seg_beg + s + 1) : K;
+        const uint32_t lid = __ldcg(D.long_id + s);
+        uint32_t T = 0;  // lane i < 28: occurrences of counter i in the chunk
+        if (lid != ~0u) {
+            T = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)lid * LOW_COUNTERS + lane) : 0u;
+        } else {
+            for (uint32_t g = beg; g < end; g += 32) {
+                const uint32_t m = (g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u;
+#pragma unroll
+                for (int c = 0; c < LOW_COUNTERS; ++c) {
+                    const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
+                    if (lane == c) T += __popc(bal);
+                }
+            }
+        }
+        uint32_t* wp = D.low + (uint64_t)b * LOW_WORDS;
+        const uint32_t fw = lane < 7 ? __ldcg(wp + lane) : 0u;
+        // pre-chunk word = final word - packed sum of the chunk's increments (mod 2^32)
+        uint32_t sw = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t t = __shfl_sync(0xffffffffu, T, (4 * (lane & 7) + k) & 31);
+            sw += t << (8 * k);
+        }
+        const uint32_t pw = fw - sw;
+        const uint32_t pwi = __shfl_sync(0xffffffffu, pw, (lane >> 2) & 7);
+        const uint32_t P = lane < LOW_COUNTERS ? (pwi >> (8 * (lane & 3))) & 0xffu : 0u;
+        uint32_t cur = P;
+        // first key (array order) that sees a selected counter > LIMIT
+        uint32_t L = ~0u, mL = 0;
+        for (uint32_t g = beg; g < end; g += 32) {
+            const uint32_t m = (g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u;
+            bool trig = false;
+            uint32_t inc = 0;
+#pragma unroll
+            for (int c = 0; c < LOW_COUNTERS; ++c) {
+                const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
+                const uint32_t cc = __shfl_sync(0xffffffffu, cur, c);
+                if (((m >> c) & 1u) && cc + __popc(bal & lt) > LIMIT) trig = true;
+                if (lane == c) inc = __popc(bal);
+            }
+            const uint32_t tb = __ballot_sync(0xffffffffu, trig);
+            if (tb) {
+                const int j = __ffs(tb) - 1;
+                const uint32_t before = (1u << j) - 1u;
+#pragma unroll
+                for (int c = 0; c < LOW_COUNTERS; ++c) {
+                    const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
+                    if (lane == c) cur += __popc(bal & before);
+                }
+                L = g + j;
+                mL = __shfl_sync(0xffffffffu, m, j);
+                break;
+            }
+            cur += inc;
+        }
+        if (L != ~0u) {
+            uint32_t H = T - (cur - P);  // increments of key L and all later keys
+            if (D.compat_v3) {          // device_sketch_v3.h:187: linking key lands on bit % 8
+                if (lane < LOW_COUNTERS && ((mL >> lane) & 1u)) H -= 1u;
+                if (lane < 8) H += __popc(mL & (0x01010101u << lane));
+            }
+            uint32_t id = 0;
+            if (lane == 0) id = atomicAdd(&ctl->next_id, 1u);
+            id = __shfl_sync(0xffffffffu, id, 0);
+            const bool ok = (uint64_t)(id - START) < D.n_high;
+            if (ok) {
+                __stcg(D.high + (uint64_t)(id - START) * HIGH_WORDS + lane, H);
+            } else if (lane == 0) {
+                atomicOr(&ctl->status, ST_POOL_FULL);
+                atomicAdd(&ctl->dropped, (unsigned long long)(end - L));
+            }
+            uint32_t word = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) word |= __shfl_sync(0xffffffffu, cur, (4 * (lane & 7) + k) & 31) << (8 * k);
+            if (lane < 7) __stcg(wp + lane, word);
+            if (lane == 7) __stcg(wp + 7, ok ? id : SATURATED);
+        } else {
+            if (lane == 7) __stcg(wp + 7, 0u);  // every key added; the words are final
+        }
+        if (lane == 0) {
+            atomicAnd(D.bitmap + (b >> 5), ~(1u << (b & 31)));
+            atomicAdd(&ctl->repaired_buckets, 1ull);
+            atomicAdd(&ctl->repaired_keys, (unsigned long long)(end - beg));
+        }
+    }
+    if (!grid_barrier(ctl)) return;
+    if (blockIdx.x == 0 && tid == 0) {
+        ctl->n_flagged = 0;
+        ctl->n_records = 0;
+        ctl->n_long = 0;
+        __threadfence();
+    }
+}
+
+// ---- query ----------------------------------------------------------------------------
+
+constexpr int QRY_THREADS = 256;
+constexpr int QRY_KPT = 4;
+
+__device__ __forceinline__ uint32_t msws_lookup(const MswsDev& D, const uint32_t* s_masks, uint32_t key) {
+    const uint32_t hv = key * D.seed;
+    const uint32_t b = fast_mod(D.fm_low, hv);
+    const uint32_t m = s_masks[fast_mod(D.fm_mask, hv)];
+    const uint4* bp = reinterpret_cast<const uint4*>(D.low + (uint64_t)b * LOW_WORDS);
+    const uint4 a = __ldg(bp), c = __ldg(bp + 1);
+    const uint32_t u[8] = {a.x, a.y, a.z, a.w, c.x, c.y, c.z, c.w};
+    // min over the selected bytes (calculation_s2_search, device_sketch_v3.h:340-357,397-402)
+    uint32_t acc = 0xffffffffu;
+#pragma unroll
+    for (int w = 0; w < 7; ++w) {
+        const uint32_t sel = expand_nibble((m >> (4 * w)) & 0xfu) * 0xffu;
+        acc = __vminu4(acc, u[w] | ~sel);
+    }
+    acc = __vminu4(acc, acc >> 16);
+    const uint32_t lo = min(acc & 0xffu, (acc >> 8) & 0xffu);
+    const uint32_t ptr = u[7];
+    uint32_t hi = 0;
+    if (ptr > START && (uint64_t)(ptr - START) < D.n_high) {  // search_high, device_sketch_v3.h:293-307, 364-395
+        const uint32_t* hb = D.high + (uint64_t)(ptr - START) * HIGH_WORDS;
+        hi = 0xffffffffu;
+        for (uint32_t mm = m; mm; mm &= mm - 1) hi = min(hi, __ldg(hb + (__ffs(mm) - 1)));
+    }
+    return lo + hi;
+}
+
+__global__ void __launch_bounds__(QRY_THREADS) k_msws_query(const uint32_t* __restrict__ keys, uint64_t n,
+                                                            uint32_t* __restrict__ out, MswsDev D) {
+    extern __shared__ __align__(16) uint32_t s_masks[];
+    for (uint32_t i = threadIdx.x; i < D.n_masks; i += blockDim.x) s_masks[i] = __ldg(D.masks + i);
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += stride * QRY_KPT) {
+        uint32_t k[QRY_KPT], r[QRY_KPT];
+#pragma unroll
+        for (int j = 0; j < QRY_KPT; ++j) {
+            const uint64_t i = base + j * stride;
+            k[j] = i < n ? __ldcs(keys + i) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < QRY_KPT; ++j) r[j] = msws_lookup(D, s_masks, k[j]);
+#pragma unroll
+        for (int j = 0; j < QRY_KPT; ++j) {
+            const uint64_t i = base + j * stride;
+            if (i < n) __stcs(out + i, r[j]);
+        }
+    }
+}
+
+// ---- launchers ----------------------------------------------------------------------------
+
+size_t msws_insert_smem(uint32_t n_masks) {
+    return (size_t)INS_STAGES * INS_TILE * 4 + INS_STAGES * 8 + (size_t)n_masks * 4;
+}
+
+cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return e;
+    L->num_sms = prop.multiProcessorCount;
+    const size_t ins_smem = msws_insert_smem(n_masks);
+    for (int agg = 0; agg < 2; ++agg) {
+        const void* fn = agg ? (const void*)k_msws_insert<1> : (const void*)k_msws_insert<0>;
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ins_smem);
+        if (e != cudaSuccess) return e;
+    }
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_insert<0>, INS_THREADS, ins_smem);
+    if (e != cudaSuccess) return e;
+    L->insert_grid = prop.multiProcessorCount * (occ > 0 ? occ : 1);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_repair, REPAIR_THREADS, 0);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    L->repair_grid = prop.multiProcessorCount * (occ < 2 ? occ : 2);
+    L->query_grid = prop.multiProcessorCount * 8;
+    return cudaSuccess;
+}
+
+cudaError_t msws_insert_pass(const uint32_t* d_keys, uint64_t n, const MswsDev& D, const MswsLaunch& L, int agg,
+                             cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const size_t smem = msws_insert_smem(D.n_masks);
+    const uint64_t tiles = (n + INS_TILE - 1) / INS_TILE;
+    const int grid = (int)std::min<uint64_t>((uint64_t)L.insert_grid, std::max<uint64_t>(1ull, tiles));
+    if (agg)
+        k_msws_insert<1><<<grid, INS_THREADS, smem, st>>>(d_keys, n, D);
+    else
+        k_msws_insert<0><<<grid, INS_THREADS, smem, st>>>(d_keys, n, D);
+    return cudaGetLastError();
+}
+
+cudaError_t msws_repair(const uint32_t* d_keys, uint64_t n, const MswsDev& D, const MswsLaunch& L, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    MswsDev Dc = D;
+    void* args[] = {(void*)&d_keys, (void*)&n, (void*)&Dc};
+    return cudaLaunchCooperativeKernel((const void*)k_msws_repair, dim3(L.repair_grid), dim3(REPAIR_THREADS), args, 0,
+                                       st);
+}
+
+cudaError_t msws_query(const uint32_t* d_keys, uint64_t n, uint32_t* d_out, const MswsDev& D, const MswsLaunch& L,
+                       cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const uint64_t want = (n + QRY_THREADS * QRY_KPT - 1) / (QRY_THREADS * QRY_KPT);
+    const int grid = (int)umin64((uint64_t)L.query_grid, std::max<uint64_t>(1ull, want));
+    k_msws_query<<<grid, QRY_THREADS, (size_t)D.n_masks * 4, st>>>(d_keys, n, d_out, D);
+    return cudaGetLastError();
+}
+
+}  // namespace qsb

@@ -1,0 +1,92 @@
+"""CPU tests of the C ABI boundary: the library loads, exports every entry point the header
+declares, and its host-side table preparation matches the reference (golden fixtures)."""
+import ctypes
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import qsketch_b200 as qs
+from qsketch_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "qsketch_c.h")
+G = os.path.join(ROOT, "tests", "golden")
+with open(os.path.join(G, "golden.json")) as f:
+    GOLD = json.load(f)
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(qs_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_bound_api():
+    assert set(declared_symbols()) == set(_lib.SIGNATURES)
+
+
+def test_library_exports_every_declared_symbol():
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (qs_[a-z0-9_]+)$", out, flags=re.M))
+    missing = set(declared_symbols()) - exported
+    assert not missing, missing
+    for name in declared_symbols():
+        assert getattr(_lib.lib, name) is not None
+
+
+def test_abi_version_and_status_strings():
+    assert _lib.lib.qs_abi_version() == 1
+    for s in range(8):
+        assert _lib.lib.qs_status_string(s)
+
+
+def test_params_default_are_reference_defaults():
+    p = _lib.qs_params()
+    _lib.lib.qs_params_default(ctypes.byref(p))
+    assert (p.kind, p.m_low, p.m_high, p.n_high, p.seed_sz, p.hash_mask_table_sz, p.hash_mask_ones) == \
+        (0, 8, 32, 1024, 1, 1021, 3)
+
+
+@pytest.mark.parametrize("case", GOLD["masks"], ids=lambda c: c["file"])
+def test_product_hashmask_matches_reference(case):
+    want = np.fromfile(os.path.join(G, case["file"]), np.uint8)
+    got = qs.generate_hashmask(case["n"], case["m_bits"], case["ones"], case["padding"], case["rng_seed"])
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("case", GOLD["seeds"], ids=lambda c: str(c["rng_seed"]))
+def test_product_seed_draw_matches_reference(case):
+    assert [int(x) for x in qs.draw_seeds(len(case["values"]), case["rng_seed"])] == case["values"]
+
+
+def test_product_primes_match_reference():
+    for x, p in GOLD["primes"].items():
+        assert qs.find_greatest_prime(int(x)) == p
+
+
+def test_number_of_buckets():
+    # device_sketch.h:371-376 with 3 ones: ((keys / factor) * 3) / m, then the prime below
+    assert qs.number_of_buckets(1 << 20, 8, 1.0) == qs.find_greatest_prime((1 << 20) * 3 // 8)
+    assert qs.number_of_buckets(1 << 27, 8, 0.5) == qs.find_greatest_prime((1 << 28) * 3 // 8)
+    assert qs.Sketch_GPU_Thread.number_of_buckets(1 << 24, 3, 1.0) == 16777213
+
+
+def test_bad_arguments_are_errors_not_crashes():
+    assert _lib.lib.qs_generate_hashmask(1, 10, 8, 9, 0, None) == _lib.QS_ERR_INVALID_ARG
+    assert _lib.lib.qs_insert(None, None, 10, None) == _lib.QS_ERR_INVALID_ARG
+    assert _lib.lib.qs_query(None, None, 10, None, None) == _lib.QS_ERR_INVALID_ARG
+    assert _lib.lib.qs_destroy(None) == _lib.QS_OK
+    assert _lib.lib.qs_create(None, None) == _lib.QS_ERR_INVALID_ARG
+
+
+def test_create_without_device_reports_no_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(qs.QsError) as ei:
+        qs.Sketch_GPU_Sub_Warp_Level(262139)
+    assert ei.value.status in (_lib.QS_ERR_NO_DEVICE, _lib.QS_ERR_CUDA)

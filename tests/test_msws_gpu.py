@@ -1,0 +1,173 @@
+"""GPU parity of the MSWS insert/query path against the sequential CPU oracle.
+
+Every comparison is bit-exact: the per-key query vector, the low table's counter words,
+which buckets are linked, and each linked bucket's high counters (high ids themselves may
+differ: allocation order is free)."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import qsketch_b200 as qs
+from qsketch_b200 import _lib, data
+
+pytestmark = pytest.mark.gpu
+
+
+def make_pair(n_low, n_high, seed=2654435769, mask_rng=1, compat=False, **kw):
+    masks = qs.generate_hashmask(1021, 32, 3, 4, mask_rng)
+    sk = qs.Sketch_GPU_Sub_Warp_Level(n_low, 8, n_high, 32, hash_seed=seed, mask_table=masks, compat_v3=compat, **kw)
+    orc = oracle.Msws(n_low, n_high, seed, masks, compat_v3=compat)
+    return sk, orc
+
+
+def assert_same_tables(sk, orc):
+    low, high = sk.tables()
+    gl, ol = low.reshape(-1, 8), orc.low.reshape(-1, 8)
+    assert np.array_equal(gl[:, :7], ol[:, :7]), "low counter words differ"
+    gp, op = gl[:, 7], ol[:, 7]
+    assert np.array_equal(gp > 1024, op > 1024), "linked buckets differ"
+    assert np.array_equal(gp == oracle.SATURATED, op == oracle.SATURATED)
+    linked = np.nonzero(op > 1024)[0]
+    if linked.size:
+        gh = high.reshape(-1, 32)[gp[linked] - 1024]
+        oh = orc.high.reshape(-1, 32)[op[linked] - 1024]
+        assert np.array_equal(gh, oh), "high buckets differ"
+    assert (gp & 0x80000000 == 0).all(), "a bucket is still flagged"
+
+
+def run_and_compare(sk, orc, keys_d, queries_d, pieces=None):
+    if pieces is None:
+        sk.insert(keys_d)
+    else:
+        off = 0
+        for p in pieces:
+            sk.insert(keys_d[off:off + p])
+            off += p
+        assert off == keys_d.numel()
+    got = sk.search(queries_d).cpu().numpy()
+    sk.sync()
+    orc.insert(keys_d.cpu().numpy())
+    want = orc.query(queries_d.cpu().numpy())
+    mism = np.nonzero(got != want)[0]
+    assert mism.size == 0, f"{mism.size} mismatches, first {mism[:5]}: got {got[mism[:5]]} want {want[mism[:5]]}"
+    assert_same_tables(sk, orc)
+    return got
+
+
+def test_uniform_small(gpu):
+    sk, orc = make_pair(65521, 1 << 12)
+    keys = data.uniform_keys(1 << 20, seed=11)
+    run_and_compare(sk, orc, keys, keys)
+
+
+def test_uniform_config1_full_size(gpu):
+    # 2^24 uniform keys into n_low = 262139 (src/test.cu:351), queries = all inserted keys
+    sk, orc = make_pair(262139, 1 << 16)
+    keys = data.uniform_keys(1 << 24, seed=1)
+    run_and_compare(sk, orc, keys, keys)
+    assert sk.stats()["linked_buckets"] == 0
+
+
+@pytest.mark.parametrize("agg", [1, 2])
+def test_zipf_heavy_links(gpu, agg):
+    sk, orc = make_pair(16381, 1 << 15, aggregate=agg)
+    keys = data.zipf_keys(1 << 22, 1 << 18, 1.1, seed=5, perm_seed=77)
+    q = data.rank_keys(77, 0, 1 << 18)
+    run_and_compare(sk, orc, keys, q)
+    st = sk.stats()
+    assert st["linked_buckets"] > 100 and st["repaired_buckets"] == st["linked_buckets"]
+
+
+def test_zipf_many_chunks_and_uneven_calls(gpu):
+    sk, orc = make_pair(8191, 1 << 14, max_batch=1 << 16)
+    keys = data.zipf_keys(3 * (1 << 18) + 77, 1 << 16, 1.2, seed=9, perm_seed=3)
+    n = keys.numel()
+    run_and_compare(sk, orc, keys, data.rank_keys(3, 0, 1 << 16), pieces=[1, 3, 5, 1000, 70001, n - 71010])
+
+
+def test_compat_v3(gpu):
+    sk, orc = make_pair(4093, 1 << 13, compat=True)
+    keys = data.zipf_keys(1 << 21, 1 << 16, 1.0, seed=21, perm_seed=8)
+    run_and_compare(sk, orc, keys, data.rank_keys(8, 0, 1 << 16))
+
+
+def test_single_heavy_key(gpu):
+    sk, orc = make_pair(1021, 64)
+    keys = torch.full((1 << 20,), 123456789, dtype=torch.uint32, device="cuda")
+    got = run_and_compare(sk, orc, keys, keys[:1])
+    assert got[0] == 1 << 20
+
+
+def test_all_keys_one_bucket_many_masks(gpu):
+    # n_low = 1: every key shares the bucket, so crossings depend on the exact order
+    sk, orc = make_pair(1, 4, seed=1)
+    keys = torch.arange(5000, dtype=torch.int64).remainder(37).to(torch.uint32).cuda()
+    run_and_compare(sk, orc, keys, torch.arange(37, dtype=torch.int64).to(torch.uint32).cuda())
+
+
+def test_unaligned_and_tiny_inputs(gpu):
+    sk, orc = make_pair(4093, 1024)
+    base = data.zipf_keys(200003, 5000, 1.3, seed=4, perm_seed=6)
+    for lo, hi in [(1, 2), (1, 6), (3, 3), (5, 1030), (2, 150001), (7, 200003)]:
+        sk.insert(base[lo:hi])
+        orc.insert(base[lo:hi].cpu().numpy())
+    sk.insert(base[:0])
+    q = data.rank_keys(6, 0, 5000)
+    assert np.array_equal(sk.search(q[1:]).cpu().numpy(), orc.query(q[1:].cpu().numpy()))
+    assert sk.search(q[:0]).numel() == 0
+    assert_same_tables(sk, orc)
+
+
+def test_pool_exhaustion_is_reported(gpu):
+    sk, orc = make_pair(4093, 8)
+    keys = data.zipf_keys(1 << 20, 1 << 12, 1.2, seed=1, perm_seed=2)
+    sk.insert(keys)
+    assert sk.status() == _lib.QS_ERR_POOL_FULL
+    with pytest.raises(qs.QsError):
+        sk.sync()
+    st = sk.stats()
+    assert st["linked_buckets"] == 7 and st["dropped_keys"] > 0
+    orc.insert(keys.cpu().numpy())
+    assert orc.pool_full and orc.next_id == 1024 + 8
+    sk.reset_status()
+    assert sk.status() == _lib.QS_OK
+
+
+def test_clear_resets(gpu):
+    sk, orc = make_pair(4093, 1 << 10)
+    keys = data.zipf_keys(1 << 20, 1 << 12, 1.2, seed=1, perm_seed=2)
+    sk.insert(keys)
+    sk.clear()
+    assert sk.stats()["next_level_id"] == 1025
+    low, high = sk.tables()
+    assert not low.any() and not high.any()
+    run_and_compare(sk, orc, keys, data.rank_keys(2, 0, 1 << 12))
+
+
+def test_host_buffers_match_device_path(gpu):
+    sk, orc = make_pair(16381, 1 << 14, max_batch=1 << 18)
+    keys = data.zipf_keys(1 << 21, 1 << 16, 1.1, seed=3, perm_seed=4)
+    hk = keys.cpu().numpy()
+    q = data.rank_keys(4, 0, 1 << 16).cpu().numpy()
+    sk.insert_host(hk)
+    got = sk.search_host(q)
+    orc.insert(hk)
+    assert np.array_equal(got, orc.query(q))
+    pinned = torch.from_numpy(q).pin_memory()
+    out = torch.empty_like(pinned).pin_memory()
+    sk.search_host(pinned, out)
+    assert np.array_equal(out.numpy(), got)
+
+
+def test_zipf_config2_full_size(gpu):
+    # 2^27 keys, Zipf s=1.1 over 2^24 ranks, 64 MB low table, 16 MB high pool
+    sk, orc = make_pair(2097143, 1 << 17)
+    keys = data.zipf_keys(1 << 27, 1 << 24, 1.1, seed=2024, perm_seed=99)
+    q = data.rank_keys(99, 0, 1 << 24)
+    sk.insert(keys)
+    got = sk.search(q).cpu().numpy()
+    sk.sync()
+    orc.insert(keys.cpu().numpy(), threads=8)
+    want = orc.query(q.cpu().numpy())
+    assert np.array_equal(got, want)
