@@ -177,6 +177,12 @@ typedef struct qs_profile {
     double query_ms;           /* query kernels */
     uint64_t insert_timed, repair_timed, query_timed;
     uint64_t insert_launches, repair_launches, query_launches;
+    /* MSWS ordered repair, measured on the device (globaltimer) since the previous
+     * qs_get_profile: invocations that found crossed buckets, and time per phase —
+     * 0 filter count, 1 tile scan, 2 filter write, 3 radix passes, 4-5 segments,
+     * 6 long-segment counts, 7 replay. */
+    uint64_t repairs_active;
+    double repair_phase_ms[8];
 } qs_profile;
 qs_status qs_set_profiling(qs_sketch *sk, int enable);
 qs_status qs_get_profile(qs_sketch *sk, qs_profile *out);

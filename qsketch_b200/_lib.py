@@ -70,6 +70,8 @@ class qs_profile(ctypes.Structure):
         ("insert_launches", ctypes.c_uint64),
         ("repair_launches", ctypes.c_uint64),
         ("query_launches", ctypes.c_uint64),
+        ("repairs_active", ctypes.c_uint64),
+        ("repair_phase_ms", ctypes.c_double * 8),
     ]
 
 

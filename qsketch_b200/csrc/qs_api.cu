@@ -209,7 +209,7 @@ qs_status insert_device(qs_sketch* sk, const uint32_t* d_keys, size_t n, cudaStr
         }
     } else {
         CK(sk->prof_begin(0, st), "profile");
-        CK(cm_insert(d_keys, n, sk->C, sk->agg, sk->cm_grid, st), "cm insert");
+        CK(cm_insert(d_keys, n, sk->C, sk->agg ? 1 : 0, sk->cm_grid, st), "cm insert");
         CK(sk->prof_end(0, st), "profile");
     }
     return QS_OK;
@@ -315,7 +315,12 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         delete sk;
         return fail(QS_ERR_INVALID_ARG, "max_batch above 2^30");
     }
-    sk->agg = (p.aggregate == 1) ? 0 : 1;
+    // aggregate: 1 none, 2 warp, 3 warp + block, 0 = default (3)
+    if (p.aggregate > 3) {
+        delete sk;
+        return fail(QS_ERR_INVALID_ARG, "aggregate out of [0, 3]");
+    }
+    sk->agg = p.aggregate == 0 ? 2 : (int)p.aggregate - 1;
     auto bail = [&](qs_status s) {
         qs_destroy(sk);
         return s;
@@ -573,6 +578,13 @@ qs_status qs_get_profile(qs_sketch* sk, qs_profile* out) {
     out->repair_launches = sk->launches[1];
     out->query_launches = sk->launches[2];
     for (int k = 0; k < 3; ++k) sk->ev_used[k] = 0;
+    if (sk->kind == QS_KIND_MSWS) {
+        Ctl c;
+        CK(cudaMemcpy(&c, sk->D.ctl, sizeof c, cudaMemcpyDeviceToHost), "read repair phases");
+        out->repairs_active = c.repairs;
+        for (int k = 0; k < 8; ++k) out->repair_phase_ms[k] = (double)c.phase_ns[k] * 1e-6;
+        CK(cudaMemset(&sk->D.ctl->repairs, 0, sizeof(unsigned long long) * 10), "reset repair phases");
+    }
     return QS_OK;
 }
 

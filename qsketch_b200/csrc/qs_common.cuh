@@ -58,7 +58,9 @@ struct Ctl {
     unsigned long long repaired_buckets;
     unsigned long long repaired_keys;
     unsigned long long inserted;
-    uint32_t pad1[16];
+    unsigned long long repairs;        // repair invocations that had flagged buckets
+    unsigned long long phase_t;        // globaltimer at the last phase mark
+    unsigned long long phase_ns[8];    // accumulated time per repair phase
 };
 
 // Everything a MSWS kernel needs, passed by value.

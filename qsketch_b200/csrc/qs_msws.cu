@@ -24,8 +24,55 @@
 namespace qsb {
 
 constexpr int INS_THREADS = 256;
+constexpr int INS_WARPS = INS_THREADS / 32;
 constexpr int INS_TILE = 2048;  // keys per TMA stage (8 KiB)
 constexpr int INS_STAGES = 3;
+constexpr int AGG_SLOTS = 1024; // per-CTA table merging the linked keys of a tile
+constexpr int AGG_PROBES = 32;
+constexpr uint32_t AGG_EMPTY = 0xffffffffu;
+
+// Aggregation modes (qs_params.aggregate): 1 none, 2 warp (equal keys of a warp merge),
+// 3 warp + block (linked keys of a whole tile merge in shared memory, so a heavy hitter
+// costs one atomic per high counter per tile instead of one per occurrence).
+enum { AGG_NONE = 0, AGG_WARP = 1, AGG_BLOCK = 2 };
+
+struct InsShared {
+    uint32_t* keys;   // [INS_STAGES][INS_TILE]
+    uint64_t* bar;    // [INS_STAGES]
+    uint32_t* akey;   // [AGG_SLOTS]
+    uint32_t* acnt;   // [AGG_SLOTS]
+    uint32_t* aid;    // [AGG_SLOTS] high id of the key's bucket
+    uint4* stage;     // [INS_WARPS][32] per-warp round staging
+    uint32_t* masks;  // [n_masks]
+    uint32_t* dropped;
+};
+
+__device__ __forceinline__ InsShared ins_carve(uint8_t* smem, uint32_t n_masks) {
+    InsShared S;
+    uint8_t* p = smem;
+    S.keys = reinterpret_cast<uint32_t*>(p);
+    p += INS_STAGES * INS_TILE * 4;
+    S.bar = reinterpret_cast<uint64_t*>(p);
+    p += INS_STAGES * 8 + 8;
+    S.akey = reinterpret_cast<uint32_t*>(p);
+    p += AGG_SLOTS * 4;
+    S.acnt = reinterpret_cast<uint32_t*>(p);
+    p += AGG_SLOTS * 4;
+    S.aid = reinterpret_cast<uint32_t*>(p);
+    p += AGG_SLOTS * 4;
+    S.stage = reinterpret_cast<uint4*>(p);
+    p += INS_WARPS * 32 * 16;
+    S.dropped = reinterpret_cast<uint32_t*>(p);
+    p += 16;
+    S.masks = reinterpret_cast<uint32_t*>(p);
+    (void)n_masks;
+    return S;
+}
+
+size_t msws_insert_smem(uint32_t n_masks) {
+    return (size_t)INS_STAGES * INS_TILE * 4 + INS_STAGES * 8 + 8 + 3 * AGG_SLOTS * 4 + INS_WARPS * 32 * 16 + 16 +
+           (size_t)n_masks * 4;
+}
 
 // ---- pass 1 -------------------------------------------------------------------------------
 
@@ -43,79 +90,142 @@ __device__ __forceinline__ void flag_bucket(const MswsDev& D, uint32_t b) {
     }
 }
 
-// Process up to 32 keys held one per lane (valid lanes: lane < cnt).
+__device__ __forceinline__ bool is_linked(const MswsDev& D, uint32_t w7) {
+    return w7 > START && (uint64_t)(w7 - START) < D.n_high;
+}
+
+__device__ __forceinline__ bool agg_insert(const InsShared& S, uint32_t key, uint32_t c, uint32_t id) {
+    if (key == AGG_EMPTY) return false;
+    const uint32_t h = (key * 0x9E3779B1u) >> 22;  // 10 bits
+    for (int p = 0; p < AGG_PROBES; ++p) {
+        const uint32_t s = (h + p) & (AGG_SLOTS - 1);
+        const uint32_t prev = atomicCAS(S.akey + s, AGG_EMPTY, key);
+        if (prev == AGG_EMPTY) {
+            S.aid[s] = id;
+            atomicAdd(S.acnt + s, c);
+            return true;
+        }
+        if (prev == key) {
+            atomicAdd(S.acnt + s, c);
+            return true;
+        }
+    }
+    return false;
+}
+
+// Sub-warp rounds over the staged entries of this warp: entry j = (target, mask, count,
+// kind); 4 entries per round, lane w of sub-warp `sub` serves entry r*4+sub.  kind 0: low
+// bucket `target`, lane w adds its nibble of 8-bit counters to word w with a returning
+// atomic (device_sketch_v3.h:131-170); kind 1: linked, lane w adds to the w-th selected
+// high counter of id `target` (insert_high, :54-65, :111-129).
+__device__ __forceinline__ void staged_rounds(const MswsDev& D, const uint4* st, int nact) {
+    const int lane = threadIdx.x & 31, sub = lane >> 3, w = lane & 7;
+    uint32_t olds[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        olds[r] = 0;
+        if (r * 4 >= nact) continue;  // warp-uniform
+        const int j = r * 4 + sub;
+        if (j >= nact) continue;
+        const uint4 e = st[j];
+        if (e.w == 0) {
+            const uint32_t nib = (w < 7) ? (e.y >> (4 * w)) & 0xfu : 0u;
+            if (nib) olds[r] = atomicAdd(D.low + (uint64_t)e.x * LOW_WORDS + w, expand_nibble(nib) * e.z);
+        } else {
+            uint32_t* hb = D.high + (uint64_t)(e.x - START) * HIGH_WORDS;
+            const int pc = __popc(e.y);
+            for (int k = w; k < pc; k += 8) atomicAdd(hb + __fns(e.y, 0, k + 1), e.z);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        if (r * 4 >= nact) continue;  // warp-uniform
+        const int j = r * 4 + sub;
+        bool cross = false;
+        uint4 e = make_uint4(0, 0, 0, 1);
+        if (j < nact) e = st[j];
+        if (e.w == 0) {
+            const uint32_t nib = (w < 7) ? (e.y >> (4 * w)) & 0xfu : 0u;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (((nib >> k) & 1u) && ((olds[r] >> (8 * k)) & 0xffu) + e.z >= CROSS) cross = true;
+        }
+        const uint32_t bal = __ballot_sync(0xffffffffu, cross);
+        if (w == 0 && ((bal >> (sub * 8)) & 0xffu)) flag_bucket(D, e.x);
+    }
+}
+
+// Up to 32 keys held one per lane (valid lanes: lane < cnt).
 template <int AGG>
-__device__ __forceinline__ void insert_group(const MswsDev& D, const uint32_t* s_masks, uint32_t key, int cnt) {
-    const int lane = threadIdx.x & 31;
-    const int sub = lane >> 3, w = lane & 7;
+__device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& S, uint32_t key, int cnt,
+                                             bool use_table) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const bool valid = lane < cnt;
     const uint32_t hv = key * D.seed;  // hash_mul_add, device_hash_function.h:6-18
     const uint32_t b = fast_mod(D.fm_low, hv);
-    const uint32_t m = s_masks[fast_mod(D.fm_mask, hv)];
+    const uint32_t m = S.masks[fast_mod(D.fm_mask, hv)];
     uint32_t c = valid ? 1u : 0u;
-    if (AGG) {  // merge equal keys of the warp: one leader carries the multiplicity
+    if (AGG != AGG_NONE) {
         const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
         const uint32_t peers = __match_any_sync(0xffffffffu, key) & vmask;
         c = (valid && lane == __ffs(peers) - 1) ? (uint32_t)__popc(peers) : 0u;
     }
     const uint32_t w7 = c ? __ldcg(D.low + (uint64_t)b * LOW_WORDS + 7) : 0u;
+    const bool linked = c && is_linked(D, w7);
+    const bool sat = c && w7 == SATURATED;
+    if (sat) atomicAdd(S.dropped, c);
+    bool direct_high = linked;
+    if (AGG == AGG_BLOCK && linked && use_table) direct_high = !agg_insert(S, key, c, w7);
+    const bool act = (c && !linked && !sat) || direct_high;
+    const uint32_t am = __ballot_sync(0xffffffffu, act);
+    uint4* st = S.stage + wid * 32;
+    if (act) st[__popc(am & lanemask_lt())] = make_uint4(direct_high ? w7 : b, m, c, direct_high ? 1u : 0u);
+    __syncwarp();
+    staged_rounds(D, st, __popc(am));
+    __syncwarp();
+}
 
-    // Issue the atomics of all 8 rounds (4 keys per round) before checking any result.
-    uint32_t olds[8];
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const int src = r * 4 + sub;
-        const uint32_t bb = __shfl_sync(0xffffffffu, b, src);
-        const uint32_t mm = __shfl_sync(0xffffffffu, m, src);
-        const uint32_t cc = __shfl_sync(0xffffffffu, c, src);
-        const uint32_t ww = __shfl_sync(0xffffffffu, w7, src);
-        olds[r] = 0;
-        if (cc == 0 || ww == SATURATED) continue;
-        if (ww > START && (uint64_t)(ww - START) < D.n_high) {
-            // linked bucket: insert_high (device_sketch_v3.h:111-129), lane w takes the
-            // w-th selected counter
-            uint32_t* hb = D.high + (uint64_t)(ww - START) * HIGH_WORDS;
-            const int pc = __popc(mm);
-            for (int k = w; k < pc; k += 8) atomicAdd(hb + __fns(mm, 0, k + 1), cc);
-        } else {
-            // packed low add (device_sketch_v3.h:131-170), lane w owns word w
-            const uint32_t nib = (w < 7) ? (mm >> (4 * w)) & 0xfu : 0u;
-            if (nib) olds[r] = atomicAdd(D.low + (uint64_t)bb * LOW_WORDS + w, expand_nibble(nib) * cc);
+// Merged linked keys of the tile: one red per selected high counter per distinct key.
+__device__ __forceinline__ void drain_table(const MswsDev& D, const InsShared& S) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint4* st = S.stage + wid * 32;
+    for (int base = wid * 32; base < AGG_SLOTS; base += INS_THREADS) {
+        const int s = base + lane;
+        const uint32_t k = S.akey[s];
+        const bool has = k != AGG_EMPTY;
+        uint32_t m = 0, c = 0, id = 0;
+        if (has) {
+            const uint32_t hv = k * D.seed;
+            m = S.masks[fast_mod(D.fm_mask, hv)];
+            c = S.acnt[s];
+            id = S.aid[s];
+            S.akey[s] = AGG_EMPTY;
+            S.acnt[s] = 0;
         }
-    }
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const int src = r * 4 + sub;
-        const uint32_t bb = __shfl_sync(0xffffffffu, b, src);
-        const uint32_t mm = __shfl_sync(0xffffffffu, m, src);
-        const uint32_t cc = __shfl_sync(0xffffffffu, c, src);
-        const uint32_t ww = __shfl_sync(0xffffffffu, w7, src);
-        const bool lowp = cc != 0 && ww != SATURATED && !(ww > START && (uint64_t)(ww - START) < D.n_high);
-        const uint32_t nib = (w < 7) ? (mm >> (4 * w)) & 0xfu : 0u;
-        bool cross = false;
-        if (lowp && nib) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (((nib >> k) & 1u) && ((olds[r] >> (8 * k)) & 0xffu) + cc >= CROSS) cross = true;
-        }
-        const uint32_t bal = __ballot_sync(0xffffffffu, cross);
-        if (w == 0 && ((bal >> (sub * 8)) & 0xffu)) flag_bucket(D, bb);
-        if (w == 0 && cc != 0 && ww == SATURATED) atomicAdd(&D.ctl->dropped, (unsigned long long)cc);
+        const uint32_t am = __ballot_sync(0xffffffffu, has);
+        if (!am) continue;
+        if (has) st[__popc(am & lanemask_lt())] = make_uint4(id, m, c, 1u);
+        __syncwarp();
+        staged_rounds(D, st, __popc(am));
+        __syncwarp();
     }
 }
 
 template <int AGG>
 __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* __restrict__ keys, uint64_t n,
-                                                             MswsDev D) {
+                                                                MswsDev D) {
     extern __shared__ __align__(128) uint8_t smem[];
-    uint32_t* s_keys = reinterpret_cast<uint32_t*>(smem);                      // STAGES * TILE
-    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_keys + INS_STAGES * INS_TILE);
-    uint32_t* s_masks = reinterpret_cast<uint32_t*>(s_bar + INS_STAGES);       // n_masks
+    const InsShared S = ins_carve(smem, D.n_masks);
     __shared__ uint32_t s_extra[8];
     __shared__ int s_ok;
 
     const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
-    for (uint32_t i = tid; i < D.n_masks; i += blockDim.x) s_masks[i] = __ldg(D.masks + i);
+    for (uint32_t i = tid; i < D.n_masks; i += blockDim.x) S.masks[i] = __ldg(D.masks + i);
+    for (int i = tid; i < AGG_SLOTS; i += blockDim.x) {
+        S.akey[i] = AGG_EMPTY;
+        S.acnt[i] = 0;
+    }
+    if (tid == 0) *S.dropped = 0;
 
     // 16-byte aligned body for the TMA bulk copies; the <= 6 ragged keys go through CTA 0.
     const uintptr_t addr = reinterpret_cast<uintptr_t>(keys);
@@ -125,7 +235,7 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
     const uint32_t* body = keys + head;
 
     if (tid == 0) {
-        for (int s = 0; s < INS_STAGES; ++s) mbar_init(&s_bar[s], 1);
+        for (int s = 0; s < INS_STAGES; ++s) mbar_init(&S.bar[s], 1);
         fence_mbar_init();
     }
     if (blockIdx.x == 0 && tid < (int)(head + tail))
@@ -133,20 +243,19 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
     __syncthreads();
     if (blockIdx.x == 0 && wid == 0 && head + tail > 0) {
         const uint32_t k = lane < (int)(head + tail) ? s_extra[lane] : 0u;
-        insert_group<AGG>(D, s_masks, k, (int)(head + tail));
+        insert_group<AGG>(D, S, k, (int)(head + tail), false);
     }
 
     const uint64_t ntiles = (body_n + INS_TILE - 1) / INS_TILE;
-    if (blockIdx.x >= ntiles) return;
-    const uint64_t my_tiles = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x;
+    const uint64_t my_tiles = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
     auto issue = [&](uint64_t i) {
         const int st = (int)(i % INS_STAGES);
         const uint64_t g = blockIdx.x + i * gridDim.x;
         const uint64_t start = g * INS_TILE;
         const uint32_t cnt = (uint32_t)umin64(INS_TILE, body_n - start);
-        mbar_arrive_expect_tx(&s_bar[st], cnt * 4u);
-        tma_bulk_g2s(s_keys + st * INS_TILE, body + start, cnt * 4u, &s_bar[st]);
+        mbar_arrive_expect_tx(&S.bar[st], cnt * 4u);
+        tma_bulk_g2s(S.keys + st * INS_TILE, body + start, cnt * 4u, &S.bar[st]);
     };
     if (tid == 0)
         for (uint64_t i = 0; i < umin64(INS_STAGES, my_tiles); ++i) issue(i);
@@ -154,34 +263,39 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
     for (uint64_t i = 0; i < my_tiles; ++i) {
         const int st = (int)(i % INS_STAGES);
         const uint32_t parity = (uint32_t)((i / INS_STAGES) & 1u);
-        if (tid == 0) s_ok = mbar_wait_bounded(&s_bar[st], parity) ? 1 : 0;
+        if (tid == 0) s_ok = mbar_wait_bounded(&S.bar[st], parity) ? 1 : 0;
         __syncthreads();
         if (!s_ok) {
             if (tid == 0) {
                 atomicOr(&D.ctl->status, ST_TIMEOUT);
                 // wait (bounded) for the copies still in flight before leaving
                 for (uint64_t j = i; j < umin64(i + INS_STAGES, my_tiles); ++j)
-                    mbar_wait_bounded(&s_bar[j % INS_STAGES], (uint32_t)((j / INS_STAGES) & 1u));
+                    mbar_wait_bounded(&S.bar[j % INS_STAGES], (uint32_t)((j / INS_STAGES) & 1u));
             }
             return;
         }
-        for (uint32_t it = 0; it < 64 && !mbar_try_wait(&s_bar[st], parity); ++it) {
+        for (uint32_t it = 0; it < 64 && !mbar_try_wait(&S.bar[st], parity); ++it) {
         }
         const uint64_t g = blockIdx.x + i * gridDim.x;
         const int cnt = (int)umin64(INS_TILE, body_n - g * INS_TILE);
-        const uint32_t* tk = s_keys + st * INS_TILE;
-        // each warp takes 32-key groups round-robin
+        const uint32_t* tk = S.keys + st * INS_TILE;
         for (int base = wid * 32; base < cnt; base += INS_THREADS) {
             const int c = min(32, cnt - base);
             const uint32_t k = lane < c ? tk[base + lane] : 0u;
-            insert_group<AGG>(D, s_masks, k, c);
+            insert_group<AGG>(D, S, k, c, true);
         }
         __syncthreads();
+        if (AGG == AGG_BLOCK) {
+            drain_table(D, S);
+            __syncthreads();
+        }
         if (tid == 0 && i + INS_STAGES < my_tiles) {
             fence_proxy_async_smem();
             issue(i + INS_STAGES);
         }
     }
+    __syncthreads();
+    if (tid == 0 && *S.dropped) atomicAdd(&D.ctl->dropped, (unsigned long long)*S.dropped);
 }
 
 // ---- ordered replay ---------------------------------------------------------------------
@@ -202,6 +316,21 @@ struct RadixSmem {
     uint32_t whist[REPAIR_THREADS / 32][256];
 };
 
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Accumulate the time since the previous mark into phase k (block 0, thread 0).
+__device__ __forceinline__ void phase_mark(Ctl* ctl, int k) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint64_t now = globaltimer();
+        if (k >= 0) ctl->phase_ns[k] += now - ctl->phase_t;
+        ctl->phase_t = now;
+    }
+}
+
 __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* __restrict__ keys, uint64_t n,
                                                                 MswsDev D) {
     __shared__ RadixSmem rs;
@@ -210,6 +339,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     Ctl* ctl = D.ctl;
     const uint32_t F = min(__ldcg(&ctl->n_flagged), D.flag_cap);
     if (F == 0) return;
+    phase_mark(ctl, -1);
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     constexpr int NW = REPAIR_THREADS / 32;
@@ -233,12 +363,14 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         if (tid == 0) __stcg(D.tile_counts + t, total);
     }
     if (!grid_barrier(ctl)) return;
+    phase_mark(ctl, 0);
     // Phase 2: exclusive scan of the tile counts.
     if (blockIdx.x == 0) {
         const uint32_t K = block_scan_array(D.tile_counts, ntk);
         if (tid == 0) __stcg(&ctl->n_records, K);
     }
     if (!grid_barrier(ctl)) return;
+    phase_mark(ctl, 1);
     const uint32_t K = __ldcg(&ctl->n_records);
     // Phase 3: stable write of (slot, mask) records in array order.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
@@ -270,6 +402,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         }
     }
     if (!grid_barrier(ctl)) return;
+    phase_mark(ctl, 2);
 
     // Phase 4: stable LSD radix sort of the records by slot, 8 bits per pass.
     const int npass = radix_passes(F);
@@ -341,6 +474,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         }
         if (!grid_barrier(ctl)) return;
     }
+    phase_mark(ctl, 3);
     const uint2* sorted = D.rec[npass & 1];
 
     // Phase 5: segment starts per slot, then segment classes.
@@ -349,6 +483,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         if (i == 0 || __ldcg(&sorted[i - 1].x) != s) __stcg(D.seg_beg + s, i);
     }
     if (!grid_barrier(ctl)) return;
+    phase_mark(ctl, 4);
     for (uint32_t s = blockIdx.x * REPAIR_THREADS + tid; s < F; s += gridDim.x * REPAIR_THREADS) {
         const uint32_t beg = __ldcg(D.seg_beg + s);
         const uint32_t end = (s + 1 < F) ? __ldcg(D.seg_beg + s + 1) : K;
@@ -363,6 +498,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         __stcg(D.long_id + s, lid);
     }
     if (!grid_barrier(ctl)) return;
+    phase_mark(ctl, 5);
 
     // Phase 6: per-counter totals of long segments; each block a contiguous record range,
     // the range's first and last slot accumulate in shared memory.
@@ -408,6 +544,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         }
     }
     if (!grid_barrier(ctl)) return;
+    phase_mark(ctl, 6);
 
     // Phase 7: replay each flagged bucket in array order, one warp per slot.
     const uint32_t lt = lanemask_lt();
@@ -501,10 +638,12 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         }
     }
     if (!grid_barrier(ctl)) return;
+    phase_mark(ctl, 7);
     if (blockIdx.x == 0 && tid == 0) {
         ctl->n_flagged = 0;
         ctl->n_records = 0;
         ctl->n_long = 0;
+        ctl->repairs += 1;
         __threadfence();
     }
 }
@@ -565,23 +704,20 @@ __global__ void __launch_bounds__(QRY_THREADS) k_msws_query(const uint32_t* __re
 
 // ---- launchers ----------------------------------------------------------------------------
 
-size_t msws_insert_smem(uint32_t n_masks) {
-    return (size_t)INS_STAGES * INS_TILE * 4 + INS_STAGES * 8 + (size_t)n_masks * 4;
-}
-
 cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
     cudaDeviceProp prop;
     cudaError_t e = cudaGetDeviceProperties(&prop, device);
     if (e != cudaSuccess) return e;
     L->num_sms = prop.multiProcessorCount;
     const size_t ins_smem = msws_insert_smem(n_masks);
-    for (int agg = 0; agg < 2; ++agg) {
-        const void* fn = agg ? (const void*)k_msws_insert<1> : (const void*)k_msws_insert<0>;
+    const void* fns[3] = {(const void*)k_msws_insert<AGG_NONE>, (const void*)k_msws_insert<AGG_WARP>,
+                          (const void*)k_msws_insert<AGG_BLOCK>};
+    for (const void* fn : fns) {
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ins_smem);
         if (e != cudaSuccess) return e;
     }
     int occ = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_insert<0>, INS_THREADS, ins_smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_insert<AGG_BLOCK>, INS_THREADS, ins_smem);
     if (e != cudaSuccess) return e;
     L->insert_grid = prop.multiProcessorCount * (occ > 0 ? occ : 1);
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_repair, REPAIR_THREADS, 0);
@@ -598,10 +734,12 @@ cudaError_t msws_insert_pass(const uint32_t* d_keys, uint64_t n, const MswsDev& 
     const size_t smem = msws_insert_smem(D.n_masks);
     const uint64_t tiles = (n + INS_TILE - 1) / INS_TILE;
     const int grid = (int)std::min<uint64_t>((uint64_t)L.insert_grid, std::max<uint64_t>(1ull, tiles));
-    if (agg)
-        k_msws_insert<1><<<grid, INS_THREADS, smem, st>>>(d_keys, n, D);
+    if (agg == AGG_BLOCK)
+        k_msws_insert<AGG_BLOCK><<<grid, INS_THREADS, smem, st>>>(d_keys, n, D);
+    else if (agg == AGG_WARP)
+        k_msws_insert<AGG_WARP><<<grid, INS_THREADS, smem, st>>>(d_keys, n, D);
     else
-        k_msws_insert<0><<<grid, INS_THREADS, smem, st>>>(d_keys, n, D);
+        k_msws_insert<AGG_NONE><<<grid, INS_THREADS, smem, st>>>(d_keys, n, D);
     return cudaGetLastError();
 }
 

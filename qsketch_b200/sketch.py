@@ -152,7 +152,9 @@ class Sketch:
     def profile(self):
         p = qs_profile()
         check(lib.qs_get_profile(self.handle, ctypes.byref(p)), "profile")
-        return {f: getattr(p, f) for f, _ in qs_profile._fields_}
+        d = {f: getattr(p, f) for f, _ in qs_profile._fields_}
+        d["repair_phase_ms"] = list(d["repair_phase_ms"])
+        return d
 
     def reset_status(self):
         check(lib.qs_reset_status(self.handle), "reset_status")

@@ -69,7 +69,7 @@ def test_uniform_config1_full_size(gpu):
     assert sk.stats()["linked_buckets"] == 0
 
 
-@pytest.mark.parametrize("agg", [1, 2])
+@pytest.mark.parametrize("agg", [1, 2, 3])
 def test_zipf_heavy_links(gpu, agg):
     sk, orc = make_pair(16381, 1 << 15, aggregate=agg)
     keys = data.zipf_keys(1 << 22, 1 << 18, 1.1, seed=5, perm_seed=77)
@@ -158,6 +158,13 @@ def test_host_buffers_match_device_path(gpu):
     out = torch.empty_like(pinned).pin_memory()
     sk.search_host(pinned, out)
     assert np.array_equal(out.numpy(), got)
+
+
+@pytest.mark.parametrize("agg", [2, 3])
+def test_uniform_aggregation_modes(gpu, agg):
+    sk, orc = make_pair(65521, 1 << 12, aggregate=agg, mask_rng=5)
+    keys = data.uniform_keys((1 << 21) + 5, seed=12)
+    run_and_compare(sk, orc, keys[3:], keys[3:])
 
 
 def test_zipf_config2_full_size(gpu):
