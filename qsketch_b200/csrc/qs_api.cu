@@ -371,7 +371,7 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         const uint64_t cap = std::min<uint64_t>(n_low, B);
         D.flag_cap = (uint32_t)cap;
         D.max_tiles = (uint32_t)((B + REPAIR_TILE - 1) / REPAIR_TILE);
-        D.long_cap = (uint32_t)(B / LONG_SEGMENT + 1);
+        D.long_cap = (uint32_t)std::min<uint64_t>(cap, 1ull << 16);  // slots with grid-computed totals
         uint32_t* masks_d = nullptr;
         CKB(sk->alloc(&D.low, n_low * LOW_WORDS), "alloc low table");
         CKB(sk->alloc(&D.high, p.n_high * HIGH_WORDS), "alloc high table");
@@ -385,7 +385,6 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         CKB(sk->alloc(&D.rec[1], B), "alloc records");
         CKB(sk->alloc(&D.hist, (uint64_t)256 * D.max_tiles), "alloc histograms");
         CKB(sk->alloc(&D.seg_beg, cap), "alloc segments");
-        CKB(sk->alloc(&D.long_id, cap), "alloc segment classes");
         CKB(sk->alloc(&D.totals, (uint64_t)D.long_cap * LOW_COUNTERS), "alloc totals");
         CKB(cudaMemcpy(masks_d, sk->masks.data(), (size_t)H * 4, cudaMemcpyHostToDevice), "upload masks");
         qs_status s = ctl_reset(sk, 0);

@@ -173,6 +173,8 @@ cudaError_t error_metrics(const uint32_t* d_est, const uint32_t* d_exact, uint64
 // kind 1: random 32 B sector loads, thread per sector (the query's access) -> sectors/s
 // kind 2: streaming 16 B loads over the buffer -> bytes/s
 // kind 3: kind 0 with returning atom.add and a prior load of the sector's last word
+// kind 4: one returning atom.add instruction per sector: 3 words + add 0 to the last word
+// kind 5: kind 0 after a prior load of the sector's last word
 __device__ __forceinline__ uint32_t probe_mix(uint32_t x) {
     x *= 0x9E3779B1u;
     x ^= x >> 16;
@@ -188,13 +190,19 @@ __global__ void k_probe(uint32_t kind, uint32_t* buf, uint64_t nsec, uint64_t no
     const int lane = threadIdx.x & 31, w = lane & 7;
     uint32_t acc = 0;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nops; i += stride) {
-        if (kind == 0 || kind == 3) {
+        if (kind == 0 || kind == 3 || kind == 4 || kind == 5) {
             const uint32_t key = (uint32_t)(i >> 3);
             const uint32_t h = probe_mix(key);
             const uint64_t s = ((uint64_t)h * nsec) >> 32;
             const uint32_t word = (w + (h & 7)) % 7;  // lanes 0..2 -> 3 distinct words of 0..6
             if (kind == 0) {
                 if (w < 3) atomicAdd(buf + s * 8 + word, 1u);
+            } else if (kind == 4) {
+                if (w < 3) acc += atomicAdd(buf + s * 8 + word, 1u);
+                if (w == 7) acc += atomicAdd(buf + s * 8 + 7, 0u);
+            } else if (kind == 5) {
+                const uint32_t v = __ldcg(buf + s * 8 + 7);
+                if (w < 3 && v != 0xdeadbeefu) atomicAdd(buf + s * 8 + word, 1u);
             } else {
                 const uint32_t v = __ldcg(buf + s * 8 + 7);
                 if (w < 3 && v != 0xdeadbeefu) acc += atomicAdd(buf + s * 8 + word, 1u);
@@ -215,7 +223,7 @@ __global__ void k_probe(uint32_t kind, uint32_t* buf, uint64_t nsec, uint64_t no
 }
 
 cudaError_t probe(uint32_t kind, uint64_t bytes, uint64_t ops, double* ops_per_s) {
-    if (kind > 3 || bytes < 64) return cudaErrorInvalidValue;
+    if (kind > 5 || bytes < 64) return cudaErrorInvalidValue;
     uint32_t* buf = nullptr;
     uint32_t* sink = nullptr;
     cudaEvent_t a = nullptr, b = nullptr;
@@ -226,7 +234,7 @@ cudaError_t probe(uint32_t kind, uint64_t bytes, uint64_t ops, double* ops_per_s
     if (e == cudaSuccess) e = cudaEventCreate(&b);
     const uint64_t nsec = bytes / 32;
     if (kind == 2) ops = nsec * 2 * 4;  // four passes of 16 B loads
-    const uint64_t thread_ops = (kind == 0 || kind == 3) ? ops * 8 : ops;
+    const uint64_t thread_ops = (kind == 0 || kind >= 3) ? ops * 8 : ops;
     float best = 1e30f;
     if (e == cudaSuccess) {
         int dev = 0, sms = 148;

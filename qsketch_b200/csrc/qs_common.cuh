@@ -84,9 +84,8 @@ struct MswsDev {
     uint2* rec[2];           // (slot, mask) records, ping-pong for the radix passes
     uint32_t* hist;          // 256 * max record tiles
     uint32_t* seg_beg;       // per slot: first record of its segment
-    uint32_t* long_id;       // per slot: index into totals or ~0u
-    uint32_t* totals;        // long slots * 28 counts
-    uint32_t long_cap;
+    uint32_t* totals;        // long_cap slots * 28 counts
+    uint32_t long_cap;       // slots whose per-counter totals are computed grid-wide
     uint32_t max_tiles;      // tiles of REPAIR_TILE elements in a chunk
 };
 
@@ -101,7 +100,6 @@ struct CmDev {
 
 constexpr int REPAIR_TILE = 4096;   // elements per tile in the ordered-replay passes
 constexpr int REPAIR_THREADS = 512; // 16 warps x 256 elements
-constexpr int LONG_SEGMENT = 256;   // segments longer than this get grid-wide counting
 constexpr int MAX_CM_ROWS = 16;
 
 // Spread a 4-bit nibble to the low bit of each byte: b0->bit0, b1->bit8, b2->bit16, b3->bit24.

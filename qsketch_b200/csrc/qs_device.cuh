@@ -82,7 +82,7 @@ __device__ __forceinline__ bool grid_barrier(Ctl* ctl) {
                     atomicOr(&ctl->status, ST_TIMEOUT);
                     break;
                 }
-                __nanosleep(128);
+                if (it > 256) __nanosleep(64);
             }
         }
         __threadfence();

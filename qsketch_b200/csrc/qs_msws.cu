@@ -300,9 +300,9 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
 
 // ---- ordered replay ---------------------------------------------------------------------
 
-__device__ __forceinline__ bool is_flagged(const MswsDev& D, uint32_t b) {
-    return (__ldcg(D.bitmap + (b >> 5)) >> (b & 31)) & 1u;
-}
+constexpr int SET_CAP = 4096;    // flagged buckets looked up in a per-block shared-memory set
+constexpr int SET_SLOTS = 8192;  // open addressing, load factor <= 1/2
+constexpr uint32_t NONE = 0xffffffffu;
 
 __device__ __forceinline__ int radix_passes(uint32_t F) {
     if (F <= 1) return 0;
@@ -310,11 +310,22 @@ __device__ __forceinline__ int radix_passes(uint32_t F) {
     return (bits + 7) / 8;
 }
 
-// Stable per-warp ranking of 256 consecutive elements by an 8-bit digit, three steps:
-// count (per warp), offsets (per digit across warps), rank + scatter.
-struct RadixSmem {
-    uint32_t whist[REPAIR_THREADS / 32][256];
-};
+// Slot of bucket b if it was flagged in this chunk, else NONE.
+__device__ __forceinline__ uint32_t flagged_slot(const MswsDev& D, const uint32_t* skey, const uint32_t* sval,
+                                                 bool use_set, uint32_t b) {
+    if (use_set) {
+        const uint32_t h = (b * 0x9E3779B1u) >> 19;  // 13 bits
+        for (int p = 0; p < SET_SLOTS; ++p) {
+            const uint32_t s = (h + p) & (SET_SLOTS - 1);
+            const uint32_t k = skey[s];
+            if (k == b) return sval[s];
+            if (k == NONE) return NONE;
+        }
+        return NONE;
+    }
+    if (!((__ldcg(D.bitmap + (b >> 5)) >> (b & 31)) & 1u)) return NONE;
+    return __ldcg(D.low + (uint64_t)b * LOW_WORDS + 7) & ~FLAG;
+}
 
 __device__ __forceinline__ uint64_t globaltimer() {
     uint64_t t;
@@ -331,11 +342,38 @@ __device__ __forceinline__ void phase_mark(Ctl* ctl, int k) {
     }
 }
 
+struct RadixSmem {
+    uint32_t whist[REPAIR_THREADS / 32][256];
+};
+
+size_t msws_repair_smem() { return (size_t)2 * SET_SLOTS * 4; }
+
+// Stable ranking of a tile of REPAIR_TILE records by the 8-bit digit at `shift`: each of
+// the 16 warps owns 256 consecutive records; per-warp digit counts, then per digit an
+// exclusive scan across warps (plus the tile's global offset when `base` is given).
+__device__ __forceinline__ void tile_count(RadixSmem& rs, const uint2* src, uint32_t K, uint32_t t, int shift) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int d = threadIdx.x; d < 256 * (REPAIR_THREADS / 32); d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
+    __syncthreads();
+    for (int r = 0; r < 256 / 32; ++r) {
+        const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
+        const bool v = i < K;
+        const uint32_t d = v ? (__ldcg(&src[i].x) >> shift) & 0xffu : 256u + lane;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* __restrict__ keys, uint64_t n,
                                                                 MswsDev D) {
     __shared__ RadixSmem rs;
     __shared__ uint32_t s_acc[2][LOW_COUNTERS];
     __shared__ uint32_t s_acc_slot[2];
+    extern __shared__ __align__(16) uint32_t s_set[];
+    uint32_t* skey = s_set;
+    uint32_t* sval = s_set + SET_SLOTS;
     Ctl* ctl = D.ctl;
     const uint32_t F = min(__ldcg(&ctl->n_flagged), D.flag_cap);
     if (F == 0) return;
@@ -343,8 +381,31 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     constexpr int NW = REPAIR_THREADS / 32;
-    constexpr int PER = REPAIR_TILE / REPAIR_THREADS;  // 8 elements per thread
+    constexpr int PER = REPAIR_TILE / REPAIR_THREADS;  // 8 consecutive keys per thread
     const uint32_t ntk = (uint32_t)((n + REPAIR_TILE - 1) / REPAIR_TILE);
+    const uint32_t nthreads = gridDim.x * REPAIR_THREADS;
+    const uint32_t gtid = blockIdx.x * REPAIR_THREADS + tid;
+
+    // Phase 0: the flagged buckets as a shared-memory set in every block; zero the totals.
+    const bool use_set = F <= (uint32_t)SET_CAP;
+    if (use_set) {
+        for (int i = tid; i < SET_SLOTS; i += REPAIR_THREADS) skey[i] = NONE;
+        __syncthreads();
+        for (uint32_t s = tid; s < F; s += REPAIR_THREADS) {
+            const uint32_t b = __ldcg(D.flag_list + s);
+            uint32_t h = (b * 0x9E3779B1u) >> 19;
+            for (int p = 0; p < SET_SLOTS; ++p, ++h) {
+                const uint32_t x = h & (SET_SLOTS - 1);
+                if (atomicCAS(skey + x, NONE, b) == NONE) {
+                    sval[x] = s;
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    const uint32_t ntot = min(F, D.long_cap);
+    for (uint32_t i = gtid; i < ntot * LOW_COUNTERS; i += nthreads) __stcg(D.totals + i, 0u);
 
     // Phase 1: count keys of flagged buckets per tile of the chunk.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
@@ -355,7 +416,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             const uint64_t i = base + j;
             if (i < n) {
                 const uint32_t hv = __ldg(keys + i) * D.seed;
-                c += is_flagged(D, fast_mod(D.fm_low, hv)) ? 1u : 0u;
+                c += flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, hv)) != NONE ? 1u : 0u;
             }
         }
         uint32_t total;
@@ -375,29 +436,27 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     // Phase 3: stable write of (slot, mask) records in array order.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
         const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
+        uint32_t slots[PER];
         uint32_t c = 0;
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
             const uint64_t i = base + j;
+            slots[j] = NONE;
             if (i < n) {
                 const uint32_t hv = __ldg(keys + i) * D.seed;
-                if (is_flagged(D, fast_mod(D.fm_low, hv))) ++c;
+                slots[j] = flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, hv));
+                c += slots[j] != NONE ? 1u : 0u;
             }
         }
         uint32_t total;
         uint32_t pos = block_exclusive_scan(c, &total) + __ldcg(D.tile_counts + t);
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
-            const uint64_t i = base + j;
-            if (i < n) {
-                const uint32_t hv = __ldg(keys + i) * D.seed;
-                const uint32_t b = fast_mod(D.fm_low, hv);
-                if (is_flagged(D, b)) {
-                    const uint32_t slot = __ldcg(D.low + (uint64_t)b * LOW_WORDS + 7) & ~FLAG;
-                    const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hv));
-                    __stcg(D.rec[0] + pos, make_uint2(slot, mask));
-                    ++pos;
-                }
+            if (slots[j] != NONE) {
+                const uint32_t hv = __ldg(keys + base + j) * D.seed;
+                const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hv));
+                __stcg(D.rec[0] + pos, make_uint2(slots[j], mask));
+                ++pos;
             }
         }
     }
@@ -411,19 +470,8 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         const uint2* src = D.rec[p & 1];
         uint2* dst = D.rec[(p + 1) & 1];
         const int shift = 8 * p;
-        // 4a: per-tile digit histograms (digit-major: hist[d * ntr + t])
-        for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {
-            for (int d = tid; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
-            __syncthreads();
-            for (int r = 0; r < 256 / 32; ++r) {
-                const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
-                const bool v = i < K;
-                const uint32_t d = v ? (__ldcg(&src[i].x) >> shift) & 0xffu : 256u + lane;
-                const uint32_t peers = __match_any_sync(0xffffffffu, d);
-                if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
-                __syncwarp();
-            }
-            __syncthreads();
+        for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {  // per-tile digit counts
+            tile_count(rs, src, K, t, shift);
             for (int d = tid; d < 256; d += REPAIR_THREADS) {
                 uint32_t s = 0;
                 for (int w = 0; w < NW; ++w) s += rs.whist[w][d];
@@ -434,19 +482,8 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         if (!grid_barrier(ctl)) return;
         if (blockIdx.x == 0) block_scan_array(D.hist, 256u * ntr);
         if (!grid_barrier(ctl)) return;
-        // 4c: stable scatter
-        for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {
-            for (int d = tid; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
-            __syncthreads();
-            for (int r = 0; r < 256 / 32; ++r) {
-                const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
-                const bool v = i < K;
-                const uint32_t d = v ? (__ldcg(&src[i].x) >> shift) & 0xffu : 256u + lane;
-                const uint32_t peers = __match_any_sync(0xffffffffu, d);
-                if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
-                __syncwarp();
-            }
-            __syncthreads();
+        for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {  // stable scatter
+            tile_count(rs, src, K, t, shift);
             for (int d = tid; d < 256; d += REPAIR_THREADS) {
                 uint32_t run = __ldcg(D.hist + (uint64_t)d * ntr + t);
                 for (int w = 0; w < NW; ++w) {
@@ -477,46 +514,26 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     phase_mark(ctl, 3);
     const uint2* sorted = D.rec[npass & 1];
 
-    // Phase 5: segment starts per slot, then segment classes.
-    for (uint32_t i = blockIdx.x * REPAIR_THREADS + tid; i < K; i += gridDim.x * REPAIR_THREADS) {
+    // Phase 5: segment starts, and per-counter totals of slots < long_cap; each block a
+    // contiguous record range whose first and last slot accumulate in shared memory.
+    for (uint32_t i = gtid; i < K; i += nthreads) {
         const uint32_t s = __ldcg(&sorted[i].x);
         if (i == 0 || __ldcg(&sorted[i - 1].x) != s) __stcg(D.seg_beg + s, i);
     }
-    if (!grid_barrier(ctl)) return;
-    phase_mark(ctl, 4);
-    for (uint32_t s = blockIdx.x * REPAIR_THREADS + tid; s < F; s += gridDim.x * REPAIR_THREADS) {
-        const uint32_t beg = __ldcg(D.seg_beg + s);
-        const uint32_t end = (s + 1 < F) ? __ldcg(D.seg_beg + s + 1) : K;
-        uint32_t lid = ~0u;
-        if (end - beg > (uint32_t)LONG_SEGMENT) {
-            const uint32_t l = atomicAdd(&ctl->n_long, 1u);
-            if (l < D.long_cap) {
-                lid = l;
-                for (int i = 0; i < LOW_COUNTERS; ++i) __stcg(D.totals + (uint64_t)l * LOW_COUNTERS + i, 0u);
-            }
-        }
-        __stcg(D.long_id + s, lid);
-    }
-    if (!grid_barrier(ctl)) return;
-    phase_mark(ctl, 5);
-
-    // Phase 6: per-counter totals of long segments; each block a contiguous record range,
-    // the range's first and last slot accumulate in shared memory.
     {
         const uint32_t per = ((K + gridDim.x - 1) / gridDim.x + 31) & ~31u;
         const uint32_t beg = min(K, blockIdx.x * per), end = min(K, beg + per);
         if (tid < 2 * LOW_COUNTERS) (&s_acc[0][0])[tid] = 0;
         if (tid == 0) {
-            s_acc_slot[0] = beg < end ? __ldcg(&sorted[beg].x) : ~0u;
-            s_acc_slot[1] = beg < end ? __ldcg(&sorted[end - 1].x) : ~0u;
+            s_acc_slot[0] = beg < end ? __ldcg(&sorted[beg].x) : NONE;
+            s_acc_slot[1] = beg < end ? __ldcg(&sorted[end - 1].x) : NONE;
         }
         __syncthreads();
         for (uint32_t g = beg + wid * 32; g < end; g += REPAIR_THREADS) {
             const uint32_t i = g + lane;
             const bool v = i < end;
-            const uint2 rec = v ? __ldcg(&sorted[i]) : make_uint2(~0u, 0u);
-            const uint32_t lid = v ? __ldcg(D.long_id + rec.x) : ~0u;
-            const bool use = v && lid != ~0u;
+            const uint2 rec = v ? __ldcg(&sorted[i]) : make_uint2(NONE, 0u);
+            const bool use = v && rec.x < D.long_cap;
             const uint32_t peers = __match_any_sync(0xffffffffu, rec.x);
             const bool leader = lane == __ffs(peers) - 1;
             const int sl = rec.x == s_acc_slot[0] ? 0 : (rec.x == s_acc_slot[1] ? 1 : -1);
@@ -527,7 +544,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
                     if (sl >= 0)
                         atomicAdd(&s_acc[sl][c], cnt);
                     else
-                        atomicAdd(D.totals + (uint64_t)lid * LOW_COUNTERS + c, cnt);
+                        atomicAdd(D.totals + (uint64_t)rec.x * LOW_COUNTERS + c, cnt);
                 }
             }
         }
@@ -537,25 +554,21 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             const uint32_t s = s_acc_slot[sl];
             const bool dup = (sl == 1 && s == s_acc_slot[0]);
             const uint32_t v = s_acc[sl][c];
-            if (s != ~0u && !dup && v) {
-                const uint32_t lid = __ldcg(D.long_id + s);
-                if (lid != ~0u) atomicAdd(D.totals + (uint64_t)lid * LOW_COUNTERS + c, v);
-            }
+            if (s < D.long_cap && !dup && v) atomicAdd(D.totals + (uint64_t)s * LOW_COUNTERS + c, v);
         }
     }
     if (!grid_barrier(ctl)) return;
-    phase_mark(ctl, 6);
+    phase_mark(ctl, 4);
 
-    // Phase 7: replay each flagged bucket in array order, one warp per slot.
+    // Phase 6: replay each flagged bucket in array order, one warp per slot.
     const uint32_t lt = lanemask_lt();
     for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) {
         const uint32_t b = __ldcg(D.flag_list + s);
         const uint32_t beg = __ldcg(D.seg_beg + s);
         const uint32_t end = (s + 1 < F) ? __ldcg(D.seg_beg + s + 1) : K;
-        const uint32_t lid = __ldcg(D.long_id + s);
         uint32_t T = 0;  // lane i < 28: occurrences of counter i in the chunk
-        if (lid != ~0u) {
-            T = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)lid * LOW_COUNTERS + lane) : 0u;
+        if (s < D.long_cap) {
+            T = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane) : 0u;
         } else {
             for (uint32_t g = beg; g < end; g += 32) {
                 const uint32_t m = (g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u;
@@ -580,7 +593,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         const uint32_t P = lane < LOW_COUNTERS ? (pwi >> (8 * (lane & 3))) & 0xffu : 0u;
         uint32_t cur = P;
         // first key (array order) that sees a selected counter > LIMIT
-        uint32_t L = ~0u, mL = 0;
+        uint32_t L = NONE, mL = 0;
         for (uint32_t g = beg; g < end; g += 32) {
             const uint32_t m = (g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u;
             bool trig = false;
@@ -607,7 +620,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             }
             cur += inc;
         }
-        if (L != ~0u) {
+        if (L != NONE) {
             uint32_t H = T - (cur - P);  // increments of key L and all later keys
             if (D.compat_v3) {          // device_sketch_v3.h:187: linking key lands on bit % 8
                 if (lane < LOW_COUNTERS && ((mL >> lane) & 1u)) H -= 1u;
@@ -638,7 +651,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         }
     }
     if (!grid_barrier(ctl)) return;
-    phase_mark(ctl, 7);
+    phase_mark(ctl, 5);
     if (blockIdx.x == 0 && tid == 0) {
         ctl->n_flagged = 0;
         ctl->n_records = 0;
@@ -720,7 +733,10 @@ cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_insert<AGG_BLOCK>, INS_THREADS, ins_smem);
     if (e != cudaSuccess) return e;
     L->insert_grid = prop.multiProcessorCount * (occ > 0 ? occ : 1);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_repair, REPAIR_THREADS, 0);
+    e = cudaFuncSetAttribute((const void*)k_msws_repair, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)msws_repair_smem());
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_repair, REPAIR_THREADS, msws_repair_smem());
     if (e != cudaSuccess) return e;
     if (occ < 1) return cudaErrorInvalidConfiguration;
     L->repair_grid = prop.multiProcessorCount * (occ < 2 ? occ : 2);
@@ -747,8 +763,8 @@ cudaError_t msws_repair(const uint32_t* d_keys, uint64_t n, const MswsDev& D, co
     if (n == 0) return cudaSuccess;
     MswsDev Dc = D;
     void* args[] = {(void*)&d_keys, (void*)&n, (void*)&Dc};
-    return cudaLaunchCooperativeKernel((const void*)k_msws_repair, dim3(L.repair_grid), dim3(REPAIR_THREADS), args, 0,
-                                       st);
+    return cudaLaunchCooperativeKernel((const void*)k_msws_repair, dim3(L.repair_grid), dim3(REPAIR_THREADS), args,
+                                       msws_repair_smem(), st);
 }
 
 cudaError_t msws_query(const uint32_t* d_keys, uint64_t n, uint32_t* d_out, const MswsDev& D, const MswsLaunch& L,
