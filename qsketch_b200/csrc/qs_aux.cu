@@ -198,8 +198,7 @@ __global__ void k_probe(uint32_t kind, uint32_t* buf, uint64_t nsec, uint64_t no
             if (kind == 0) {
                 if (w < 3) atomicAdd(buf + s * 8 + word, 1u);
             } else if (kind == 4) {
-                if (w < 3) acc += atomicAdd(buf + s * 8 + word, 1u);
-                if (w == 7) acc += atomicAdd(buf + s * 8 + 7, 0u);
+                if (w < 3 || w == 7) acc += atomicAdd(buf + s * 8 + (w == 7 ? 7u : word), w == 7 ? 0u : 1u);
             } else if (kind == 5) {
                 const uint32_t v = __ldcg(buf + s * 8 + 7);
                 if (w < 3 && v != 0xdeadbeefu) atomicAdd(buf + s * 8 + word, 1u);

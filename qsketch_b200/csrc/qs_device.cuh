@@ -126,16 +126,37 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
 }
 
 // Exclusive scan in place of a global array a[0..len) by one block; returns the total.
+// a must be 16-byte aligned; each thread owns a run of a multiple of 4 entries.
 __device__ __forceinline__ uint32_t block_scan_array(uint32_t* a, uint32_t len) {
-    const uint32_t per = (len + blockDim.x - 1) / blockDim.x;
-    const uint32_t beg = threadIdx.x * per;
+    const uint32_t per = ((len + blockDim.x - 1) / blockDim.x + 3) & ~3u;
+    const uint32_t beg = min(len, threadIdx.x * per);
     const uint32_t end = min(len, beg + per);
-    uint32_t sum = 0;
-    for (uint32_t i = beg; i < end; ++i) sum += __ldcg(a + i);
+    uint32_t sum = 0, i = beg;
+#pragma unroll 4
+    for (; i + 4 <= end; i += 4) {
+        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(a + i));
+        sum += v.x + v.y + v.z + v.w;
+    }
+    for (; i < end; ++i) sum += __ldcg(a + i);
     uint32_t total;
     uint32_t run = block_exclusive_scan(sum, &total);
-    for (uint32_t i = beg; i < end; ++i) {
-        uint32_t t = __ldcg(a + i);
+    i = beg;
+#pragma unroll 4
+    for (; i + 4 <= end; i += 4) {
+        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(a + i));
+        uint4 o;
+        o.x = run;
+        run += v.x;
+        o.y = run;
+        run += v.y;
+        o.z = run;
+        run += v.z;
+        o.w = run;
+        run += v.w;
+        __stcg(reinterpret_cast<uint4*>(a + i), o);
+    }
+    for (; i < end; ++i) {
+        const uint32_t t = __ldcg(a + i);
         __stcg(a + i, run);
         run += t;
     }

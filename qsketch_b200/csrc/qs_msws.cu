@@ -35,6 +35,14 @@ constexpr uint32_t AGG_EMPTY = 0xffffffffu;
 // 3 warp + block (linked keys of a whole tile merge in shared memory, so a heavy hitter
 // costs one atomic per high counter per tile instead of one per occurrence).
 enum { AGG_NONE = 0, AGG_WARP = 1, AGG_BLOCK = 2 };
+// Routing of a tile's keys between the low and the high level:
+// ROUTE_PRELOAD loads each bucket's index word first, then sends linked keys to the high
+// level (through the tile table) and the others to the packed low atomics;
+// ROUTE_FUSED skips the load: lane 7 of each sub-warp adds 0 to the index word in the same
+// atomic instruction that adds the low counters, and the rare key that finds its bucket
+// linked takes its low increments back (u32 addition is invertible) and counts high.
+// A CTA picks the mode of its next tile from the linked share of the last one.
+enum { ROUTE_PRELOAD = 0, ROUTE_FUSED = 1 };
 
 struct InsShared {
     uint32_t* keys;   // [INS_STAGES][INS_TILE]
@@ -44,7 +52,8 @@ struct InsShared {
     uint32_t* aid;    // [AGG_SLOTS] high id of the key's bucket
     uint4* stage;     // [INS_WARPS][32] per-warp round staging
     uint32_t* masks;  // [n_masks]
-    uint32_t* dropped;
+    uint32_t* misc;   // [0] keys dropped (saturated buckets), [1] linked keys in this tile,
+                      // [2] routing mode of this tile (ROUTE_*)
 };
 
 __device__ __forceinline__ InsShared ins_carve(uint8_t* smem, uint32_t n_masks) {
@@ -62,7 +71,7 @@ __device__ __forceinline__ InsShared ins_carve(uint8_t* smem, uint32_t n_masks) 
     p += AGG_SLOTS * 4;
     S.stage = reinterpret_cast<uint4*>(p);
     p += INS_WARPS * 32 * 16;
-    S.dropped = reinterpret_cast<uint32_t*>(p);
+    S.misc = reinterpret_cast<uint32_t*>(p);
     p += 16;
     S.masks = reinterpret_cast<uint32_t*>(p);
     (void)n_masks;
@@ -155,10 +164,59 @@ __device__ __forceinline__ void staged_rounds(const MswsDev& D, const uint4* st,
     }
 }
 
+// ROUTE_FUSED rounds: entry j = (bucket, mask, count, key).  Returns the linked count.
+__device__ __forceinline__ uint32_t staged_rounds_fused(const MswsDev& D, const InsShared& S, const uint4* st,
+                                                        int nact) {
+    const int lane = threadIdx.x & 31, sub = lane >> 3, w = lane & 7;
+    uint32_t olds[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        olds[r] = 0;
+        if (r * 4 >= nact) continue;  // warp-uniform
+        const int j = r * 4 + sub;
+        if (j >= nact) continue;
+        const uint4 e = st[j];
+        const uint32_t nib = (w < 7) ? (e.y >> (4 * w)) & 0xfu : 0u;
+        if (nib || w == 7)
+            olds[r] = atomicAdd(D.low + (uint64_t)e.x * LOW_WORDS + w, w == 7 ? 0u : expand_nibble(nib) * e.z);
+    }
+    uint32_t linked_keys = 0;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        if (r * 4 >= nact) continue;  // warp-uniform
+        const int j = r * 4 + sub;
+        const bool ve = j < nact;
+        uint4 e = make_uint4(0, 0, 0, 0);
+        if (ve) e = st[j];
+        const uint32_t ptr = __shfl_sync(0xffffffffu, olds[r], (lane & ~7) | 7);
+        const bool linked = ve && is_linked(D, ptr);
+        const bool sat = ve && ptr == SATURATED;
+        const uint32_t nib = (w < 7) ? (e.y >> (4 * w)) & 0xfu : 0u;
+        if ((linked || sat) && nib) atomicAdd(D.low + (uint64_t)e.x * LOW_WORDS + w, 0u - expand_nibble(nib) * e.z);
+        bool cross = false;
+        if (ve && !linked && !sat && nib) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (((nib >> k) & 1u) && ((olds[r] >> (8 * k)) & 0xffu) + e.z >= CROSS) cross = true;
+        }
+        const uint32_t bal = __ballot_sync(0xffffffffu, cross);
+        if (w == 0) {
+            if ((bal >> (sub * 8)) & 0xffu) flag_bucket(D, e.x);
+            if (sat) atomicAdd(S.misc + 0, e.z);
+            if (linked) {  // rare in this mode: count high directly
+                uint32_t* hb = D.high + (uint64_t)(ptr - START) * HIGH_WORDS;
+                for (uint32_t mm = e.y; mm; mm &= mm - 1) atomicAdd(hb + (__ffs(mm) - 1), e.z);
+                linked_keys += e.z;
+            }
+        }
+    }
+    return linked_keys;
+}
+
 // Up to 32 keys held one per lane (valid lanes: lane < cnt).
 template <int AGG>
 __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& S, uint32_t key, int cnt,
-                                             bool use_table) {
+                                             bool use_table, int route) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const bool valid = lane < cnt;
     const uint32_t hv = key * D.seed;  // hash_mul_add, device_hash_function.h:6-18
@@ -170,15 +228,25 @@ __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& 
         const uint32_t peers = __match_any_sync(0xffffffffu, key) & vmask;
         c = (valid && lane == __ffs(peers) - 1) ? (uint32_t)__popc(peers) : 0u;
     }
+    uint4* st = S.stage + wid * 32;
+    if (route == ROUTE_FUSED) {
+        const uint32_t am = __ballot_sync(0xffffffffu, c != 0);
+        if (c) st[__popc(am & lanemask_lt())] = make_uint4(b, m, c, key);
+        __syncwarp();
+        const uint32_t lk = staged_rounds_fused(D, S, st, __popc(am));
+        if (lk) atomicAdd(S.misc + 1, lk);
+        __syncwarp();
+        return;
+    }
     const uint32_t w7 = c ? __ldcg(D.low + (uint64_t)b * LOW_WORDS + 7) : 0u;
     const bool linked = c && is_linked(D, w7);
     const bool sat = c && w7 == SATURATED;
-    if (sat) atomicAdd(S.dropped, c);
+    if (sat) atomicAdd(S.misc + 0, c);
+    if (linked) atomicAdd(S.misc + 1, c);
     bool direct_high = linked;
     if (AGG == AGG_BLOCK && linked && use_table) direct_high = !agg_insert(S, key, c, w7);
     const bool act = (c && !linked && !sat) || direct_high;
     const uint32_t am = __ballot_sync(0xffffffffu, act);
-    uint4* st = S.stage + wid * 32;
     if (act) st[__popc(am & lanemask_lt())] = make_uint4(direct_high ? w7 : b, m, c, direct_high ? 1u : 0u);
     __syncwarp();
     staged_rounds(D, st, __popc(am));
@@ -225,7 +293,11 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
         S.akey[i] = AGG_EMPTY;
         S.acnt[i] = 0;
     }
-    if (tid == 0) *S.dropped = 0;
+    if (tid == 0) {
+        S.misc[0] = 0;
+        S.misc[1] = 0;
+        S.misc[2] = __ldcg(&D.ctl->next_id) == FIRST_ID ? ROUTE_FUSED : ROUTE_PRELOAD;
+    }
 
     // 16-byte aligned body for the TMA bulk copies; the <= 6 ragged keys go through CTA 0.
     const uintptr_t addr = reinterpret_cast<uintptr_t>(keys);
@@ -243,7 +315,7 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
     __syncthreads();
     if (blockIdx.x == 0 && wid == 0 && head + tail > 0) {
         const uint32_t k = lane < (int)(head + tail) ? s_extra[lane] : 0u;
-        insert_group<AGG>(D, S, k, (int)(head + tail), false);
+        insert_group<AGG>(D, S, k, (int)(head + tail), false, ROUTE_PRELOAD);
     }
 
     const uint64_t ntiles = (body_n + INS_TILE - 1) / INS_TILE;
@@ -279,12 +351,17 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
         const uint64_t g = blockIdx.x + i * gridDim.x;
         const int cnt = (int)umin64(INS_TILE, body_n - g * INS_TILE);
         const uint32_t* tk = S.keys + st * INS_TILE;
+        const int route = (int)S.misc[2];
         for (int base = wid * 32; base < cnt; base += INS_THREADS) {
             const int c = min(32, cnt - base);
             const uint32_t k = lane < c ? tk[base + lane] : 0u;
-            insert_group<AGG>(D, S, k, c, true);
+            insert_group<AGG>(D, S, k, c, true, route);
         }
         __syncthreads();
+        if (tid == 0) {  // next tile: fused while under 1/16 of the keys find their bucket linked
+            S.misc[2] = S.misc[1] * 16u < (uint32_t)cnt ? ROUTE_FUSED : ROUTE_PRELOAD;
+            S.misc[1] = 0;
+        }
         if (AGG == AGG_BLOCK) {
             drain_table(D, S);
             __syncthreads();
@@ -295,7 +372,7 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
         }
     }
     __syncthreads();
-    if (tid == 0 && *S.dropped) atomicAdd(&D.ctl->dropped, (unsigned long long)*S.dropped);
+    if (tid == 0 && S.misc[0]) atomicAdd(&D.ctl->dropped, (unsigned long long)S.misc[0]);
 }
 
 // ---- ordered replay ---------------------------------------------------------------------
@@ -407,75 +484,99 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     const uint32_t ntot = min(F, D.long_cap);
     for (uint32_t i = gtid; i < ntot * LOW_COUNTERS; i += nthreads) __stcg(D.totals + i, 0u);
 
-    // Phase 1: count keys of flagged buckets per tile of the chunk.
+    // Phases 1-3 are the first (digit 0) pass of a stable LSD radix sort by slot whose
+    // input is the key chunk itself: keys of unflagged buckets drop out, the others become
+    // (slot, mask) records, ordered by digit 0 and, within a digit, by array position.
+    // Warp w of a tile owns keys [w*256, w*256+256) in 8 rounds of 32, so (warp, round,
+    // lane) is array order.
+    const int npass = max(1, radix_passes(F));
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
-        const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
-        uint32_t c = 0;
-#pragma unroll
-        for (int j = 0; j < PER; ++j) {
-            const uint64_t i = base + j;
-            if (i < n) {
-                const uint32_t hv = __ldg(keys + i) * D.seed;
-                c += flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, hv)) != NONE ? 1u : 0u;
-            }
+        for (int d = tid; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
+        __syncthreads();
+        for (int r = 0; r < 8; ++r) {
+            const uint64_t i = (uint64_t)t * REPAIR_TILE + wid * 256 + r * 32 + lane;
+            uint32_t slot = NONE;
+            if (i < n) slot = flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, __ldg(keys + i) * D.seed));
+            const bool v = slot != NONE;
+            const uint32_t d = v ? (slot & 0xffu) : 256u + lane;
+            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
+            __syncwarp();
         }
-        uint32_t total;
-        block_exclusive_scan(c, &total);
-        if (tid == 0) __stcg(D.tile_counts + t, total);
+        __syncthreads();
+        for (int d = tid; d < 256; d += REPAIR_THREADS) {
+            uint32_t sum = 0;
+            for (int w = 0; w < NW; ++w) sum += rs.whist[w][d];
+            __stcg(D.hist + (uint64_t)d * ntk + t, sum);
+        }
+        __syncthreads();
     }
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 0);
-    // Phase 2: exclusive scan of the tile counts.
     if (blockIdx.x == 0) {
-        const uint32_t K = block_scan_array(D.tile_counts, ntk);
+        const uint32_t K = block_scan_array(D.hist, 256u * ntk);
         if (tid == 0) __stcg(&ctl->n_records, K);
     }
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 1);
     const uint32_t K = __ldcg(&ctl->n_records);
-    // Phase 3: stable write of (slot, mask) records in array order.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
-        const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
-        uint32_t slots[PER];
-        uint32_t c = 0;
+        for (int d = tid; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
+        __syncthreads();
+        uint32_t slots[8];
 #pragma unroll
-        for (int j = 0; j < PER; ++j) {
-            const uint64_t i = base + j;
-            slots[j] = NONE;
-            if (i < n) {
+        for (int r = 0; r < 8; ++r) {
+            const uint64_t i = (uint64_t)t * REPAIR_TILE + wid * 256 + r * 32 + lane;
+            slots[r] = NONE;
+            if (i < n) slots[r] = flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, __ldg(keys + i) * D.seed));
+            const bool v = slots[r] != NONE;
+            const uint32_t d = v ? (slots[r] & 0xffu) : 256u + lane;
+            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        for (int d = tid; d < 256; d += REPAIR_THREADS) {
+            uint32_t run = __ldcg(D.hist + (uint64_t)d * ntk + t);
+            for (int w = 0; w < NW; ++w) {
+                const uint32_t x = rs.whist[w][d];
+                rs.whist[w][d] = run;
+                run += x;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const uint64_t i = (uint64_t)t * REPAIR_TILE + wid * 256 + r * 32 + lane;
+            const bool v = slots[r] != NONE;
+            const uint32_t d = v ? (slots[r] & 0xffu) : 256u + lane;
+            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            if (v) {
                 const uint32_t hv = __ldg(keys + i) * D.seed;
-                slots[j] = flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, hv));
-                c += slots[j] != NONE ? 1u : 0u;
-            }
-        }
-        uint32_t total;
-        uint32_t pos = block_exclusive_scan(c, &total) + __ldcg(D.tile_counts + t);
-#pragma unroll
-        for (int j = 0; j < PER; ++j) {
-            if (slots[j] != NONE) {
-                const uint32_t hv = __ldg(keys + base + j) * D.seed;
                 const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hv));
-                __stcg(D.rec[0] + pos, make_uint2(slots[j], mask));
-                ++pos;
+                __stcg(D.rec[0] + rs.whist[wid][d] + __popc(peers & lanemask_lt()), make_uint2(slots[r], mask));
             }
+            __syncwarp();
+            if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
+            __syncwarp();
         }
+        __syncthreads();
     }
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 2);
 
-    // Phase 4: stable LSD radix sort of the records by slot, 8 bits per pass.
-    const int npass = radix_passes(F);
+    // Phase 4: the remaining radix passes over the records, 8 bits each.
     const uint32_t ntr = (K + REPAIR_TILE - 1) / REPAIR_TILE;
-    for (int p = 0; p < npass; ++p) {
-        const uint2* src = D.rec[p & 1];
-        uint2* dst = D.rec[(p + 1) & 1];
+    for (int p = 1; p < npass; ++p) {
+        const uint2* src = D.rec[(p - 1) & 1];
+        uint2* dst = D.rec[p & 1];
         const int shift = 8 * p;
         for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {  // per-tile digit counts
             tile_count(rs, src, K, t, shift);
             for (int d = tid; d < 256; d += REPAIR_THREADS) {
-                uint32_t s = 0;
-                for (int w = 0; w < NW; ++w) s += rs.whist[w][d];
-                __stcg(D.hist + (uint64_t)d * ntr + t, s);
+                uint32_t sum = 0;
+                for (int w = 0; w < NW; ++w) sum += rs.whist[w][d];
+                __stcg(D.hist + (uint64_t)d * ntr + t, sum);
             }
             __syncthreads();
         }
@@ -512,7 +613,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         if (!grid_barrier(ctl)) return;
     }
     phase_mark(ctl, 3);
-    const uint2* sorted = D.rec[npass & 1];
+    const uint2* sorted = D.rec[(npass - 1) & 1];
 
     // Phase 5: segment starts, and per-counter totals of slots < long_cap; each block a
     // contiguous record range whose first and last slot accumulate in shared memory.

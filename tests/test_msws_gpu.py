@@ -92,6 +92,21 @@ def test_compat_v3(gpu):
     run_and_compare(sk, orc, keys, data.rank_keys(8, 0, 1 << 16))
 
 
+def test_few_links_fused_routing(gpu):
+    # a handful of heavy keys inside a uniform stream: after the first chunk links their
+    # buckets, tiles run in the fused routing mode, where a linked key takes its low
+    # increments back and counts in the high bucket
+    sk, orc = make_pair(65521, 1 << 10, max_batch=1 << 18)
+    uni = data.uniform_keys(1 << 21, seed=31)
+    heavy = torch.tensor([7, 11, 13, 1 << 31], dtype=torch.int64).to(torch.uint32).cuda()
+    idx = torch.arange(1 << 21, device="cuda") % 97 == 0
+    keys = uni.clone()
+    keys[idx] = heavy[(torch.arange(int(idx.sum()), device="cuda") % 4)]
+    q = torch.cat([heavy, uni[:4096]])
+    run_and_compare(sk, orc, keys, q)
+    assert sk.stats()["linked_buckets"] >= 4
+
+
 def test_single_heavy_key(gpu):
     sk, orc = make_pair(1021, 64)
     keys = torch.full((1 << 20,), 123456789, dtype=torch.uint32, device="cuda")
