@@ -92,6 +92,9 @@ typedef struct qs_params {
                                     else 8 (one lane per bucket word) */
     uint32_t aggregate;          /* 0 = autotune, 1 = off, 2 = warp, 3 = block
                                     pre-aggregation of duplicate keys */
+    uint32_t route;              /* insert routing between the levels: 0 = adaptive per
+                                    tile, 1 = load each bucket's index word first,
+                                    2 = read it with the counter atomic */
 } qs_params;
 
 typedef struct qs_sketch qs_sketch;

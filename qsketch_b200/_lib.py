@@ -44,6 +44,7 @@ class qs_params(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("lanes_per_key", ctypes.c_uint32),
         ("aggregate", ctypes.c_uint32),
+        ("route", ctypes.c_uint32),
     ]
 
 

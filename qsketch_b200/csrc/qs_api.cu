@@ -367,6 +367,8 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         D.seed = sk->seeds[0];
         D.n_masks = H;
         D.compat_v3 = (p.flags & QS_FLAG_COMPAT_V3) ? 1u : 0u;
+        if (p.route > 2) return bail(fail(QS_ERR_INVALID_ARG, "route out of [0, 2]"));
+        D.route = p.route;
         const uint64_t B = sk->max_batch;
         const uint64_t cap = std::min<uint64_t>(n_low, B);
         D.flag_cap = (uint32_t)cap;

@@ -86,6 +86,7 @@ struct MswsDev {
     uint32_t* seg_beg;       // per slot: first record of its segment
     uint32_t* totals;        // long_cap slots * 28 counts
     uint32_t long_cap;       // slots whose per-counter totals are computed grid-wide
+    uint32_t route;          // 0 adaptive, 1 preload, 2 fused (pass-1 routing)
     uint32_t max_tiles;      // tiles of REPAIR_TILE elements in a chunk
 };
 

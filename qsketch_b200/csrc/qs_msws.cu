@@ -296,7 +296,9 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
     if (tid == 0) {
         S.misc[0] = 0;
         S.misc[1] = 0;
-        S.misc[2] = __ldcg(&D.ctl->next_id) == FIRST_ID ? ROUTE_FUSED : ROUTE_PRELOAD;
+        S.misc[2] = D.route == 1 ? ROUTE_PRELOAD
+                    : D.route == 2 ? ROUTE_FUSED
+                                   : (__ldcg(&D.ctl->next_id) == FIRST_ID ? ROUTE_FUSED : ROUTE_PRELOAD);
     }
 
     // 16-byte aligned body for the TMA bulk copies; the <= 6 ragged keys go through CTA 0.
@@ -358,8 +360,8 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
             insert_group<AGG>(D, S, k, c, true, route);
         }
         __syncthreads();
-        if (tid == 0) {  // next tile: fused while under 1/16 of the keys find their bucket linked
-            S.misc[2] = S.misc[1] * 16u < (uint32_t)cnt ? ROUTE_FUSED : ROUTE_PRELOAD;
+        if (tid == 0) {  // adaptive: the next tile is fused while under 1/16 of the keys are linked
+            if (D.route == 0) S.misc[2] = S.misc[1] * 16u < (uint32_t)cnt ? ROUTE_FUSED : ROUTE_PRELOAD;
             S.misc[1] = 0;
         }
         if (AGG == AGG_BLOCK) {
@@ -443,6 +445,159 @@ __device__ __forceinline__ void tile_count(RadixSmem& rs, const uint2* src, uint
     __syncthreads();
 }
 
+// Replay flagged bucket `s` (one warp): its records sorted[seg_beg[s] .. next segment) are
+// the chunk's keys of that bucket in array order.  Restores the pre-chunk counters, finds
+// the first key that sees a selected counter above LIMIT (the sequential low->high switch
+// of device_sketch_v3.h:160-190), links the bucket there and writes the final words.
+__device__ __forceinline__ void replay_slot(const MswsDev& D, const uint2* sorted, uint32_t s, uint32_t F, uint32_t K,
+                                            bool use_totals) {
+    Ctl* ctl = D.ctl;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = lanemask_lt();
+    const uint32_t b = __ldcg(D.flag_list + s);
+    const uint32_t beg = __ldcg(D.seg_beg + s);
+    const uint32_t end = (s + 1 < F) ? __ldcg(D.seg_beg + s + 1) : K;
+    uint32_t T = 0;  // lane i < 28: occurrences of counter i in the chunk
+    if (use_totals && s < D.long_cap) {
+        T = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane) : 0u;
+    } else {
+        for (uint32_t g = beg; g < end; g += 32) {
+            const uint32_t m = (g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u;
+#pragma unroll
+            for (int c = 0; c < LOW_COUNTERS; ++c) {
+                const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
+                if (lane == c) T += __popc(bal);
+            }
+        }
+    }
+    uint32_t* wp = D.low + (uint64_t)b * LOW_WORDS;
+    const uint32_t fw = lane < 7 ? __ldcg(wp + lane) : 0u;
+    // pre-chunk word = final word - packed sum of the chunk's increments (mod 2^32)
+    uint32_t sw = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t t = __shfl_sync(0xffffffffu, T, (4 * (lane & 7) + k) & 31);
+        sw += t << (8 * k);
+    }
+    const uint32_t pw = fw - sw;
+    const uint32_t pwi = __shfl_sync(0xffffffffu, pw, (lane >> 2) & 7);
+    const uint32_t P = lane < LOW_COUNTERS ? (pwi >> (8 * (lane & 3))) & 0xffu : 0u;
+    uint32_t cur = P;
+    // first key (array order) that sees a selected counter > LIMIT
+    uint32_t L = NONE, mL = 0;
+    for (uint32_t g = beg; g < end; g += 32) {
+        const uint32_t m = (g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u;
+        bool trig = false;
+        uint32_t inc = 0;
+#pragma unroll
+        for (int c = 0; c < LOW_COUNTERS; ++c) {
+            const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
+            const uint32_t cc = __shfl_sync(0xffffffffu, cur, c);
+            if (((m >> c) & 1u) && cc + __popc(bal & lt) > LIMIT) trig = true;
+            if (lane == c) inc = __popc(bal);
+        }
+        const uint32_t tb = __ballot_sync(0xffffffffu, trig);
+        if (tb) {
+            const int j = __ffs(tb) - 1;
+            const uint32_t before = (1u << j) - 1u;
+#pragma unroll
+            for (int c = 0; c < LOW_COUNTERS; ++c) {
+                const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
+                if (lane == c) cur += __popc(bal & before);
+            }
+            L = g + j;
+            mL = __shfl_sync(0xffffffffu, m, j);
+            break;
+        }
+        cur += inc;
+    }
+    if (L != NONE) {
+        uint32_t H = T - (cur - P);  // increments of key L and all later keys
+        if (D.compat_v3) {          // device_sketch_v3.h:187: linking key lands on bit % 8
+            if (lane < LOW_COUNTERS && ((mL >> lane) & 1u)) H -= 1u;
+            if (lane < 8) H += __popc(mL & (0x01010101u << lane));
+        }
+        uint32_t id = 0;
+        if (lane == 0) id = atomicAdd(&ctl->next_id, 1u);
+        id = __shfl_sync(0xffffffffu, id, 0);
+        const bool ok = (uint64_t)(id - START) < D.n_high;
+        if (ok) {
+            __stcg(D.high + (uint64_t)(id - START) * HIGH_WORDS + lane, H);
+        } else if (lane == 0) {
+            atomicOr(&ctl->status, ST_POOL_FULL);
+            atomicAdd(&ctl->dropped, (unsigned long long)(end - L));
+        }
+        uint32_t word = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) word |= __shfl_sync(0xffffffffu, cur, (4 * (lane & 7) + k) & 31) << (8 * k);
+        if (lane < 7) __stcg(wp + lane, word);
+        if (lane == 7) __stcg(wp + 7, ok ? id : SATURATED);
+    } else {
+        if (lane == 7) __stcg(wp + 7, 0u);  // every key added; the words are final
+    }
+    if (lane == 0) {
+        atomicAnd(D.bitmap + (b >> 5), ~(1u << (b & 31)));
+        atomicAdd(&ctl->repaired_buckets, 1ull);
+        atomicAdd(&ctl->repaired_keys, (unsigned long long)(end - beg));
+    }
+}
+
+constexpr uint32_t SMALL_K = 1u << 17;  // at most this many records: block 0 finishes alone
+
+// Stable LSD radix sort of the K records by slot inside one block (tiles in array order,
+// block syncs only); returns the buffer holding the sorted records.
+__device__ __forceinline__ const uint2* block_sort_records(const MswsDev& D, RadixSmem& rs, uint32_t* base,
+                                                          uint32_t K, uint32_t F) {
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    constexpr int NW = REPAIR_THREADS / 32;
+    const int npass = radix_passes(F);
+    const uint32_t ntr = (K + REPAIR_TILE - 1) / REPAIR_TILE;
+    for (int p = 0; p < npass; ++p) {
+        const uint2* src = D.rec[p & 1];
+        uint2* dst = D.rec[(p + 1) & 1];
+        const int shift = 8 * p;
+        if (tid < 256) base[tid] = 0;
+        for (uint32_t t = 0; t < ntr; ++t) {
+            tile_count(rs, src, K, t, shift);
+            for (int d = tid; d < 256; d += REPAIR_THREADS) {
+                uint32_t sum = 0;
+                for (int w = 0; w < NW; ++w) sum += rs.whist[w][d];
+                base[d] += sum;
+            }
+            __syncthreads();
+        }
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan(tid < 256 ? base[tid] : 0u, &total);
+        if (tid < 256) base[tid] = ex;
+        for (uint32_t t = 0; t < ntr; ++t) {
+            tile_count(rs, src, K, t, shift);
+            for (int d = tid; d < 256; d += REPAIR_THREADS) {
+                uint32_t run = base[d];
+                for (int w = 0; w < NW; ++w) {
+                    const uint32_t x = rs.whist[w][d];
+                    rs.whist[w][d] = run;
+                    run += x;
+                }
+                base[d] = run;
+            }
+            __syncthreads();
+            for (int r = 0; r < 256 / 32; ++r) {
+                const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
+                const bool v = i < K;
+                const uint2 rec = v ? __ldcg(&src[i]) : make_uint2(0, 0);
+                const uint32_t d = v ? (rec.x >> shift) & 0xffu : 256u + lane;
+                const uint32_t peers = __match_any_sync(0xffffffffu, d);
+                if (v) __stcg(dst + rs.whist[wid][d] + __popc(peers & lanemask_lt()), rec);
+                __syncwarp();
+                if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
+                __syncwarp();
+            }
+            __syncthreads();
+        }
+    }
+    return D.rec[npass & 1];
+}
+
 __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* __restrict__ keys, uint64_t n,
                                                                 MswsDev D) {
     __shared__ RadixSmem rs;
@@ -484,99 +639,98 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     const uint32_t ntot = min(F, D.long_cap);
     for (uint32_t i = gtid; i < ntot * LOW_COUNTERS; i += nthreads) __stcg(D.totals + i, 0u);
 
-    // Phases 1-3 are the first (digit 0) pass of a stable LSD radix sort by slot whose
-    // input is the key chunk itself: keys of unflagged buckets drop out, the others become
-    // (slot, mask) records, ordered by digit 0 and, within a digit, by array position.
-    // Warp w of a tile owns keys [w*256, w*256+256) in 8 rounds of 32, so (warp, round,
-    // lane) is array order.
-    const int npass = max(1, radix_passes(F));
+    // Phase 1: count keys of flagged buckets per tile of the chunk.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
-        for (int d = tid; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
-        __syncthreads();
-        for (int r = 0; r < 8; ++r) {
-            const uint64_t i = (uint64_t)t * REPAIR_TILE + wid * 256 + r * 32 + lane;
-            uint32_t slot = NONE;
-            if (i < n) slot = flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, __ldg(keys + i) * D.seed));
-            const bool v = slot != NONE;
-            const uint32_t d = v ? (slot & 0xffu) : 256u + lane;
-            const uint32_t peers = __match_any_sync(0xffffffffu, d);
-            if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
-            __syncwarp();
+        const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
+        uint32_t c = 0;
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const uint64_t i = base + j;
+            if (i < n) {
+                const uint32_t hv = __ldg(keys + i) * D.seed;
+                c += flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, hv)) != NONE ? 1u : 0u;
+            }
         }
-        __syncthreads();
-        for (int d = tid; d < 256; d += REPAIR_THREADS) {
-            uint32_t sum = 0;
-            for (int w = 0; w < NW; ++w) sum += rs.whist[w][d];
-            __stcg(D.hist + (uint64_t)d * ntk + t, sum);
-        }
-        __syncthreads();
+        uint32_t total;
+        block_exclusive_scan(c, &total);
+        if (tid == 0) __stcg(D.tile_counts + t, total);
     }
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 0);
+    // Phase 2: exclusive scan of the tile counts.
     if (blockIdx.x == 0) {
-        const uint32_t K = block_scan_array(D.hist, 256u * ntk);
+        const uint32_t K = block_scan_array(D.tile_counts, ntk);
         if (tid == 0) __stcg(&ctl->n_records, K);
     }
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 1);
     const uint32_t K = __ldcg(&ctl->n_records);
+    // Phase 3: stable write of (slot, mask) records in array order.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
-        for (int d = tid; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
-        __syncthreads();
-        uint32_t slots[8];
+        const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
+        uint32_t slots[PER];
+        uint32_t c = 0;
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const uint64_t i = (uint64_t)t * REPAIR_TILE + wid * 256 + r * 32 + lane;
-            slots[r] = NONE;
-            if (i < n) slots[r] = flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, __ldg(keys + i) * D.seed));
-            const bool v = slots[r] != NONE;
-            const uint32_t d = v ? (slots[r] & 0xffu) : 256u + lane;
-            const uint32_t peers = __match_any_sync(0xffffffffu, d);
-            if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
-            __syncwarp();
-        }
-        __syncthreads();
-        for (int d = tid; d < 256; d += REPAIR_THREADS) {
-            uint32_t run = __ldcg(D.hist + (uint64_t)d * ntk + t);
-            for (int w = 0; w < NW; ++w) {
-                const uint32_t x = rs.whist[w][d];
-                rs.whist[w][d] = run;
-                run += x;
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const uint64_t i = (uint64_t)t * REPAIR_TILE + wid * 256 + r * 32 + lane;
-            const bool v = slots[r] != NONE;
-            const uint32_t d = v ? (slots[r] & 0xffu) : 256u + lane;
-            const uint32_t peers = __match_any_sync(0xffffffffu, d);
-            if (v) {
+        for (int j = 0; j < PER; ++j) {
+            const uint64_t i = base + j;
+            slots[j] = NONE;
+            if (i < n) {
                 const uint32_t hv = __ldg(keys + i) * D.seed;
-                const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hv));
-                __stcg(D.rec[0] + rs.whist[wid][d] + __popc(peers & lanemask_lt()), make_uint2(slots[r], mask));
+                slots[j] = flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, hv));
+                c += slots[j] != NONE ? 1u : 0u;
             }
-            __syncwarp();
-            if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
-            __syncwarp();
         }
-        __syncthreads();
+        uint32_t total;
+        uint32_t pos = block_exclusive_scan(c, &total) + __ldcg(D.tile_counts + t);
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            if (slots[j] != NONE) {
+                const uint32_t hv = __ldg(keys + base + j) * D.seed;
+                const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hv));
+                __stcg(D.rec[0] + pos, make_uint2(slots[j], mask));
+                ++pos;
+            }
+        }
     }
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 2);
 
-    // Phase 4: the remaining radix passes over the records, 8 bits each.
+    // Few records (every chunk after the first on skewed streams): block 0 sorts and replays
+    // alone, with block syncs instead of grid barriers.
+    if (K <= SMALL_K) {
+        if (blockIdx.x != 0) return;
+        const uint2* srt = block_sort_records(D, rs, s_set, K, F);
+        for (uint32_t i = tid; i < K; i += REPAIR_THREADS) {
+            const uint32_t sl = __ldcg(&srt[i].x);
+            if (i == 0 || __ldcg(&srt[i - 1].x) != sl) __stcg(D.seg_beg + sl, i);
+        }
+        __syncthreads();
+        phase_mark(ctl, 3);
+        for (uint32_t sl = wid; sl < F; sl += NW) replay_slot(D, srt, sl, F, K, false);
+        __syncthreads();
+        phase_mark(ctl, 5);
+        if (tid == 0) {
+            ctl->n_flagged = 0;
+            ctl->n_records = 0;
+            ctl->repairs += 1;
+            __threadfence();
+        }
+        return;
+    }
+
+    // Phase 4: stable LSD radix sort of the records by slot, 8 bits per pass.
+    const int npass = radix_passes(F);
     const uint32_t ntr = (K + REPAIR_TILE - 1) / REPAIR_TILE;
-    for (int p = 1; p < npass; ++p) {
-        const uint2* src = D.rec[(p - 1) & 1];
-        uint2* dst = D.rec[p & 1];
+    for (int p = 0; p < npass; ++p) {
+        const uint2* src = D.rec[p & 1];
+        uint2* dst = D.rec[(p + 1) & 1];
         const int shift = 8 * p;
         for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {  // per-tile digit counts
             tile_count(rs, src, K, t, shift);
             for (int d = tid; d < 256; d += REPAIR_THREADS) {
-                uint32_t sum = 0;
-                for (int w = 0; w < NW; ++w) sum += rs.whist[w][d];
-                __stcg(D.hist + (uint64_t)d * ntr + t, sum);
+                uint32_t s = 0;
+                for (int w = 0; w < NW; ++w) s += rs.whist[w][d];
+                __stcg(D.hist + (uint64_t)d * ntr + t, s);
             }
             __syncthreads();
         }
@@ -613,7 +767,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         if (!grid_barrier(ctl)) return;
     }
     phase_mark(ctl, 3);
-    const uint2* sorted = D.rec[(npass - 1) & 1];
+    const uint2* sorted = D.rec[npass & 1];
 
     // Phase 5: segment starts, and per-counter totals of slots < long_cap; each block a
     // contiguous record range whose first and last slot accumulate in shared memory.
@@ -662,95 +816,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     phase_mark(ctl, 4);
 
     // Phase 6: replay each flagged bucket in array order, one warp per slot.
-    const uint32_t lt = lanemask_lt();
-    for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) {
-        const uint32_t b = __ldcg(D.flag_list + s);
-        const uint32_t beg = __ldcg(D.seg_beg + s);
-        const uint32_t end = (s + 1 < F) ? __ldcg(D.seg_beg + s + 1) : K;
-        uint32_t T = 0;  // lane i < 28: occurrences of counter i in the chunk
-        if (s < D.long_cap) {
-            T = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane) : 0u;
-        } else {
-            for (uint32_t g = beg; g < end; g += 32) {
-                const uint32_t m = (g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u;
-#pragma unroll
-                for (int c = 0; c < LOW_COUNTERS; ++c) {
-                    const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
-                    if (lane == c) T += __popc(bal);
-                }
-            }
-        }
-        uint32_t* wp = D.low + (uint64_t)b * LOW_WORDS;
-        const uint32_t fw = lane < 7 ? __ldcg(wp + lane) : 0u;
-        // pre-chunk word = final word - packed sum of the chunk's increments (mod 2^32)
-        uint32_t sw = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const uint32_t t = __shfl_sync(0xffffffffu, T, (4 * (lane & 7) + k) & 31);
-            sw += t << (8 * k);
-        }
-        const uint32_t pw = fw - sw;
-        const uint32_t pwi = __shfl_sync(0xffffffffu, pw, (lane >> 2) & 7);
-        const uint32_t P = lane < LOW_COUNTERS ? (pwi >> (8 * (lane & 3))) & 0xffu : 0u;
-        uint32_t cur = P;
-        // first key (array order) that sees a selected counter > LIMIT
-        uint32_t L = NONE, mL = 0;
-        for (uint32_t g = beg; g < end; g += 32) {
-            const uint32_t m = (g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u;
-            bool trig = false;
-            uint32_t inc = 0;
-#pragma unroll
-            for (int c = 0; c < LOW_COUNTERS; ++c) {
-                const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
-                const uint32_t cc = __shfl_sync(0xffffffffu, cur, c);
-                if (((m >> c) & 1u) && cc + __popc(bal & lt) > LIMIT) trig = true;
-                if (lane == c) inc = __popc(bal);
-            }
-            const uint32_t tb = __ballot_sync(0xffffffffu, trig);
-            if (tb) {
-                const int j = __ffs(tb) - 1;
-                const uint32_t before = (1u << j) - 1u;
-#pragma unroll
-                for (int c = 0; c < LOW_COUNTERS; ++c) {
-                    const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
-                    if (lane == c) cur += __popc(bal & before);
-                }
-                L = g + j;
-                mL = __shfl_sync(0xffffffffu, m, j);
-                break;
-            }
-            cur += inc;
-        }
-        if (L != NONE) {
-            uint32_t H = T - (cur - P);  // increments of key L and all later keys
-            if (D.compat_v3) {          // device_sketch_v3.h:187: linking key lands on bit % 8
-                if (lane < LOW_COUNTERS && ((mL >> lane) & 1u)) H -= 1u;
-                if (lane < 8) H += __popc(mL & (0x01010101u << lane));
-            }
-            uint32_t id = 0;
-            if (lane == 0) id = atomicAdd(&ctl->next_id, 1u);
-            id = __shfl_sync(0xffffffffu, id, 0);
-            const bool ok = (uint64_t)(id - START) < D.n_high;
-            if (ok) {
-                __stcg(D.high + (uint64_t)(id - START) * HIGH_WORDS + lane, H);
-            } else if (lane == 0) {
-                atomicOr(&ctl->status, ST_POOL_FULL);
-                atomicAdd(&ctl->dropped, (unsigned long long)(end - L));
-            }
-            uint32_t word = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) word |= __shfl_sync(0xffffffffu, cur, (4 * (lane & 7) + k) & 31) << (8 * k);
-            if (lane < 7) __stcg(wp + lane, word);
-            if (lane == 7) __stcg(wp + 7, ok ? id : SATURATED);
-        } else {
-            if (lane == 7) __stcg(wp + 7, 0u);  // every key added; the words are final
-        }
-        if (lane == 0) {
-            atomicAnd(D.bitmap + (b >> 5), ~(1u << (b & 31)));
-            atomicAdd(&ctl->repaired_buckets, 1ull);
-            atomicAdd(&ctl->repaired_keys, (unsigned long long)(end - beg));
-        }
-    }
+    for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) replay_slot(D, sorted, s, F, K, true);
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 5);
     if (blockIdx.x == 0 && tid == 0) {

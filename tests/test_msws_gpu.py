@@ -69,9 +69,9 @@ def test_uniform_config1_full_size(gpu):
     assert sk.stats()["linked_buckets"] == 0
 
 
-@pytest.mark.parametrize("agg", [1, 2, 3])
-def test_zipf_heavy_links(gpu, agg):
-    sk, orc = make_pair(16381, 1 << 15, aggregate=agg)
+@pytest.mark.parametrize("agg,route", [(1, 0), (2, 0), (3, 0), (3, 1), (3, 2)])
+def test_zipf_heavy_links(gpu, agg, route):
+    sk, orc = make_pair(16381, 1 << 15, aggregate=agg, route=route)
     keys = data.zipf_keys(1 << 22, 1 << 18, 1.1, seed=5, perm_seed=77)
     q = data.rank_keys(77, 0, 1 << 18)
     run_and_compare(sk, orc, keys, q)
@@ -97,13 +97,13 @@ def test_few_links_fused_routing(gpu):
     # buckets, tiles run in the fused routing mode, where a linked key takes its low
     # increments back and counts in the high bucket
     sk, orc = make_pair(65521, 1 << 10, max_batch=1 << 18)
-    uni = data.uniform_keys(1 << 21, seed=31)
-    heavy = torch.tensor([7, 11, 13, 1 << 31], dtype=torch.int64).to(torch.uint32).cuda()
-    idx = torch.arange(1 << 21, device="cuda") % 97 == 0
-    keys = uni.clone()
-    keys[idx] = heavy[(torch.arange(int(idx.sum()), device="cuda") % 4)]
-    q = torch.cat([heavy, uni[:4096]])
-    run_and_compare(sk, orc, keys, q)
+    uni = data.uniform_keys(1 << 21, seed=31).cpu().numpy()
+    heavy = np.array([7, 11, 13, 1 << 31], np.uint32)
+    keys = uni.copy()
+    pos = np.arange(0, keys.size, 97)
+    keys[pos] = heavy[np.arange(pos.size) % 4]
+    q = np.concatenate([heavy, uni[:4096]])
+    run_and_compare(sk, orc, torch.from_numpy(keys).cuda(), torch.from_numpy(q).cuda())
     assert sk.stats()["linked_buckets"] >= 4
 
 
@@ -175,9 +175,9 @@ def test_host_buffers_match_device_path(gpu):
     assert np.array_equal(out.numpy(), got)
 
 
-@pytest.mark.parametrize("agg", [2, 3])
-def test_uniform_aggregation_modes(gpu, agg):
-    sk, orc = make_pair(65521, 1 << 12, aggregate=agg, mask_rng=5)
+@pytest.mark.parametrize("agg,route", [(2, 0), (3, 1), (3, 2), (1, 2)])
+def test_uniform_aggregation_and_routing_modes(gpu, agg, route):
+    sk, orc = make_pair(65521, 1 << 12, aggregate=agg, route=route, mask_rng=5)
     keys = data.uniform_keys((1 << 21) + 5, seed=12)
     run_and_compare(sk, orc, keys[3:], keys[3:])
 
