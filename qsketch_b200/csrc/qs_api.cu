@@ -368,7 +368,7 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         D.n_masks = H;
         D.compat_v3 = (p.flags & QS_FLAG_COMPAT_V3) ? 1u : 0u;
         if (p.route > 2) return bail(fail(QS_ERR_INVALID_ARG, "route out of [0, 2]"));
-        D.route = p.route;
+        D.route = p.route == 0 ? 1u : p.route;  // default: load the index word first
         const uint64_t B = sk->max_batch;
         const uint64_t cap = std::min<uint64_t>(n_low, B);
         D.flag_cap = (uint32_t)cap;

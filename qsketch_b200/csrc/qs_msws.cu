@@ -445,75 +445,74 @@ __device__ __forceinline__ void tile_count(RadixSmem& rs, const uint2* src, uint
     __syncthreads();
 }
 
-// Replay flagged bucket `s` (one warp): its records sorted[seg_beg[s] .. next segment) are
-// the chunk's keys of that bucket in array order.  Restores the pre-chunk counters, finds
-// the first key that sees a selected counter above LIMIT (the sequential low->high switch
-// of device_sketch_v3.h:160-190), links the bucket there and writes the final words.
-__device__ __forceinline__ void replay_slot(const MswsDev& D, const uint2* sorted, uint32_t s, uint32_t F, uint32_t K,
-                                            bool use_totals) {
-    Ctl* ctl = D.ctl;
+// ---- per-bucket replay (one warp per flagged bucket; lane i keeps counter i) ------------
+// The chunk's keys of a flagged bucket, in array order, are replayed with the sequential
+// semantics of device_sketch_v3.h:88-191: the pre-chunk counters are restored (final word
+// minus the packed sum of the chunk's increments, mod 2^32), the first key that sees a
+// selected counter above LIMIT is found (the low->high switch of :160-190), the bucket is
+// linked there (atomic_malloc, :69-85) and that key and all later ones count high.
+
+// Lane c accumulates the occurrences of counter c among the 32 masks of the warp.
+__device__ __forceinline__ void count_counters(uint32_t m, uint32_t& T) {
     const int lane = threadIdx.x & 31;
-    const uint32_t lt = lanemask_lt();
-    const uint32_t b = __ldcg(D.flag_list + s);
-    const uint32_t beg = __ldcg(D.seg_beg + s);
-    const uint32_t end = (s + 1 < F) ? __ldcg(D.seg_beg + s + 1) : K;
-    uint32_t T = 0;  // lane i < 28: occurrences of counter i in the chunk
-    if (use_totals && s < D.long_cap) {
-        T = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane) : 0u;
-    } else {
-        for (uint32_t g = beg; g < end; g += 32) {
-            const uint32_t m = (g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u;
 #pragma unroll
-            for (int c = 0; c < LOW_COUNTERS; ++c) {
-                const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
-                if (lane == c) T += __popc(bal);
-            }
-        }
+    for (int c = 0; c < LOW_COUNTERS; ++c) {
+        const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
+        if (lane == c) T += __popc(bal);
     }
-    uint32_t* wp = D.low + (uint64_t)b * LOW_WORDS;
+}
+
+// Pre-chunk counter of lane i from the bucket's final words and the chunk totals T.
+__device__ __forceinline__ uint32_t pre_counters(const uint32_t* wp, uint32_t T) {
+    const int lane = threadIdx.x & 31;
     const uint32_t fw = lane < 7 ? __ldcg(wp + lane) : 0u;
-    // pre-chunk word = final word - packed sum of the chunk's increments (mod 2^32)
     uint32_t sw = 0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint32_t t = __shfl_sync(0xffffffffu, T, (4 * (lane & 7) + k) & 31);
-        sw += t << (8 * k);
+    for (int k = 0; k < 4; ++k) sw += __shfl_sync(0xffffffffu, T, (4 * (lane & 7) + k) & 31) << (8 * k);
+    const uint32_t pwi = __shfl_sync(0xffffffffu, fw - sw, (lane >> 2) & 7);
+    return lane < LOW_COUNTERS ? (pwi >> (8 * (lane & 3))) & 0xffu : 0u;
+}
+
+// 32 consecutive records (mask m, 0 for lanes that are not this bucket's): returns the lane
+// of the first record that sees a selected counter above LIMIT, or -1; `cur` advances over
+// the records before it (all 32 when none triggers).
+__device__ __forceinline__ int link_step(uint32_t m, uint32_t& cur) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = lanemask_lt();
+    bool trig = false;
+    uint32_t inc = 0;
+#pragma unroll
+    for (int c = 0; c < LOW_COUNTERS; ++c) {
+        const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
+        const uint32_t cc = __shfl_sync(0xffffffffu, cur, c);
+        if (((m >> c) & 1u) && cc + __popc(bal & lt) > LIMIT) trig = true;
+        if (lane == c) inc = __popc(bal);
     }
-    const uint32_t pw = fw - sw;
-    const uint32_t pwi = __shfl_sync(0xffffffffu, pw, (lane >> 2) & 7);
-    const uint32_t P = lane < LOW_COUNTERS ? (pwi >> (8 * (lane & 3))) & 0xffu : 0u;
-    uint32_t cur = P;
-    // first key (array order) that sees a selected counter > LIMIT
-    uint32_t L = NONE, mL = 0;
-    for (uint32_t g = beg; g < end; g += 32) {
-        const uint32_t m = (g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u;
-        bool trig = false;
-        uint32_t inc = 0;
-#pragma unroll
-        for (int c = 0; c < LOW_COUNTERS; ++c) {
-            const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
-            const uint32_t cc = __shfl_sync(0xffffffffu, cur, c);
-            if (((m >> c) & 1u) && cc + __popc(bal & lt) > LIMIT) trig = true;
-            if (lane == c) inc = __popc(bal);
-        }
-        const uint32_t tb = __ballot_sync(0xffffffffu, trig);
-        if (tb) {
-            const int j = __ffs(tb) - 1;
-            const uint32_t before = (1u << j) - 1u;
-#pragma unroll
-            for (int c = 0; c < LOW_COUNTERS; ++c) {
-                const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
-                if (lane == c) cur += __popc(bal & before);
-            }
-            L = g + j;
-            mL = __shfl_sync(0xffffffffu, m, j);
-            break;
-        }
+    const uint32_t tb = __ballot_sync(0xffffffffu, trig);
+    if (!tb) {
         cur += inc;
+        return -1;
     }
-    if (L != NONE) {
-        uint32_t H = T - (cur - P);  // increments of key L and all later keys
-        if (D.compat_v3) {          // device_sketch_v3.h:187: linking key lands on bit % 8
+    const int j = __ffs(tb) - 1;
+    const uint32_t before = (1u << j) - 1u;
+#pragma unroll
+    for (int c = 0; c < LOW_COUNTERS; ++c) {
+        const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
+        if (lane == c) cur += __popc(bal & before);
+    }
+    return j;
+}
+
+// Final words of bucket b.  found: a key switched it to the high level; n_after: keys at
+// or after that key; n_total: the bucket's keys in the chunk; mL: the switching key's mask.
+__device__ __forceinline__ void finish_bucket(const MswsDev& D, uint32_t b, bool found, uint32_t n_after,
+                                              uint32_t n_total, uint32_t T, uint32_t P, uint32_t cur, uint32_t mL) {
+    Ctl* ctl = D.ctl;
+    const int lane = threadIdx.x & 31;
+    uint32_t* wp = D.low + (uint64_t)b * LOW_WORDS;
+    if (found) {
+        uint32_t H = T - (cur - P);  // increments of the switching key and all later keys
+        if (D.compat_v3) {          // device_sketch_v3.h:187: the switching key lands on bit % 8
             if (lane < LOW_COUNTERS && ((mL >> lane) & 1u)) H -= 1u;
             if (lane < 8) H += __popc(mL & (0x01010101u << lane));
         }
@@ -525,77 +524,108 @@ __device__ __forceinline__ void replay_slot(const MswsDev& D, const uint2* sorte
             __stcg(D.high + (uint64_t)(id - START) * HIGH_WORDS + lane, H);
         } else if (lane == 0) {
             atomicOr(&ctl->status, ST_POOL_FULL);
-            atomicAdd(&ctl->dropped, (unsigned long long)(end - L));
+            atomicAdd(&ctl->dropped, (unsigned long long)n_after);
         }
         uint32_t word = 0;
 #pragma unroll
         for (int k = 0; k < 4; ++k) word |= __shfl_sync(0xffffffffu, cur, (4 * (lane & 7) + k) & 31) << (8 * k);
         if (lane < 7) __stcg(wp + lane, word);
         if (lane == 7) __stcg(wp + 7, ok ? id : SATURATED);
-    } else {
-        if (lane == 7) __stcg(wp + 7, 0u);  // every key added; the words are final
+    } else if (lane == 7) {
+        __stcg(wp + 7, 0u);  // every key added to the low level; the words are final
     }
     if (lane == 0) {
         atomicAnd(D.bitmap + (b >> 5), ~(1u << (b & 31)));
         atomicAdd(&ctl->repaired_buckets, 1ull);
-        atomicAdd(&ctl->repaired_keys, (unsigned long long)(end - beg));
+        atomicAdd(&ctl->repaired_keys, (unsigned long long)n_total);
     }
 }
 
-constexpr uint32_t SMALL_K = 1u << 17;  // at most this many records: block 0 finishes alone
-
-// Stable LSD radix sort of the K records by slot inside one block (tiles in array order,
-// block syncs only); returns the buffer holding the sorted records.
-__device__ __forceinline__ const uint2* block_sort_records(const MswsDev& D, RadixSmem& rs, uint32_t* base,
-                                                          uint32_t K, uint32_t F) {
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    constexpr int NW = REPAIR_THREADS / 32;
-    const int npass = radix_passes(F);
-    const uint32_t ntr = (K + REPAIR_TILE - 1) / REPAIR_TILE;
-    for (int p = 0; p < npass; ++p) {
-        const uint2* src = D.rec[p & 1];
-        uint2* dst = D.rec[(p + 1) & 1];
-        const int shift = 8 * p;
-        if (tid < 256) base[tid] = 0;
-        for (uint32_t t = 0; t < ntr; ++t) {
-            tile_count(rs, src, K, t, shift);
-            for (int d = tid; d < 256; d += REPAIR_THREADS) {
-                uint32_t sum = 0;
-                for (int w = 0; w < NW; ++w) sum += rs.whist[w][d];
-                base[d] += sum;
-            }
-            __syncthreads();
-        }
-        uint32_t total;
-        const uint32_t ex = block_exclusive_scan(tid < 256 ? base[tid] : 0u, &total);
-        if (tid < 256) base[tid] = ex;
-        for (uint32_t t = 0; t < ntr; ++t) {
-            tile_count(rs, src, K, t, shift);
-            for (int d = tid; d < 256; d += REPAIR_THREADS) {
-                uint32_t run = base[d];
-                for (int w = 0; w < NW; ++w) {
-                    const uint32_t x = rs.whist[w][d];
-                    rs.whist[w][d] = run;
-                    run += x;
-                }
-                base[d] = run;
-            }
-            __syncthreads();
-            for (int r = 0; r < 256 / 32; ++r) {
-                const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
-                const bool v = i < K;
-                const uint2 rec = v ? __ldcg(&src[i]) : make_uint2(0, 0);
-                const uint32_t d = v ? (rec.x >> shift) & 0xffu : 256u + lane;
-                const uint32_t peers = __match_any_sync(0xffffffffu, d);
-                if (v) __stcg(dst + rs.whist[wid][d] + __popc(peers & lanemask_lt()), rec);
-                __syncwarp();
-                if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
-                __syncwarp();
-            }
-            __syncthreads();
+// Replay slot s from its segment of the slot-sorted records.
+__device__ __forceinline__ void replay_slot(const MswsDev& D, const uint2* sorted, uint32_t s, uint32_t F, uint32_t K,
+                                            bool use_totals) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t b = __ldcg(D.flag_list + s);
+    const uint32_t beg = __ldcg(D.seg_beg + s);
+    const uint32_t end = (s + 1 < F) ? __ldcg(D.seg_beg + s + 1) : K;
+    uint32_t T = 0;
+    if (use_totals && s < D.long_cap) {
+        T = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane) : 0u;
+    } else {
+        for (uint32_t g = beg; g < end; g += 32) count_counters((g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u, T);
+    }
+    const uint32_t P = pre_counters(D.low + (uint64_t)b * LOW_WORDS, T);
+    uint32_t cur = P, mL = 0, L = NONE;
+    for (uint32_t g = beg; g < end; g += 32) {
+        const uint32_t m = (g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u;
+        const int j = link_step(m, cur);
+        if (j >= 0) {
+            L = g + j;
+            mL = __shfl_sync(0xffffffffu, m, j);
+            break;
         }
     }
-    return D.rec[npass & 1];
+    finish_bucket(D, b, L != NONE, L != NONE ? end - L : 0u, end - beg, T, P, cur, mL);
+}
+
+// Without a sort: the block's 16 warps take 16 flagged buckets and stream the array-ordered
+// records through shared memory tile by tile, each warp keeping its own bucket's records.
+// Two passes: counter totals, then the switching key.
+constexpr uint32_t SCAN_K_MAX = 1u << 16;
+
+__device__ __forceinline__ void replay_scan(const MswsDev& D, uint2* tile, uint32_t F, uint32_t K) {
+    constexpr int NW = REPAIR_THREADS / 32;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const uint2* recs = D.rec[0];
+    for (uint32_t g0 = blockIdx.x * NW; g0 < F; g0 += gridDim.x * NW) {
+        const uint32_t s = g0 + wid;
+        const bool has = s < F;
+        uint32_t T = 0, nrec = 0;
+        for (uint32_t t0 = 0; t0 < K; t0 += REPAIR_TILE) {
+            const uint32_t cnt = min((uint32_t)REPAIR_TILE, K - t0);
+            __syncthreads();
+            for (uint32_t i = tid; i < cnt; i += REPAIR_THREADS) tile[i] = __ldcg(recs + t0 + i);
+            __syncthreads();
+            if (has) {
+                for (uint32_t r = 0; r < cnt; r += 32) {
+                    const uint2 rec = r + lane < cnt ? tile[r + lane] : make_uint2(NONE, 0u);
+                    const bool mt = rec.x == s;
+                    const uint32_t bal = __ballot_sync(0xffffffffu, mt);
+                    if (!bal) continue;
+                    count_counters(mt ? rec.y : 0u, T);
+                    nrec += __popc(bal);
+                }
+            }
+        }
+        const uint32_t b = has ? __ldcg(D.flag_list + s) : 0u;
+        const uint32_t P = has ? pre_counters(D.low + (uint64_t)b * LOW_WORDS, T) : 0u;
+        uint32_t cur = P, mL = 0, nbefore = 0;
+        bool found = false;
+        for (uint32_t t0 = 0; t0 < K; t0 += REPAIR_TILE) {
+            if (__syncthreads_and(!has || found)) break;
+            const uint32_t cnt = min((uint32_t)REPAIR_TILE, K - t0);
+            for (uint32_t i = tid; i < cnt; i += REPAIR_THREADS) tile[i] = __ldcg(recs + t0 + i);
+            __syncthreads();
+            if (has && !found) {
+                for (uint32_t r = 0; r < cnt; r += 32) {
+                    const uint2 rec = r + lane < cnt ? tile[r + lane] : make_uint2(NONE, 0u);
+                    const bool mt = rec.x == s;
+                    const uint32_t bal = __ballot_sync(0xffffffffu, mt);
+                    if (!bal) continue;
+                    const uint32_t m = mt ? rec.y : 0u;
+                    const int j = link_step(m, cur);
+                    if (j >= 0) {
+                        found = true;
+                        nbefore += __popc(bal & ((1u << j) - 1u));
+                        mL = __shfl_sync(0xffffffffu, m, j);
+                        break;
+                    }
+                    nbefore += __popc(bal);
+                }
+            }
+        }
+        if (has) finish_bucket(D, b, found, nrec - nbefore, nrec, T, P, cur, mL);
+    }
 }
 
 __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* __restrict__ keys, uint64_t n,
@@ -695,21 +725,14 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 2);
 
-    // Few records (every chunk after the first on skewed streams): block 0 sorts and replays
-    // alone, with block syncs instead of grid barriers.
-    if (K <= SMALL_K) {
-        if (blockIdx.x != 0) return;
-        const uint2* srt = block_sort_records(D, rs, s_set, K, F);
-        for (uint32_t i = tid; i < K; i += REPAIR_THREADS) {
-            const uint32_t sl = __ldcg(&srt[i].x);
-            if (i == 0 || __ldcg(&srt[i - 1].x) != sl) __stcg(D.seg_beg + sl, i);
-        }
-        __syncthreads();
-        phase_mark(ctl, 3);
-        for (uint32_t sl = wid; sl < F; sl += NW) replay_slot(D, srt, sl, F, K, false);
-        __syncthreads();
+    // Few records x few buckets (every chunk after the first on skewed streams): no sort.
+    // Each flagged bucket's warp streams the whole array-ordered record list, which stays
+    // in L2, and keeps its own records.
+    if (K <= SCAN_K_MAX && F <= 2u * gridDim.x * NW) {
+        replay_scan(D, reinterpret_cast<uint2*>(s_set), F, K);
+        if (!grid_barrier(ctl)) return;
         phase_mark(ctl, 5);
-        if (tid == 0) {
+        if (blockIdx.x == 0 && tid == 0) {
             ctl->n_flagged = 0;
             ctl->n_records = 0;
             ctl->repairs += 1;
