@@ -568,66 +568,6 @@ __device__ __forceinline__ void replay_slot(const MswsDev& D, const uint2* sorte
     finish_bucket(D, b, L != NONE, L != NONE ? end - L : 0u, end - beg, T, P, cur, mL);
 }
 
-// Without a sort: the block's 16 warps take 16 flagged buckets and stream the array-ordered
-// records through shared memory tile by tile, each warp keeping its own bucket's records.
-// Two passes: counter totals, then the switching key.
-constexpr uint32_t SCAN_K_MAX = 1u << 16;
-
-__device__ __forceinline__ void replay_scan(const MswsDev& D, uint2* tile, uint32_t F, uint32_t K) {
-    constexpr int NW = REPAIR_THREADS / 32;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const uint2* recs = D.rec[0];
-    for (uint32_t g0 = blockIdx.x * NW; g0 < F; g0 += gridDim.x * NW) {
-        const uint32_t s = g0 + wid;
-        const bool has = s < F;
-        uint32_t T = 0, nrec = 0;
-        for (uint32_t t0 = 0; t0 < K; t0 += REPAIR_TILE) {
-            const uint32_t cnt = min((uint32_t)REPAIR_TILE, K - t0);
-            __syncthreads();
-            for (uint32_t i = tid; i < cnt; i += REPAIR_THREADS) tile[i] = __ldcg(recs + t0 + i);
-            __syncthreads();
-            if (has) {
-                for (uint32_t r = 0; r < cnt; r += 32) {
-                    const uint2 rec = r + lane < cnt ? tile[r + lane] : make_uint2(NONE, 0u);
-                    const bool mt = rec.x == s;
-                    const uint32_t bal = __ballot_sync(0xffffffffu, mt);
-                    if (!bal) continue;
-                    count_counters(mt ? rec.y : 0u, T);
-                    nrec += __popc(bal);
-                }
-            }
-        }
-        const uint32_t b = has ? __ldcg(D.flag_list + s) : 0u;
-        const uint32_t P = has ? pre_counters(D.low + (uint64_t)b * LOW_WORDS, T) : 0u;
-        uint32_t cur = P, mL = 0, nbefore = 0;
-        bool found = false;
-        for (uint32_t t0 = 0; t0 < K; t0 += REPAIR_TILE) {
-            if (__syncthreads_and(!has || found)) break;
-            const uint32_t cnt = min((uint32_t)REPAIR_TILE, K - t0);
-            for (uint32_t i = tid; i < cnt; i += REPAIR_THREADS) tile[i] = __ldcg(recs + t0 + i);
-            __syncthreads();
-            if (has && !found) {
-                for (uint32_t r = 0; r < cnt; r += 32) {
-                    const uint2 rec = r + lane < cnt ? tile[r + lane] : make_uint2(NONE, 0u);
-                    const bool mt = rec.x == s;
-                    const uint32_t bal = __ballot_sync(0xffffffffu, mt);
-                    if (!bal) continue;
-                    const uint32_t m = mt ? rec.y : 0u;
-                    const int j = link_step(m, cur);
-                    if (j >= 0) {
-                        found = true;
-                        nbefore += __popc(bal & ((1u << j) - 1u));
-                        mL = __shfl_sync(0xffffffffu, m, j);
-                        break;
-                    }
-                    nbefore += __popc(bal);
-                }
-            }
-        }
-        if (has) finish_bucket(D, b, found, nrec - nbefore, nrec, T, P, cur, mL);
-    }
-}
-
 __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* __restrict__ keys, uint64_t n,
                                                                 MswsDev D) {
     __shared__ RadixSmem rs;
@@ -724,22 +664,6 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     }
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 2);
-
-    // Few records x few buckets (every chunk after the first on skewed streams): no sort.
-    // Each flagged bucket's warp streams the whole array-ordered record list, which stays
-    // in L2, and keeps its own records.
-    if (K <= SCAN_K_MAX && F <= 2u * gridDim.x * NW) {
-        replay_scan(D, reinterpret_cast<uint2*>(s_set), F, K);
-        if (!grid_barrier(ctl)) return;
-        phase_mark(ctl, 5);
-        if (blockIdx.x == 0 && tid == 0) {
-            ctl->n_flagged = 0;
-            ctl->n_records = 0;
-            ctl->repairs += 1;
-            __threadfence();
-        }
-        return;
-    }
 
     // Phase 4: stable LSD radix sort of the records by slot, 8 bits per pass.
     const int npass = radix_passes(F);
