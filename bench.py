@@ -34,6 +34,9 @@ CONFIGS = {
                  n_ranks=1 << 24, s=1.1, n_low=2097143, n_high=1 << 17, n_query=1 << 24),
     "uniform": dict(workload="uniform_2^24keys_nlow262139_high8MB_query2^24", kind=0, n_keys=1 << 24, n_ranks=0,
                     s=0.0, n_low=262139, n_high=1 << 16, n_query=1 << 24),
+    # a smaller skewed case for Nsight Compute captures (key stream still larger than L2)
+    "zipf_prof": dict(workload="zipf1.1_2^25keys_2^22ranks_low16MB_high4MB_query2^22", kind=1, n_keys=1 << 25,
+                      n_ranks=1 << 22, s=1.1, n_low=524287, n_high=1 << 15, n_query=1 << 22),
 }
 INSERT_BYTES_PER_KEY = 68  # 4 B key + 32 B bucket sector read + 32 B write-back
 QUERY_BYTES_PER_KEY = 40   # 4 B key + 32 B bucket sector + 4 B result
