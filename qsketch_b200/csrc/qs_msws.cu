@@ -836,11 +836,13 @@ cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
     cudaError_t e = cudaGetDeviceProperties(&prop, device);
     if (e != cudaSuccess) return e;
     L->num_sms = prop.multiProcessorCount;
+    // The dynamic shared-memory cap is a per-kernel attribute shared by every sketch of the
+    // process: set it for the largest mask table (16384 words); the launch passes the actual size.
     const size_t ins_smem = msws_insert_smem(n_masks);
     const void* fns[3] = {(const void*)k_msws_insert<AGG_NONE>, (const void*)k_msws_insert<AGG_WARP>,
                           (const void*)k_msws_insert<AGG_BLOCK>};
     for (const void* fn : fns) {
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ins_smem);
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msws_insert_smem(16384));
         if (e != cudaSuccess) return e;
     }
     int occ = 0;

@@ -107,6 +107,25 @@ def test_few_links_fused_routing(gpu):
     assert sk.stats()["linked_buckets"] >= 4
 
 
+def test_sketches_with_different_mask_tables_coexist(gpu):
+    # a small-table sketch created after a large-table one must not break the first
+    big = qs.generate_hashmask(16384, 32, 3, 4, 2)
+    a = qs.Sketch_GPU_Sub_Warp_Level(4093, 8, 1024, 32, 1, 16384, hash_seed=12345, mask_table=big)
+    b, orc_b = make_pair(4093, 1024)
+    keys = data.zipf_keys(1 << 19, 1 << 12, 1.1, seed=3, perm_seed=5)
+    a.insert(keys)
+    b.insert(keys)
+    a.sync()
+    b.sync()
+    orc_a = oracle.Msws(4093, 1024, 12345, big)
+    hk = keys.cpu().numpy()
+    orc_a.insert(hk)
+    orc_b.insert(hk)
+    q = data.rank_keys(5, 0, 1 << 12)
+    assert np.array_equal(a.search(q).cpu().numpy(), orc_a.query(q.cpu().numpy()))
+    assert np.array_equal(b.search(q).cpu().numpy(), orc_b.query(q.cpu().numpy()))
+
+
 def test_single_heavy_key(gpu):
     sk, orc = make_pair(1021, 64)
     keys = torch.full((1 << 20,), 123456789, dtype=torch.uint32, device="cuda")
