@@ -845,6 +845,8 @@ cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msws_insert_smem(16384));
         if (e != cudaSuccess) return e;
     }
+    e = cudaFuncSetAttribute((const void*)k_msws_query, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * 4);
+    if (e != cudaSuccess) return e;
     int occ = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_insert<AGG_BLOCK>, INS_THREADS, ins_smem);
     if (e != cudaSuccess) return e;
