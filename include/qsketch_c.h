@@ -227,6 +227,39 @@ qs_status qs_error_metrics(const uint32_t *d_est, const uint32_t *d_exact, size_
  * returning operations per second (sectors/s or bytes/s for kind 2). */
 qs_status qs_probe(uint32_t kind, uint64_t bytes, uint64_t ops, double *ops_per_s);
 
+/* ---- MSWS insert for callers that cannot allocate device memory ------------------------
+ * No counterpart in the reference: its classes allocate their own tables
+ * (device_sketch.h:83-114) and the harness allocates key buffers per batch.
+ *
+ * For code that runs inside an engine owning all device memory (a fixed arena set up at
+ * start-up, say) and may not call cudaMalloc/cudaFree while serving — those calls
+ * synchronise the device and fragment the arena.  The caller keeps the sketch in its own
+ * memory and passes it in: the low table (n_low*8 u32, 32-byte aligned), the high pool
+ * (n_high*32 u32), a state block of QS_MSWS_STATE_BYTES, and the device mask words
+ * (n_masks u32, bits 0..27, e.g. from qs_generate_hashmask).  A new sketch is all three
+ * zero-filled.  The call allocates nothing: the ordered replay's scratch is a fixed
+ * QS_NOALLOC_SCRATCH_BYTES array inside the library, which every GPU that loads the library
+ * holds until the process exits.  Results equal qs_insert's on a sketch with the same
+ * seed, masks and tables; query those tables by your own means or copy them into a
+ * qs_create'd sketch.
+ *
+ * Limits: n <= QS_NOALLOC_MAX_KEYS per call and n_low <= QS_NOALLOC_MAX_BUCKETS, else
+ * QS_ERR_CAPACITY before anything runs.  The first call on each device looks up the scratch
+ * array's device address (with that device current) and configures the kernels; make that
+ * first call before any stream capture.  Every call shares the one scratch array and leaves
+ * its contents behind (the call clears what must start at zero), so calls that overlap on
+ * the GPU — different streams or host threads without ordering between them — race and
+ * corrupt each other: order them.  Device status (pool full, timeouts) is latched in the
+ * state block's status word (second u32). */
+#define QS_NOALLOC_MAX_KEYS (1u << 18)
+#define QS_NOALLOC_MAX_BUCKETS (1ull << 26)
+#define QS_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define QS_MSWS_STATE_BYTES 256u
+qs_status qs_msws_insert_noalloc(uint32_t *d_low, uint64_t n_low, uint32_t *d_high, uint64_t n_high,
+                                 void *d_state, const uint32_t *d_masks, uint32_t n_masks,
+                                 uint32_t hash_seed, uint32_t flags, const uint32_t *d_keys, size_t n,
+                                 void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -110,7 +110,11 @@ SIGNATURES = {
     "qs_rank_histogram": (_I, [_P, _SZ, _P, _U64, _P]),
     "qs_error_metrics": (_I, [_P, _P, _SZ, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _P]),
     "qs_probe": (_I, [_U32, _U64, _U64, ctypes.POINTER(ctypes.c_double)]),
+    "qs_msws_insert_noalloc": (_I, [_P, _U64, _P, _U64, _P, _P, _U32, _U32, _U32, _P, _SZ, _P]),
 }
+QS_NOALLOC_MAX_KEYS = 1 << 18
+QS_NOALLOC_MAX_BUCKETS = 1 << 26
+QS_MSWS_STATE_BYTES = 256
 
 
 def _load():

@@ -61,6 +61,10 @@ const uint64_t kPrimes[] = {402653171, 268435399, 201326557, 134217689, 10066329
 
 }  // namespace
 
+namespace qsb {
+void set_last_error(const char* text) { g_err = text; }
+}  // namespace qsb
+
 struct qs_sketch {
     qs_params p{};
     int device = 0;

@@ -35,4 +35,7 @@ cudaError_t error_metrics(const uint32_t* d_est, const uint32_t* d_exact, uint64
                           cudaStream_t st);
 cudaError_t probe(uint32_t kind, uint64_t bytes, uint64_t ops, double* ops_per_s);
 
+// Text returned by qs_last_error_string() on this host thread.
+void set_last_error(const char* text);
+
 }  // namespace qsb

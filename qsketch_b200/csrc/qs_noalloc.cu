@@ -78,7 +78,7 @@ static qs_status na_setup(int dev, NaDevice** out, char* err, size_t errlen) {
             snprintf(err, errlen, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
             return e == cudaErrorNoKernelImageForDevice ? QS_ERR_NO_DEVICE : QS_ERR_CUDA;
         }
-        e = msws_configure(dev, 16384, &d.launch);
+        e = msws_configure(dev, 1021, &d.launch);  // grid sized for the default mask table
         if (e != cudaSuccess) {
             snprintf(err, errlen, "kernel configuration: %s", cudaGetErrorString(e));
             return QS_ERR_CUDA;
@@ -94,38 +94,36 @@ static qs_status na_setup(int dev, NaDevice** out, char* err, size_t errlen) {
 
 using namespace qsb;
 
-extern "C" qs_status qs_set_error_text(const char* text);
-
 extern "C" qs_status qs_msws_insert_noalloc(uint32_t* d_low, uint64_t n_low, uint32_t* d_high, uint64_t n_high,
                                             void* d_state, const uint32_t* d_masks, uint32_t n_masks,
                                             uint32_t hash_seed, uint32_t flags, const uint32_t* d_keys, size_t n,
                                             void* stream) {
-    char err[256];
+    char err[320];
     if (!d_low || !d_high || !d_state || !d_masks || (!d_keys && n))
-        return qs_set_error_text("qs_msws_insert_noalloc: null pointer"), QS_ERR_INVALID_ARG;
+        return set_last_error("qs_msws_insert_noalloc: null pointer"), QS_ERR_INVALID_ARG;
     if (n_low == 0 || n_high < 2 || n_high > (1ull << 30) || n_masks == 0 || n_masks > 16384 || hash_seed == 0)
-        return qs_set_error_text("qs_msws_insert_noalloc: n_low, n_high, n_masks or hash_seed out of range"),
+        return set_last_error("qs_msws_insert_noalloc: n_low, n_high, n_masks or hash_seed out of range"),
                QS_ERR_INVALID_ARG;
     if (n > NA_MAX_KEYS || n_low > NA_MAX_BUCKETS) {
         snprintf(err, sizeof err,
                  "qs_msws_insert_noalloc: %zu keys / %llu buckets exceed the fixed scratch (at most %llu keys per "
                  "call and %llu low buckets); split the call or use qs_create/qs_insert",
                  n, (unsigned long long)n_low, (unsigned long long)NA_MAX_KEYS, (unsigned long long)NA_MAX_BUCKETS);
-        return qs_set_error_text(err), QS_ERR_CAPACITY;
+        return set_last_error(err), QS_ERR_CAPACITY;
     }
     if ((reinterpret_cast<uintptr_t>(d_keys) | reinterpret_cast<uintptr_t>(d_low) |
          reinterpret_cast<uintptr_t>(d_high) | reinterpret_cast<uintptr_t>(d_state)) & 3u)
-        return qs_set_error_text("qs_msws_insert_noalloc: pointers must be 4-byte aligned"), QS_ERR_INVALID_ARG;
+        return set_last_error("qs_msws_insert_noalloc: pointers must be 4-byte aligned"), QS_ERR_INVALID_ARG;
     if (reinterpret_cast<uintptr_t>(d_low) & 31u)
-        return qs_set_error_text("qs_msws_insert_noalloc: the low table must be 32-byte aligned"), QS_ERR_INVALID_ARG;
+        return set_last_error("qs_msws_insert_noalloc: the low table must be 32-byte aligned"), QS_ERR_INVALID_ARG;
     if (n == 0) return QS_OK;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES)
-        return qs_set_error_text("qs_msws_insert_noalloc: no current CUDA device"), QS_ERR_NO_DEVICE;
+        return set_last_error("qs_msws_insert_noalloc: no current CUDA device"), QS_ERR_NO_DEVICE;
     NaDevice* nd = nullptr;
     qs_status s = na_setup(dev, &nd, err, sizeof err);
-    if (s != QS_OK) return qs_set_error_text(err), s;
+    if (s != QS_OK) return set_last_error(err), s;
 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     MswsDev D{};
@@ -165,7 +163,7 @@ extern "C" qs_status qs_msws_insert_noalloc(uint32_t* d_low, uint64_t n_low, uin
     if (e == cudaSuccess) e = msws_repair(d_keys, n, D, nd->launch, st);
     if (e != cudaSuccess) {
         snprintf(err, sizeof err, "qs_msws_insert_noalloc: %s", cudaGetErrorString(e));
-        return qs_set_error_text(err), QS_ERR_CUDA;
+        return set_last_error(err), QS_ERR_CUDA;
     }
     return QS_OK;
 }
