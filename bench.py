@@ -34,6 +34,11 @@ CONFIGS = {
                  n_ranks=1 << 24, s=1.1, n_low=2097143, n_high=1 << 17, n_query=1 << 24),
     "uniform": dict(workload="uniform_2^24keys_nlow262139_high8MB_query2^24", kind=0, n_keys=1 << 24, n_ranks=0,
                     s=0.0, n_low=262139, n_high=1 << 16, n_query=1 << 24),
+    # HBM-bound mixed workload: 2^28 operations in 2^20-key batches, each batch 90 % inserts
+    # then 10 % queries; Zipf 0.8 over 2^26 ranks; 256 MB low table (> L2), 64 MB high pool
+    "mixed": dict(workload="mixed_2^28ops_batch2^20_90ins10qry_zipf0.8_2^26ranks_low256MB_high64MB", kind=2,
+                  n_keys=1 << 28, n_ranks=1 << 26, s=0.8, n_low=8388593, n_high=1 << 19, n_query=0,
+                  batch=1 << 20, insert_frac=0.9),
     # a smaller skewed case for Nsight Compute captures (key stream still larger than L2)
     "zipf_prof": dict(workload="zipf1.1_2^25keys_2^22ranks_low16MB_high4MB_query2^22", kind=1, n_keys=1 << 25,
                       n_ranks=1 << 22, s=1.1, n_low=524287, n_high=1 << 15, n_query=1 << 22),
@@ -174,15 +179,42 @@ def run_ours(args, cfg):
         queries = data.rank_keys(perm_seed, 0, cfg["n_query"])
         exact = data.rank_histogram(ranks, cfg["n_ranks"])[:cfg["n_query"]].contiguous()
         del ranks
+    elif cfg["kind"] == 2:
+        keys = data.zipf_keys(cfg["n_keys"], cfg["n_ranks"], cfg["s"], seed=seed, perm_seed=perm_seed)
+        exact = None
     else:
         keys = data.uniform_keys(cfg["n_keys"], seed=seed)
         queries = keys[:cfg["n_query"]]
         exact = None
+    if cfg["kind"] == 2:  # per batch: the first 90 % insert, the rest query
+        B = cfg["batch"]
+        ni_b = int(B * cfg["insert_frac"])
+        nbat = cfg["n_keys"] // B
+        ins_views = [keys[b * B:b * B + ni_b] for b in range(nbat)]
+        q_views = [keys[b * B + ni_b:(b + 1) * B] for b in range(nbat)]
+        queries = torch.cat(q_views)
+        cfg = dict(cfg, n_query=queries.numel())
     out = torch.empty(cfg["n_query"], dtype=torch.uint32, device="cuda")
     sk = qs.Sketch_GPU_Sub_Warp_Level(cfg["n_low"], 8, cfg["n_high"], 32, hash_seed=SEED, mask_rng=1)
     n_ins, n_q = cfg["n_keys"], cfg["n_query"]
+    if cfg["kind"] == 2:
+        n_ins = n_ins - n_q
+        out_views = list(torch.split(out, [v.numel() for v in q_views]))
+
+    def step_mixed(ev=None):
+        sk.clear()
+        if ev:
+            ev[0].record(stream)
+        for iv, qv, ov in zip(ins_views, q_views, out_views):
+            sk.insert(iv)
+            sk.search(qv, counts=ov)
+        if ev:
+            ev[1].record(stream)
+            ev[2].record(stream)
 
     def step(ev=None):
+        if cfg["kind"] == 2:
+            return step_mixed(ev)
         sk.clear()
         if ev:
             ev[0].record(stream)
@@ -248,6 +280,9 @@ def run_ours(args, cfg):
         if k:
             traffic = k["dram_bytes_per_unit"] * per_launch_units
     atomic_peak = data.probe(0, max(64 << 20, cfg["n_low"] * 32), 1 << 26) if rank == 0 else None
+    if cfg["kind"] == 2:  # inserts and queries interleave: split their rates by kernel time
+        ins_ms = prof["insert_ms"] + prof["repair_ms"]
+        q_ms = prof["query_ms"]
     ins_rate = per_launch_units / (avg_ms * 1e-3) if dom == "insert" else n_ins / (prof["insert_ms"] * 1e-3)
 
     # end to end through the host-buffer C ABI calls: pinned keys in, counts out
@@ -255,16 +290,26 @@ def run_ours(args, cfg):
     hq = queries.cpu().pin_memory()
     ho = torch.empty(n_q, dtype=torch.uint32).pin_memory()
     e2e_steps = max(1, min(args.steps, 5))
-    sk.clear()
-    sk.insert_host(hk)
-    sk.search_host(hq, ho)
+
+    def e2e_step():
+        sk.clear()
+        if cfg["kind"] == 2:
+            B, qo = cfg["batch"], 0
+            for b in range(len(ins_views)):
+                sk.insert_host(hk[b * B:b * B + ni_b])
+                nq_b = B - ni_b
+                sk.search_host(hk[b * B + ni_b:(b + 1) * B], ho[qo:qo + nq_b])
+                qo += nq_b
+        else:
+            sk.insert_host(hk)
+            sk.search_host(hq, ho)
+
+    e2e_step()
     torch.cuda.synchronize()
     barrier()
     w0 = time.perf_counter()
     for _ in range(e2e_steps):
-        sk.clear()
-        sk.insert_host(hk)
-        sk.search_host(hq, ho)
+        e2e_step()
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks((time.perf_counter() - w0) * 1e3 / e2e_steps)
     barrier()
@@ -284,6 +329,8 @@ def run_ours(args, cfg):
             "insert_gkeys_per_s": round(world * n_ins / (ins_ms * 1e6), 4),
             "query_gkeys_per_s": round(world * n_q / (q_ms * 1e6), 4),
             "avg_rel_error": rel, "mean_est_over_exact": ratio,
+            "hbm_gbs_algorithmic": round((n_ins * INSERT_BYTES_PER_KEY + n_q * QUERY_BYTES_PER_KEY) /
+                                         (ms_per_step * 1e-3) / 1e9, 1),
             "e2e": {"value": round(world * (n_ins + n_q) / (e2e_ms * 1e6), 4), "unit": "Gkeys/s",
                     "h2d_bytes_per_step": (n_ins + n_q) * 4, "d2h_bytes_per_step": n_q * 4,
                     "ms_per_step": round(e2e_ms, 3), "api": "qs_insert_host + qs_query_host"},

@@ -212,3 +212,30 @@ def test_zipf_config2_full_size(gpu):
     orc.insert(keys.cpu().numpy(), threads=8)
     want = orc.query(q.cpu().numpy())
     assert np.array_equal(got, want)
+
+
+def run_mixed(sk, orc, keys, batch, frac=0.9, threads=1):
+    """Per batch: insert the first `frac` of it, then query the rest (configuration 3)."""
+    ni = int(batch * frac)
+    hk = keys.cpu().numpy()
+    for b in range(keys.numel() // batch):
+        sk.insert(keys[b * batch:b * batch + ni])
+        got = sk.search(keys[b * batch + ni:(b + 1) * batch]).cpu().numpy()
+        orc.insert(hk[b * batch:b * batch + ni], threads=threads)
+        want = orc.query(hk[b * batch + ni:(b + 1) * batch])
+        assert np.array_equal(got, want), f"batch {b}: {(got != want).sum()} estimates differ"
+
+
+def test_mixed_interleaved_small(gpu):
+    sk, orc = make_pair(65521, 1 << 13)
+    run_mixed(sk, orc, data.zipf_keys(1 << 22, 1 << 22, 0.8, seed=41, perm_seed=42), 1 << 18)
+    sk.sync()
+    assert_same_tables(sk, orc)
+
+
+def test_mixed_config3_full_size(gpu):
+    # 2^28 operations in 2^20 batches (90 % inserts then 10 % queries), Zipf 0.8 over 2^26,
+    # 256 MB low table (n_low = 8388593), 64 MB high pool
+    sk, orc = make_pair(8388593, 1 << 19)
+    run_mixed(sk, orc, data.zipf_keys(1 << 28, 1 << 26, 0.8, seed=1000, perm_seed=99), 1 << 20, threads=8)
+    sk.sync()
