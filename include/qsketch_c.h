@@ -211,6 +211,11 @@ qs_status qs_get_tables(qs_sketch *sk, uint32_t *h_low, uint32_t *h_high);
 qs_status qs_gen_keys(uint32_t kind, uint64_t seed, uint64_t n_ranks, double s,
                       uint64_t perm_seed, uint32_t *d_keys, uint32_t *d_ranks, size_t n,
                       void *stream);
+/* Structured keys (learned-split workload): key = class << 16 | suffix, the class id is a
+ * Zipf(s_class) rank over n_class <= 2^16 classes, the suffix a Zipf(s_suffix) rank over 2^16
+ * under the class's own seeded permutation of 16-bit values. */
+qs_status qs_gen_class_keys(uint64_t seed, uint32_t n_class, double s_class, double s_suffix, uint64_t perm_seed,
+                            uint32_t *d_keys, size_t n, void *stream);
 /* The key that qs_gen_keys(kind 1) maps rank r to, for r in [first, first+n). */
 qs_status qs_gen_rank_keys(uint64_t perm_seed, uint64_t first, uint32_t *d_keys, size_t n,
                            void *stream);
@@ -226,6 +231,63 @@ qs_status qs_error_metrics(const uint32_t *d_est, const uint32_t *d_exact, size_
  * 1 random 32 B sector load, 2 streaming read) over a device buffer of `bytes`,
  * returning operations per second (sectors/s or bytes/s for kind 2). */
 qs_status qs_probe(uint32_t kind, uint64_t bytes, uint64_t ops, double *ops_per_s);
+
+/* ---- learned heavy-hitter split (no counterpart in the reference) ------------------------
+ * An MLP 32 -> 128 -> 128 -> 1 over the key's bits (BF16 weights, FP32 accumulation on the
+ * tensor cores, weighted binary cross-entropy, Adam) decides which keys are heavy.  The
+ * first `warmup_keys` keys go to the MSWS sketch alone; then the network is trained on the
+ * warm-up window's distinct keys, labelled heavy when the sketch's estimate is in the top
+ * `heavy_fraction`, and the warm-up keys it predicts heavy are admitted to an exact
+ * open-addressing table (u32 key + u32 count).  Afterwards each key found in the table counts
+ * there exactly; every other key goes to the sketch, and keys the network predicts heavy are
+ * admitted at the end of their chunk (in key order, while the table is below max fill).  A
+ * query returns table count + sketch estimate.  Sketch, table and network share
+ * `budget_bytes` (sketch low:high = 4:1). */
+typedef struct qs_learned_params {
+    uint64_t budget_bytes;     /* default 64 MiB */
+    uint32_t table_slots;      /* power of two, default 2^17 (1 MiB) */
+    float table_max_fill;      /* admission stops at this load factor, default 0.75 */
+    uint64_t warmup_keys;      /* default 2^24 */
+    double heavy_fraction;     /* default 0.005 */
+    uint32_t epochs;           /* default 4 */
+    uint32_t batch;            /* training batch, default 4096 */
+    float lr;                  /* Adam step, default 2e-3 */
+    float max_pos_weight;      /* positive-class weight cap, default 64 */
+    uint32_t hash_seed;        /* sketch hash multiplier, 0 = draw from seed_rng */
+    uint32_t seed_rng, mask_rng, init_seed;
+    uint64_t max_batch;        /* keys per routing chunk, default 2^22 */
+    int32_t device;
+} qs_learned_params;
+
+typedef struct qs_learned qs_learned;
+
+typedef struct qs_learned_info {
+    uint64_t budget_bytes, sketch_bytes, table_bytes, mlp_bytes;
+    uint64_t n_low, n_high, table_slots, table_fill;
+    uint64_t warmup_keys, warmup_seen, train_examples, train_positives, admitted_after_warmup;
+    uint32_t threshold, trained, epochs, steps;
+    float pos_weight, loss_first, loss_last, train_precision, train_recall;
+    double train_ms;
+} qs_learned_info;
+
+#define QS_MLP_PARAMS 20865u /* W1[128x32] | W2[128x128] | b1[128] | b2[128] | w3[128] | b3 */
+
+void qs_learned_params_default(qs_learned_params *p);
+qs_status qs_learned_create(const qs_learned_params *p, qs_learned **out);
+qs_status qs_learned_destroy(qs_learned *lk);
+qs_status qs_learned_insert(qs_learned *lk, const uint32_t *d_keys, size_t n, void *stream);
+qs_status qs_learned_query(qs_learned *lk, const uint32_t *d_keys, size_t n, uint32_t *d_counts, void *stream);
+qs_status qs_learned_get_info(qs_learned *lk, qs_learned_info *out);
+/* The classifier alone (tests and tooling): fp32 parameters in the layout above. */
+qs_status qs_mlp_get_params(qs_learned *lk, float *h_params);
+qs_status qs_mlp_set_params(qs_learned *lk, const float *h_params);
+qs_status qs_mlp_forward(qs_learned *lk, const uint32_t *d_keys, size_t n, float *d_logits, void *stream);
+/* Gradient of the weighted BCE (mean over n) at the current parameters; loss = mean loss. */
+qs_status qs_mlp_grads(qs_learned *lk, const uint32_t *d_keys, const uint8_t *d_labels, size_t n, float pos_weight,
+                       float *h_grads, double *loss);
+/* Adam training over (keys, labels) in the given order, batches of `batch`. */
+qs_status qs_mlp_train(qs_learned *lk, const uint32_t *d_keys, const uint8_t *d_labels, size_t n, uint32_t epochs,
+                       uint32_t batch, float lr, float pos_weight, double *last_loss);
 
 /* ---- MSWS insert for callers that cannot allocate device memory ------------------------
  * No counterpart in the reference: its classes allocate their own tables

@@ -76,6 +76,37 @@ class qs_profile(ctypes.Structure):
     ]
 
 
+class qs_learned_params(ctypes.Structure):
+    _fields_ = [
+        ("budget_bytes", ctypes.c_uint64),
+        ("table_slots", ctypes.c_uint32),
+        ("table_max_fill", ctypes.c_float),
+        ("warmup_keys", ctypes.c_uint64),
+        ("heavy_fraction", ctypes.c_double),
+        ("epochs", ctypes.c_uint32),
+        ("batch", ctypes.c_uint32),
+        ("lr", ctypes.c_float),
+        ("max_pos_weight", ctypes.c_float),
+        ("hash_seed", ctypes.c_uint32),
+        ("seed_rng", ctypes.c_uint32),
+        ("mask_rng", ctypes.c_uint32),
+        ("init_seed", ctypes.c_uint32),
+        ("max_batch", ctypes.c_uint64),
+        ("device", ctypes.c_int32),
+    ]
+
+
+class qs_learned_info(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "budget_bytes", "sketch_bytes", "table_bytes", "mlp_bytes", "n_low", "n_high", "table_slots", "table_fill",
+        "warmup_keys", "warmup_seen", "train_examples", "train_positives", "admitted_after_warmup")] + \
+        [(n, ctypes.c_uint32) for n in ("threshold", "trained", "epochs", "steps")] + \
+        [(n, ctypes.c_float) for n in ("pos_weight", "loss_first", "loss_last", "train_precision", "train_recall")] + \
+        [("train_ms", ctypes.c_double)]
+
+
+QS_MLP_PARAMS = 20865
+
 # Every symbol include/qsketch_c.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
@@ -107,10 +138,23 @@ SIGNATURES = {
     "qs_get_tables": (_I, [_P, _P, _P]),
     "qs_gen_keys": (_I, [_U32, _U64, _U64, ctypes.c_double, _U64, _P, _P, _SZ, _P]),
     "qs_gen_rank_keys": (_I, [_U64, _U64, _P, _SZ, _P]),
+    "qs_gen_class_keys": (_I, [_U64, _U32, ctypes.c_double, ctypes.c_double, _U64, _P, _SZ, _P]),
     "qs_rank_histogram": (_I, [_P, _SZ, _P, _U64, _P]),
     "qs_error_metrics": (_I, [_P, _P, _SZ, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _P]),
     "qs_probe": (_I, [_U32, _U64, _U64, ctypes.POINTER(ctypes.c_double)]),
     "qs_msws_insert_noalloc": (_I, [_P, _U64, _P, _U64, _P, _P, _U32, _U32, _U32, _P, _SZ, _P]),
+    "qs_learned_params_default": (None, [ctypes.POINTER(qs_learned_params)]),
+    "qs_learned_create": (_I, [ctypes.POINTER(qs_learned_params), ctypes.POINTER(_P)]),
+    "qs_learned_destroy": (_I, [_P]),
+    "qs_learned_insert": (_I, [_P, _P, _SZ, _P]),
+    "qs_learned_query": (_I, [_P, _P, _SZ, _P, _P]),
+    "qs_learned_get_info": (_I, [_P, ctypes.POINTER(qs_learned_info)]),
+    "qs_mlp_get_params": (_I, [_P, _P]),
+    "qs_mlp_set_params": (_I, [_P, _P]),
+    "qs_mlp_forward": (_I, [_P, _P, _SZ, _P, _P]),
+    "qs_mlp_grads": (_I, [_P, _P, _P, _SZ, ctypes.c_float, _P, ctypes.POINTER(ctypes.c_double)]),
+    "qs_mlp_train": (_I, [_P, _P, _P, _SZ, _U32, _U32, ctypes.c_float, ctypes.c_float,
+                          ctypes.POINTER(ctypes.c_double)]),
 }
 QS_NOALLOC_MAX_KEYS = 1 << 18
 QS_NOALLOC_MAX_BUCKETS = 1 << 26

@@ -1,7 +1,10 @@
 // qs_api.cu — the C ABI (include/qsketch_c.h): sketch construction, host-side table
 // preparation (seeds, hash masks, prime sizing) and the stream-ordered launch sequence.
 #include <algorithm>
+#include <chrono>
+#include <cmath>
 #include <cstdarg>
+#include <functional>
 #include <cstdio>
 #include <cstring>
 #include <limits>
@@ -200,15 +203,20 @@ qs_status setup_io(qs_sketch* sk) {
     return QS_OK;
 }
 
-qs_status insert_device(qs_sketch* sk, const uint32_t* d_keys, size_t n, cudaStream_t st) {
+// skip: optional bitmap over the keys (bit set = the key is not for this sketch); chunk
+// offsets are multiples of max_batch, itself a multiple of 32.
+qs_status insert_device(qs_sketch* sk, const uint32_t* d_keys, size_t n, cudaStream_t st,
+                        const uint32_t* skip = nullptr) {
     if (sk->kind == QS_KIND_MSWS) {
         for (size_t off = 0; off < n; off += sk->max_batch) {
             const uint64_t c = std::min<uint64_t>(sk->max_batch, n - off);
+            MswsDev D = sk->D;
+            D.skip = skip ? skip + off / 32 : nullptr;
             CK(sk->prof_begin(0, st), "profile");
-            CK(msws_insert_pass(d_keys + off, c, sk->D, sk->L, sk->agg, st), "msws insert");
+            CK(msws_insert_pass(d_keys + off, c, D, sk->L, sk->agg, st), "msws insert");
             CK(sk->prof_end(0, st), "profile");
             CK(sk->prof_begin(1, st), "profile");
-            CK(msws_repair(d_keys + off, c, sk->D, sk->L, st), "msws repair");
+            CK(msws_repair(d_keys + off, c, D, sk->L, st), "msws repair");
             CK(sk->prof_end(1, st), "profile");
         }
     } else {
@@ -315,9 +323,9 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
     sk->device = dev;
     sk->kind = p.kind;
     sk->max_batch = p.max_batch ? p.max_batch : (1ull << 22);
-    if (sk->max_batch > (1ull << 30)) {
+    if (sk->max_batch > (1ull << 30) || (sk->max_batch & 31)) {
         delete sk;
-        return fail(QS_ERR_INVALID_ARG, "max_batch above 2^30");
+        return fail(QS_ERR_INVALID_ARG, "max_batch must be a multiple of 32 and at most 2^30");
     }
     // aggregate: 1 none, 2 warp, 3 warp + block, 0 = default (3)
     if (p.aggregate > 3) {
@@ -641,6 +649,15 @@ qs_status qs_gen_keys(uint32_t kind, uint64_t seed, uint64_t n_ranks, double s, 
     return QS_OK;
 }
 
+qs_status qs_gen_class_keys(uint64_t seed, uint32_t n_class, double s_class, double s_suffix, uint64_t perm_seed,
+                            uint32_t* d_keys, size_t n, void* stream) {
+    if ((!d_keys && n) || n_class == 0 || n_class > 65536 || s_class <= 0 || s_suffix <= 0)
+        return fail(QS_ERR_INVALID_ARG, "gen_class_keys: bad arguments");
+    CK(gen_class_keys(seed, n_class, s_class, s_suffix, perm_seed, d_keys, n, static_cast<cudaStream_t>(stream)),
+       "gen_class_keys");
+    return QS_OK;
+}
+
 qs_status qs_gen_rank_keys(uint64_t perm_seed, uint64_t first, uint32_t* d_keys, size_t n, void* stream) {
     if (!d_keys && n) return fail(QS_ERR_INVALID_ARG, "gen_rank_keys: null output");
     CK(gen_rank_keys(perm_seed, first, d_keys, n, static_cast<cudaStream_t>(stream)), "gen_rank_keys");
@@ -674,6 +691,454 @@ qs_status qs_error_metrics(const uint32_t* d_est, const uint32_t* d_exact, size_
 qs_status qs_probe(uint32_t kind, uint64_t bytes, uint64_t ops, double* ops_per_s) {
     if (!ops_per_s) return fail(QS_ERR_INVALID_ARG, "probe: null output");
     CK(probe(kind, bytes, ops, ops_per_s), "probe");
+    return QS_OK;
+}
+
+}  // extern "C"
+
+// =====================================================================================
+// Learned heavy-hitter split
+// =====================================================================================
+struct qs_learned {
+    qs_learned_params p{};
+    qs_sketch* sk = nullptr;
+    int device = 0;
+    TableDev T{};
+    RouteDev R{};
+    MlpDev M{};
+    std::vector<void*> allocs;
+    uint32_t* warm = nullptr;
+    uint64_t warm_seen = 0;
+    uint32_t* d_sorted = nullptr;   // admission order upload buffer
+    uint32_t admit_cap = 0;
+    float* d_loss = nullptr;
+    uint8_t* d_labels_tmp = nullptr;
+    qs_learned_info info{};
+    uint32_t adam_step = 0;
+
+    template <class X>
+    cudaError_t alloc(X** ptr, size_t count, int fill = 0) {
+        void* v = nullptr;
+        const size_t bytes = std::max<size_t>(count * sizeof(X), 256);
+        cudaError_t e = cudaMalloc(&v, bytes);
+        if (e != cudaSuccess) return e;
+        allocs.push_back(v);
+        e = cudaMemset(v, fill, bytes);
+        *ptr = static_cast<X*>(v);
+        return e;
+    }
+};
+
+namespace {
+
+qs_status mlp_init_params(qs_learned* lk) {
+    // He-uniform hidden layers, Glorot-uniform output, zero biases; deterministic in init_seed
+    std::vector<float> h(MLP_PARAMS, 0.0f);
+    std::mt19937 g(lk->p.init_seed);
+    auto fill = [&](size_t off, size_t n, float bound) {
+        std::uniform_real_distribution<float> d(-bound, bound);
+        for (size_t i = 0; i < n; ++i) h[off + i] = d(g);
+    };
+    fill(0, MLP_W1_N, std::sqrt(6.0f / 32.0f));
+    fill(MLP_W1_N, MLP_W2_N, std::sqrt(6.0f / 128.0f));
+    fill(MLP_BF16_PARAMS + 256, 128, std::sqrt(6.0f / 129.0f));
+    CK(cudaMemcpy(lk->M.params, h.data(), h.size() * 4, cudaMemcpyHostToDevice), "mlp init");
+    CK(mlp_refresh_bf16(lk->M, 0), "mlp bf16");
+    CK(cudaMemset(lk->M.adam_m, 0, MLP_PARAMS * 4), "adam m");
+    CK(cudaMemset(lk->M.adam_v, 0, MLP_PARAMS * 4), "adam v");
+    CK(cudaMemset(lk->M.grads, 0, MLP_PARAMS * 4), "grads");
+    CK(cudaDeviceSynchronize(), "mlp init sync");
+    lk->adam_step = 0;
+    return QS_OK;
+}
+
+// One pass of Adam over the examples in order; returns the mean loss of the last batch.
+qs_status mlp_train_pass(qs_learned* lk, const uint32_t* d_keys, const uint8_t* d_labels, uint64_t n, uint32_t batch,
+                         float lr, float pos_weight, double* last_loss, cudaStream_t st) {
+    float h_loss = 0.0f;
+    for (uint64_t off = 0; off < n; off += batch) {
+        const uint64_t b = std::min<uint64_t>(batch, n - off);
+        CK(cudaMemsetAsync(lk->d_loss, 0, 4, st), "loss reset");
+        CK(mlp_backward(d_keys + off, d_labels + off, b, pos_weight, 1.0f / (float)b, lk->M, lk->d_loss, st),
+           "mlp backward");
+        CK(mlp_adam(lk->M, ++lk->adam_step, lr, st), "adam");
+        if (off + batch >= n) {
+            CK(cudaMemcpyAsync(&h_loss, lk->d_loss, 4, cudaMemcpyDeviceToHost, st), "loss");
+            CK(cudaStreamSynchronize(st), "train sync");
+            h_loss /= (float)b;
+        }
+    }
+    *last_loss = h_loss;
+    return QS_OK;
+}
+
+qs_status learned_train(qs_learned* lk, cudaStream_t st) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const uint64_t W = lk->warm_seen;
+    uint32_t set_slots = 1;
+    while (set_slots < 2 * W) set_slots <<= 1;
+    uint32_t *d_set = nullptr, *d_distinct = nullptr, *d_cnt = nullptr, *d_est = nullptr;
+    float* d_logit = nullptr;
+    uint8_t* d_lab = nullptr;
+    uint32_t* d_perm_keys = nullptr;
+    auto cleanup = [&] {
+        for (void* v : {(void*)d_set, (void*)d_distinct, (void*)d_cnt, (void*)d_est, (void*)d_logit, (void*)d_lab,
+                        (void*)d_perm_keys})
+            if (v) cudaFree(v);
+    };
+#define CKT(expr, what)                                 \
+    do {                                                \
+        cudaError_t _e = (expr);                        \
+        if (_e != cudaSuccess) {                        \
+            cleanup();                                  \
+            return cuda_fail(_e, what);                 \
+        }                                               \
+    } while (0)
+    CKT(cudaMalloc(&d_set, (size_t)set_slots * 4), "train set");
+    CKT(cudaMalloc(&d_distinct, W * 4 + 4), "train distinct");
+    CKT(cudaMalloc(&d_cnt, 8), "train count");
+    CKT(distinct_keys(lk->warm, W, d_set, set_slots, d_distinct, d_cnt, st), "distinct");
+    uint32_t hc[2] = {0, 0};
+    CKT(cudaMemcpyAsync(hc, d_cnt, 8, cudaMemcpyDeviceToHost, st), "distinct count");
+    CKT(cudaStreamSynchronize(st), "distinct sync");
+    const uint64_t D = hc[0];
+    std::vector<uint32_t> keys(D);
+    CKT(cudaMemcpy(keys.data(), d_distinct, D * 4, cudaMemcpyDeviceToHost), "distinct copy");
+    std::sort(keys.begin(), keys.end());  // a fixed order, whatever the set's layout
+    CKT(cudaMemcpy(d_distinct, keys.data(), D * 4, cudaMemcpyHostToDevice), "distinct upload");
+    // labels from the sketch's own estimates
+    CKT(cudaMalloc(&d_est, D * 4 + 4), "train est");
+    qs_status s = query_device(lk->sk, d_distinct, D, d_est, st);
+    if (s != QS_OK) {
+        cleanup();
+        return s;
+    }
+    std::vector<uint32_t> est(D);
+    CKT(cudaMemcpyAsync(est.data(), d_est, D * 4, cudaMemcpyDeviceToHost, st), "est copy");
+    CKT(cudaStreamSynchronize(st), "est sync");
+    const uint64_t k = std::max<uint64_t>(1, (uint64_t)std::ceil(lk->p.heavy_fraction * (double)D));
+    std::vector<uint32_t> tmp(est);
+    std::nth_element(tmp.begin(), tmp.begin() + (k - 1), tmp.end(), std::greater<uint32_t>());
+    const uint32_t thr = tmp[k - 1];
+    std::vector<uint8_t> lab(D);
+    uint64_t npos = 0;
+    for (uint64_t i = 0; i < D; ++i) npos += (lab[i] = est[i] >= thr ? 1 : 0);
+    const float pw = std::min(lk->p.max_pos_weight, (float)(D - npos) / (float)std::max<uint64_t>(1, npos));
+    // epochs over a seeded shuffle of the examples
+    CKT(cudaMalloc(&d_lab, D + 4), "train labels");
+    CKT(cudaMalloc(&d_perm_keys, D * 4 + 4), "train keys");
+    std::vector<uint32_t> perm(D), pk(D);
+    std::vector<uint8_t> pl(D);
+    for (uint64_t i = 0; i < D; ++i) perm[i] = (uint32_t)i;
+    std::mt19937 g(lk->p.init_seed ^ 0x5bd1e995u);
+    double loss = 0.0, first = -1.0;
+    for (uint32_t ep = 0; ep < lk->p.epochs; ++ep) {
+        std::shuffle(perm.begin(), perm.end(), g);
+        for (uint64_t i = 0; i < D; ++i) {
+            pk[i] = keys[perm[i]];
+            pl[i] = lab[perm[i]];
+        }
+        CKT(cudaMemcpy(d_perm_keys, pk.data(), D * 4, cudaMemcpyHostToDevice), "train keys upload");
+        CKT(cudaMemcpy(d_lab, pl.data(), D, cudaMemcpyHostToDevice), "train labels upload");
+        s = mlp_train_pass(lk, d_perm_keys, d_lab, D, lk->p.batch, lk->p.lr, pw, &loss, st);
+        if (s != QS_OK) {
+            cleanup();
+            return s;
+        }
+        if (first < 0) first = loss;
+    }
+    // predictions on the warm-up keys: admit the predicted heavy, most confident first
+    CKT(cudaMalloc(&d_logit, D * 4 + 4), "train logits");
+    CKT(mlp_forward(d_distinct, D, lk->M, d_logit, st), "train forward");
+    std::vector<float> z(D);
+    CKT(cudaMemcpyAsync(z.data(), d_logit, D * 4, cudaMemcpyDeviceToHost, st), "logit copy");
+    CKT(cudaStreamSynchronize(st), "logit sync");
+    uint64_t tp = 0, fp = 0, fn = 0;
+    std::vector<std::pair<float, uint32_t>> heavy;
+    for (uint64_t i = 0; i < D; ++i) {
+        const bool pred = z[i] > 0.0f;
+        tp += pred && lab[i];
+        fp += pred && !lab[i];
+        fn += !pred && lab[i];
+        if (pred) heavy.push_back({-z[i], keys[i]});
+    }
+    std::sort(heavy.begin(), heavy.end());
+    const uint32_t take = (uint32_t)std::min<uint64_t>(heavy.size(), lk->T.max_fill);
+    std::vector<uint32_t> order(take);
+    for (uint32_t i = 0; i < take; ++i) order[i] = heavy[i].second;
+    if (take) {
+        CKT(cudaMemcpy(lk->d_sorted, order.data(), take * 4, cudaMemcpyHostToDevice), "admit upload");
+        CKT(table_admit(lk->T, lk->d_sorted, take, st), "admit");
+    }
+    CKT(cudaStreamSynchronize(st), "admit sync");
+    cleanup();
+#undef CKT
+    qs_learned_info& I = lk->info;
+    I.trained = 1;
+    I.train_examples = D;
+    I.train_positives = npos;
+    I.threshold = thr;
+    I.pos_weight = pw;
+    I.loss_first = (float)first;
+    I.loss_last = (float)loss;
+    I.train_precision = tp + fp ? (float)tp / (float)(tp + fp) : 0.0f;
+    I.train_recall = tp + fn ? (float)tp / (float)(tp + fn) : 0.0f;
+    I.epochs = lk->p.epochs;
+    I.steps = lk->adam_step;
+    I.train_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return QS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void qs_learned_params_default(qs_learned_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->budget_bytes = 64ull << 20;
+    p->table_slots = 1u << 17;
+    p->table_max_fill = 0.75f;
+    p->warmup_keys = 1ull << 24;
+    p->heavy_fraction = 0.005;
+    p->epochs = 4;
+    p->batch = 4096;
+    p->lr = 2e-3f;
+    p->max_pos_weight = 64.0f;
+    p->seed_rng = 1;
+    p->mask_rng = 1;
+    p->init_seed = 1;
+    p->max_batch = 1ull << 22;
+    p->device = -1;
+}
+
+qs_status qs_learned_create(const qs_learned_params* p, qs_learned** out) {
+    if (!p || !out) return fail(QS_ERR_INVALID_ARG, "qs_learned_create: null argument");
+    *out = nullptr;
+    if (p->table_slots < 64 || (p->table_slots & (p->table_slots - 1)))
+        return fail(QS_ERR_INVALID_ARG, "table_slots must be a power of two >= 64");
+    if (p->warmup_keys == 0 || p->heavy_fraction <= 0 || p->heavy_fraction >= 1 || p->batch == 0 || p->epochs == 0)
+        return fail(QS_ERR_INVALID_ARG, "learned params out of range");
+    const uint64_t mlp_bytes = (uint64_t)MLP_BF16_PARAMS * 2 + (uint64_t)(MLP_PARAMS - MLP_BF16_PARAMS) * 4;
+    const uint64_t table_bytes = (uint64_t)p->table_slots * 8;
+    if (p->budget_bytes < table_bytes + mlp_bytes + (1u << 16))
+        return fail(QS_ERR_INVALID_ARG, "budget too small for table + network + sketch");
+    const uint64_t sketch_bytes = p->budget_bytes - table_bytes - mlp_bytes;
+    qs_params sp;
+    qs_params_default(&sp);
+    sp.n_low = qs_find_greatest_prime(sketch_bytes * 4 / 5 / 32);
+    sp.n_high = (sketch_bytes - sp.n_low * 32) / 128;
+    sp.hash_seed = p->hash_seed;
+    sp.seed_rng = p->seed_rng;
+    sp.mask_rng = p->mask_rng;
+    sp.max_batch = p->max_batch ? p->max_batch : (1ull << 22);
+    sp.device = p->device;
+    qs_learned* lk = new qs_learned();
+    lk->p = *p;
+    if (!lk->p.max_batch) lk->p.max_batch = sp.max_batch;
+    qs_status s = qs_create(&sp, &lk->sk);
+    if (s != QS_OK) {
+        delete lk;
+        return s;
+    }
+    lk->device = lk->sk->device;
+    DeviceGuard guard(lk->device);
+    auto bail = [&](qs_status st) {
+        qs_learned_destroy(lk);
+        return st;
+    };
+    const uint64_t B = lk->sk->max_batch;
+    TableDev& T = lk->T;
+    T.slots = p->table_slots;
+    T.max_fill = (uint32_t)std::max(1.0f, p->table_max_fill * (float)p->table_slots);
+    CKB(lk->alloc(&T.keys, T.slots, 0xff), "table keys");
+    CKB(lk->alloc(&T.counts, T.slots), "table counts");
+    CKB(lk->alloc(&T.fill, 1), "table fill");
+    RouteDev& R = lk->R;
+    R.cand_slots = 1u << 18;
+    CKB(lk->alloc(&R.skip, B / 32 + 1), "route skip");
+    CKB(lk->alloc(&R.misses, B), "route misses");
+    CKB(lk->alloc(&R.n_misses, 1), "route misses count");
+    CKB(lk->alloc(&R.cand_keys, R.cand_slots, 0xff), "candidates");
+    CKB(lk->alloc(&R.n_cand, 1), "candidate count");
+    CKB(lk->alloc(&R.cand_list, R.cand_slots), "candidate list");
+    lk->admit_cap = std::max<uint32_t>(T.max_fill, R.cand_slots);
+    CKB(lk->alloc(&lk->d_sorted, lk->admit_cap), "admission buffer");
+    MlpDev& M = lk->M;
+    CKB(lk->alloc(&M.params, MLP_PARAMS), "mlp params");
+    CKB(lk->alloc(&M.grads, MLP_PARAMS), "mlp grads");
+    CKB(lk->alloc(&M.adam_m, MLP_PARAMS), "adam m");
+    CKB(lk->alloc(&M.adam_v, MLP_PARAMS), "adam v");
+    CKB(lk->alloc(&M.W1, MLP_BF16_PARAMS), "mlp bf16");
+    M.W2 = M.W1 + MLP_W1_N;
+    M.b1 = M.params + MLP_BF16_PARAMS;
+    M.b2 = M.b1 + 128;
+    M.w3 = M.b2 + 128;
+    M.b3 = M.w3 + 128;
+    M.gW1 = M.grads;
+    M.gW2 = M.grads + MLP_W1_N;
+    M.gb1 = M.grads + MLP_BF16_PARAMS;
+    M.gb2 = M.gb1 + 128;
+    M.g3 = M.gb2 + 128;
+    M.gb3 = M.g3 + 128;
+    CKB(lk->alloc(&lk->d_loss, 4), "loss");
+    CKB(lk->alloc(&lk->warm, p->warmup_keys), "warm-up keys");
+    cudaError_t e = mlp_configure();
+    if (e != cudaSuccess) return bail(cuda_fail(e, "mlp configure"));
+    s = mlp_init_params(lk);
+    if (s != QS_OK) return bail(s);
+    qs_learned_info& I = lk->info;
+    I.budget_bytes = p->budget_bytes;
+    I.sketch_bytes = sp.n_low * 32 + sp.n_high * 128;
+    I.table_bytes = table_bytes;
+    I.mlp_bytes = mlp_bytes;
+    I.n_low = sp.n_low;
+    I.n_high = sp.n_high;
+    I.table_slots = T.slots;
+    I.warmup_keys = p->warmup_keys;
+    *out = lk;
+    return QS_OK;
+}
+
+qs_status qs_learned_destroy(qs_learned* lk) {
+    if (!lk) return QS_OK;
+    {
+        DeviceGuard guard(lk->device);
+        cudaDeviceSynchronize();
+        for (void* v : lk->allocs) cudaFree(v);
+        if (lk->sk) qs_destroy(lk->sk);
+    }
+    delete lk;
+    return QS_OK;
+}
+
+qs_status qs_learned_insert(qs_learned* lk, const uint32_t* d_keys, size_t n, void* stream) {
+    if (!lk) return fail(QS_ERR_INVALID_ARG, "null learned sketch");
+    if (n == 0) return QS_OK;
+    if (!d_keys || (reinterpret_cast<uintptr_t>(d_keys) & 3u)) return fail(QS_ERR_INVALID_ARG, "bad keys pointer");
+    DeviceGuard guard(lk->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    size_t off = 0;
+    while (off < n) {
+        if (lk->warm_seen < lk->p.warmup_keys) {
+            const uint64_t take = std::min<uint64_t>(n - off, lk->p.warmup_keys - lk->warm_seen);
+            CK(cudaMemcpyAsync(lk->warm + lk->warm_seen, d_keys + off, take * 4, cudaMemcpyDeviceToDevice, st),
+               "warm-up copy");
+            qs_status s = insert_device(lk->sk, d_keys + off, take, st);
+            if (s != QS_OK) return s;
+            lk->warm_seen += take;
+            off += take;
+            if (lk->warm_seen == lk->p.warmup_keys) {
+                s = learned_train(lk, st);
+                if (s != QS_OK) return s;
+            }
+            continue;
+        }
+        // route a chunk: table hits count exactly and are skipped by the sketch insert
+        uint64_t c = std::min<uint64_t>(n - off, lk->sk->max_batch);
+        CK(cudaMemsetAsync(lk->R.n_misses, 0, 4, st), "misses reset");
+        CK(route_chunk(d_keys + off, c, lk->T, lk->R, st), "route");
+        CK(classify_misses(lk->M, lk->R, c, st), "classify");
+        qs_status s = insert_device(lk->sk, d_keys + off, c, st, lk->R.skip);
+        if (s != QS_OK) return s;
+        uint32_t ncand = 0;
+        CK(cudaMemcpyAsync(&ncand, lk->R.n_cand, 4, cudaMemcpyDeviceToHost, st), "candidates");
+        CK(cudaStreamSynchronize(st), "candidate sync");
+        if (ncand) {
+            ncand = std::min(ncand, lk->R.cand_slots);
+            std::vector<uint32_t> cand(ncand);
+            CK(cudaMemcpy(cand.data(), lk->R.cand_list, ncand * 4, cudaMemcpyDeviceToHost), "candidate copy");
+            std::sort(cand.begin(), cand.end());
+            const uint32_t take = std::min<uint32_t>(ncand, lk->admit_cap);
+            CK(cudaMemcpy(lk->d_sorted, cand.data(), take * 4, cudaMemcpyHostToDevice), "admit upload");
+            uint32_t before = 0, after = 0;
+            CK(cudaMemcpy(&before, lk->T.fill, 4, cudaMemcpyDeviceToHost), "fill");
+            CK(table_admit(lk->T, lk->d_sorted, take, st), "admit");
+            CK(cudaMemcpyAsync(&after, lk->T.fill, 4, cudaMemcpyDeviceToHost, st), "fill");
+            CK(cudaMemsetAsync(lk->R.cand_keys, 0xff, (size_t)lk->R.cand_slots * 4, st), "candidate reset");
+            CK(cudaMemsetAsync(lk->R.n_cand, 0, 4, st), "candidate reset");
+            CK(cudaStreamSynchronize(st), "admit sync");
+            lk->info.admitted_after_warmup += after - before;
+        }
+        off += c;
+    }
+    return QS_OK;
+}
+
+qs_status qs_learned_query(qs_learned* lk, const uint32_t* d_keys, size_t n, uint32_t* d_counts, void* stream) {
+    if (!lk) return fail(QS_ERR_INVALID_ARG, "null learned sketch");
+    if (n == 0) return QS_OK;
+    if (!d_keys || !d_counts) return fail(QS_ERR_INVALID_ARG, "null keys or counts");
+    DeviceGuard guard(lk->device);
+    CK(learned_query(d_keys, n, lk->T, lk->sk->D, lk->sk->L, d_counts, static_cast<cudaStream_t>(stream)),
+       "learned query");
+    return QS_OK;
+}
+
+qs_status qs_learned_get_info(qs_learned* lk, qs_learned_info* out) {
+    if (!lk || !out) return fail(QS_ERR_INVALID_ARG, "null argument");
+    DeviceGuard guard(lk->device);
+    CK(cudaDeviceSynchronize(), "info sync");
+    uint32_t fill = 0;
+    CK(cudaMemcpy(&fill, lk->T.fill, 4, cudaMemcpyDeviceToHost), "fill");
+    *out = lk->info;
+    out->table_fill = fill;
+    out->warmup_seen = lk->warm_seen;
+    return QS_OK;
+}
+
+qs_status qs_mlp_get_params(qs_learned* lk, float* h) {
+    if (!lk || !h) return fail(QS_ERR_INVALID_ARG, "null argument");
+    DeviceGuard guard(lk->device);
+    CK(cudaDeviceSynchronize(), "sync");
+    CK(cudaMemcpy(h, lk->M.params, MLP_PARAMS * 4, cudaMemcpyDeviceToHost), "params copy");
+    return QS_OK;
+}
+
+qs_status qs_mlp_set_params(qs_learned* lk, const float* h) {
+    if (!lk || !h) return fail(QS_ERR_INVALID_ARG, "null argument");
+    DeviceGuard guard(lk->device);
+    CK(cudaDeviceSynchronize(), "sync");
+    CK(cudaMemcpy(lk->M.params, h, MLP_PARAMS * 4, cudaMemcpyHostToDevice), "params copy");
+    CK(mlp_refresh_bf16(lk->M, 0), "bf16");
+    CK(cudaMemset(lk->M.adam_m, 0, MLP_PARAMS * 4), "adam m");
+    CK(cudaMemset(lk->M.adam_v, 0, MLP_PARAMS * 4), "adam v");
+    CK(cudaDeviceSynchronize(), "sync");
+    lk->adam_step = 0;
+    return QS_OK;
+}
+
+qs_status qs_mlp_forward(qs_learned* lk, const uint32_t* d_keys, size_t n, float* d_logits, void* stream) {
+    if (!lk || (!d_keys && n) || (!d_logits && n)) return fail(QS_ERR_INVALID_ARG, "null argument");
+    DeviceGuard guard(lk->device);
+    CK(mlp_forward(d_keys, n, lk->M, d_logits, static_cast<cudaStream_t>(stream)), "mlp forward");
+    return QS_OK;
+}
+
+qs_status qs_mlp_grads(qs_learned* lk, const uint32_t* d_keys, const uint8_t* d_labels, size_t n, float pos_weight,
+                       float* h_grads, double* loss) {
+    if (!lk || !d_keys || !d_labels || !h_grads || !loss || n == 0) return fail(QS_ERR_INVALID_ARG, "bad argument");
+    DeviceGuard guard(lk->device);
+    CK(cudaDeviceSynchronize(), "sync");
+    CK(cudaMemset(lk->M.grads, 0, MLP_PARAMS * 4), "grads reset");
+    CK(cudaMemset(lk->d_loss, 0, 4), "loss reset");
+    CK(mlp_backward(d_keys, d_labels, n, pos_weight, 1.0f / (float)n, lk->M, lk->d_loss, 0), "mlp backward");
+    float l = 0;
+    CK(cudaMemcpy(&l, lk->d_loss, 4, cudaMemcpyDeviceToHost), "loss copy");
+    CK(cudaMemcpy(h_grads, lk->M.grads, MLP_PARAMS * 4, cudaMemcpyDeviceToHost), "grads copy");
+    CK(cudaMemset(lk->M.grads, 0, MLP_PARAMS * 4), "grads reset");
+    *loss = (double)l / (double)n;
+    return QS_OK;
+}
+
+qs_status qs_mlp_train(qs_learned* lk, const uint32_t* d_keys, const uint8_t* d_labels, size_t n, uint32_t epochs,
+                       uint32_t batch, float lr, float pos_weight, double* last_loss) {
+    if (!lk || !d_keys || !d_labels || !last_loss || n == 0 || batch == 0) return fail(QS_ERR_INVALID_ARG, "bad argument");
+    DeviceGuard guard(lk->device);
+    for (uint32_t e = 0; e < epochs; ++e) {
+        qs_status s = mlp_train_pass(lk, d_keys, d_labels, n, batch, lr, pos_weight, last_loss, 0);
+        if (s != QS_OK) return s;
+    }
     return QS_OK;
 }
 

@@ -89,6 +89,42 @@ __global__ void k_gen_keys(uint32_t kind, uint64_t seed, ZipfParams zp, uint64_t
     }
 }
 
+// Seeded bijection of 16-bit values (odd multiplies mod 2^16 and xor-shifts invert).
+__device__ __forceinline__ uint32_t perm16(uint32_t r, uint32_t k) {
+    uint32_t x = (r ^ k) & 0xffffu;
+    x = (x * 0x9E35u) & 0xffffu;
+    x ^= x >> 7;
+    x = (x * (((k >> 16) | 1u) & 0xffffu)) & 0xffffu;
+    x ^= x >> 9;
+    x = (x * 0x6A27u) & 0xffffu;
+    return x ^ (x >> 8);
+}
+
+// key = class << 16 | suffix: class rank ~ Zipf(s_class) over n_class classes (the class id
+// is its rank), suffix rank ~ Zipf(s_suffix) over 2^16 mapped by the class's own permutation.
+__global__ void k_gen_class_keys(uint64_t seed, ZipfParams zc, ZipfParams zs, uint64_t perm_seed, uint32_t* keys,
+                                 uint64_t n) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        double kc = 1.0, ks = 1.0;
+        for (uint32_t a = 0; a < 64; ++a) {
+            const double u = zc.hxn + uniform01(seed, i, a) * (zc.hx1 - zc.hxn);
+            const double x = zHinv(u, zc.s);
+            kc = fmin(fmax(floor(x + 0.5), 1.0), zc.N);
+            if (kc - x <= zc.sconst || u >= zH(kc + 0.5, zc.s) - zh(kc, zc.s)) break;
+        }
+        for (uint32_t a = 0; a < 64; ++a) {
+            const double u = zs.hxn + uniform01(seed ^ 0x5851F42D4C957F2Dull, i, a) * (zs.hx1 - zs.hxn);
+            const double x = zHinv(u, zs.s);
+            ks = fmin(fmax(floor(x + 0.5), 1.0), zs.N);
+            if (ks - x <= zs.sconst || u >= zH(ks + 0.5, zs.s) - zh(ks, zs.s)) break;
+        }
+        const uint32_t c = (uint32_t)kc - 1u, r = (uint32_t)ks - 1u;
+        const uint32_t k = (uint32_t)splitmix64(perm_seed ^ ((uint64_t)c << 20));
+        keys[i] = (c << 16) | perm16(r, k);
+    }
+}
+
 __global__ void k_gen_rank_keys(uint64_t perm_seed, uint64_t first, uint32_t* keys, uint64_t n) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
@@ -145,6 +181,14 @@ cudaError_t gen_keys(uint32_t kind, uint64_t seed, uint64_t n_ranks, double s, u
     if (n == 0) return cudaSuccess;
     ZipfParams z = make_zipf(s > 0 ? s : 1.0, n_ranks ? n_ranks : 1);
     k_gen_keys<<<148 * 8, 256, 0, st>>>(kind, seed, z, perm_seed, d_keys, d_ranks, n);
+    return cudaGetLastError();
+}
+
+cudaError_t gen_class_keys(uint64_t seed, uint32_t n_class, double s_class, double s_suffix, uint64_t perm_seed,
+                           uint32_t* d_keys, uint64_t n, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_gen_class_keys<<<148 * 8, 256, 0, st>>>(seed, make_zipf(s_class, n_class), make_zipf(s_suffix, 1u << 16),
+                                              perm_seed, d_keys, n);
     return cudaGetLastError();
 }
 

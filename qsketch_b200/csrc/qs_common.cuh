@@ -87,6 +87,7 @@ struct MswsDev {
     uint32_t* totals;        // long_cap slots * 28 counts
     uint32_t long_cap;       // slots whose per-counter totals are computed grid-wide
     uint32_t route;          // 0 adaptive, 1 preload, 2 fused (pass-1 routing)
+    const uint32_t* skip;    // optional: bit i set = key i of the chunk is not for this sketch
     uint32_t max_tiles;      // tiles of REPAIR_TILE elements in a chunk
 };
 

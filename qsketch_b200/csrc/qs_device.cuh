@@ -163,4 +163,27 @@ __device__ __forceinline__ uint32_t block_scan_array(uint32_t* a, uint32_t len) 
     return total;
 }
 
+// ---- exact table of the learned split -----------------------------------------------------
+__host__ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x85EBCA6Bu;
+    x ^= x >> 13;
+    x *= 0xC2B2AE35u;
+    x ^= x >> 16;
+    return x;
+}
+
+// Slot of `key` in an open-addressing table (linear probing, TBL_PROBES slots), or -1.
+__device__ __forceinline__ int table_find(const uint32_t* keys, uint32_t slots, uint32_t key) {
+    if (key == 0xffffffffu) return -1;
+    const uint32_t h = mix32(key) & (slots - 1);
+    for (int p = 0; p < 32; ++p) {
+        const uint32_t s = (h + p) & (slots - 1);
+        const uint32_t k = __ldg(keys + s);
+        if (k == key) return (int)s;
+        if (k == 0xffffffffu) return -1;
+    }
+    return -1;
+}
+
 }  // namespace qsb

@@ -2,6 +2,7 @@
 #pragma once
 #include <algorithm>
 #include <cstdint>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include "qs_common.cuh"
 
@@ -30,6 +31,8 @@ cudaError_t cm_query(const uint32_t* d_keys, uint64_t n, uint32_t* d_out, const 
 cudaError_t gen_keys(uint32_t kind, uint64_t seed, uint64_t n_ranks, double s, uint64_t perm_seed, uint32_t* d_keys,
                      uint32_t* d_ranks, uint64_t n, cudaStream_t st);
 cudaError_t gen_rank_keys(uint64_t perm_seed, uint64_t first, uint32_t* d_keys, uint64_t n, cudaStream_t st);
+cudaError_t gen_class_keys(uint64_t seed, uint32_t n_class, double s_class, double s_suffix, uint64_t perm_seed,
+                           uint32_t* d_keys, uint64_t n, cudaStream_t st);
 cudaError_t rank_histogram(const uint32_t* d_ranks, uint64_t n, uint32_t* d_hist, uint64_t n_ranks, cudaStream_t st);
 cudaError_t error_metrics(const uint32_t* d_est, const uint32_t* d_exact, uint64_t n, double* d_acc,
                           cudaStream_t st);
@@ -37,5 +40,58 @@ cudaError_t probe(uint32_t kind, uint64_t bytes, uint64_t ops, double* ops_per_s
 
 // Text returned by qs_last_error_string() on this host thread.
 void set_last_error(const char* text);
+
+// ---- learned split: MLP 32 -> 128 -> 128 -> 1 ---------------------------------------------
+constexpr uint32_t MLP_W1_N = 128 * 32, MLP_W2_N = 128 * 128;
+constexpr uint32_t MLP_BF16_PARAMS = MLP_W1_N + MLP_W2_N;           // W1 | W2 in bf16
+constexpr uint32_t MLP_PARAMS = MLP_BF16_PARAMS + 128 + 128 + 128 + 1;  // + b1 | b2 | w3 | b3
+
+struct MlpDev {
+    __nv_bfloat16* W1;  // bf16 copies, W2 = W1 + MLP_W1_N
+    __nv_bfloat16* W2;
+    float* params;      // fp32 master: W1 | W2 | b1 | b2 | w3 | b3
+    float *b1, *b2, *w3, *b3;
+    float* grads;       // same layout
+    float *gW1, *gW2, *gb1, *gb2, *g3, *gb3;
+    float *adam_m, *adam_v;
+};
+
+size_t mlp_smem_bytes();
+cudaError_t mlp_configure();
+cudaError_t mlp_forward(const uint32_t* d_keys, uint64_t n, const MlpDev& M, float* d_logits, cudaStream_t st);
+cudaError_t mlp_backward(const uint32_t* d_keys, const uint8_t* d_labels, uint64_t n, float pos_weight,
+                         float inv_batch, const MlpDev& M, float* d_loss, cudaStream_t st);
+cudaError_t mlp_adam(const MlpDev& M, uint32_t step, float lr, cudaStream_t st);
+cudaError_t mlp_refresh_bf16(const MlpDev& M, cudaStream_t st);
+
+// ---- learned split: exact table of heavy keys and routing -----------------------------------
+constexpr uint32_t TBL_EMPTY = 0xffffffffu;
+constexpr int TBL_PROBES = 32;
+
+struct TableDev {
+    uint32_t* keys;    // slots, TBL_EMPTY when free
+    uint32_t* counts;  // exact counts of the admitted keys
+    uint32_t slots;    // power of two
+    uint32_t max_fill; // admission stops at this many keys
+    uint32_t* fill;    // device counter of admitted keys
+};
+
+struct RouteDev {
+    uint32_t* skip;         // 1 bit per key of the chunk: counted in the exact table
+    uint32_t* misses;       // distinct-per-warp keys that missed the table (unordered)
+    uint32_t* n_misses;
+    uint32_t* cand_keys;    // candidate set (open addressing), TBL_EMPTY when free
+    uint32_t cand_slots;    // power of two
+    uint32_t* n_cand;
+    uint32_t* cand_list;    // admitted-order list of candidates
+};
+
+cudaError_t route_chunk(const uint32_t* d_keys, uint64_t n, const TableDev& T, const RouteDev& R, cudaStream_t st);
+cudaError_t classify_misses(const MlpDev& M, const RouteDev& R, uint64_t max_misses, cudaStream_t st);
+cudaError_t table_admit(const TableDev& T, const uint32_t* d_sorted, uint32_t count, cudaStream_t st);
+cudaError_t learned_query(const uint32_t* d_keys, uint64_t n, const TableDev& T, const MswsDev& D, const MswsLaunch& L,
+                          uint32_t* d_out, cudaStream_t st);
+cudaError_t distinct_keys(const uint32_t* d_keys, uint64_t n, uint32_t* d_set, uint32_t set_slots, uint32_t* d_out,
+                          uint32_t* d_count, cudaStream_t st);
 
 }  // namespace qsb

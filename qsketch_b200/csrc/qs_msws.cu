@@ -216,9 +216,9 @@ __device__ __forceinline__ uint32_t staged_rounds_fused(const MswsDev& D, const 
 // Up to 32 keys held one per lane (valid lanes: lane < cnt).
 template <int AGG>
 __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& S, uint32_t key, int cnt,
-                                             bool use_table, int route) {
+                                             bool use_table, int route, uint64_t idx) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const bool valid = lane < cnt;
+    const bool valid = lane < cnt && !(D.skip && ((__ldg(D.skip + (idx >> 5)) >> (idx & 31)) & 1u));
     const uint32_t hv = key * D.seed;  // hash_mul_add, device_hash_function.h:6-18
     const uint32_t b = fast_mod(D.fm_low, hv);
     const uint32_t m = S.masks[fast_mod(D.fm_mask, hv)];
@@ -317,7 +317,8 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
     __syncthreads();
     if (blockIdx.x == 0 && wid == 0 && head + tail > 0) {
         const uint32_t k = lane < (int)(head + tail) ? s_extra[lane] : 0u;
-        insert_group<AGG>(D, S, k, (int)(head + tail), false, ROUTE_PRELOAD);
+        const uint64_t idx = lane < (int)head ? (uint64_t)lane : head + body_n + (lane - head);
+        insert_group<AGG>(D, S, k, (int)(head + tail), false, ROUTE_PRELOAD, idx);
     }
 
     const uint64_t ntiles = (body_n + INS_TILE - 1) / INS_TILE;
@@ -357,7 +358,7 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
         for (int base = wid * 32; base < cnt; base += INS_THREADS) {
             const int c = min(32, cnt - base);
             const uint32_t k = lane < c ? tk[base + lane] : 0u;
-            insert_group<AGG>(D, S, k, c, true, route);
+            insert_group<AGG>(D, S, k, c, true, route, head + g * INS_TILE + base + lane);
         }
         __syncthreads();
         if (tid == 0) {  // adaptive: the next tile is fused while under 1/16 of the keys are linked
@@ -616,7 +617,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
             const uint64_t i = base + j;
-            if (i < n) {
+            if (i < n && !(D.skip && ((__ldg(D.skip + (i >> 5)) >> (i & 31)) & 1u))) {
                 const uint32_t hv = __ldg(keys + i) * D.seed;
                 c += flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, hv)) != NONE ? 1u : 0u;
             }
@@ -644,7 +645,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         for (int j = 0; j < PER; ++j) {
             const uint64_t i = base + j;
             slots[j] = NONE;
-            if (i < n) {
+            if (i < n && !(D.skip && ((__ldg(D.skip + (i >> 5)) >> (i & 31)) & 1u))) {
                 const uint32_t hv = __ldg(keys + i) * D.seed;
                 slots[j] = flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, hv));
                 c += slots[j] != NONE ? 1u : 0u;
@@ -829,6 +830,32 @@ __global__ void __launch_bounds__(QRY_THREADS) k_msws_query(const uint32_t* __re
     }
 }
 
+// Learned split query: exact count of a key in the heavy table (if admitted) plus the MSWS
+// estimate (its occurrences before admission live in the sketch).
+__global__ void __launch_bounds__(QRY_THREADS) k_learned_query(const uint32_t* __restrict__ keys, uint64_t n,
+                                                               TableDev T, uint32_t* __restrict__ out, MswsDev D) {
+    extern __shared__ __align__(16) uint32_t s_masks[];
+    for (uint32_t i = threadIdx.x; i < D.n_masks; i += blockDim.x) s_masks[i] = __ldg(D.masks + i);
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t key = __ldcs(keys + i);
+        uint32_t r = msws_lookup(D, s_masks, key);
+        const int s = table_find(T.keys, T.slots, key);
+        if (s >= 0) r += __ldcg(T.counts + s);
+        __stcs(out + i, r);
+    }
+}
+
+cudaError_t learned_query(const uint32_t* d_keys, uint64_t n, const TableDev& T, const MswsDev& D, const MswsLaunch& L,
+                          uint32_t* d_out, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const uint64_t want = (n + QRY_THREADS - 1) / QRY_THREADS;
+    const int grid = (int)std::min<uint64_t>((uint64_t)L.query_grid, std::max<uint64_t>(1ull, want));
+    k_learned_query<<<grid, QRY_THREADS, (size_t)D.n_masks * 4, st>>>(d_keys, n, T, d_out, D);
+    return cudaGetLastError();
+}
+
 // ---- launchers ----------------------------------------------------------------------------
 
 cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
@@ -846,6 +873,8 @@ cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
         if (e != cudaSuccess) return e;
     }
     e = cudaFuncSetAttribute((const void*)k_msws_query, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * 4);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute((const void*)k_learned_query, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * 4);
     if (e != cudaSuccess) return e;
     int occ = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_insert<AGG_BLOCK>, INS_THREADS, ins_smem);

@@ -30,6 +30,20 @@ def zipf_keys(n, n_ranks, s, seed, perm_seed, with_ranks=False, device="cuda", s
     return (keys, ranks) if with_ranks else keys
 
 
+def class_keys(n, seed, perm_seed, n_class=1 << 16, s_class=1.0, s_suffix=1.2, device="cuda", stream=None):
+    """class << 16 | suffix keys of the learned-split workload."""
+    keys = torch.empty(n, dtype=torch.uint32, device=device)
+    check(lib.qs_gen_class_keys(seed, n_class, float(s_class), float(s_suffix), perm_seed, keys.data_ptr(), n,
+                                _s(stream)), "class_keys")
+    return keys
+
+
+def exact_counts(keys):
+    """Distinct keys (ascending) and their exact counts (torch sort/unique on the device)."""
+    u, c = torch.unique(keys.to(torch.int64), return_counts=True)
+    return u.to(torch.uint32), c.to(torch.uint32)
+
+
 def rank_keys(perm_seed, first, n, device="cuda", stream=None):
     """The distinct keys of ranks [first, first+n) of a zipf_keys stream."""
     keys = torch.empty(n, dtype=torch.uint32, device=device)

@@ -1,0 +1,94 @@
+"""GPU tests of the learned heavy-hitter split: the classifier's forward and gradients against
+the CPU oracle (oracle/mlp.py), training, and the end-to-end gain over the plain sketch at
+equal bytes."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from oracle import mlp
+from qsketch_b200 import data
+from qsketch_b200.learned import LearnedSketch, plain_equal_bytes
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(1e-30, np.linalg.norm(b)))
+
+
+@pytest.fixture(scope="module")
+def net(gpu):
+    # a warm-up longer than anything inserted here: the network is driven directly
+    return LearnedSketch(budget_bytes=4 << 20, table_slots=1 << 12, warmup_keys=1 << 30)
+
+
+def test_forward_matches_oracle(net):
+    p = mlp.init_params(5)
+    net.set_mlp_params(p)
+    keys = data.uniform_keys(3000, seed=3)
+    got = net.mlp_forward(keys).cpu().numpy()
+    want, _ = mlp.forward(p, keys.cpu().numpy(), emulate=True)
+    assert rel(got, want) < 2e-3
+    assert np.abs(got - want).max() < 0.02 * np.abs(want).max()
+    want32, _ = mlp.forward(p, keys.cpu().numpy(), emulate=False)
+    assert rel(got, want32) < 2e-2  # bf16 weights and activations vs fp32
+
+
+def test_gradients_match_oracle(net):
+    p = mlp.init_params(6)
+    net.set_mlp_params(p)
+    keys = data.uniform_keys(4096, seed=4)
+    rng = np.random.default_rng(7)
+    labels = torch.from_numpy((rng.random(4096) < 0.1).astype(np.uint8)).cuda()
+    g, loss = net.mlp_grads(keys, labels, 5.0)
+    want_loss, want = mlp.loss_and_grads(p, keys.cpu().numpy(), labels.cpu().numpy(), 5.0, emulate=True)
+    _, want32 = mlp.loss_and_grads(p, keys.cpu().numpy(), labels.cpu().numpy(), 5.0, emulate=False)
+    assert abs(loss - want_loss) <= 1e-3 * abs(want_loss)
+    blocks = {"W1": slice(0, 4096), "W2": slice(4096, 20480), "b1": slice(20480, 20608),
+              "b2": slice(20608, 20736), "w3": slice(20736, 20864), "b3": slice(20864, 20865)}
+    for name, sl in blocks.items():
+        assert rel(g[sl], want[sl]) < 2e-2, (name, rel(g[sl], want[sl]))   # same rounding points
+        assert rel(g[sl], want32[sl]) < 8e-2, (name, rel(g[sl], want32[sl]))  # vs plain fp32
+
+
+def test_training_learns_a_bit_rule(net):
+    net.set_mlp_params(mlp.init_params(8))
+    keys = data.uniform_keys(1 << 16, seed=9)
+    labels = ((keys.cpu().numpy() >> 28) == 0).astype(np.uint8)  # 1/16 positives
+    lab = torch.from_numpy(labels).cuda()
+    _, before = net.mlp_grads(keys, lab, 15.0)
+    after = net.mlp_train(keys, lab, epochs=8, batch=1024, lr=3e-3, pos_weight=15.0)
+    assert after < 0.5 * before
+    fresh = data.uniform_keys(1 << 14, seed=10)
+    z = net.mlp_forward(fresh).cpu().numpy()
+    truth = (fresh.cpu().numpy() >> 28) == 0
+    assert ((z > 0) == truth).mean() > 0.97
+
+
+def run_learned_vs_plain(n_keys, warmup, budget, table_slots, seed=5):
+    keys = data.class_keys(n_keys, seed=seed, perm_seed=11, n_class=1 << 12)
+    lk = LearnedSketch(budget_bytes=budget, table_slots=table_slots, warmup_keys=warmup, hash_seed=2654435769,
+                       max_batch=1 << 20, epochs=4)
+    lk.insert(keys)
+    plain = plain_equal_bytes(budget, hash_seed=2654435769)
+    plain.insert(keys)
+    uniq, exact = data.exact_counts(keys)
+    return lk, plain, uniq, exact, keys
+
+
+def test_learned_split_beats_plain_at_equal_bytes(gpu):
+    budget = 6 << 20
+    lk, plain, uniq, exact, keys = run_learned_vs_plain(1 << 22, 1 << 20, budget, 1 << 14)
+    info = lk.info()
+    assert info["trained"] == 1 and info["table_fill"] > 0
+    assert info["sketch_bytes"] + info["table_bytes"] + info["mlp_bytes"] <= budget
+    est_l = lk.search(uniq)
+    est_p = plain.search(uniq)
+    assert bool((est_l >= exact).all()) and bool((est_p >= exact).all())  # never below the truth
+    re_l, _ = data.error_metrics(est_l, exact)
+    re_p, _ = data.error_metrics(est_p, exact)
+    assert re_l < re_p, (re_l, re_p, info)
+    # deterministic: the same stream and parameters give the same estimates
+    lk2, _, _, _, _ = run_learned_vs_plain(1 << 22, 1 << 20, budget, 1 << 14)
+    assert torch.equal(lk2.search(uniq), est_l)
