@@ -240,8 +240,10 @@ qs_status qs_probe(uint32_t kind, uint64_t bytes, uint64_t ops, double *ops_per_
  * `heavy_fraction`, and the warm-up keys it predicts heavy are admitted to an exact
  * open-addressing table (u32 key + u32 count).  Afterwards each key found in the table counts
  * there exactly; every other key goes to the sketch, and keys the network predicts heavy are
- * admitted at the end of their chunk (in key order, while the table is below max fill).  A
- * query returns table count + sketch estimate.  Sketch, table and network share
+ * admitted at the end of their chunk.  The network decides which keys may enter the table;
+ * when more are eligible than the table holds (max fill), the sketch's own estimates rank
+ * them (ties by key), so admission is deterministic.  A query returns table count + sketch
+ * estimate.  Sketch, table and network share
  * `budget_bytes` (sketch low:high = 4:1). */
 typedef struct qs_learned_params {
     uint64_t budget_bytes;     /* default 64 MiB */

@@ -710,6 +710,7 @@ struct qs_learned {
     uint32_t* warm = nullptr;
     uint64_t warm_seen = 0;
     uint32_t* d_sorted = nullptr;   // admission order upload buffer
+    uint32_t* d_cand_est = nullptr; // sketch estimates of the chunk's candidates
     uint32_t admit_cap = 0;
     float* d_loss = nullptr;
     uint8_t* d_labels_tmp = nullptr;
@@ -854,14 +855,15 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     CKT(cudaMemcpyAsync(z.data(), d_logit, D * 4, cudaMemcpyDeviceToHost, st), "logit copy");
     CKT(cudaStreamSynchronize(st), "logit sync");
     uint64_t tp = 0, fp = 0, fn = 0;
-    std::vector<std::pair<float, uint32_t>> heavy;
+    std::vector<std::pair<double, uint32_t>> heavy;
     for (uint64_t i = 0; i < D; ++i) {
         const bool pred = z[i] > 0.0f;
         tp += pred && lab[i];
         fp += pred && !lab[i];
         fn += !pred && lab[i];
-        if (pred) heavy.push_back({-z[i], keys[i]});
+        if (pred) heavy.push_back({-(double)est[i], keys[i]});
     }
+    // the network decides who may enter the table; the sketch's own counts rank them
     std::sort(heavy.begin(), heavy.end());
     const uint32_t take = (uint32_t)std::min<uint64_t>(heavy.size(), lk->T.max_fill);
     std::vector<uint32_t> order(take);
@@ -964,12 +966,15 @@ qs_status qs_learned_create(const qs_learned_params* p, qs_learned** out) {
     CKB(lk->alloc(&R.cand_list, R.cand_slots), "candidate list");
     lk->admit_cap = std::max<uint32_t>(T.max_fill, R.cand_slots);
     CKB(lk->alloc(&lk->d_sorted, lk->admit_cap), "admission buffer");
+    CKB(lk->alloc(&lk->d_cand_est, lk->admit_cap), "candidate estimates");
     MlpDev& M = lk->M;
     CKB(lk->alloc(&M.params, MLP_PARAMS), "mlp params");
     CKB(lk->alloc(&M.grads, MLP_PARAMS), "mlp grads");
     CKB(lk->alloc(&M.adam_m, MLP_PARAMS), "adam m");
     CKB(lk->alloc(&M.adam_v, MLP_PARAMS), "adam v");
     CKB(lk->alloc(&M.W1, MLP_BF16_PARAMS), "mlp bf16");
+    CKB(lk->alloc(&M.partials, (uint64_t)MLP_MAX_TILES * MLP_PARAMS), "mlp partial gradients");
+    CKB(lk->alloc(&M.ploss, MLP_MAX_TILES), "mlp partial losses");
     M.W2 = M.W1 + MLP_W1_N;
     M.b1 = M.params + MLP_BF16_PARAMS;
     M.b2 = M.b1 + 128;
@@ -1046,10 +1051,18 @@ qs_status qs_learned_insert(qs_learned* lk, const uint32_t* d_keys, size_t n, vo
         CK(cudaStreamSynchronize(st), "candidate sync");
         if (ncand) {
             ncand = std::min(ncand, lk->R.cand_slots);
-            std::vector<uint32_t> cand(ncand);
-            CK(cudaMemcpy(cand.data(), lk->R.cand_list, ncand * 4, cudaMemcpyDeviceToHost), "candidate copy");
-            std::sort(cand.begin(), cand.end());
+            // rank the chunk's candidates by the sketch's estimate (ties by key), admit in order
+            std::vector<uint32_t> cand(ncand), cest(ncand);
+            s = query_device(lk->sk, lk->R.cand_list, ncand, lk->d_cand_est, st);
+            if (s != QS_OK) return s;
+            CK(cudaMemcpyAsync(cand.data(), lk->R.cand_list, ncand * 4, cudaMemcpyDeviceToHost, st), "candidate copy");
+            CK(cudaMemcpyAsync(cest.data(), lk->d_cand_est, ncand * 4, cudaMemcpyDeviceToHost, st), "estimate copy");
+            CK(cudaStreamSynchronize(st), "candidate sync");
+            std::vector<std::pair<int64_t, uint32_t>> order(ncand);
+            for (uint32_t i = 0; i < ncand; ++i) order[i] = {-(int64_t)cest[i], cand[i]};
+            std::sort(order.begin(), order.end());
             const uint32_t take = std::min<uint32_t>(ncand, lk->admit_cap);
+            for (uint32_t i = 0; i < take; ++i) cand[i] = order[i].second;
             CK(cudaMemcpy(lk->d_sorted, cand.data(), take * 4, cudaMemcpyHostToDevice), "admit upload");
             uint32_t before = 0, after = 0;
             CK(cudaMemcpy(&before, lk->T.fill, 4, cudaMemcpyDeviceToHost), "fill");

@@ -54,7 +54,10 @@ struct MlpDev {
     float* grads;       // same layout
     float *gW1, *gW2, *gb1, *gb2, *g3, *gb3;
     float *adam_m, *adam_v;
+    float* partials;    // MLP_MAX_TILES * MLP_PARAMS per-tile gradients (fixed-order reduction)
+    float* ploss;       // MLP_MAX_TILES tile losses
 };
+constexpr uint32_t MLP_MAX_TILES = 256;  // 64-example tiles per backward launch
 
 size_t mlp_smem_bytes();
 cudaError_t mlp_configure();

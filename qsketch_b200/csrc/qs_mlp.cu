@@ -169,100 +169,127 @@ __device__ __forceinline__ void gemm_aT_b(MlpSmem& S, const __nv_bfloat16* A, co
     }
 }
 
-// Gradients of the weighted BCE over a batch, accumulated (atomicAdd) into M.g*.
-// labels[i] in {0,1}; the loss sum goes to *loss (unnormalised, then divided by B).
+// Gradients of the weighted BCE over examples [tile0*64, ...): CTA b handles tile tile0+b and
+// writes its partial gradient (fp32, MLP_PARAMS) to partials + b*MLP_PARAMS and its loss sum
+// to ploss[b]; k_mlp_reduce then adds the partials in tile order, so the result does not
+// depend on scheduling.
 __global__ void __launch_bounds__(MLP_THREADS) k_mlp_backward(const uint32_t* __restrict__ keys,
                                                               const uint8_t* __restrict__ labels, uint64_t n,
-                                                              float pos_weight, float inv_batch, MlpDev M,
-                                                              float* loss) {
+                                                              uint64_t tile0, float pos_weight, float inv_batch,
+                                                              MlpDev M, float* __restrict__ partials,
+                                                              float* __restrict__ ploss) {
     extern __shared__ __align__(128) uint8_t smem_raw[];
     MlpSmem& S = *reinterpret_cast<MlpSmem*>(smem_raw);
-    load_weights(S, M);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (uint64_t base = (uint64_t)blockIdx.x * MLP_T; base < n; base += (uint64_t)gridDim.x * MLP_T) {
-        load_features(S, keys, base, n);
-        __syncthreads();
-        forward_tile(S, M);
-        // loss and dz
-        float lsum = 0.0f, dzsum = 0.0f;
-        if (tid < MLP_T) {
-            const uint64_t i = base + tid;
-            float dz = 0.0f;
-            if (i < n) {
-                const float z = S.z[tid];
-                const float y = labels[i] ? 1.0f : 0.0f;
-                const float w = labels[i] ? pos_weight : 1.0f;
-                const float p = 1.0f / (1.0f + __expf(-z));
-                // log(1+e^-|z|) form of the BCE
-                const float l = fmaxf(z, 0.0f) - z * y + log1pf(__expf(-fabsf(z)));
-                lsum = w * l;
-                dz = (p - y) * w * inv_batch;
-            }
-            S.dz[tid] = dz;
-            dzsum = dz;
+    float* G = partials + (uint64_t)blockIdx.x * MLP_PARAMS;
+    float* gW1 = G;
+    float* gW2 = G + MLP_W1_N;
+    float* gb1 = G + MLP_BF16_PARAMS;
+    float* gb2 = gb1 + MLP_H;
+    float* g3 = gb2 + MLP_H;
+    float* gb3 = g3 + MLP_H;
+    const uint64_t base = (tile0 + blockIdx.x) * MLP_T;
+    load_weights(S, M);
+    load_features(S, keys, base, n);
+    __syncthreads();
+    forward_tile(S, M);
+    // loss and dz
+    float lsum = 0.0f, dzsum = 0.0f;
+    if (tid < MLP_T) {
+        const uint64_t i = base + tid;
+        float dz = 0.0f;
+        if (i < n) {
+            const float z = S.z[tid];
+            const float y = labels[i] ? 1.0f : 0.0f;
+            const float w = labels[i] ? pos_weight : 1.0f;
+            const float p = 1.0f / (1.0f + __expf(-z));
+            const float l = fmaxf(z, 0.0f) - z * y + log1pf(__expf(-fabsf(z)));  // log(1+e^-|z|) form
+            lsum = w * l;
+            dz = (p - y) * w * inv_batch;
         }
-        if (warp < 2) {
+        S.dz[tid] = dz;
+        dzsum = dz;
+    }
+    __shared__ float s_red[2][2];
+    if (warp < 2) {
 #pragma unroll
-            for (int o = 16; o; o >>= 1) {
-                lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
-                dzsum += __shfl_xor_sync(0xffffffffu, dzsum, o);
-            }
-            if (lane == 0) {
-                atomicAdd(loss, lsum);
-                atomicAdd(M.gb3, dzsum);
-            }
+        for (int o = 16; o; o >>= 1) {
+            lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+            dzsum += __shfl_xor_sync(0xffffffffu, dzsum, o);
         }
-        __syncthreads();
-        // dh2, g3
-        for (int i = tid; i < MLP_T * MLP_H; i += blockDim.x) {
-            const int r = i / MLP_H, j = i % MLP_H;
-            const float h = __bfloat162float(S.H2[i]);
-            S.D2[i] = __float2bfloat16(h > 0.0f ? S.dz[r] * S.w3[j] : 0.0f);
+        if (lane == 0) {
+            s_red[warp][0] = lsum;
+            s_red[warp][1] = dzsum;
         }
-        for (int j = tid; j < MLP_H; j += blockDim.x) {
-            float g = 0.0f;
-            for (int r = 0; r < MLP_T; ++r) g += __bfloat162float(S.H2[r * MLP_H + j]) * S.dz[r];
-            atomicAdd(M.g3 + j, g);
-        }
-        __syncthreads();
-        // gb2 = colsum(dh2); gW2 = dh2^T h1
-        for (int j = tid; j < MLP_H; j += blockDim.x) {
-            float g = 0.0f;
-            for (int r = 0; r < MLP_T; ++r) g += __bfloat162float(S.D2[r * MLP_H + j]);
-            atomicAdd(M.gb2 + j, g);
-        }
-        gemm_aT_b<MLP_H>(S, S.D2, S.H1);
-        __syncthreads();
-        for (int i = tid; i < MLP_H * MLP_H; i += blockDim.x) atomicAdd(M.gW2 + i, S.F[i]);
-        __syncthreads();
-        // dh1 = (dh2 W2) * [h1 > 0]: B = W2 row-major [128][128] used as is
-        for (int t = warp; t < (MLP_T / 16) * (MLP_H / 16); t += MLP_THREADS / 32) {
-            const int tr = t / (MLP_H / 16), tc = t % (MLP_H / 16);
-            wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
-            wmma::fill_fragment(acc, 0.0f);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        ploss[blockIdx.x] = s_red[0][0] + s_red[1][0];
+        *gb3 = s_red[0][1] + s_red[1][1];
+    }
+    // dh2, g3
+    for (int i = tid; i < MLP_T * MLP_H; i += blockDim.x) {
+        const int r = i / MLP_H, j = i % MLP_H;
+        const float h = __bfloat162float(S.H2[i]);
+        S.D2[i] = __float2bfloat16(h > 0.0f ? S.dz[r] * S.w3[j] : 0.0f);
+    }
+    for (int j = tid; j < MLP_H; j += blockDim.x) {
+        float g = 0.0f;
+        for (int r = 0; r < MLP_T; ++r) g += __bfloat162float(S.H2[r * MLP_H + j]) * S.dz[r];
+        g3[j] = g;
+    }
+    __syncthreads();
+    // gb2 = colsum(dh2); gW2 = dh2^T h1
+    for (int j = tid; j < MLP_H; j += blockDim.x) {
+        float g = 0.0f;
+        for (int r = 0; r < MLP_T; ++r) g += __bfloat162float(S.D2[r * MLP_H + j]);
+        gb2[j] = g;
+    }
+    gemm_aT_b<MLP_H>(S, S.D2, S.H1);
+    __syncthreads();
+    for (int i = tid; i < MLP_H * MLP_H; i += blockDim.x) gW2[i] = S.F[i];
+    __syncthreads();
+    // dh1 = (dh2 W2) * [h1 > 0]: B = W2 row-major [128][128] used as is
+    for (int t = warp; t < (MLP_T / 16) * (MLP_H / 16); t += MLP_THREADS / 32) {
+        const int tr = t / (MLP_H / 16), tc = t % (MLP_H / 16);
+        wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
+        wmma::fill_fragment(acc, 0.0f);
 #pragma unroll
-            for (int k = 0; k < MLP_H; k += 16) {
-                wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> a;
-                wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> b;
-                wmma::load_matrix_sync(a, S.D2 + tr * 16 * MLP_H + k, MLP_H);
-                wmma::load_matrix_sync(b, S.W2 + k * MLP_H + tc * 16, MLP_H);
-                wmma::mma_sync(acc, a, b, acc);
-            }
-            wmma::store_matrix_sync(S.F + tr * 16 * MLP_H + tc * 16, acc, MLP_H, wmma::mem_row_major);
+        for (int k = 0; k < MLP_H; k += 16) {
+            wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> a;
+            wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> b;
+            wmma::load_matrix_sync(a, S.D2 + tr * 16 * MLP_H + k, MLP_H);
+            wmma::load_matrix_sync(b, S.W2 + k * MLP_H + tc * 16, MLP_H);
+            wmma::mma_sync(acc, a, b, acc);
         }
-        __syncthreads();
-        for (int i = tid; i < MLP_T * MLP_H; i += blockDim.x)
-            S.D1[i] = __float2bfloat16(__bfloat162float(S.H1[i]) > 0.0f ? S.F[i] : 0.0f);
-        __syncthreads();
-        for (int j = tid; j < MLP_H; j += blockDim.x) {
-            float g = 0.0f;
-            for (int r = 0; r < MLP_T; ++r) g += __bfloat162float(S.D1[r * MLP_H + j]);
-            atomicAdd(M.gb1 + j, g);
-        }
-        gemm_aT_b<MLP_IN>(S, S.D1, S.X);
-        __syncthreads();
-        for (int i = tid; i < MLP_H * MLP_IN; i += blockDim.x) atomicAdd(M.gW1 + i, S.F[i]);
-        __syncthreads();
+        wmma::store_matrix_sync(S.F + tr * 16 * MLP_H + tc * 16, acc, MLP_H, wmma::mem_row_major);
+    }
+    __syncthreads();
+    for (int i = tid; i < MLP_T * MLP_H; i += blockDim.x)
+        S.D1[i] = __float2bfloat16(__bfloat162float(S.H1[i]) > 0.0f ? S.F[i] : 0.0f);
+    __syncthreads();
+    for (int j = tid; j < MLP_H; j += blockDim.x) {
+        float g = 0.0f;
+        for (int r = 0; r < MLP_T; ++r) g += __bfloat162float(S.D1[r * MLP_H + j]);
+        gb1[j] = g;
+    }
+    gemm_aT_b<MLP_IN>(S, S.D1, S.X);
+    __syncthreads();
+    for (int i = tid; i < MLP_H * MLP_IN; i += blockDim.x) gW1[i] = S.F[i];
+}
+
+// grads += sum over tiles (in order) of the partial gradients; *loss += sum of the tile losses.
+__global__ void k_mlp_reduce(const float* __restrict__ partials, const float* __restrict__ ploss, uint32_t tiles,
+                             float* __restrict__ grads, float* __restrict__ loss) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < MLP_PARAMS; i += gridDim.x * blockDim.x) {
+        float s = grads[i];
+        for (uint32_t t = 0; t < tiles; ++t) s += partials[(uint64_t)t * MLP_PARAMS + i];
+        grads[i] = s;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        float s = *loss;
+        for (uint32_t t = 0; t < tiles; ++t) s += ploss[t];
+        *loss = s;
     }
 }
 
@@ -318,10 +345,13 @@ cudaError_t classify_misses(const MlpDev& M, const RouteDev& R, uint64_t max_mis
 
 cudaError_t mlp_backward(const uint32_t* d_keys, const uint8_t* d_labels, uint64_t n, float pos_weight,
                          float inv_batch, const MlpDev& M, float* d_loss, cudaStream_t st) {
-    if (n == 0) return cudaSuccess;
     const uint64_t tiles = (n + MLP_T - 1) / MLP_T;
-    const int grid = (int)std::min<uint64_t>(tiles, 148ull * 2);
-    k_mlp_backward<<<grid, MLP_THREADS, mlp_smem_bytes(), st>>>(d_keys, d_labels, n, pos_weight, inv_batch, M, d_loss);
+    for (uint64_t t0 = 0; t0 < tiles; t0 += MLP_MAX_TILES) {
+        const uint32_t nt = (uint32_t)std::min<uint64_t>(MLP_MAX_TILES, tiles - t0);
+        k_mlp_backward<<<nt, MLP_THREADS, mlp_smem_bytes(), st>>>(d_keys, d_labels, n, t0, pos_weight, inv_batch, M,
+                                                                   M.partials, M.ploss);
+        k_mlp_reduce<<<82, 256, 0, st>>>(M.partials, M.ploss, nt, M.grads, d_loss);
+    }
     return cudaGetLastError();
 }
 

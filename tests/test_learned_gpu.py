@@ -85,9 +85,11 @@ def test_learned_split_beats_plain_at_equal_bytes(gpu):
     assert info["sketch_bytes"] + info["table_bytes"] + info["mlp_bytes"] <= budget
     est_l = lk.search(uniq)
     est_p = plain.search(uniq)
-    assert bool((est_l >= exact).all()) and bool((est_p >= exact).all())  # never below the truth
+    ex = exact.to(torch.int64)
+    assert bool((est_l.to(torch.int64) >= ex).all()) and bool((est_p.to(torch.int64) >= ex).all())  # no undercount
     re_l, _ = data.error_metrics(est_l, exact)
     re_p, _ = data.error_metrics(est_p, exact)
+    print("learned vs plain avg relative error:", re_l, re_p, info)
     assert re_l < re_p, (re_l, re_p, info)
     # deterministic: the same stream and parameters give the same estimates
     lk2, _, _, _, _ = run_learned_vs_plain(1 << 22, 1 << 20, budget, 1 << 14)
