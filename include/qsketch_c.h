@@ -255,6 +255,8 @@ typedef struct qs_learned_params {
     uint32_t batch;            /* training batch, default 4096 */
     float lr;                  /* Adam step, default 2e-3 */
     float max_pos_weight;      /* positive-class weight cap, default 64 */
+    float eligible_recall;     /* the logit cut for table eligibility keeps this share of
+                                  the labelled-heavy warm-up keys, default 0.95 */
     uint32_t hash_seed;        /* sketch hash multiplier, 0 = draw from seed_rng */
     uint32_t seed_rng, mask_rng, init_seed;
     uint64_t max_batch;        /* keys per routing chunk, default 2^22 */
@@ -268,7 +270,7 @@ typedef struct qs_learned_info {
     uint64_t n_low, n_high, table_slots, table_fill;
     uint64_t warmup_keys, warmup_seen, train_examples, train_positives, admitted_after_warmup;
     uint32_t threshold, trained, epochs, steps;
-    float pos_weight, loss_first, loss_last, train_precision, train_recall;
+    float pos_weight, loss_first, loss_last, train_precision, train_recall, logit_threshold;
     double train_ms;
 } qs_learned_info;
 

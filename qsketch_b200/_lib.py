@@ -87,6 +87,7 @@ class qs_learned_params(ctypes.Structure):
         ("batch", ctypes.c_uint32),
         ("lr", ctypes.c_float),
         ("max_pos_weight", ctypes.c_float),
+        ("eligible_recall", ctypes.c_float),
         ("hash_seed", ctypes.c_uint32),
         ("seed_rng", ctypes.c_uint32),
         ("mask_rng", ctypes.c_uint32),
@@ -101,7 +102,8 @@ class qs_learned_info(ctypes.Structure):
         "budget_bytes", "sketch_bytes", "table_bytes", "mlp_bytes", "n_low", "n_high", "table_slots", "table_fill",
         "warmup_keys", "warmup_seen", "train_examples", "train_positives", "admitted_after_warmup")] + \
         [(n, ctypes.c_uint32) for n in ("threshold", "trained", "epochs", "steps")] + \
-        [(n, ctypes.c_float) for n in ("pos_weight", "loss_first", "loss_last", "train_precision", "train_recall")] + \
+        [(n, ctypes.c_float) for n in ("pos_weight", "loss_first", "loss_last", "train_precision", "train_recall",
+                                       "logit_threshold")] + \
         [("train_ms", ctypes.c_double)]
 
 

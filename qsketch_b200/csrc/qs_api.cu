@@ -854,10 +854,22 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     std::vector<float> z(D);
     CKT(cudaMemcpyAsync(z.data(), d_logit, D * 4, cudaMemcpyDeviceToHost, st), "logit copy");
     CKT(cudaStreamSynchronize(st), "logit sync");
+    // eligibility cut: the largest logit threshold that keeps `eligible_recall` of the
+    // labelled-heavy warm-up keys (the network filters, the sketch's counts rank)
+    std::vector<float> zpos;
+    for (uint64_t i = 0; i < D; ++i)
+        if (lab[i]) zpos.push_back(z[i]);
+    float zthr = 0.0f;
+    if (!zpos.empty()) {
+        std::sort(zpos.begin(), zpos.end());
+        const double miss = std::min(1.0, std::max(0.0, 1.0 - (double)lk->p.eligible_recall));
+        zthr = std::min(0.0f, zpos[(size_t)std::floor(miss * (double)(zpos.size() - 1))]);
+    }
+    lk->R.z_threshold = zthr;
     uint64_t tp = 0, fp = 0, fn = 0;
     std::vector<std::pair<double, uint32_t>> heavy;
     for (uint64_t i = 0; i < D; ++i) {
-        const bool pred = z[i] > 0.0f;
+        const bool pred = z[i] >= zthr;
         tp += pred && lab[i];
         fp += pred && !lab[i];
         fn += !pred && lab[i];
@@ -885,6 +897,7 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     I.loss_last = (float)loss;
     I.train_precision = tp + fp ? (float)tp / (float)(tp + fp) : 0.0f;
     I.train_recall = tp + fn ? (float)tp / (float)(tp + fn) : 0.0f;
+    I.logit_threshold = zthr;
     I.epochs = lk->p.epochs;
     I.steps = lk->adam_step;
     I.train_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -907,6 +920,7 @@ void qs_learned_params_default(qs_learned_params* p) {
     p->batch = 4096;
     p->lr = 2e-3f;
     p->max_pos_weight = 64.0f;
+    p->eligible_recall = 0.95f;
     p->seed_rng = 1;
     p->mask_rng = 1;
     p->init_seed = 1;

@@ -87,6 +87,7 @@ struct RouteDev {
     uint32_t cand_slots;    // power of two
     uint32_t* n_cand;
     uint32_t* cand_list;    // admitted-order list of candidates
+    float z_threshold;      // a key is a candidate when its logit is >= this
 };
 
 cudaError_t route_chunk(const uint32_t* d_keys, uint64_t n, const TableDev& T, const RouteDev& R, cudaStream_t st);

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(MLP_THREADS) k_mlp_forward(const uint32_t* __r
     }
 }
 
-// Classify the keys that missed the exact table; keys predicted heavy (z > 0) join the
+// Classify the keys that missed the exact table; keys predicted heavy (z >= threshold) join the
 // candidate set (deduplicated; order of arrival does not matter, admission sorts them).
 __global__ void __launch_bounds__(MLP_THREADS) k_mlp_classify(MlpDev M, RouteDev R, uint64_t max_misses) {
     extern __shared__ __align__(128) uint8_t smem_raw[];
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(MLP_THREADS) k_mlp_classify(MlpDev M, RouteDev
         load_features(S, R.misses, base, n);
         __syncthreads();
         forward_tile(S, M);
-        if (threadIdx.x < MLP_T && base + threadIdx.x < n && S.z[threadIdx.x] > 0.0f) {
+        if (threadIdx.x < MLP_T && base + threadIdx.x < n && S.z[threadIdx.x] >= R.z_threshold) {
             const uint32_t key = R.misses[base + threadIdx.x];
             if (key != 0xffffffffu) {
                 uint32_t h = mix32(key) & (R.cand_slots - 1);
