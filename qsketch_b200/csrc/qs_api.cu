@@ -716,6 +716,7 @@ struct qs_learned {
     uint8_t* d_labels_tmp = nullptr;
     qs_learned_info info{};
     uint32_t adam_step = 0;
+    bool table_full = false;  // no admission possible: routing skips the classifier
 
     template <class X>
     cudaError_t alloc(X** ptr, size_t count, int fill = 0) {
@@ -884,7 +885,10 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
         CKT(cudaMemcpy(lk->d_sorted, order.data(), take * 4, cudaMemcpyHostToDevice), "admit upload");
         CKT(table_admit(lk->T, lk->d_sorted, take, st), "admit");
     }
+    uint32_t fill = 0;
+    CKT(cudaMemcpyAsync(&fill, lk->T.fill, 4, cudaMemcpyDeviceToHost, st), "fill");
     CKT(cudaStreamSynchronize(st), "admit sync");
+    lk->table_full = fill >= lk->T.max_fill;
     cleanup();
 #undef CKT
     qs_learned_info& I = lk->info;
@@ -1057,9 +1061,13 @@ qs_status qs_learned_insert(qs_learned* lk, const uint32_t* d_keys, size_t n, vo
         uint64_t c = std::min<uint64_t>(n - off, lk->sk->max_batch);
         CK(cudaMemsetAsync(lk->R.n_misses, 0, 4, st), "misses reset");
         CK(route_chunk(d_keys + off, c, lk->T, lk->R, st), "route");
-        CK(classify_misses(lk->M, lk->R, c, st), "classify");
+        if (!lk->table_full) CK(classify_misses(lk->M, lk->R, c, st), "classify");
         qs_status s = insert_device(lk->sk, d_keys + off, c, st, lk->R.skip);
         if (s != QS_OK) return s;
+        if (lk->table_full) {
+            off += c;
+            continue;
+        }
         uint32_t ncand = 0;
         CK(cudaMemcpyAsync(&ncand, lk->R.n_cand, 4, cudaMemcpyDeviceToHost, st), "candidates");
         CK(cudaStreamSynchronize(st), "candidate sync");
@@ -1086,6 +1094,7 @@ qs_status qs_learned_insert(qs_learned* lk, const uint32_t* d_keys, size_t n, vo
             CK(cudaMemsetAsync(lk->R.n_cand, 0, 4, st), "candidate reset");
             CK(cudaStreamSynchronize(st), "admit sync");
             lk->info.admitted_after_warmup += after - before;
+            lk->table_full = after >= lk->T.max_fill;
         }
         off += c;
     }

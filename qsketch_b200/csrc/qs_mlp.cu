@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(MLP_THREADS) k_mlp_classify(MlpDev M, RouteDev
             const uint32_t key = R.misses[base + threadIdx.x];
             if (key != 0xffffffffu) {
                 uint32_t h = mix32(key) & (R.cand_slots - 1);
-                for (uint32_t p = 0; p < R.cand_slots; ++p, h = (h + 1) & (R.cand_slots - 1)) {
+                for (uint32_t p = 0; p < 64; ++p, h = (h + 1) & (R.cand_slots - 1)) {  // a full set drops
                     const uint32_t prev = atomicCAS(R.cand_keys + h, 0xffffffffu, key);
                     if (prev == 0xffffffffu) {
                         const uint32_t at = atomicAdd(R.n_cand, 1u);
