@@ -1,12 +1,16 @@
 #!/usr/bin/env python
 """QSketch insert/query throughput on B200 — one JSON line on rank 0.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config zipf|uniform]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config zipf|uniform|mixed|learned|zipf_prof]
 
 A step is one pass of the hot path over one batch of synthetic input: clear the sketch,
 insert the whole key stream, query the distinct keys.  The default workload is the
 Zipf-skewed stream (2^27 keys, Zipf s=1.1 over 2^24 ranks, 64 MB low table, 16 MB high
-pool, query the 2^24 distinct keys); `--config uniform` is the 2^24-key uniform case.
+pool, query the 2^24 distinct keys); `--config uniform` is the 2^24-key uniform case,
+`--config mixed` the HBM-bound interleaved insert/query stream, and `--config learned` the
+learned heavy-hitter split against the plain sketch at equal bytes (relative error of both,
+throughput with and without the warm-up/training phase).
 For N > 1 (torchrun, one process per GPU) every rank runs its own sketch over its own
 seeded stream: the path has no data exchange, so this is weak scaling with no collective
 on the data path.  `--impl reference` times the CPU restatement of the reference path
@@ -39,6 +43,11 @@ CONFIGS = {
     "mixed": dict(workload="mixed_2^28ops_batch2^20_90ins10qry_zipf0.8_2^26ranks_low256MB_high64MB", kind=2,
                   n_keys=1 << 28, n_ranks=1 << 26, s=0.8, n_low=8388593, n_high=1 << 19, n_query=0,
                   batch=1 << 20, insert_frac=0.9),
+    # learned heavy-hitter split vs the plain sketch at equal bytes: 2^28 keys (class<<16)|suffix,
+    # class Zipf 1.0 over 2^16, suffix Zipf 1.2 over 2^16 permuted per class; 64 MB each form
+    "learned": dict(workload="class_keys_2^28_classZipf1.0_suffixZipf1.2_64MB_learned_vs_plain", kind=3,
+                    n_keys=1 << 28, n_ranks=0, s=0.0, budget=64 << 20, warmup=1 << 24, table_slots=1 << 17,
+                    n_low=0, n_high=0, n_query=0),
     # a smaller skewed case for Nsight Compute captures (key stream still larger than L2)
     "zipf_prof": dict(workload="zipf1.1_2^25keys_2^22ranks_low16MB_high4MB_query2^22", kind=1, n_keys=1 << 25,
                       n_ranks=1 << 22, s=1.1, n_low=524287, n_high=1 << 15, n_query=1 << 22),
@@ -144,14 +153,12 @@ def dist_setup(gpus):
     return world, rank, local
 
 
-def run_ours(args, cfg):
+def init_ranks(args):
+    """One process per GPU; returns (world, rank, local, barrier, max_over_ranks)."""
     import datetime
 
     import torch
     import torch.distributed as dist
-
-    import qsketch_b200 as qs
-    from qsketch_b200 import data
 
     world, rank, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
@@ -169,6 +176,20 @@ def run_ours(args, cfg):
         t = torch.tensor([x], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    return world, rank, local, barrier, max_over_ranks
+
+
+def run_ours(args, cfg):
+    import torch
+    import torch.distributed as dist
+
+    import qsketch_b200 as qs
+    from qsketch_b200 import data
+
+    if cfg["kind"] == 3:
+        return run_learned(args, cfg)
+    world, rank, local, barrier, max_over_ranks = init_ranks(args)
 
     stream = torch.cuda.current_stream()
     seed = 1000 + rank
@@ -356,6 +377,143 @@ def run_ours(args, cfg):
         dist.destroy_process_group()
 
 
+def run_learned(args, cfg):
+    """Learned split vs plain MSWS at equal bytes.  A step is: a fresh learned sketch (created
+    outside the timed events) takes the whole stream — warm-up inserts, training, routed
+    inserts — then answers the distinct keys.  The plain sketch with the same budget runs the
+    same step beside it."""
+    import torch
+    import torch.distributed as dist
+
+    from qsketch_b200 import data
+    from qsketch_b200.learned import LearnedSketch, plain_equal_bytes
+
+    world, rank, local, barrier, max_over_ranks = init_ranks(args)
+    stream = torch.cuda.current_stream()
+    n, warm = cfg["n_keys"], cfg["warmup"]
+    keys = data.class_keys(n, seed=5 + rank, perm_seed=11 + 7919 * rank)
+    uniq, exact = data.exact_counts(keys)
+    n_q = uniq.numel()
+    out_l = torch.empty(n_q, dtype=torch.uint32, device="cuda")
+    out_p = torch.empty_like(out_l)
+    params = dict(budget_bytes=cfg["budget"], warmup_keys=warm, table_slots=cfg["table_slots"], hash_seed=SEED)
+    plain = plain_equal_bytes(cfg["budget"], hash_seed=SEED)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def learned_step(e):
+        lk = LearnedSketch(**params)
+        torch.cuda.synchronize()
+        e[0].record(stream)
+        lk.insert(keys[:warm])
+        e[1].record(stream)
+        lk.insert(keys[warm:])
+        e[2].record(stream)
+        lk.search(uniq, counts=out_l)
+        e[3].record(stream)
+        torch.cuda.synchronize()
+        return lk
+
+    def plain_step(e):
+        plain.clear()
+        e[0].record(stream)
+        plain.insert(keys)
+        e[1].record(stream)
+        plain.search(uniq, counts=out_p)
+        e[2].record(stream)
+
+    for _ in range(args.warmup):
+        learned_step([ev() for _ in range(4)]).close()
+        plain_step([ev() for _ in range(3)])
+    torch.cuda.synchronize()
+    le = [[ev() for _ in range(4)] for _ in range(args.steps)]
+    pe = [[ev() for _ in range(3)] for _ in range(args.steps)]
+    lk = None
+    with Clocks(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            if lk is not None:
+                lk.close()
+            lk = learned_step(le[i])
+        for i in range(args.steps):
+            plain_step(pe[i])
+        torch.cuda.synchronize()
+        barrier()
+    K = args.steps
+    warm_ms = max_over_ranks(sum(e[0].elapsed_time(e[1]) for e in le) / K)
+    rest_ms = max_over_ranks(sum(e[1].elapsed_time(e[2]) for e in le) / K)
+    lq_ms = max_over_ranks(sum(e[2].elapsed_time(e[3]) for e in le) / K)
+    p_ins_ms = max_over_ranks(sum(e[0].elapsed_time(e[1]) for e in pe) / K)
+    p_q_ms = max_over_ranks(sum(e[1].elapsed_time(e[2]) for e in pe) / K)
+    ms_per_step = warm_ms + rest_ms + lq_ms
+    info = lk.info()
+    re_l, ratio_l = data.error_metrics(out_l, exact)
+    re_p, ratio_p = data.error_metrics(out_p, exact)
+
+    # end to end: keys from pinned host memory, counts back to the host, inside the timed region
+    hk = keys.cpu().pin_memory()
+    hu = uniq.cpu().pin_memory()
+    ho = torch.empty(n_q, dtype=torch.uint32).pin_memory()
+    dk = torch.empty_like(keys)
+    du = torch.empty_like(uniq)
+    lk.close()
+    lk2 = LearnedSketch(**params)
+    torch.cuda.synchronize()
+    barrier()
+    w0 = time.perf_counter()
+    dk.copy_(hk, non_blocking=True)
+    lk2.insert(dk)
+    du.copy_(hu, non_blocking=True)
+    lk2.search(du, counts=out_l)
+    ho.copy_(out_l, non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks((time.perf_counter() - w0) * 1e3)
+    lk2.close()
+
+    rest_keys = n - warm
+    achieved = rest_keys * INSERT_BYTES_PER_KEY / (rest_ms * 1e-3) / 1e9
+    hbm, peak_kind = peaks()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(world * (n + n_q) / (ms_per_step * 1e6), 4), "unit": "Gkeys/s",
+            "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 sketch, bf16/fp32 MLP",
+            "data": "synthetic: seeded (class<<16)|suffix keys, class Zipf 1.0, suffix Zipf 1.2 permuted per class",
+            "config": {"workload": cfg["workload"], "n_keys": n, "n_query": n_q, "budget_bytes": cfg["budget"],
+                       "warmup_keys": warm, "table_slots": cfg["table_slots"],
+                       "l2": "key stream of %d MB per step > 126 MB L2" % (n * 4 >> 20),
+                       "parallelism": "independent sketch per GPU" if world > 1 else "single GPU"},
+            "avg_rel_error": re_l, "avg_rel_error_plain": re_p, "re_ratio_learned_over_plain": re_l / re_p,
+            "mean_est_over_exact": ratio_l, "mean_est_over_exact_plain": ratio_p,
+            "learned": {"warmup_and_train_ms": round(warm_ms, 3), "routed_insert_ms": round(rest_ms, 3),
+                        "routed_insert_gkeys_per_s": round(world * rest_keys / (rest_ms * 1e6), 4),
+                        "whole_stream_insert_gkeys_per_s": round(world * n / ((warm_ms + rest_ms) * 1e6), 4),
+                        "query_gkeys_per_s": round(world * n_q / (lq_ms * 1e6), 4),
+                        "train_ms": round(info["train_ms"], 2), "table_fill": info["table_fill"],
+                        "train_precision": info["train_precision"], "train_recall": info["train_recall"],
+                        "sketch_bytes": info["sketch_bytes"], "table_bytes": info["table_bytes"],
+                        "mlp_bytes": info["mlp_bytes"]},
+            "plain": {"insert_gkeys_per_s": round(world * n / (p_ins_ms * 1e6), 4),
+                      "query_gkeys_per_s": round(world * n_q / (p_q_ms * 1e6), 4),
+                      "value": round(world * (n + n_q) / ((p_ins_ms + p_q_ms) * 1e6), 4)},
+            "e2e": {"value": round(world * (n + n_q) / (e2e_ms * 1e6), 4), "unit": "Gkeys/s",
+                    "h2d_bytes_per_step": (n + n_q) * 4, "d2h_bytes_per_step": n_q * 4,
+                    "ms_per_step": round(e2e_ms, 3), "api": "qs_learned_insert + qs_learned_query"},
+            "gpu_launches": None,
+            "roofline": {"bound": "hbm", "kernel": "routed insert (k_route + k_msws_insert + k_msws_repair)",
+                         "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4), "traffic": None, "peak_source": peak_kind,
+                         "bytes_per_unit": INSERT_BYTES_PER_KEY, "units": rest_keys},
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    plain.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 # ---------------------------------------------------------------------------------------
 def host_zipf_keys(n, n_ranks, s, seed):
     """Bounded Zipf(s) over n_ranks by inverse CDF (numpy), ranks mapped by a seeded bijection."""
@@ -404,6 +562,10 @@ def cpu_baseline(cfg, keys, queries):
 def run_reference(args, cfg):
     world, rank, _ = dist_setup(args.gpus)
     if rank != 0:
+        return
+    if cfg["kind"] == 3:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned heavy-hitter split; "
+                          "its plain path is timed under --config zipf, uniform and mixed"}), flush=True)
         return
     threads = os.cpu_count() or 1
     ni = min(cfg["n_keys"], 1 << 24)

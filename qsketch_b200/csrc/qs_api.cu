@@ -1060,6 +1060,7 @@ qs_status qs_learned_insert(qs_learned* lk, const uint32_t* d_keys, size_t n, vo
         // route a chunk: table hits count exactly and are skipped by the sketch insert
         uint64_t c = std::min<uint64_t>(n - off, lk->sk->max_batch);
         CK(cudaMemsetAsync(lk->R.n_misses, 0, 4, st), "misses reset");
+        lk->R.collect = lk->table_full ? 0u : 1u;
         CK(route_chunk(d_keys + off, c, lk->T, lk->R, st), "route");
         if (!lk->table_full) CK(classify_misses(lk->M, lk->R, c, st), "classify");
         qs_status s = insert_device(lk->sk, d_keys + off, c, st, lk->R.skip);

@@ -88,6 +88,7 @@ struct RouteDev {
     uint32_t* n_cand;
     uint32_t* cand_list;    // admitted-order list of candidates
     float z_threshold;      // a key is a candidate when its logit is >= this
+    uint32_t collect;       // k_route fills `misses` only while this is set
 };
 
 cudaError_t route_chunk(const uint32_t* d_keys, uint64_t n, const TableDev& T, const RouteDev& R, cudaStream_t st);
