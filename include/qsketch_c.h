@@ -293,6 +293,64 @@ qs_status qs_mlp_grads(qs_learned *lk, const uint32_t *d_keys, const uint8_t *d_
 qs_status qs_mlp_train(qs_learned *lk, const uint32_t *d_keys, const uint8_t *d_labels, size_t n, uint32_t epochs,
                        uint32_t batch, float lr, float pos_weight, double *last_loss);
 
+/* ---- batched uneven streams (no counterpart in the reference) ---------------------------
+ * One handle owns n_streams independent MSWS sketches (stream s: n_low[s] low buckets,
+ * n_high[s] high buckets, hash multiplier seed[s]; one mask table for all) laid out in one
+ * table arena.  A call takes the keys of every stream at once as one flat device array and
+ * device offsets: stream s is d_keys[d_offsets[s] .. d_offsets[s+1]), offsets non-decreasing
+ * from d_offsets[0] = 0 (else QS_ERR_INVALID_ARG at the next sync), empty streams allowed.
+ * One persistent launch inserts all streams (tiles of one stream each, taken from a device
+ * work queue), followed by the ordered replay; each stream's result is that of inserting its
+ * keys alone, in order, into a qs_create'd sketch with the same n_low, n_high, seed and
+ * masks.  Long batches run in windows of max_batch keys.  The _graph variants record the
+ * whole launch sequence once per (d_keys, d_offsets, d_counts, max_total) in a CUDA graph and
+ * replay it; sizes are read on the device, so refill the same buffers and call again.
+ * Insert graphs take at most max_total <= max_batch keys (more latches QS_ERR_CAPACITY and
+ * the rest is not inserted). */
+typedef struct qs_batch_params {
+    uint32_t n_streams;           /* 1 .. 2^20 */
+    const uint64_t *n_low;        /* host [n_streams], each >= 1; sum < 2^32 */
+    const uint64_t *n_high;       /* host [n_streams], each >= 2; sum <= 2^30 */
+    const uint32_t *hash_seeds;   /* host [n_streams] or NULL: stream s takes draw s of seed_rng */
+    uint32_t seed_rng, mask_rng;
+    uint32_t hash_mask_table_sz;  /* default 1021 */
+    uint32_t hash_mask_ones;      /* default 3 */
+    const uint8_t *mask_table;    /* optional, hash_mask_table_sz*4 bytes */
+    uint32_t flags;               /* QS_FLAG_COMPAT_V3 */
+    uint32_t aggregate, route;    /* as qs_params */
+    uint64_t max_batch;           /* keys per window (replay scratch), default 2^22 */
+    int32_t device;
+} qs_batch_params;
+
+typedef struct qs_batch qs_batch;
+
+typedef struct qs_batch_info {
+    uint64_t n_streams, low_buckets, high_buckets, table_bytes, max_batch;
+    uint64_t inserts, queries, graph_launches, launches;
+    uint32_t graph_capture;       /* 1: CUDA-graph capture works here; 0: _graph calls run eagerly */
+    uint32_t streams_pool_full;   /* streams whose high pool ran out */
+} qs_batch_info;
+
+void qs_batch_params_default(qs_batch_params *p);
+qs_status qs_batch_create(const qs_batch_params *p, qs_batch **out);
+qs_status qs_batch_destroy(qs_batch *b);
+/* total = d_offsets[n_streams] as the host knows it (windows are planned from it). */
+qs_status qs_batch_insert(qs_batch *b, const uint32_t *d_keys, const uint64_t *d_offsets, uint64_t total,
+                          void *stream);
+qs_status qs_batch_query(qs_batch *b, const uint32_t *d_keys, const uint64_t *d_offsets, uint64_t total,
+                         uint32_t *d_counts, void *stream);
+qs_status qs_batch_insert_graph(qs_batch *b, const uint32_t *d_keys, const uint64_t *d_offsets, uint64_t max_total,
+                                void *stream);
+qs_status qs_batch_query_graph(qs_batch *b, const uint32_t *d_keys, const uint64_t *d_offsets, uint64_t max_total,
+                               uint32_t *d_counts, void *stream);
+qs_status qs_batch_clear(qs_batch *b, void *stream);
+/* Waits for `stream`; returns the first latched error (any stream's pool running out is
+ * QS_ERR_POOL_FULL; qs_batch_stream_status tells which). */
+qs_status qs_batch_sync(qs_batch *b, void *stream);
+qs_status qs_batch_stream_status(qs_batch *b, uint32_t *h_status /* [n_streams]: bit 0 pool full */);
+qs_status qs_batch_seeds(qs_batch *b, uint32_t *h_seeds /* [n_streams] */);
+qs_status qs_batch_get_info(qs_batch *b, qs_batch_info *out);
+
 /* ---- MSWS insert for callers that cannot allocate device memory ------------------------
  * No counterpart in the reference: its classes allocate their own tables
  * (device_sketch.h:83-114) and the harness allocates key buffers per batch.

@@ -107,6 +107,31 @@ class qs_learned_info(ctypes.Structure):
         [("train_ms", ctypes.c_double)]
 
 
+class qs_batch_params(ctypes.Structure):
+    _fields_ = [
+        ("n_streams", ctypes.c_uint32),
+        ("n_low", ctypes.c_void_p),
+        ("n_high", ctypes.c_void_p),
+        ("hash_seeds", ctypes.c_void_p),
+        ("seed_rng", ctypes.c_uint32),
+        ("mask_rng", ctypes.c_uint32),
+        ("hash_mask_table_sz", ctypes.c_uint32),
+        ("hash_mask_ones", ctypes.c_uint32),
+        ("mask_table", ctypes.c_void_p),
+        ("flags", ctypes.c_uint32),
+        ("aggregate", ctypes.c_uint32),
+        ("route", ctypes.c_uint32),
+        ("max_batch", ctypes.c_uint64),
+        ("device", ctypes.c_int32),
+    ]
+
+
+class qs_batch_info(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "n_streams", "low_buckets", "high_buckets", "table_bytes", "max_batch", "inserts", "queries",
+        "graph_launches", "launches")] + [("graph_capture", ctypes.c_uint32), ("streams_pool_full", ctypes.c_uint32)]
+
+
 QS_MLP_PARAMS = 20865
 
 # Every symbol include/qsketch_c.h declares, with its ctypes signature.
@@ -145,6 +170,18 @@ SIGNATURES = {
     "qs_error_metrics": (_I, [_P, _P, _SZ, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _P]),
     "qs_probe": (_I, [_U32, _U64, _U64, ctypes.POINTER(ctypes.c_double)]),
     "qs_msws_insert_noalloc": (_I, [_P, _U64, _P, _U64, _P, _P, _U32, _U32, _U32, _P, _SZ, _P]),
+    "qs_batch_params_default": (None, [ctypes.POINTER(qs_batch_params)]),
+    "qs_batch_create": (_I, [ctypes.POINTER(qs_batch_params), ctypes.POINTER(_P)]),
+    "qs_batch_destroy": (_I, [_P]),
+    "qs_batch_insert": (_I, [_P, _P, _P, _U64, _P]),
+    "qs_batch_query": (_I, [_P, _P, _P, _U64, _P, _P]),
+    "qs_batch_insert_graph": (_I, [_P, _P, _P, _U64, _P]),
+    "qs_batch_query_graph": (_I, [_P, _P, _P, _U64, _P, _P]),
+    "qs_batch_clear": (_I, [_P, _P]),
+    "qs_batch_sync": (_I, [_P, _P]),
+    "qs_batch_stream_status": (_I, [_P, _P]),
+    "qs_batch_seeds": (_I, [_P, _P]),
+    "qs_batch_get_info": (_I, [_P, ctypes.POINTER(qs_batch_info)]),
     "qs_learned_params_default": (None, [ctypes.POINTER(qs_learned_params)]),
     "qs_learned_create": (_I, [ctypes.POINTER(qs_learned_params), ctypes.POINTER(_P)]),
     "qs_learned_destroy": (_I, [_P]),

@@ -1180,3 +1180,332 @@ qs_status qs_mlp_train(qs_learned* lk, const uint32_t* d_keys, const uint8_t* d_
 }
 
 }  // extern "C"
+
+// ---- batched uneven streams ----------------------------------------------------------------
+// All streams' sketches live in one arena sketch (its low table, pool, masks, control block
+// and replay scratch); the batch adds the per-stream descriptors and the work-queue state.
+struct qs_batch {
+    qs_sketch* sk = nullptr;
+    uint32_t S = 0;
+    std::vector<uint32_t> seeds;
+    BatchDev B{};
+    cudaStream_t cap = nullptr;  // capture stream for the graph variants
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        const void* keys = nullptr;
+        const void* offs = nullptr;
+        const void* out = nullptr;
+        uint64_t max_total = 0;
+    } g[2];  // 0 insert, 1 query
+    int graph_ok = -1;  // -1 not tried, 1 works, 0 capture unsupported here
+    qs_batch_info info{};
+};
+
+namespace {
+
+qs_status batch_insert_seq(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets, uint64_t c0, uint64_t c1,
+                           bool strict, cudaStream_t st) {
+    qs_sketch* sk = b->sk;
+    BatchDev B = b->B;
+    B.key_off = d_offsets;
+    CK(batch_plan(B, sk->D.ctl, c0, c1, strict, st), "batch plan");
+    CK(batch_insert_pass(d_keys, sk->D, B, sk->L, sk->agg, st), "batch insert");
+    CK(batch_repair(d_keys + c0, sk->D, B, sk->L, st), "batch repair");
+    b->info.launches += 3;
+    return QS_OK;
+}
+
+qs_status batch_query_seq(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets, uint64_t total,
+                          uint32_t* d_counts, cudaStream_t st) {
+    qs_sketch* sk = b->sk;
+    BatchDev B = b->B;
+    B.key_off = d_offsets;
+    CK(batch_plan(B, sk->D.ctl, 0, total, false, st), "batch plan");
+    CK(batch_query(d_keys, d_counts, sk->D, B, sk->L, st), "batch query");
+    b->info.launches += 2;
+    return QS_OK;
+}
+
+// Record `seq` into graph slot k (unless it is already recorded for these buffers) and launch
+// it on `st`.  Returns false when capture does not work here; the caller then runs eagerly.
+template <class F>
+qs_status batch_graph(qs_batch* b, int k, const void* keys, const void* offs, const void* out, uint64_t max_total,
+                      cudaStream_t st, F seq, bool* ran) {
+    *ran = false;
+    if (b->graph_ok == 0) return QS_OK;
+    qs_batch::Graph& g = b->g[k];
+    if (!g.exec || g.keys != keys || g.offs != offs || g.out != out || g.max_total != max_total) {
+        if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
+        if (!b->cap) CK(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking), "capture stream");
+        const uint64_t launches = b->info.launches;
+        cudaError_t e = cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return cuda_fail(e, "begin capture");
+        const qs_status s = seq(b->cap);
+        cudaGraph_t graph = nullptr;
+        e = cudaStreamEndCapture(b->cap, &graph);
+        b->info.launches = launches;
+        cudaGraphExec_t exec = nullptr;
+        if (s == QS_OK && e == cudaSuccess && graph) e = cudaGraphInstantiate(&exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (s != QS_OK || e != cudaSuccess || !exec) {
+            cudaGetLastError();  // capture is not supported for this sequence: run eagerly from now on
+            b->graph_ok = 0;
+            return QS_OK;
+        }
+        b->graph_ok = 1;
+        g.exec = exec;
+        g.keys = keys;
+        g.offs = offs;
+        g.out = out;
+        g.max_total = max_total;
+    }
+    CK(cudaGraphLaunch(g.exec, st), "graph launch");
+    ++b->info.graph_launches;
+    *ran = true;
+    return QS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void qs_batch_params_default(qs_batch_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->seed_rng = 1;
+    p->mask_rng = 1;
+    p->hash_mask_table_sz = 1021;
+    p->hash_mask_ones = 3;
+    p->max_batch = 1ull << 22;
+    p->device = -1;
+}
+
+qs_status qs_batch_create(const qs_batch_params* p, qs_batch** out) {
+    if (!p || !out) return fail(QS_ERR_INVALID_ARG, "qs_batch_create: null argument");
+    *out = nullptr;
+    const uint32_t S = p->n_streams;
+    if (S == 0 || S > (1u << 20)) return fail(QS_ERR_INVALID_ARG, "n_streams out of [1, 2^20]");
+    if (!p->n_low || !p->n_high) return fail(QS_ERR_INVALID_ARG, "n_low and n_high arrays are required");
+    uint64_t tl = 0, th = 0;
+    for (uint32_t s = 0; s < S; ++s) {
+        if (p->n_low[s] == 0 || p->n_high[s] < 2) return fail(QS_ERR_INVALID_ARG, "stream %u: n_low >= 1 and n_high >= 2", s);
+        tl += p->n_low[s];
+        th += p->n_high[s];
+        if (tl > 0xffffffffull || th > (1ull << 30))
+            return fail(QS_ERR_INVALID_ARG, "total buckets exceed 2^32 - 1 low or 2^30 high");
+    }
+    qs_params ap;
+    qs_params_default(&ap);
+    ap.kind = QS_KIND_MSWS;
+    ap.n_low = tl;
+    ap.n_high = th;
+    ap.hash_seed = 1;  // the arena's own multiplier is not used: every stream has its own
+    ap.mask_rng = p->mask_rng;
+    ap.hash_mask_table_sz = p->hash_mask_table_sz;
+    ap.hash_mask_ones = p->hash_mask_ones;
+    ap.mask_table = p->mask_table;
+    ap.flags = p->flags;
+    ap.max_batch = p->max_batch;
+    ap.device = p->device;
+    ap.aggregate = p->aggregate;
+    ap.route = p->route;
+    qs_batch* b = new qs_batch();
+    qs_status s = qs_create(&ap, &b->sk);
+    if (s != QS_OK) {
+        delete b;
+        return s;
+    }
+    b->S = S;
+    auto bail = [&](qs_status st) {
+        qs_batch_destroy(b);
+        return st;
+    };
+    qs_sketch* sk = b->sk;
+    DeviceGuard guard(sk->device);
+    b->seeds.resize(S);
+    if (p->hash_seeds)
+        std::memcpy(b->seeds.data(), p->hash_seeds, (size_t)S * 4);
+    else
+        draw_seeds(p->seed_rng, S, b->seeds.data());
+    std::vector<StreamDesc> desc(S);
+    uint64_t lb = 0, hb = 0;
+    for (uint32_t i = 0; i < S; ++i) {
+        if (b->seeds[i] == 0) return bail(fail(QS_ERR_INVALID_ARG, "stream %u: hash seed 0", i));
+        desc[i].fm_low = make_fastmod((uint32_t)p->n_low[i]);
+        desc[i].seed = b->seeds[i];
+        desc[i].low_base = (uint32_t)lb;
+        desc[i].high_base = (uint32_t)hb;
+        desc[i].n_high = (uint32_t)p->n_high[i];
+        lb += p->n_low[i];
+        hb += p->n_high[i];
+    }
+    BatchDev& B = b->B;
+    B.n_streams = S;
+    StreamDesc* d_desc = nullptr;
+    CKB(sk->alloc(&d_desc, S), "alloc stream descriptors");
+    B.desc = d_desc;
+    CKB(sk->alloc(&B.lo, S), "alloc windows");
+    CKB(sk->alloc(&B.hi, S), "alloc windows");
+    CKB(sk->alloc(&B.item_off, (uint64_t)S + 1), "alloc work items");
+    CKB(sk->alloc(&B.win, 2), "alloc window");
+    CKB(sk->alloc(&B.work, 1), "alloc work queue");
+    CKB(sk->alloc(&B.next_id, S), "alloc allocators");
+    CKB(sk->alloc(&B.status, S), "alloc stream status");
+    CKB(cudaMemcpy(d_desc, desc.data(), (size_t)S * sizeof(StreamDesc), cudaMemcpyHostToDevice), "upload descriptors");
+    std::vector<uint32_t> first(S, FIRST_ID);
+    CKB(cudaMemcpy(B.next_id, first.data(), (size_t)S * 4, cudaMemcpyHostToDevice), "init allocators");
+    b->info.n_streams = S;
+    b->info.low_buckets = tl;
+    b->info.high_buckets = th;
+    b->info.table_bytes = tl * 32 + th * 128;
+    b->info.max_batch = sk->max_batch;
+    *out = b;
+    return QS_OK;
+}
+
+qs_status qs_batch_destroy(qs_batch* b) {
+    if (!b) return QS_OK;
+    if (b->sk) {
+        DeviceGuard guard(b->sk->device);
+        cudaDeviceSynchronize();
+        for (auto& g : b->g)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (b->cap) cudaStreamDestroy(b->cap);
+    }
+    qs_destroy(b->sk);
+    delete b;
+    return QS_OK;
+}
+
+static qs_status batch_args(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets) {
+    if (!b) return fail(QS_ERR_INVALID_ARG, "null batch");
+    if (!d_keys || !d_offsets) return fail(QS_ERR_INVALID_ARG, "null keys or offsets");
+    if ((reinterpret_cast<uintptr_t>(d_keys) & 3u) || (reinterpret_cast<uintptr_t>(d_offsets) & 7u))
+        return fail(QS_ERR_INVALID_ARG, "keys must be 4-byte and offsets 8-byte aligned");
+    return QS_OK;
+}
+
+qs_status qs_batch_insert(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets, uint64_t total,
+                          void* stream) {
+    qs_status s = batch_args(b, d_keys, d_offsets);
+    if (s != QS_OK || total == 0) return s;
+    DeviceGuard guard(b->sk->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const uint64_t mb = b->sk->max_batch;
+    for (uint64_t c0 = 0; c0 < total; c0 += mb) {
+        s = batch_insert_seq(b, d_keys, d_offsets, c0, std::min(total, c0 + mb), false, st);
+        if (s != QS_OK) return s;
+    }
+    ++b->info.inserts;
+    return QS_OK;
+}
+
+qs_status qs_batch_query(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets, uint64_t total,
+                         uint32_t* d_counts, void* stream) {
+    qs_status s = batch_args(b, d_keys, d_offsets);
+    if (s != QS_OK || total == 0) return s;
+    if (!d_counts) return fail(QS_ERR_INVALID_ARG, "null counts");
+    if (total > (uint64_t)0xffffffffu * 2048u) return fail(QS_ERR_CAPACITY, "query batch too large");
+    DeviceGuard guard(b->sk->device);
+    s = batch_query_seq(b, d_keys, d_offsets, total, d_counts, static_cast<cudaStream_t>(stream));
+    if (s == QS_OK) ++b->info.queries;
+    return s;
+}
+
+qs_status qs_batch_insert_graph(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets, uint64_t max_total,
+                                void* stream) {
+    qs_status s = batch_args(b, d_keys, d_offsets);
+    if (s != QS_OK || max_total == 0) return s;
+    if (max_total > b->sk->max_batch)
+        return fail(QS_ERR_CAPACITY, "insert graph: max_total %llu exceeds max_batch %llu",
+                    (unsigned long long)max_total, (unsigned long long)b->sk->max_batch);
+    DeviceGuard guard(b->sk->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    bool ran = false;
+    s = batch_graph(b, 0, d_keys, d_offsets, nullptr, max_total, st,
+                    [&](cudaStream_t cs) { return batch_insert_seq(b, d_keys, d_offsets, 0, max_total, true, cs); },
+                    &ran);
+    if (s == QS_OK && !ran) s = batch_insert_seq(b, d_keys, d_offsets, 0, max_total, true, st);
+    if (s == QS_OK) ++b->info.inserts;
+    return s;
+}
+
+qs_status qs_batch_query_graph(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets, uint64_t max_total,
+                               uint32_t* d_counts, void* stream) {
+    qs_status s = batch_args(b, d_keys, d_offsets);
+    if (s != QS_OK || max_total == 0) return s;
+    if (!d_counts) return fail(QS_ERR_INVALID_ARG, "null counts");
+    if (max_total > (uint64_t)0xffffffffu * 2048u) return fail(QS_ERR_CAPACITY, "query batch too large");
+    DeviceGuard guard(b->sk->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    bool ran = false;
+    s = batch_graph(b, 1, d_keys, d_offsets, d_counts, max_total, st,
+                    [&](cudaStream_t cs) { return batch_query_seq(b, d_keys, d_offsets, max_total, d_counts, cs); },
+                    &ran);
+    if (s == QS_OK && !ran) s = batch_query_seq(b, d_keys, d_offsets, max_total, d_counts, st);
+    if (s == QS_OK) ++b->info.queries;
+    return s;
+}
+
+qs_status qs_batch_clear(qs_batch* b, void* stream) {
+    if (!b) return fail(QS_ERR_INVALID_ARG, "null batch");
+    qs_status s = qs_clear(b->sk, stream);
+    if (s != QS_OK) return s;
+    DeviceGuard guard(b->sk->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::vector<uint32_t> first(b->S, FIRST_ID);
+    CK(cudaMemcpyAsync(b->B.next_id, first.data(), (size_t)b->S * 4, cudaMemcpyHostToDevice, st), "reset allocators");
+    CK(cudaMemsetAsync(b->B.status, 0, (size_t)b->S * 4, st), "reset stream status");
+    CK(cudaStreamSynchronize(st), "clear sync");  // the host vector above must outlive the copy
+    return QS_OK;
+}
+
+qs_status qs_batch_sync(qs_batch* b, void* stream) {
+    if (!b) return fail(QS_ERR_INVALID_ARG, "null batch");
+    DeviceGuard guard(b->sk->device);
+    CK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "stream sync");
+    Ctl c;
+    CK(cudaMemcpy(&c, b->sk->D.ctl, sizeof c, cudaMemcpyDeviceToHost), "read status");
+    if (c.status & ST_BAD_OFFSETS) return fail(QS_ERR_INVALID_ARG, "batch offsets are not non-decreasing from 0");
+    if (c.status & ST_TIMEOUT) return fail(QS_ERR_TIMEOUT, "a bounded device wait timed out");
+    if (c.status & ST_CAPACITY) return fail(QS_ERR_CAPACITY, "batch larger than its window or flag list");
+    std::vector<uint32_t> st(b->S);
+    CK(cudaMemcpy(st.data(), b->B.status, (size_t)b->S * 4, cudaMemcpyDeviceToHost), "read stream status");
+    uint32_t full = 0;
+    for (uint32_t v : st) full += (v & ST_POOL_FULL) ? 1u : 0u;
+    if (full)
+        return fail(QS_ERR_POOL_FULL, "%u stream(s) ran out of high buckets (%llu keys dropped)", full,
+                    (unsigned long long)c.dropped);
+    return QS_OK;
+}
+
+qs_status qs_batch_stream_status(qs_batch* b, uint32_t* h_status) {
+    if (!b || !h_status) return fail(QS_ERR_INVALID_ARG, "null argument");
+    DeviceGuard guard(b->sk->device);
+    CK(cudaDeviceSynchronize(), "status sync");
+    CK(cudaMemcpy(h_status, b->B.status, (size_t)b->S * 4, cudaMemcpyDeviceToHost), "read stream status");
+    return QS_OK;
+}
+
+qs_status qs_batch_seeds(qs_batch* b, uint32_t* h_seeds) {
+    if (!b || !h_seeds) return fail(QS_ERR_INVALID_ARG, "null argument");
+    std::memcpy(h_seeds, b->seeds.data(), (size_t)b->S * 4);
+    return QS_OK;
+}
+
+qs_status qs_batch_get_info(qs_batch* b, qs_batch_info* out) {
+    if (!b || !out) return fail(QS_ERR_INVALID_ARG, "null argument");
+    std::vector<uint32_t> st(b->S);
+    qs_status s = qs_batch_stream_status(b, st.data());
+    if (s != QS_OK) return s;
+    *out = b->info;
+    out->graph_capture = b->graph_ok == 0 ? 0u : 1u;
+    out->streams_pool_full = 0;
+    for (uint32_t v : st) out->streams_pool_full += (v & ST_POOL_FULL) ? 1u : 0u;
+    return QS_OK;
+}
+
+}  // extern "C"

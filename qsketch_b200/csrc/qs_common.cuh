@@ -20,6 +20,7 @@ constexpr int HIGH_WORDS = 32;         // 128 B high bucket of u32 counters
 constexpr uint32_t ST_POOL_FULL = 1u;
 constexpr uint32_t ST_TIMEOUT = 2u;
 constexpr uint32_t ST_CAPACITY = 4u;
+constexpr uint32_t ST_BAD_OFFSETS = 8u;  // batched streams: offsets not non-decreasing from 0
 
 // Lemire-Kaser-Kurz direct remainder ("Faster Remainder by Direct Computation", 2019):
 // for d < 2^32 and M = ceil(2^64 / d), a % d == mulhi64(M * a mod 2^64, d) for all
@@ -89,6 +90,33 @@ struct MswsDev {
     uint32_t route;          // 0 adaptive, 1 preload, 2 fused (pass-1 routing)
     const uint32_t* skip;    // optional: bit i set = key i of the chunk is not for this sketch
     uint32_t max_tiles;      // tiles of REPAIR_TILE elements in a chunk
+};
+
+// Batched streams: many per-stream MSWS sketches share one low-table arena and one high
+// pool arena.  A stream's sketch is the bucket range [low_base, low_base + fm_low.d) of the
+// low arena and the id range (high_base + START, high_base + START + n_high) of the pool, so
+// a bucket or a high id is one global number and pass 1, the flag machinery and the
+// ordered replay work unchanged; only hashing and allocation read the stream's descriptor.
+struct StreamDesc {
+    FastMod fm_low;      // d = the stream's low bucket count
+    uint32_t seed;       // the stream's hash multiplier
+    uint32_t low_base;   // first bucket of the stream's sketch in the low arena
+    uint32_t high_base;  // global high id = high_base + the stream's own id (from FIRST_ID)
+    uint32_t n_high;     // the stream's pool size in buckets (own ids < START + n_high)
+};
+
+struct BatchDev {
+    const StreamDesc* desc;   // [n_streams]
+    const uint64_t* key_off;  // [n_streams + 1] caller's offsets: stream s = keys[off[s], off[s+1])
+    uint64_t* lo;             // [n_streams] window-clipped first key of each stream
+    uint64_t* hi;             // [n_streams] window-clipped end
+    uint32_t* item_off;       // [n_streams + 1] prefix of work items (key tiles) per stream
+    uint64_t* win;            // [2] the window [c0, c1) of the flat key array this call covers
+    uint32_t* work;           // work-queue head
+    uint32_t* next_id;        // [n_streams] per-stream bump allocators (from FIRST_ID)
+    uint32_t* status;         // [n_streams] latched ST_* bits per stream
+    uint32_t n_streams;       // 0: not a batch
+    uint32_t pad;
 };
 
 struct CmDev {

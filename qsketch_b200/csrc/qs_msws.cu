@@ -213,14 +213,16 @@ __device__ __forceinline__ uint32_t staged_rounds_fused(const MswsDev& D, const 
     return linked_keys;
 }
 
-// Up to 32 keys held one per lane (valid lanes: lane < cnt).
+// Up to 32 keys held one per lane (valid lanes: lane < cnt), all of one sketch: hash
+// multiplier `seed`, `fm_low.d` buckets starting at bucket `base` of the table.
 template <int AGG>
 __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& S, uint32_t key, int cnt,
-                                             bool use_table, int route, uint64_t idx) {
+                                             bool use_table, int route, uint64_t idx, uint32_t seed,
+                                             const FastMod& fm_low, uint32_t base) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const bool valid = lane < cnt && !(D.skip && ((__ldg(D.skip + (idx >> 5)) >> (idx & 31)) & 1u));
-    const uint32_t hv = key * D.seed;  // hash_mul_add, device_hash_function.h:6-18
-    const uint32_t b = fast_mod(D.fm_low, hv);
+    const uint32_t hv = key * seed;  // hash_mul_add, device_hash_function.h:6-18
+    const uint32_t b = base + fast_mod(fm_low, hv);
     const uint32_t m = S.masks[fast_mod(D.fm_mask, hv)];
     uint32_t c = valid ? 1u : 0u;
     if (AGG != AGG_NONE) {
@@ -253,8 +255,9 @@ __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& 
     __syncwarp();
 }
 
-// Merged linked keys of the tile: one red per selected high counter per distinct key.
-__device__ __forceinline__ void drain_table(const MswsDev& D, const InsShared& S) {
+// Merged linked keys of the tile: one red per selected high counter per distinct key (the
+// tile's keys share the hash multiplier `seed`).
+__device__ __forceinline__ void drain_table(const MswsDev& D, const InsShared& S, uint32_t seed) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint4* st = S.stage + wid * 32;
     for (int base = wid * 32; base < AGG_SLOTS; base += INS_THREADS) {
@@ -263,7 +266,7 @@ __device__ __forceinline__ void drain_table(const MswsDev& D, const InsShared& S
         const bool has = k != AGG_EMPTY;
         uint32_t m = 0, c = 0, id = 0;
         if (has) {
-            const uint32_t hv = k * D.seed;
+            const uint32_t hv = k * seed;
             m = S.masks[fast_mod(D.fm_mask, hv)];
             c = S.acnt[s];
             id = S.aid[s];
@@ -318,7 +321,7 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
     if (blockIdx.x == 0 && wid == 0 && head + tail > 0) {
         const uint32_t k = lane < (int)(head + tail) ? s_extra[lane] : 0u;
         const uint64_t idx = lane < (int)head ? (uint64_t)lane : head + body_n + (lane - head);
-        insert_group<AGG>(D, S, k, (int)(head + tail), false, ROUTE_PRELOAD, idx);
+        insert_group<AGG>(D, S, k, (int)(head + tail), false, ROUTE_PRELOAD, idx, D.seed, D.fm_low, 0u);
     }
 
     const uint64_t ntiles = (body_n + INS_TILE - 1) / INS_TILE;
@@ -358,7 +361,7 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
         for (int base = wid * 32; base < cnt; base += INS_THREADS) {
             const int c = min(32, cnt - base);
             const uint32_t k = lane < c ? tk[base + lane] : 0u;
-            insert_group<AGG>(D, S, k, c, true, route, head + g * INS_TILE + base + lane);
+            insert_group<AGG>(D, S, k, c, true, route, head + g * INS_TILE + base + lane, D.seed, D.fm_low, 0u);
         }
         __syncthreads();
         if (tid == 0) {  // adaptive: the next tile is fused while under 1/16 of the keys are linked
@@ -366,7 +369,7 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
             S.misc[1] = 0;
         }
         if (AGG == AGG_BLOCK) {
-            drain_table(D, S);
+            drain_table(D, S, D.seed);
             __syncthreads();
         }
         if (tid == 0 && i + INS_STAGES < my_tiles) {
@@ -421,6 +424,55 @@ __device__ __forceinline__ void phase_mark(Ctl* ctl, int k) {
         ctl->phase_t = now;
     }
 }
+
+// Batched streams: the stream of flat key index f (< key_off[n_streams]), i.e. the last s
+// with key_off[s] <= f, which is never an empty stream.
+__device__ __forceinline__ uint32_t stream_of_key(const BatchDev& B, uint64_t f) {
+    uint32_t lo = 0, hi = B.n_streams;  // key_off[lo] <= f < key_off[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(B.key_off + mid) <= f)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// The stream whose bucket range holds global bucket g (bases strictly increase).
+__device__ __forceinline__ uint32_t stream_of_bucket(const BatchDev& B, uint32_t g) {
+    uint32_t lo = 0, hi = B.n_streams;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(&B.desc[mid].low_base) <= g)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Hashing of the repair's key passes: one sketch, or a stream cursor over flat key indices
+// that only moves forward (a thread walks consecutive keys).
+template <bool BATCH>
+struct KeyHash {
+    uint32_t s = 0;
+    __device__ __forceinline__ void start(const BatchDev& B, uint64_t f) {
+        if (BATCH) s = stream_of_key(B, f);
+    }
+    __device__ __forceinline__ uint32_t bucket(const MswsDev& D, const BatchDev& B, uint64_t f, uint32_t key,
+                                               uint32_t& hv) {
+        if (!BATCH) {
+            hv = key * D.seed;
+            return fast_mod(D.fm_low, hv);
+        }
+        while (f >= __ldg(B.key_off + s + 1)) ++s;
+        const StreamDesc* sd = B.desc + s;
+        hv = key * __ldg(&sd->seed);
+        const FastMod fm{__ldg(&sd->fm_low.M), __ldg(&sd->fm_low.d), 0u};
+        return __ldg(&sd->low_base) + fast_mod(fm, hv);
+    }
+};
 
 struct RadixSmem {
     uint32_t whist[REPAIR_THREADS / 32][256];
@@ -506,8 +558,10 @@ __device__ __forceinline__ int link_step(uint32_t m, uint32_t& cur) {
 
 // Final words of bucket b.  found: a key switched it to the high level; n_after: keys at
 // or after that key; n_total: the bucket's keys in the chunk; mL: the switching key's mask.
-__device__ __forceinline__ void finish_bucket(const MswsDev& D, uint32_t b, bool found, uint32_t n_after,
-                                              uint32_t n_total, uint32_t T, uint32_t P, uint32_t cur, uint32_t mL) {
+template <bool BATCH>
+__device__ __forceinline__ void finish_bucket(const MswsDev& D, const BatchDev& B, uint32_t b, bool found,
+                                              uint32_t n_after, uint32_t n_total, uint32_t T, uint32_t P,
+                                              uint32_t cur, uint32_t mL) {
     Ctl* ctl = D.ctl;
     const int lane = threadIdx.x & 31;
     uint32_t* wp = D.low + (uint64_t)b * LOW_WORDS;
@@ -518,9 +572,23 @@ __device__ __forceinline__ void finish_bucket(const MswsDev& D, uint32_t b, bool
             if (lane < 8) H += __popc(mL & (0x01010101u << lane));
         }
         uint32_t id = 0;
-        if (lane == 0) id = atomicAdd(&ctl->next_id, 1u);
-        id = __shfl_sync(0xffffffffu, id, 0);
-        const bool ok = (uint64_t)(id - START) < D.n_high;
+        bool ok;
+        if (BATCH) {  // the stream's own allocator and pool bound; the id is global
+            uint32_t own = 0, s = 0;
+            if (lane == 0) {
+                s = stream_of_bucket(B, b);
+                own = atomicAdd(B.next_id + s, 1u);
+            }
+            own = __shfl_sync(0xffffffffu, own, 0);
+            s = __shfl_sync(0xffffffffu, s, 0);
+            ok = (uint64_t)(own - START) < __ldg(&B.desc[s].n_high);
+            id = own + __ldg(&B.desc[s].high_base);
+            if (!ok && lane == 0) atomicOr(B.status + s, ST_POOL_FULL);
+        } else {
+            if (lane == 0) id = atomicAdd(&ctl->next_id, 1u);
+            id = __shfl_sync(0xffffffffu, id, 0);
+            ok = (uint64_t)(id - START) < D.n_high;
+        }
         if (ok) {
             __stcg(D.high + (uint64_t)(id - START) * HIGH_WORDS + lane, H);
         } else if (lane == 0) {
@@ -543,8 +611,9 @@ __device__ __forceinline__ void finish_bucket(const MswsDev& D, uint32_t b, bool
 }
 
 // Replay slot s from its segment of the slot-sorted records.
-__device__ __forceinline__ void replay_slot(const MswsDev& D, const uint2* sorted, uint32_t s, uint32_t F, uint32_t K,
-                                            bool use_totals) {
+template <bool BATCH>
+__device__ __forceinline__ void replay_slot(const MswsDev& D, const BatchDev& B, const uint2* sorted, uint32_t s,
+                                            uint32_t F, uint32_t K, bool use_totals) {
     const int lane = threadIdx.x & 31;
     const uint32_t b = __ldcg(D.flag_list + s);
     const uint32_t beg = __ldcg(D.seg_beg + s);
@@ -566,11 +635,14 @@ __device__ __forceinline__ void replay_slot(const MswsDev& D, const uint2* sorte
             break;
         }
     }
-    finish_bucket(D, b, L != NONE, L != NONE ? end - L : 0u, end - beg, T, P, cur, mL);
+    finish_bucket<BATCH>(D, B, b, L != NONE, L != NONE ? end - L : 0u, end - beg, T, P, cur, mL);
 }
 
+// BATCH: the keys are the window of a batch's flat key array that starts at flat index
+// B.win[0]; n is read from the window (the launch's own n is ignored).
+template <bool BATCH>
 __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* __restrict__ keys, uint64_t n,
-                                                                MswsDev D) {
+                                                                MswsDev D, BatchDev B) {
     __shared__ RadixSmem rs;
     __shared__ uint32_t s_acc[2][LOW_COUNTERS];
     __shared__ uint32_t s_acc_slot[2];
@@ -581,6 +653,8 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     const uint32_t F = min(__ldcg(&ctl->n_flagged), D.flag_cap);
     if (F == 0) return;
     phase_mark(ctl, -1);
+    const uint64_t c0 = BATCH ? __ldcg(B.win) : 0ull;
+    if (BATCH) n = __ldcg(B.win + 1) - c0;
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     constexpr int NW = REPAIR_THREADS / 32;
@@ -614,12 +688,15 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
         const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
         uint32_t c = 0;
+        KeyHash<BATCH> kh;
+        if (base < n) kh.start(B, c0 + base);
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
             const uint64_t i = base + j;
             if (i < n && !(D.skip && ((__ldg(D.skip + (i >> 5)) >> (i & 31)) & 1u))) {
-                const uint32_t hv = __ldg(keys + i) * D.seed;
-                c += flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, hv)) != NONE ? 1u : 0u;
+                uint32_t hv;
+                const uint32_t b = kh.bucket(D, B, c0 + i, __ldg(keys + i), hv);
+                c += flagged_slot(D, skey, sval, use_set, b) != NONE ? 1u : 0u;
             }
         }
         uint32_t total;
@@ -639,15 +716,18 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     // Phase 3: stable write of (slot, mask) records in array order.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
         const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
-        uint32_t slots[PER];
+        uint32_t slots[PER], hvs[PER];
         uint32_t c = 0;
+        KeyHash<BATCH> kh;
+        if (base < n) kh.start(B, c0 + base);
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
             const uint64_t i = base + j;
             slots[j] = NONE;
+            hvs[j] = 0;
             if (i < n && !(D.skip && ((__ldg(D.skip + (i >> 5)) >> (i & 31)) & 1u))) {
-                const uint32_t hv = __ldg(keys + i) * D.seed;
-                slots[j] = flagged_slot(D, skey, sval, use_set, fast_mod(D.fm_low, hv));
+                const uint32_t b = kh.bucket(D, B, c0 + i, __ldg(keys + i), hvs[j]);
+                slots[j] = flagged_slot(D, skey, sval, use_set, b);
                 c += slots[j] != NONE ? 1u : 0u;
             }
         }
@@ -656,8 +736,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
             if (slots[j] != NONE) {
-                const uint32_t hv = __ldg(keys + base + j) * D.seed;
-                const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hv));
+                const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hvs[j]));
                 __stcg(D.rec[0] + pos, make_uint2(slots[j], mask));
                 ++pos;
             }
@@ -764,7 +843,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     phase_mark(ctl, 4);
 
     // Phase 6: replay each flagged bucket in array order, one warp per slot.
-    for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) replay_slot(D, sorted, s, F, K, true);
+    for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) replay_slot<BATCH>(D, B, sorted, s, F, K, true);
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 5);
     if (blockIdx.x == 0 && tid == 0) {
@@ -781,9 +860,10 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
 constexpr int QRY_THREADS = 256;
 constexpr int QRY_KPT = 4;
 
-__device__ __forceinline__ uint32_t msws_lookup(const MswsDev& D, const uint32_t* s_masks, uint32_t key) {
-    const uint32_t hv = key * D.seed;
-    const uint32_t b = fast_mod(D.fm_low, hv);
+__device__ __forceinline__ uint32_t msws_lookup(const MswsDev& D, const uint32_t* s_masks, uint32_t key,
+                                                uint32_t seed, const FastMod& fm_low, uint32_t base) {
+    const uint32_t hv = key * seed;
+    const uint32_t b = base + fast_mod(fm_low, hv);
     const uint32_t m = s_masks[fast_mod(D.fm_mask, hv)];
     const uint4* bp = reinterpret_cast<const uint4*>(D.low + (uint64_t)b * LOW_WORDS);
     const uint4 a = __ldg(bp), c = __ldg(bp + 1);
@@ -821,7 +901,7 @@ __global__ void __launch_bounds__(QRY_THREADS) k_msws_query(const uint32_t* __re
             k[j] = i < n ? __ldcs(keys + i) : 0u;
         }
 #pragma unroll
-        for (int j = 0; j < QRY_KPT; ++j) r[j] = msws_lookup(D, s_masks, k[j]);
+        for (int j = 0; j < QRY_KPT; ++j) r[j] = msws_lookup(D, s_masks, k[j], D.seed, D.fm_low, 0u);
 #pragma unroll
         for (int j = 0; j < QRY_KPT; ++j) {
             const uint64_t i = base + j * stride;
@@ -840,7 +920,7 @@ __global__ void __launch_bounds__(QRY_THREADS) k_learned_query(const uint32_t* _
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t key = __ldcs(keys + i);
-        uint32_t r = msws_lookup(D, s_masks, key);
+        uint32_t r = msws_lookup(D, s_masks, key, D.seed, D.fm_low, 0u);
         const int s = table_find(T.keys, T.slots, key);
         if (s >= 0) r += __ldcg(T.counts + s);
         __stcs(out + i, r);
@@ -854,6 +934,143 @@ cudaError_t learned_query(const uint32_t* d_keys, uint64_t n, const TableDev& T,
     const int grid = (int)std::min<uint64_t>((uint64_t)L.query_grid, std::max<uint64_t>(1ull, want));
     k_learned_query<<<grid, QRY_THREADS, (size_t)D.n_masks * 4, st>>>(d_keys, n, T, d_out, D);
     return cudaGetLastError();
+}
+
+// ---- batched streams -------------------------------------------------------------------
+// Many per-stream sketches (StreamDesc) in one arena.  A call covers the window [c0, c1) of
+// the caller's flat key array, stream s being keys[key_off[s], key_off[s+1]).  Work items
+// are tiles of at most INS_TILE keys of one stream; every size is read on the device, so
+// the launch sequence can be recorded once in a CUDA graph and replayed on new contents.
+
+// One block: clip the streams to the window, count their tiles, prefix-sum the counts,
+// reset the work queue.  Offsets that are not non-decreasing from 0 latch ST_BAD_OFFSETS
+// and empty the window; strict mode latches ST_CAPACITY if the keys run past c1.
+__global__ void __launch_bounds__(1024) k_batch_plan(BatchDev B, uint64_t c0, uint64_t c1, uint32_t strict,
+                                                     Ctl* ctl) {
+    const uint32_t S = B.n_streams;
+    bool bad = false;
+    for (uint32_t s = threadIdx.x; s < S; s += blockDim.x)
+        bad |= __ldcg(B.key_off + s + 1) < __ldcg(B.key_off + s);
+    bad = __syncthreads_or(bad) || __ldcg(B.key_off) != 0;
+    const uint64_t total = __ldcg(B.key_off + S);
+    const uint64_t e = bad ? c0 : umin64(c1, total);
+    const uint64_t b0 = umin64(c0, e);
+    for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
+        const uint64_t lo = umin64(e, max(__ldcg(B.key_off + s), b0));
+        const uint64_t hi = umin64(e, max(__ldcg(B.key_off + s + 1), lo));
+        B.lo[s] = lo;
+        B.hi[s] = hi;
+        B.item_off[s] = (uint32_t)((hi - lo + INS_TILE - 1) / INS_TILE);
+    }
+    __syncthreads();
+    const uint32_t items = block_scan_array(B.item_off, S);
+    if (threadIdx.x == 0) {
+        B.item_off[S] = items;
+        B.win[0] = b0;
+        B.win[1] = e;
+        *B.work = 0;
+        if (bad) atomicOr(&ctl->status, ST_BAD_OFFSETS);
+        if (strict && !bad && total > c1) atomicOr(&ctl->status, ST_CAPACITY);
+    }
+}
+
+// The stream of work item `it` (< item_off[n_streams]): the last s with item_off[s] <= it.
+__device__ __forceinline__ uint32_t stream_of_item(const BatchDev& B, uint32_t it) {
+    uint32_t lo = 0, hi = B.n_streams;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldcg(B.item_off + mid) <= it)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Pass 1 over a batch: a persistent grid pulls tiles from the work queue; a tile's keys
+// all belong to one stream, so they hash with its descriptor and the tile's shared-memory
+// merge table never mixes sketches.  Everything after hashing is the single-sketch pass 1.
+template <int AGG>
+__global__ void __launch_bounds__(INS_THREADS, 4) k_batch_insert(const uint32_t* __restrict__ keys, MswsDev D,
+                                                                 BatchDev B) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    const InsShared S = ins_carve(smem, D.n_masks);
+    __shared__ uint32_t s_item, s_stream;
+    const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
+    for (uint32_t i = tid; i < D.n_masks; i += blockDim.x) S.masks[i] = __ldg(D.masks + i);
+    for (int i = tid; i < AGG_SLOTS; i += blockDim.x) {
+        S.akey[i] = AGG_EMPTY;
+        S.acnt[i] = 0;
+    }
+    if (tid == 0) {
+        S.misc[0] = 0;
+        S.misc[1] = 0;
+        S.misc[2] = D.route == 2 ? ROUTE_FUSED : ROUTE_PRELOAD;
+    }
+    const uint32_t n_items = __ldcg(B.item_off + B.n_streams);
+    for (;;) {
+        if (tid == 0) {
+            const uint32_t it = atomicAdd(B.work, 1u);
+            s_item = it;
+            if (it < n_items) s_stream = stream_of_item(B, it);
+        }
+        __syncthreads();
+        const uint32_t it = s_item;
+        if (it >= n_items) break;
+        const uint32_t s = s_stream;
+        const StreamDesc* sd = B.desc + s;
+        const uint32_t seed = __ldg(&sd->seed), base = __ldg(&sd->low_base);
+        const FastMod fm{__ldg(&sd->fm_low.M), __ldg(&sd->fm_low.d), 0u};
+        const uint64_t t0 = __ldcg(B.lo + s) + (uint64_t)(it - __ldcg(B.item_off + s)) * INS_TILE;
+        const int cnt = (int)umin64(INS_TILE, __ldcg(B.hi + s) - t0);
+        const int route = (int)S.misc[2];
+        for (int b = wid * 32; b < cnt; b += INS_THREADS) {
+            const int c = min(32, cnt - b);
+            const uint32_t k = lane < c ? __ldcs(keys + t0 + b + lane) : 0u;
+            insert_group<AGG>(D, S, k, c, true, route, 0, seed, fm, base);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            if (D.route == 0) S.misc[2] = S.misc[1] * 16u < (uint32_t)cnt ? ROUTE_FUSED : ROUTE_PRELOAD;
+            S.misc[1] = 0;
+        }
+        if (AGG == AGG_BLOCK) drain_table(D, S, seed);
+        __syncthreads();
+    }
+    if (tid == 0 && S.misc[0]) atomicAdd(&D.ctl->dropped, (unsigned long long)S.misc[0]);
+}
+
+// Query over a batch: static tiles, each stream's keys with its own descriptor.
+__global__ void __launch_bounds__(QRY_THREADS) k_batch_query(const uint32_t* __restrict__ keys,
+                                                             uint32_t* __restrict__ out, MswsDev D, BatchDev B) {
+    extern __shared__ __align__(16) uint32_t s_masks[];
+    __shared__ uint32_t s_stream;
+    for (uint32_t i = threadIdx.x; i < D.n_masks; i += blockDim.x) s_masks[i] = __ldg(D.masks + i);
+    const uint32_t n_items = __ldcg(B.item_off + B.n_streams);
+    for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+        if (threadIdx.x == 0) s_stream = stream_of_item(B, it);
+        __syncthreads();
+        const uint32_t s = s_stream;
+        __syncthreads();
+        const StreamDesc* sd = B.desc + s;
+        const uint32_t seed = __ldg(&sd->seed), base = __ldg(&sd->low_base);
+        const FastMod fm{__ldg(&sd->fm_low.M), __ldg(&sd->fm_low.d), 0u};
+        const uint64_t t0 = __ldcg(B.lo + s) + (uint64_t)(it - __ldcg(B.item_off + s)) * INS_TILE;
+        const uint32_t cnt = (uint32_t)umin64(INS_TILE, __ldcg(B.hi + s) - t0);
+        constexpr int PER = INS_TILE / QRY_THREADS;
+        uint32_t k[PER];
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const uint32_t i = threadIdx.x + j * QRY_THREADS;
+            k[j] = i < cnt ? __ldcs(keys + t0 + i) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const uint32_t i = threadIdx.x + j * QRY_THREADS;
+            const uint32_t r = msws_lookup(D, s_masks, k[j], seed, fm, base);
+            if (i < cnt) __stcs(out + t0 + i, r);
+        }
+    }
 }
 
 // ---- launchers ----------------------------------------------------------------------------
@@ -876,14 +1093,28 @@ cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute((const void*)k_learned_query, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * 4);
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute((const void*)k_batch_query, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * 4);
+    if (e != cudaSuccess) return e;
+    const void* bfns[3] = {(const void*)k_batch_insert<AGG_NONE>, (const void*)k_batch_insert<AGG_WARP>,
+                           (const void*)k_batch_insert<AGG_BLOCK>};
+    for (const void* fn : bfns) {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msws_insert_smem(16384));
+        if (e != cudaSuccess) return e;
+    }
     int occ = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_insert<AGG_BLOCK>, INS_THREADS, ins_smem);
     if (e != cudaSuccess) return e;
     L->insert_grid = prop.multiProcessorCount * (occ > 0 ? occ : 1);
-    e = cudaFuncSetAttribute((const void*)k_msws_repair, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)msws_repair_smem());
+    for (const void* fn : {(const void*)k_msws_repair<false>, (const void*)k_msws_repair<true>}) {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msws_repair_smem());
+        if (e != cudaSuccess) return e;
+    }
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_repair<true>, REPAIR_THREADS, msws_repair_smem());
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_repair, REPAIR_THREADS, msws_repair_smem());
+    int occ_single = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_single, k_msws_repair<false>, REPAIR_THREADS,
+                                                      msws_repair_smem());
+    occ = std::min(occ, occ_single);
     if (e != cudaSuccess) return e;
     if (occ < 1) return cudaErrorInvalidConfiguration;
     L->repair_grid = prop.multiProcessorCount * (occ < 2 ? occ : 2);
@@ -909,9 +1140,44 @@ cudaError_t msws_insert_pass(const uint32_t* d_keys, uint64_t n, const MswsDev& 
 cudaError_t msws_repair(const uint32_t* d_keys, uint64_t n, const MswsDev& D, const MswsLaunch& L, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     MswsDev Dc = D;
-    void* args[] = {(void*)&d_keys, (void*)&n, (void*)&Dc};
-    return cudaLaunchCooperativeKernel((const void*)k_msws_repair, dim3(L.repair_grid), dim3(REPAIR_THREADS), args,
-                                       msws_repair_smem(), st);
+    BatchDev Bn{};
+    void* args[] = {(void*)&d_keys, (void*)&n, (void*)&Dc, (void*)&Bn};
+    return cudaLaunchCooperativeKernel((const void*)k_msws_repair<false>, dim3(L.repair_grid), dim3(REPAIR_THREADS),
+                                       args, msws_repair_smem(), st);
+}
+
+cudaError_t batch_plan(const BatchDev& B, Ctl* ctl, uint64_t c0, uint64_t c1, bool strict, cudaStream_t st) {
+    k_batch_plan<<<1, 1024, 0, st>>>(B, c0, c1, strict ? 1u : 0u, ctl);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_insert_pass(const uint32_t* d_keys, const MswsDev& D, const BatchDev& B, const MswsLaunch& L,
+                              int agg, cudaStream_t st) {
+    const size_t smem = msws_insert_smem(D.n_masks);
+    if (agg == AGG_BLOCK)
+        k_batch_insert<AGG_BLOCK><<<L.insert_grid, INS_THREADS, smem, st>>>(d_keys, D, B);
+    else if (agg == AGG_WARP)
+        k_batch_insert<AGG_WARP><<<L.insert_grid, INS_THREADS, smem, st>>>(d_keys, D, B);
+    else
+        k_batch_insert<AGG_NONE><<<L.insert_grid, INS_THREADS, smem, st>>>(d_keys, D, B);
+    return cudaGetLastError();
+}
+
+// d_window: the caller's flat key array advanced to the window start c0.
+cudaError_t batch_repair(const uint32_t* d_window, const MswsDev& D, const BatchDev& B, const MswsLaunch& L,
+                         cudaStream_t st) {
+    MswsDev Dc = D;
+    BatchDev Bc = B;
+    uint64_t n = 0;  // read from the window on the device
+    void* args[] = {(void*)&d_window, (void*)&n, (void*)&Dc, (void*)&Bc};
+    return cudaLaunchCooperativeKernel((const void*)k_msws_repair<true>, dim3(L.repair_grid), dim3(REPAIR_THREADS),
+                                       args, msws_repair_smem(), st);
+}
+
+cudaError_t batch_query(const uint32_t* d_keys, uint32_t* d_out, const MswsDev& D, const BatchDev& B,
+                        const MswsLaunch& L, cudaStream_t st) {
+    k_batch_query<<<L.query_grid, QRY_THREADS, (size_t)D.n_masks * 4, st>>>(d_keys, d_out, D, B);
+    return cudaGetLastError();
 }
 
 cudaError_t msws_query(const uint32_t* d_keys, uint64_t n, uint32_t* d_out, const MswsDev& D, const MswsLaunch& L,

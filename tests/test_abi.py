@@ -90,3 +90,22 @@ def test_create_without_device_reports_no_device():
     with pytest.raises(qs.QsError) as ei:
         qs.Sketch_GPU_Sub_Warp_Level(262139)
     assert ei.value.status in (_lib.QS_ERR_NO_DEVICE, _lib.QS_ERR_CUDA)
+
+
+def test_batch_bad_arguments_are_errors():
+    from qsketch_b200._lib import qs_batch_params
+    p = qs_batch_params()
+    _lib.lib.qs_batch_params_default(ctypes.byref(p))
+    assert p.hash_mask_table_sz == 1021 and p.hash_mask_ones == 3 and p.max_batch == 1 << 22
+    h = ctypes.c_void_p()
+    assert _lib.lib.qs_batch_create(ctypes.byref(p), ctypes.byref(h)) == _lib.QS_ERR_INVALID_ARG  # 0 streams
+    nl = np.array([1021, 0], np.uint64)
+    nh = np.array([64, 64], np.uint64)
+    p.n_streams, p.n_low, p.n_high = 2, nl.ctypes.data, nh.ctypes.data
+    assert _lib.lib.qs_batch_create(ctypes.byref(p), ctypes.byref(h)) == _lib.QS_ERR_INVALID_ARG  # n_low 0
+    nl[1] = 509
+    nh[1] = 1
+    assert _lib.lib.qs_batch_create(ctypes.byref(p), ctypes.byref(h)) == _lib.QS_ERR_INVALID_ARG  # n_high < 2
+    assert _lib.lib.qs_batch_insert(None, None, None, 10, None) == _lib.QS_ERR_INVALID_ARG
+    assert _lib.lib.qs_batch_query(None, None, None, 10, None, None) == _lib.QS_ERR_INVALID_ARG
+    assert _lib.lib.qs_batch_destroy(None) == _lib.QS_OK
