@@ -2,15 +2,16 @@
 """QSketch insert/query throughput on B200 — one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config zipf|uniform|mixed|learned|zipf_prof]
+                    [--config zipf|uniform|mixed|learned|batched|zipf_prof]
 
 A step is one pass of the hot path over one batch of synthetic input: clear the sketch,
 insert the whole key stream, query the distinct keys.  The default workload is the
 Zipf-skewed stream (2^27 keys, Zipf s=1.1 over 2^24 ranks, 64 MB low table, 16 MB high
 pool, query the 2^24 distinct keys); `--config uniform` is the 2^24-key uniform case,
-`--config mixed` the HBM-bound interleaved insert/query stream, and `--config learned` the
+`--config mixed` the HBM-bound interleaved insert/query stream, `--config learned` the
 learned heavy-hitter split against the plain sketch at equal bytes (relative error of both,
-throughput with and without the warm-up/training phase).
+throughput with and without the warm-up/training phase), and `--config batched` 512 uneven
+streams with one sketch each, inserted and queried as one batch.
 For N > 1 (torchrun, one process per GPU) every rank runs its own sketch over its own
 seeded stream: the path has no data exchange, so this is weak scaling with no collective
 on the data path.  `--impl reference` times the CPU restatement of the reference path
@@ -48,6 +49,11 @@ CONFIGS = {
     "learned": dict(workload="class_keys_2^28_classZipf1.0_suffixZipf1.2_64MB_learned_vs_plain", kind=3,
                     n_keys=1 << 28, n_ranks=0, s=0.0, budget=64 << 20, warmup=1 << 24, table_slots=1 << 17,
                     n_low=0, n_high=0, n_query=0),
+    # batched uneven streams: 512 per-stream sketches, lengths log-uniform in [2^10, 2^22],
+    # Zipf s ~ U[0.6, 1.4] over 2^20 ranks, sketch sizes log-uniform in [32 KB, 16 MB],
+    # n_low = prime <= bytes/32, high pool bytes/4; inserted and queried in one batch each
+    "batched": dict(workload="512_streams_len_2^10..2^22_zipf0.6..1.4_2^20ranks_sketch32KB..16MB_pool_bytes/4",
+                    kind=4, n_streams=512, n_keys=0, n_ranks=1 << 20, s=0.0, n_low=0, n_high=0, n_query=0),
     # a smaller skewed case for Nsight Compute captures (key stream still larger than L2)
     "zipf_prof": dict(workload="zipf1.1_2^25keys_2^22ranks_low16MB_high4MB_query2^22", kind=1, n_keys=1 << 25,
                       n_ranks=1 << 22, s=1.1, n_low=524287, n_high=1 << 15, n_query=1 << 22),
@@ -189,6 +195,8 @@ def run_ours(args, cfg):
 
     if cfg["kind"] == 3:
         return run_learned(args, cfg)
+    if cfg["kind"] == 4:
+        return run_batched(args, cfg)
     world, rank, local, barrier, max_over_ranks = init_ranks(args)
 
     stream = torch.cuda.current_stream()
@@ -514,6 +522,179 @@ def run_learned(args, cfg):
         dist.destroy_process_group()
 
 
+def run_batched(args, cfg):
+    """512 uneven streams, each with its own sketch, in one batch (qs_batch_*).  A step is:
+    clear every sketch, insert every stream, query every stream's keys.  Beside it: the same
+    streams through 512 separate sketches one call after another, and the latency of a small
+    serving batch eager vs replayed from a CUDA graph."""
+    import torch
+    import torch.distributed as dist
+
+    import qsketch_b200 as qs
+    from qsketch_b200 import data
+    from qsketch_b200.batch import BatchedSketches
+
+    world, rank, local, barrier, max_over_ranks = init_ranks(args)
+    stream = torch.cuda.current_stream()
+    S = cfg["n_streams"]
+    w = data.uneven_streams(S, seed=1000 + rank, n_ranks=cfg["n_ranks"])
+    keys, offs = w["keys"], w["offsets"]
+    total = keys.numel()
+    out = torch.empty(total, dtype=torch.uint32, device="cuda")
+    b = BatchedSketches(w["n_low"], w["n_high"], seed_rng=1 + rank, max_batch=1 << 22)
+
+    def step(ev=None):
+        b.clear()
+        if ev:
+            ev[0].record(stream)
+        b.insert(keys, offs, total)
+        if ev:
+            ev[1].record(stream)
+        b.search(keys, offs, total, counts=out)
+        if ev:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = b.info()["launches"]
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for i in range(args.steps):
+            step(evs[i])
+        t1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    K = args.steps
+    ms_per_step = max_over_ranks(t0.elapsed_time(t1)) / K
+    ins_ms = max_over_ranks(sum(e[0].elapsed_time(e[1]) for e in evs) / K)
+    q_ms = max_over_ranks(sum(e[1].elapsed_time(e[2]) for e in evs) / K)
+    launches = b.info()["launches"] - launches0
+    info = b.info()
+
+    # per-kernel times of one instrumented step
+    b.set_profiling(True)
+    step()
+    torch.cuda.synchronize()
+    prof = b.profile()
+    b.set_profiling(False)
+    hbm, peak_kind = peaks()
+    avg_ins = prof["insert_ms"] / max(1, prof["insert_timed"])
+    per_launch = total / max(1, prof["insert_timed"])
+    achieved = per_launch * INSERT_BYTES_PER_KEY / (avg_ins * 1e-3) / 1e9
+
+    # the same streams through separate sketches, one call after another (one pass)
+    alone = [qs.Sketch_GPU_Sub_Warp_Level(int(w["n_low"][s]), 8, int(w["n_high"][s]), 32,
+                                          hash_seed=int(sd), max_batch=1 << 20)
+             for s, sd in enumerate(b.seeds())]
+    off = offs.cpu().numpy()
+    out2 = torch.empty_like(out)
+
+    def alone_pass():
+        for s in range(S):
+            alone[s].clear()
+            alone[s].insert(keys[off[s]:off[s + 1]])
+            alone[s].search(keys[off[s]:off[s + 1]], counts=out2[off[s]:off[s + 1]])
+
+    alone_pass()
+    torch.cuda.synchronize()
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    alone_pass()
+    a1.record(stream)
+    torch.cuda.synchronize()
+    alone_ms = a0.elapsed_time(a1)
+    for sk in alone:
+        sk.close()
+
+    # serving latency: the first 1024 keys of every stream (2^19 keys), eager vs graph replay
+    nsv = np.minimum(w["lengths"], 1024)
+    sv_keys = torch.cat([keys[off[s]:off[s] + nsv[s]] for s in range(S)])
+    sv_offs = torch.tensor(np.concatenate([[0], np.cumsum(nsv)]), dtype=torch.int64, device="cuda")
+    sv_out = torch.empty_like(sv_keys)
+    bs = BatchedSketches(w["n_low"], w["n_high"], seed_rng=1 + rank, max_batch=1 << 20)
+
+    def serve(graph):
+        if graph:
+            bs.insert_graph(sv_keys, sv_offs)
+            bs.search_graph(sv_keys, sv_offs, sv_out)
+        else:
+            bs.insert(sv_keys, sv_offs, sv_keys.numel())
+            bs.search(sv_keys, sv_offs, sv_keys.numel(), counts=sv_out)
+
+    lat = {}
+    for graph in (False, True):
+        for _ in range(3):
+            serve(graph)
+        torch.cuda.synchronize()
+        reps = 20
+        h0 = time.perf_counter()
+        for _ in range(reps):
+            serve(graph)
+        torch.cuda.synchronize()
+        lat["graph" if graph else "eager"] = (time.perf_counter() - h0) * 1e3 / reps
+    graph_ok = bs.info()["graph_capture"]
+    bs.close()
+
+    # end to end: keys and offsets from pinned host memory, counts back, inside the timed region
+    hk = keys.cpu().pin_memory()
+    ho_offs = offs.cpu().pin_memory()
+    hout = torch.empty(total, dtype=torch.uint32).pin_memory()
+    dk = torch.empty_like(keys)
+    do = torch.empty_like(offs)
+    b.clear()
+    torch.cuda.synchronize()
+    barrier()
+    w0 = time.perf_counter()
+    dk.copy_(hk, non_blocking=True)
+    do.copy_(ho_offs, non_blocking=True)
+    b.insert(dk, do, total)
+    b.search(dk, do, total, counts=out)
+    hout.copy_(out, non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks((time.perf_counter() - w0) * 1e3)
+    status = b.status()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(world * 2 * total / (ms_per_step * 1e6), 4), "unit": "Gkeys/s",
+            "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic: per stream seeded Zipf(s) ranks by rejection-inversion mapped to distinct u32 keys",
+            "config": {"workload": cfg["workload"], "n_streams": S, "n_keys": total, "n_query": total,
+                       "table_bytes": int(info["table_bytes"]), "streams_pool_full": int(info["streams_pool_full"]),
+                       "l2": "key stream of %d MB and tables of %d MB per step > 126 MB L2"
+                             % (total * 4 >> 20, info["table_bytes"] >> 20),
+                       "parallelism": "independent batch per GPU" if world > 1 else "single GPU"},
+            "insert_gkeys_per_s": round(world * total / (ins_ms * 1e6), 4),
+            "query_gkeys_per_s": round(world * total / (q_ms * 1e6), 4),
+            "alone": {"ms": round(alone_ms, 3), "gkeys_per_s": round(2 * total / (alone_ms * 1e6), 4),
+                      "note": "the same streams through 512 separate sketches, one insert + one query call each"},
+            "serving_batch": {"keys": int(sv_keys.numel()), "eager_ms": round(lat["eager"], 4),
+                              "graph_ms": round(lat["graph"], 4), "graph_capture": int(graph_ok),
+                              "note": "insert + query of the first 1024 keys of every stream, host wall time"},
+            "status": int(status),
+            "e2e": {"value": round(world * 2 * total / (e2e_ms * 1e6), 4), "unit": "Gkeys/s",
+                    "h2d_bytes_per_step": total * 4 + (S + 1) * 8, "d2h_bytes_per_step": total * 4,
+                    "ms_per_step": round(e2e_ms, 3), "api": "qs_batch_insert + qs_batch_query"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "k_batch_insert", "achieved": round(achieved, 1), "peak": hbm,
+                         "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+                         "peak_source": peak_kind, "bytes_per_unit": INSERT_BYTES_PER_KEY,
+                         "units_per_launch": per_launch, "avg_launch_ms": round(avg_ins, 5)},
+            "kernel_ms_per_step": {"insert": round(prof["insert_ms"], 4), "repair": round(prof["repair_ms"], 4),
+                                   "query": round(prof["query_ms"], 4)},
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 # ---------------------------------------------------------------------------------------
 def host_zipf_keys(n, n_ranks, s, seed):
     """Bounded Zipf(s) over n_ranks by inverse CDF (numpy), ranks mapped by a seeded bijection."""
@@ -563,9 +744,10 @@ def run_reference(args, cfg):
     world, rank, _ = dist_setup(args.gpus)
     if rank != 0:
         return
-    if cfg["kind"] == 3:
-        print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned heavy-hitter split; "
-                          "its plain path is timed under --config zipf, uniform and mixed"}), flush=True)
+    if cfg["kind"] in (3, 4):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned heavy-hitter split "
+                          "and no batched multi-sketch path; its plain path is timed under --config zipf, "
+                          "uniform and mixed"}), flush=True)
         return
     threads = os.cpu_count() or 1
     ni = min(cfg["n_keys"], 1 << 24)

@@ -350,6 +350,9 @@ qs_status qs_batch_sync(qs_batch *b, void *stream);
 qs_status qs_batch_stream_status(qs_batch *b, uint32_t *h_status /* [n_streams]: bit 0 pool full */);
 qs_status qs_batch_seeds(qs_batch *b, uint32_t *h_seeds /* [n_streams] */);
 qs_status qs_batch_get_info(qs_batch *b, qs_batch_info *out);
+/* The arena sketch behind the batch, for qs_set_profiling / qs_get_profile / qs_get_stats
+ * (eager calls are timed per launch: insert = pass 1, repair, query); owned by the batch. */
+qs_sketch *qs_batch_arena(qs_batch *b);
 
 /* ---- MSWS insert for callers that cannot allocate device memory ------------------------
  * No counterpart in the reference: its classes allocate their own tables

@@ -182,6 +182,7 @@ SIGNATURES = {
     "qs_batch_stream_status": (_I, [_P, _P]),
     "qs_batch_seeds": (_I, [_P, _P]),
     "qs_batch_get_info": (_I, [_P, ctypes.POINTER(qs_batch_info)]),
+    "qs_batch_arena": (_P, [_P]),
     "qs_learned_params_default": (None, [ctypes.POINTER(qs_learned_params)]),
     "qs_learned_create": (_I, [ctypes.POINTER(qs_learned_params), ctypes.POINTER(_P)]),
     "qs_learned_destroy": (_I, [_P]),

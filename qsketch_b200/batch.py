@@ -119,6 +119,18 @@ class BatchedSketches:
         check(lib.qs_batch_get_info(self.handle, ctypes.byref(i)), "info")
         return {f: getattr(i, f) for f, _ in qs_batch_info._fields_}
 
+    def set_profiling(self, enable=True):
+        check(lib.qs_set_profiling(lib.qs_batch_arena(self.handle), 1 if enable else 0), "set_profiling")
+
+    def profile(self):
+        """Per-launch CUDA-event times of eager calls since the last read (qs_get_profile)."""
+        from ._lib import qs_profile
+        p = qs_profile()
+        check(lib.qs_get_profile(lib.qs_batch_arena(self.handle), ctypes.byref(p)), "profile")
+        d = {f: getattr(p, f) for f, _ in qs_profile._fields_}
+        d["repair_phase_ms"] = list(p.repair_phase_ms)
+        return d
+
     def close(self):
         if self._h:
             lib.qs_batch_destroy(self._h)

@@ -1203,25 +1203,32 @@ struct qs_batch {
 
 namespace {
 
+// `timed`: bracket the launches with the arena sketch's profiling events (not while capturing).
 qs_status batch_insert_seq(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets, uint64_t c0, uint64_t c1,
-                           bool strict, cudaStream_t st) {
+                           bool strict, cudaStream_t st, bool timed = true) {
     qs_sketch* sk = b->sk;
     BatchDev B = b->B;
     B.key_off = d_offsets;
     CK(batch_plan(B, sk->D.ctl, c0, c1, strict, st), "batch plan");
+    if (timed) CK(sk->prof_begin(0, st), "profile");
     CK(batch_insert_pass(d_keys, sk->D, B, sk->L, sk->agg, st), "batch insert");
+    if (timed) CK(sk->prof_end(0, st), "profile");
+    if (timed) CK(sk->prof_begin(1, st), "profile");
     CK(batch_repair(d_keys + c0, sk->D, B, sk->L, st), "batch repair");
+    if (timed) CK(sk->prof_end(1, st), "profile");
     b->info.launches += 3;
     return QS_OK;
 }
 
 qs_status batch_query_seq(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets, uint64_t total,
-                          uint32_t* d_counts, cudaStream_t st) {
+                          uint32_t* d_counts, cudaStream_t st, bool timed = true) {
     qs_sketch* sk = b->sk;
     BatchDev B = b->B;
     B.key_off = d_offsets;
     CK(batch_plan(B, sk->D.ctl, 0, total, false, st), "batch plan");
+    if (timed) CK(sk->prof_begin(2, st), "profile");
     CK(batch_query(d_keys, d_counts, sk->D, B, sk->L, st), "batch query");
+    if (timed) CK(sk->prof_end(2, st), "profile");
     b->info.launches += 2;
     return QS_OK;
 }
@@ -1426,7 +1433,7 @@ qs_status qs_batch_insert_graph(qs_batch* b, const uint32_t* d_keys, const uint6
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     bool ran = false;
     s = batch_graph(b, 0, d_keys, d_offsets, nullptr, max_total, st,
-                    [&](cudaStream_t cs) { return batch_insert_seq(b, d_keys, d_offsets, 0, max_total, true, cs); },
+                    [&](cudaStream_t cs) { return batch_insert_seq(b, d_keys, d_offsets, 0, max_total, true, cs, false); },
                     &ran);
     if (s == QS_OK && !ran) s = batch_insert_seq(b, d_keys, d_offsets, 0, max_total, true, st);
     if (s == QS_OK) ++b->info.inserts;
@@ -1443,7 +1450,9 @@ qs_status qs_batch_query_graph(qs_batch* b, const uint32_t* d_keys, const uint64
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     bool ran = false;
     s = batch_graph(b, 1, d_keys, d_offsets, d_counts, max_total, st,
-                    [&](cudaStream_t cs) { return batch_query_seq(b, d_keys, d_offsets, max_total, d_counts, cs); },
+                    [&](cudaStream_t cs) {
+                        return batch_query_seq(b, d_keys, d_offsets, max_total, d_counts, cs, false);
+                    },
                     &ran);
     if (s == QS_OK && !ran) s = batch_query_seq(b, d_keys, d_offsets, max_total, d_counts, st);
     if (s == QS_OK) ++b->info.queries;
@@ -1495,6 +1504,8 @@ qs_status qs_batch_seeds(qs_batch* b, uint32_t* h_seeds) {
     std::memcpy(h_seeds, b->seeds.data(), (size_t)b->S * 4);
     return QS_OK;
 }
+
+qs_sketch* qs_batch_arena(qs_batch* b) { return b ? b->sk : nullptr; }
 
 qs_status qs_batch_get_info(qs_batch* b, qs_batch_info* out) {
     if (!b || !out) return fail(QS_ERR_INVALID_ARG, "null argument");
