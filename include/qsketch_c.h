@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define QS_ABI_VERSION 1u
+#define QS_ABI_VERSION 2u
 
 /* Status codes.  The reference returns 0 from every call and ignores CUDA errors in
  * release builds (include/qsketch.h:104-105); these replace that. */
@@ -88,13 +88,18 @@ typedef struct qs_params {
     uint64_t max_batch;          /* keys per internal insert chunk (scratch sizing);
                                     0 = 1<<22 */
     int32_t device;              /* CUDA device ordinal; -1 = current */
-    uint32_t lanes_per_key;      /* sub-warp width for the insert kernel: 0 = autotune,
-                                    else 8 (one lane per bucket word) */
-    uint32_t aggregate;          /* 0 = autotune, 1 = off, 2 = warp, 3 = block
-                                    pre-aggregation of duplicate keys */
-    uint32_t route;              /* insert routing between the levels: 0 = adaptive per
-                                    tile, 1 = load each bucket's index word first,
-                                    2 = read it with the counter atomic */
+    /* Insert-kernel knobs; none changes any result.  When lanes_per_key, aggregate, route
+     * and ctas_per_sm are all 0, qs_create takes them (and max_batch, if 0) from the
+     * autotuner's entry for the sketch's size class (qs_autotune), else the defaults
+     * 8 / 3 / 1 / 0. */
+    uint32_t lanes_per_key;      /* lanes serving one key in pass 1: 4, 8 (one lane per
+                                    bucket word, the reference's sub-warp), 16 or 32 */
+    uint32_t aggregate;          /* 1 = off, 2 = warp, 3 = warp + block pre-aggregation
+                                    of duplicate keys */
+    uint32_t route;              /* insert routing between the levels: 1 = load each
+                                    bucket's index word first, 2 = read it with the counter
+                                    atomic (8 lanes per key only), 3 = adaptive per tile */
+    uint32_t ctas_per_sm;        /* pass-1 CTAs per SM, 0 = as many as fit */
 } qs_params;
 
 typedef struct qs_sketch qs_sketch;
@@ -293,6 +298,27 @@ qs_status qs_mlp_grads(qs_learned *lk, const uint32_t *d_keys, const uint8_t *d_
 qs_status qs_mlp_train(qs_learned *lk, const uint32_t *d_keys, const uint8_t *d_labels, size_t n, uint32_t epochs,
                        uint32_t batch, float lr, float pos_weight, double *last_loss);
 
+/* ---- autotuner (no counterpart in the reference) -----------------------------------------
+ * Times pass-1 knob settings (lanes per key, aggregation, routing, CTAs per SM, chunk size
+ * max_batch; every setting gives identical results) on a scratch sketch built from `base`
+ * over the caller's sample keys (device memory, inserted `reps` times after a clear), by a
+ * coordinate search from the defaults: lanes per key, then aggregation, routing, CTAs per
+ * SM, chunk size.  The fastest setting is returned in *best, recorded in a process-wide
+ * table for the size class floor(log2(n_low)) of `base`, and used by later qs_create calls
+ * of that class whose knobs are all 0.  h_all (may be null) receives up to max_all of the
+ * timed settings, *n_all how many were timed. */
+typedef struct qs_tune_config {
+    uint32_t lanes_per_key, aggregate, route, ctas_per_sm;
+    uint64_t max_batch;
+    double insert_ms; /* mean time of one insert of the sample (pass 1 + ordered replay) */
+} qs_tune_config;
+
+qs_status qs_autotune(const qs_params *base, const uint32_t *d_keys, size_t n, uint32_t reps, qs_tune_config *best,
+                      qs_tune_config *h_all, uint32_t max_all, uint32_t *n_all);
+/* The recorded setting for n_low's size class; QS_ERR_INVALID_ARG when there is none. */
+qs_status qs_autotune_lookup(uint64_t n_low, qs_tune_config *out);
+void qs_autotune_reset(void);
+
 /* ---- batched uneven streams (no counterpart in the reference) ---------------------------
  * One handle owns n_streams independent MSWS sketches (stream s: n_low[s] low buckets,
  * n_high[s] high buckets, hash multiplier seed[s]; one mask table for all) laid out in one
@@ -318,6 +344,7 @@ typedef struct qs_batch_params {
     const uint8_t *mask_table;    /* optional, hash_mask_table_sz*4 bytes */
     uint32_t flags;               /* QS_FLAG_COMPAT_V3 */
     uint32_t aggregate, route;    /* as qs_params */
+    uint32_t lanes_per_key, ctas_per_sm; /* as qs_params */
     uint64_t max_batch;           /* keys per window (replay scratch), default 2^22 */
     int32_t device;
 } qs_batch_params;

@@ -45,6 +45,7 @@ class qs_params(ctypes.Structure):
         ("lanes_per_key", ctypes.c_uint32),
         ("aggregate", ctypes.c_uint32),
         ("route", ctypes.c_uint32),
+        ("ctas_per_sm", ctypes.c_uint32),
     ]
 
 
@@ -121,9 +122,16 @@ class qs_batch_params(ctypes.Structure):
         ("flags", ctypes.c_uint32),
         ("aggregate", ctypes.c_uint32),
         ("route", ctypes.c_uint32),
+        ("lanes_per_key", ctypes.c_uint32),
+        ("ctas_per_sm", ctypes.c_uint32),
         ("max_batch", ctypes.c_uint64),
         ("device", ctypes.c_int32),
     ]
+
+
+class qs_tune_config(ctypes.Structure):
+    _fields_ = [("lanes_per_key", ctypes.c_uint32), ("aggregate", ctypes.c_uint32), ("route", ctypes.c_uint32),
+                ("ctas_per_sm", ctypes.c_uint32), ("max_batch", ctypes.c_uint64), ("insert_ms", ctypes.c_double)]
 
 
 class qs_batch_info(ctypes.Structure):
@@ -170,6 +178,10 @@ SIGNATURES = {
     "qs_error_metrics": (_I, [_P, _P, _SZ, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _P]),
     "qs_probe": (_I, [_U32, _U64, _U64, ctypes.POINTER(ctypes.c_double)]),
     "qs_msws_insert_noalloc": (_I, [_P, _U64, _P, _U64, _P, _P, _U32, _U32, _U32, _P, _SZ, _P]),
+    "qs_autotune": (_I, [ctypes.POINTER(qs_params), _P, _SZ, _U32, ctypes.POINTER(qs_tune_config), _P, _U32,
+                         ctypes.POINTER(_U32)]),
+    "qs_autotune_lookup": (_I, [_U64, ctypes.POINTER(qs_tune_config)]),
+    "qs_autotune_reset": (None, []),
     "qs_batch_params_default": (None, [ctypes.POINTER(qs_batch_params)]),
     "qs_batch_create": (_I, [ctypes.POINTER(qs_batch_params), ctypes.POINTER(_P)]),
     "qs_batch_destroy": (_I, [_P]),

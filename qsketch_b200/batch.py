@@ -27,7 +27,8 @@ class BatchedSketches:
     """n_streams MSWS sketches updated together (qs_batch_create)."""
 
     def __init__(self, n_low, n_high, *, hash_seeds=None, seed_rng=1, mask_rng=1, hash_mask_table_sz=1021,
-                 hash_mask_ones=3, compat_v3=False, aggregate=0, route=0, max_batch=0, device=None):
+                 hash_mask_ones=3, compat_v3=False, aggregate=0, route=0, lanes_per_key=0, ctas_per_sm=0,
+                 max_batch=0, device=None):
         nl = np.ascontiguousarray(n_low, dtype=np.uint64)
         nh = np.ascontiguousarray(n_high, dtype=np.uint64)
         if nl.shape != nh.shape or nl.ndim != 1:
@@ -47,6 +48,7 @@ class BatchedSketches:
         p.hash_mask_table_sz, p.hash_mask_ones = hash_mask_table_sz, hash_mask_ones
         p.flags = QS_FLAG_COMPAT_V3 if compat_v3 else 0
         p.aggregate, p.route = aggregate, route
+        p.lanes_per_key, p.ctas_per_sm = lanes_per_key, ctas_per_sm
         if max_batch:
             p.max_batch = max_batch
         if device is None:

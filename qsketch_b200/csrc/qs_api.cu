@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <mutex>
 #include <random>
 #include <string>
@@ -61,6 +62,20 @@ const uint64_t kPrimes[] = {402653171, 268435399, 201326557, 134217689, 10066329
                             6143,      4093,      3067,      2039,      1531,      1021,     761,      509,
                             383,       251,       191,       127,       89,        61,       47,       31,
                             23,        13,        11,        7,         5,         3,        2};
+
+// Autotuner table: the fastest pass-1 setting per size class floor(log2(n_low)).
+std::mutex g_tune_mu;
+std::map<int, qs_tune_config> g_tune;
+
+int size_class(uint64_t n_low) { return n_low ? 63 - __builtin_clzll(n_low) : 0; }
+
+bool tune_lookup(uint64_t n_low, qs_tune_config* out) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(size_class(n_low));
+    if (it == g_tune.end()) return false;
+    *out = it->second;
+    return true;
+}
 
 }  // namespace
 
@@ -346,8 +361,21 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         if (p.n_high < 2 || p.n_high > (1ull << 30)) return bail(fail(QS_ERR_INVALID_ARG, "n_high out of [2, 2^30]"));
         const uint32_t H = p.hash_mask_table_sz;
         if (H == 0 || H > 16384) return bail(fail(QS_ERR_INVALID_ARG, "hash_mask_table_sz out of [1, 16384]"));
-        if (p.lanes_per_key != 0 && p.lanes_per_key != 8)
-            return bail(fail(QS_ERR_INVALID_ARG, "lanes_per_key must be 0 or 8"));
+        // insert knobs: explicit, else the autotuner's entry for this size class, else defaults
+        qs_tune_config tc{};
+        const bool tuned = p.lanes_per_key == 0 && p.aggregate == 0 && p.route == 0 && p.ctas_per_sm == 0 &&
+                           tune_lookup(n_low, &tc);
+        const uint32_t lpk = tuned ? tc.lanes_per_key : (p.lanes_per_key ? p.lanes_per_key : 8u);
+        const uint32_t route = tuned ? tc.route : (p.route ? p.route : 1u);
+        if (lpk != 4 && lpk != 8 && lpk != 16 && lpk != 32)
+            return bail(fail(QS_ERR_INVALID_ARG, "lanes_per_key must be 0, 4, 8, 16 or 32"));
+        if (route > 3) return bail(fail(QS_ERR_INVALID_ARG, "route out of [0, 3]"));
+        if (route == 2 && lpk != 8) return bail(fail(QS_ERR_INVALID_ARG, "route 2 needs 8 lanes per key"));
+        if (p.ctas_per_sm > 64) return bail(fail(QS_ERR_INVALID_ARG, "ctas_per_sm out of [0, 64]"));
+        if (tuned) {
+            sk->agg = (int)tc.aggregate - 1;
+            if (!p.max_batch && tc.max_batch) sk->max_batch = tc.max_batch;
+        }
         std::vector<uint8_t> bytes((size_t)H * 4);
         if (p.mask_table) {
             std::memcpy(bytes.data(), p.mask_table, bytes.size());
@@ -379,8 +407,7 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         D.seed = sk->seeds[0];
         D.n_masks = H;
         D.compat_v3 = (p.flags & QS_FLAG_COMPAT_V3) ? 1u : 0u;
-        if (p.route > 2) return bail(fail(QS_ERR_INVALID_ARG, "route out of [0, 2]"));
-        D.route = p.route == 0 ? 1u : p.route;  // default: load the index word first
+        D.route = route == 3 ? 0u : route;  // 0 in the kernel = adaptive per tile
         const uint64_t B = sk->max_batch;
         const uint64_t cap = std::min<uint64_t>(n_low, B);
         D.flag_cap = (uint32_t)cap;
@@ -406,6 +433,8 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         CKB(cudaStreamSynchronize(0), "create sync");
         e = msws_configure(dev, H, &sk->L);
         if (e != cudaSuccess) return bail(cuda_fail(e, "configure kernels"));
+        sk->L.lanes_per_key = (int)lpk;
+        sk->L.ctas_per_sm = tuned ? (int)tc.ctas_per_sm : (int)p.ctas_per_sm;
     } else {
         const uint32_t rows = p.m_low;
         if (rows == 0 || rows > (uint32_t)MAX_CM_ROWS) return bail(fail(QS_ERR_INVALID_ARG, "cm rows out of [1, 16]"));
@@ -1319,6 +1348,8 @@ qs_status qs_batch_create(const qs_batch_params* p, qs_batch** out) {
     ap.device = p->device;
     ap.aggregate = p->aggregate;
     ap.route = p->route;
+    ap.lanes_per_key = p->lanes_per_key;
+    ap.ctas_per_sm = p->ctas_per_sm;
     qs_batch* b = new qs_batch();
     qs_status s = qs_create(&ap, &b->sk);
     if (s != QS_OK) {
@@ -1517,6 +1548,128 @@ qs_status qs_batch_get_info(qs_batch* b, qs_batch_info* out) {
     out->streams_pool_full = 0;
     for (uint32_t v : st) out->streams_pool_full += (v & ST_POOL_FULL) ? 1u : 0u;
     return QS_OK;
+}
+
+}  // extern "C"
+
+// ---- autotuner ------------------------------------------------------------------------------
+
+extern "C" {
+
+void qs_autotune_reset(void) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.clear();
+}
+
+qs_status qs_autotune_lookup(uint64_t n_low, qs_tune_config* out) {
+    if (!out) return fail(QS_ERR_INVALID_ARG, "null output");
+    if (!tune_lookup(n_low, out)) return fail(QS_ERR_INVALID_ARG, "no tuned setting for this size class");
+    return QS_OK;
+}
+
+qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, uint32_t reps, qs_tune_config* best,
+                      qs_tune_config* h_all, uint32_t max_all, uint32_t* n_all) {
+    if (!base || !d_keys || !best || n == 0) return fail(QS_ERR_INVALID_ARG, "qs_autotune: bad argument");
+    if (base->kind != QS_KIND_MSWS) return fail(QS_ERR_INVALID_ARG, "qs_autotune: MSWS sketches only");
+    if (reinterpret_cast<uintptr_t>(d_keys) & 3u) return fail(QS_ERR_INVALID_ARG, "keys not 4-byte aligned");
+    reps = std::max(1u, reps);
+    // chunk sizes worth trying: 2^20 .. 2^24, none far beyond the sample
+    std::vector<uint64_t> mbs;
+    for (uint64_t mb = 1ull << 20; mb <= (1ull << 24); mb <<= 1)
+        if (mb <= std::max<uint64_t>(1ull << 20, 2 * (uint64_t)n)) mbs.push_back(mb);
+    qs_params p = *base;
+    p.lanes_per_key = 8;
+    p.aggregate = 3;
+    p.route = 1;
+    p.ctas_per_sm = 0;
+    p.max_batch = mbs.back();
+    qs_sketch* sk = nullptr;
+    qs_status s = qs_create(&p, &sk);
+    if (s != QS_OK) return s;
+    DeviceGuard guard(sk->device);
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto cleanup = [&](qs_status r) {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (st) cudaStreamDestroy(st);
+        qs_destroy(sk);
+        return r;
+    };
+    cudaError_t ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) return cleanup(cuda_fail(ce, "autotune setup"));
+    const uint64_t alloc_mb = sk->max_batch;
+    uint32_t timed = 0;
+    auto run = [&](qs_tune_config& c) -> qs_status {
+        sk->L.lanes_per_key = (int)c.lanes_per_key;
+        sk->L.ctas_per_sm = (int)c.ctas_per_sm;
+        sk->agg = (int)c.aggregate - 1;
+        sk->D.route = c.route == 3 ? 0u : c.route;
+        sk->max_batch = std::min(c.max_batch, alloc_mb);
+        double tot = 0;
+        for (uint32_t r = 0; r <= reps; ++r) {  // the first round warms up
+            qs_status q = qs_clear(sk, st);
+            if (q != QS_OK) return q;
+            CK(cudaEventRecord(e0, st), "autotune event");
+            q = insert_device(sk, d_keys, n, st);
+            if (q != QS_OK) return q;
+            CK(cudaEventRecord(e1, st), "autotune event");
+            CK(cudaEventSynchronize(e1), "autotune sync");
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, e0, e1), "autotune time");
+            if (r) tot += ms;
+        }
+        c.insert_ms = tot / reps;
+        if (h_all && timed < max_all) h_all[timed] = c;
+        ++timed;
+        return QS_OK;
+    };
+    qs_tune_config cur{8u, 3u, 1u, 0u, std::min<uint64_t>(1ull << 22, mbs.back()), 0.0};
+    s = run(cur);
+    if (s != QS_OK) return cleanup(s);
+    auto consider = [&](qs_tune_config c) -> qs_status {
+        qs_status q = run(c);
+        if (q == QS_OK && c.insert_ms < cur.insert_ms) cur = c;
+        return q;
+    };
+    for (uint32_t lpk : {4u, 16u, 32u}) {
+        qs_tune_config c = cur;
+        c.lanes_per_key = lpk;
+        if ((s = consider(c)) != QS_OK) return cleanup(s);
+    }
+    for (uint32_t agg : {1u, 2u, 3u}) {
+        if (agg == cur.aggregate) continue;
+        qs_tune_config c = cur;
+        c.aggregate = agg;
+        if ((s = consider(c)) != QS_OK) return cleanup(s);
+    }
+    for (uint32_t route : {2u, 3u}) {
+        if (route == 2 && cur.lanes_per_key != 8) continue;
+        qs_tune_config c = cur;
+        c.route = route;
+        if ((s = consider(c)) != QS_OK) return cleanup(s);
+    }
+    for (uint32_t ctas : {1u, 2u, 3u}) {
+        qs_tune_config c = cur;
+        c.ctas_per_sm = ctas;
+        if ((s = consider(c)) != QS_OK) return cleanup(s);
+    }
+    for (uint64_t mb : mbs) {
+        if (mb == cur.max_batch) continue;
+        qs_tune_config c = cur;
+        c.max_batch = mb;
+        if ((s = consider(c)) != QS_OK) return cleanup(s);
+    }
+    if (n_all) *n_all = timed;
+    *best = cur;
+    {
+        const uint64_t n_low = sk->D.n_low;
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[size_class(n_low)] = cur;
+    }
+    return cleanup(QS_OK);
 }
 
 }  // extern "C"

@@ -13,6 +13,9 @@ struct MswsLaunch {
     int insert_grid;
     int repair_grid;
     int query_grid;
+    int ins_occ[3][4];       // resident pass-1 CTAs per SM by [aggregation][lanes-per-key index]
+    int lanes_per_key = 8;   // pass-1 sub-warp width: 4, 8, 16 or 32
+    int ctas_per_sm = 0;     // pass-1 CTAs per SM, 0 = as many as fit
 };
 
 size_t msws_insert_smem(uint32_t n_masks);

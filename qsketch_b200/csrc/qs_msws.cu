@@ -123,44 +123,60 @@ __device__ __forceinline__ bool agg_insert(const InsShared& S, uint32_t key, uin
 }
 
 // Sub-warp rounds over the staged entries of this warp: entry j = (target, mask, count,
-// kind); 4 entries per round, lane w of sub-warp `sub` serves entry r*4+sub.  kind 0: low
-// bucket `target`, lane w adds its nibble of 8-bit counters to word w with a returning
-// atomic (device_sketch_v3.h:131-170); kind 1: linked, lane w adds to the w-th selected
-// high counter of id `target` (insert_high, :54-65, :111-129).
+// kind).  LPK lanes serve one entry (32/LPK entries per round, LPK rounds for 32 entries);
+// lane w of a group owns bucket words w, w+LPK, ... (LPK = 8: one word per lane, the
+// reference's sub-warp mapping, device_sketch_v3.h:131-170; LPK = 4: two words per lane;
+// LPK = 16, 32: lanes past the eighth idle).  kind 0: low bucket `target`, each owned word
+// gets its nibble of 8-bit counters with one returning atomic; kind 1: linked, the owning
+// lanes add to the selected high counters of id `target` (insert_high, :54-65, :111-129).
+template <int LPK>
 __device__ __forceinline__ void staged_rounds(const MswsDev& D, const uint4* st, int nact) {
-    const int lane = threadIdx.x & 31, sub = lane >> 3, w = lane & 7;
-    uint32_t olds[8];
+    static_assert(LPK == 4 || LPK == 8 || LPK == 16 || LPK == 32, "lanes per key");
+    constexpr int KPR = 32 / LPK;                // entries per round
+    constexpr int WPL = LPK >= 8 ? 1 : 8 / LPK;  // bucket words per lane
+    const int lane = threadIdx.x & 31, sub = lane / LPK, w = lane % LPK;
+    uint32_t olds[LPK][WPL];
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        olds[r] = 0;
-        if (r * 4 >= nact) continue;  // warp-uniform
-        const int j = r * 4 + sub;
+    for (int r = 0; r < LPK; ++r) {
+#pragma unroll
+        for (int h = 0; h < WPL; ++h) olds[r][h] = 0;
+        if (r * KPR >= nact) continue;  // warp-uniform
+        const int j = r * KPR + sub;
         if (j >= nact) continue;
         const uint4 e = st[j];
         if (e.w == 0) {
-            const uint32_t nib = (w < 7) ? (e.y >> (4 * w)) & 0xfu : 0u;
-            if (nib) olds[r] = atomicAdd(D.low + (uint64_t)e.x * LOW_WORDS + w, expand_nibble(nib) * e.z);
+#pragma unroll
+            for (int h = 0; h < WPL; ++h) {
+                const int ww = w + h * LPK;
+                const uint32_t nib = (ww < 7) ? (e.y >> (4 * ww)) & 0xfu : 0u;
+                if (nib) olds[r][h] = atomicAdd(D.low + (uint64_t)e.x * LOW_WORDS + ww, expand_nibble(nib) * e.z);
+            }
         } else {
             uint32_t* hb = D.high + (uint64_t)(e.x - START) * HIGH_WORDS;
             const int pc = __popc(e.y);
-            for (int k = w; k < pc; k += 8) atomicAdd(hb + __fns(e.y, 0, k + 1), e.z);
+            for (int k = w; k < pc; k += LPK) atomicAdd(hb + __fns(e.y, 0, k + 1), e.z);
         }
     }
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        if (r * 4 >= nact) continue;  // warp-uniform
-        const int j = r * 4 + sub;
+    for (int r = 0; r < LPK; ++r) {
+        if (r * KPR >= nact) continue;  // warp-uniform
+        const int j = r * KPR + sub;
         bool cross = false;
         uint4 e = make_uint4(0, 0, 0, 1);
         if (j < nact) e = st[j];
         if (e.w == 0) {
-            const uint32_t nib = (w < 7) ? (e.y >> (4 * w)) & 0xfu : 0u;
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (((nib >> k) & 1u) && ((olds[r] >> (8 * k)) & 0xffu) + e.z >= CROSS) cross = true;
+            for (int h = 0; h < WPL; ++h) {
+                const int ww = w + h * LPK;
+                const uint32_t nib = (ww < 7) ? (e.y >> (4 * ww)) & 0xfu : 0u;
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (((nib >> k) & 1u) && ((olds[r][h] >> (8 * k)) & 0xffu) + e.z >= CROSS) cross = true;
+            }
         }
         const uint32_t bal = __ballot_sync(0xffffffffu, cross);
-        if (w == 0 && ((bal >> (sub * 8)) & 0xffu)) flag_bucket(D, e.x);
+        const uint32_t grp = LPK == 32 ? bal : (bal >> (sub * LPK)) & ((1u << (LPK & 31)) - 1u);
+        if (w == 0 && grp) flag_bucket(D, e.x);
     }
 }
 
@@ -215,7 +231,7 @@ __device__ __forceinline__ uint32_t staged_rounds_fused(const MswsDev& D, const 
 
 // Up to 32 keys held one per lane (valid lanes: lane < cnt), all of one sketch: hash
 // multiplier `seed`, `fm_low.d` buckets starting at bucket `base` of the table.
-template <int AGG>
+template <int AGG, int LPK>
 __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& S, uint32_t key, int cnt,
                                              bool use_table, int route, uint64_t idx, uint32_t seed,
                                              const FastMod& fm_low, uint32_t base) {
@@ -231,7 +247,7 @@ __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& 
         c = (valid && lane == __ffs(peers) - 1) ? (uint32_t)__popc(peers) : 0u;
     }
     uint4* st = S.stage + wid * 32;
-    if (route == ROUTE_FUSED) {
+    if (LPK == 8 && route == ROUTE_FUSED) {  // the fused form exists for 8 lanes per key
         const uint32_t am = __ballot_sync(0xffffffffu, c != 0);
         if (c) st[__popc(am & lanemask_lt())] = make_uint4(b, m, c, key);
         __syncwarp();
@@ -251,12 +267,13 @@ __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& 
     const uint32_t am = __ballot_sync(0xffffffffu, act);
     if (act) st[__popc(am & lanemask_lt())] = make_uint4(direct_high ? w7 : b, m, c, direct_high ? 1u : 0u);
     __syncwarp();
-    staged_rounds(D, st, __popc(am));
+    staged_rounds<LPK>(D, st, __popc(am));
     __syncwarp();
 }
 
 // Merged linked keys of the tile: one red per selected high counter per distinct key (the
 // tile's keys share the hash multiplier `seed`).
+template <int LPK>
 __device__ __forceinline__ void drain_table(const MswsDev& D, const InsShared& S, uint32_t seed) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint4* st = S.stage + wid * 32;
@@ -277,12 +294,12 @@ __device__ __forceinline__ void drain_table(const MswsDev& D, const InsShared& S
         if (!am) continue;
         if (has) st[__popc(am & lanemask_lt())] = make_uint4(id, m, c, 1u);
         __syncwarp();
-        staged_rounds(D, st, __popc(am));
+        staged_rounds<LPK>(D, st, __popc(am));
         __syncwarp();
     }
 }
 
-template <int AGG>
+template <int AGG, int LPK>
 __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* __restrict__ keys, uint64_t n,
                                                                 MswsDev D) {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -321,7 +338,7 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
     if (blockIdx.x == 0 && wid == 0 && head + tail > 0) {
         const uint32_t k = lane < (int)(head + tail) ? s_extra[lane] : 0u;
         const uint64_t idx = lane < (int)head ? (uint64_t)lane : head + body_n + (lane - head);
-        insert_group<AGG>(D, S, k, (int)(head + tail), false, ROUTE_PRELOAD, idx, D.seed, D.fm_low, 0u);
+        insert_group<AGG, LPK>(D, S, k, (int)(head + tail), false, ROUTE_PRELOAD, idx, D.seed, D.fm_low, 0u);
     }
 
     const uint64_t ntiles = (body_n + INS_TILE - 1) / INS_TILE;
@@ -361,7 +378,8 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
         for (int base = wid * 32; base < cnt; base += INS_THREADS) {
             const int c = min(32, cnt - base);
             const uint32_t k = lane < c ? tk[base + lane] : 0u;
-            insert_group<AGG>(D, S, k, c, true, route, head + g * INS_TILE + base + lane, D.seed, D.fm_low, 0u);
+            insert_group<AGG, LPK>(D, S, k, c, true, route, head + g * INS_TILE + base + lane, D.seed, D.fm_low,
+                                   0u);
         }
         __syncthreads();
         if (tid == 0) {  // adaptive: the next tile is fused while under 1/16 of the keys are linked
@@ -369,7 +387,7 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
             S.misc[1] = 0;
         }
         if (AGG == AGG_BLOCK) {
-            drain_table(D, S, D.seed);
+            drain_table<LPK>(D, S, D.seed);
             __syncthreads();
         }
         if (tid == 0 && i + INS_STAGES < my_tiles) {
@@ -990,7 +1008,7 @@ __device__ __forceinline__ uint32_t stream_of_item(const BatchDev& B, uint32_t i
 // Pass 1 over a batch: a persistent grid pulls tiles from the work queue; a tile's keys
 // all belong to one stream, so they hash with its descriptor and the tile's shared-memory
 // merge table never mixes sketches.  Everything after hashing is the single-sketch pass 1.
-template <int AGG>
+template <int AGG, int LPK>
 __global__ void __launch_bounds__(INS_THREADS, 4) k_batch_insert(const uint32_t* __restrict__ keys, MswsDev D,
                                                                  BatchDev B) {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -1027,14 +1045,14 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_batch_insert(const uint32_t*
         for (int b = wid * 32; b < cnt; b += INS_THREADS) {
             const int c = min(32, cnt - b);
             const uint32_t k = lane < c ? __ldcs(keys + t0 + b + lane) : 0u;
-            insert_group<AGG>(D, S, k, c, true, route, 0, seed, fm, base);
+            insert_group<AGG, LPK>(D, S, k, c, true, route, 0, seed, fm, base);
         }
         __syncthreads();
         if (tid == 0) {
             if (D.route == 0) S.misc[2] = S.misc[1] * 16u < (uint32_t)cnt ? ROUTE_FUSED : ROUTE_PRELOAD;
             S.misc[1] = 0;
         }
-        if (AGG == AGG_BLOCK) drain_table(D, S, seed);
+        if (AGG == AGG_BLOCK) drain_table<LPK>(D, S, seed);
         __syncthreads();
     }
     if (tid == 0 && S.misc[0]) atomicAdd(&D.ctl->dropped, (unsigned long long)S.misc[0]);
@@ -1075,6 +1093,32 @@ __global__ void __launch_bounds__(QRY_THREADS) k_batch_query(const uint32_t* __r
 
 // ---- launchers ----------------------------------------------------------------------------
 
+// Pass-1 kernels by aggregation mode and lanes per key (4, 8, 16, 32).
+int lpk_index(int lpk) { return lpk == 4 ? 0 : lpk == 16 ? 2 : lpk == 32 ? 3 : 1; }
+
+template <int AGG>
+const void* ins_fn(int li, bool batch) {
+    switch (li) {
+        case 0: return batch ? (const void*)k_batch_insert<AGG, 4> : (const void*)k_msws_insert<AGG, 4>;
+        case 2: return batch ? (const void*)k_batch_insert<AGG, 16> : (const void*)k_msws_insert<AGG, 16>;
+        case 3: return batch ? (const void*)k_batch_insert<AGG, 32> : (const void*)k_msws_insert<AGG, 32>;
+        default: return batch ? (const void*)k_batch_insert<AGG, 8> : (const void*)k_msws_insert<AGG, 8>;
+    }
+}
+
+const void* ins_fn(int agg, int li, bool batch) {
+    return agg == AGG_BLOCK ? ins_fn<AGG_BLOCK>(li, batch)
+           : agg == AGG_WARP ? ins_fn<AGG_WARP>(li, batch)
+                             : ins_fn<AGG_NONE>(li, batch);
+}
+
+// Persistent pass-1 grid: ctas_per_sm CTAs per SM (0 = as many as fit), at most the occupancy.
+int ins_grid(const MswsLaunch& L, int agg, int li) {
+    const int occ = std::max(1, L.ins_occ[agg][li]);
+    const int per = L.ctas_per_sm > 0 ? std::min(L.ctas_per_sm, occ) : occ;
+    return L.num_sms * per;
+}
+
 cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
     cudaDeviceProp prop;
     cudaError_t e = cudaGetDeviceProperties(&prop, device);
@@ -1083,28 +1127,26 @@ cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
     // The dynamic shared-memory cap is a per-kernel attribute shared by every sketch of the
     // process: set it for the largest mask table (16384 words); the launch passes the actual size.
     const size_t ins_smem = msws_insert_smem(n_masks);
-    const void* fns[3] = {(const void*)k_msws_insert<AGG_NONE>, (const void*)k_msws_insert<AGG_WARP>,
-                          (const void*)k_msws_insert<AGG_BLOCK>};
-    for (const void* fn : fns) {
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msws_insert_smem(16384));
-        if (e != cudaSuccess) return e;
-    }
+    for (int agg = 0; agg < 3; ++agg)
+        for (int li = 0; li < 4; ++li)
+            for (int batch = 0; batch < 2; ++batch) {
+                const void* fn = ins_fn(agg, li, batch != 0);
+                e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)msws_insert_smem(16384));
+                if (e != cudaSuccess) return e;
+                if (!batch) {
+                    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&L->ins_occ[agg][li], fn, INS_THREADS, ins_smem);
+                    if (e != cudaSuccess) return e;
+                }
+            }
     e = cudaFuncSetAttribute((const void*)k_msws_query, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * 4);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute((const void*)k_learned_query, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * 4);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute((const void*)k_batch_query, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * 4);
     if (e != cudaSuccess) return e;
-    const void* bfns[3] = {(const void*)k_batch_insert<AGG_NONE>, (const void*)k_batch_insert<AGG_WARP>,
-                           (const void*)k_batch_insert<AGG_BLOCK>};
-    for (const void* fn : bfns) {
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msws_insert_smem(16384));
-        if (e != cudaSuccess) return e;
-    }
     int occ = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_msws_insert<AGG_BLOCK>, INS_THREADS, ins_smem);
-    if (e != cudaSuccess) return e;
-    L->insert_grid = prop.multiProcessorCount * (occ > 0 ? occ : 1);
+    L->insert_grid = prop.multiProcessorCount * std::max(1, L->ins_occ[AGG_BLOCK][1]);
     for (const void* fn : {(const void*)k_msws_repair<false>, (const void*)k_msws_repair<true>}) {
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msws_repair_smem());
         if (e != cudaSuccess) return e;
@@ -1126,15 +1168,12 @@ cudaError_t msws_insert_pass(const uint32_t* d_keys, uint64_t n, const MswsDev& 
                              cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     const size_t smem = msws_insert_smem(D.n_masks);
+    const int li = lpk_index(L.lanes_per_key);
     const uint64_t tiles = (n + INS_TILE - 1) / INS_TILE;
-    const int grid = (int)std::min<uint64_t>((uint64_t)L.insert_grid, std::max<uint64_t>(1ull, tiles));
-    if (agg == AGG_BLOCK)
-        k_msws_insert<AGG_BLOCK><<<grid, INS_THREADS, smem, st>>>(d_keys, n, D);
-    else if (agg == AGG_WARP)
-        k_msws_insert<AGG_WARP><<<grid, INS_THREADS, smem, st>>>(d_keys, n, D);
-    else
-        k_msws_insert<AGG_NONE><<<grid, INS_THREADS, smem, st>>>(d_keys, n, D);
-    return cudaGetLastError();
+    const int grid = (int)std::min<uint64_t>((uint64_t)ins_grid(L, agg, li), std::max<uint64_t>(1ull, tiles));
+    MswsDev Dc = D;
+    void* args[] = {(void*)&d_keys, (void*)&n, (void*)&Dc};
+    return cudaLaunchKernel(ins_fn(agg, li, false), dim3(grid), dim3(INS_THREADS), args, smem, st);
 }
 
 cudaError_t msws_repair(const uint32_t* d_keys, uint64_t n, const MswsDev& D, const MswsLaunch& L, cudaStream_t st) {
@@ -1154,13 +1193,11 @@ cudaError_t batch_plan(const BatchDev& B, Ctl* ctl, uint64_t c0, uint64_t c1, bo
 cudaError_t batch_insert_pass(const uint32_t* d_keys, const MswsDev& D, const BatchDev& B, const MswsLaunch& L,
                               int agg, cudaStream_t st) {
     const size_t smem = msws_insert_smem(D.n_masks);
-    if (agg == AGG_BLOCK)
-        k_batch_insert<AGG_BLOCK><<<L.insert_grid, INS_THREADS, smem, st>>>(d_keys, D, B);
-    else if (agg == AGG_WARP)
-        k_batch_insert<AGG_WARP><<<L.insert_grid, INS_THREADS, smem, st>>>(d_keys, D, B);
-    else
-        k_batch_insert<AGG_NONE><<<L.insert_grid, INS_THREADS, smem, st>>>(d_keys, D, B);
-    return cudaGetLastError();
+    const int li = lpk_index(L.lanes_per_key);
+    MswsDev Dc = D;
+    BatchDev Bc = B;
+    void* args[] = {(void*)&d_keys, (void*)&Dc, (void*)&Bc};
+    return cudaLaunchKernel(ins_fn(agg, li, true), dim3(ins_grid(L, agg, li)), dim3(INS_THREADS), args, smem, st);
 }
 
 // d_window: the caller's flat key array advanced to the window start c0.

@@ -39,7 +39,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version_and_status_strings():
-    assert _lib.lib.qs_abi_version() == 1
+    assert _lib.lib.qs_abi_version() == 2
     for s in range(8):
         assert _lib.lib.qs_status_string(s)
 
@@ -109,3 +109,20 @@ def test_batch_bad_arguments_are_errors():
     assert _lib.lib.qs_batch_insert(None, None, None, 10, None) == _lib.QS_ERR_INVALID_ARG
     assert _lib.lib.qs_batch_query(None, None, None, 10, None, None) == _lib.QS_ERR_INVALID_ARG
     assert _lib.lib.qs_batch_destroy(None) == _lib.QS_OK
+
+
+def test_autotune_table_empty_and_bad_arguments():
+    from qsketch_b200 import autotune
+    autotune.reset()
+    assert autotune.lookup(1 << 20) is None
+    assert _lib.lib.qs_autotune(None, None, 0, 1, None, None, 0, None) == _lib.QS_ERR_INVALID_ARG
+
+
+def test_knob_validation_happens_before_any_device_work():
+    # lanes_per_key outside {0, 4, 8, 16, 32} is rejected; without a GPU the device check
+    # comes first, so only check that an invalid value never reports success.
+    p = _lib.qs_params()
+    _lib.lib.qs_params_default(ctypes.byref(p))
+    p.n_low, p.lanes_per_key = 1021, 12
+    h = ctypes.c_void_p()
+    assert _lib.lib.qs_create(ctypes.byref(p), ctypes.byref(h)) != _lib.QS_OK

@@ -45,10 +45,10 @@ def check_streams(b, w, got, streams=None):
         assert torch.equal(g, want), f"stream {s}: {(g != want).sum().item()} of {g.numel()} estimates differ"
 
 
-@pytest.mark.parametrize("max_batch", [1 << 16, 1 << 22])
-def test_batch_equals_each_stream_alone(gpu, max_batch):
+@pytest.mark.parametrize("max_batch,lpk", [(1 << 16, 8), (1 << 22, 8), (1 << 18, 4), (1 << 18, 16)])
+def test_batch_equals_each_stream_alone(gpu, max_batch, lpk):
     w = workload(64, seed=3, max_len=1 << 17)
-    b = BatchedSketches(w["n_low"], w["n_high"], seed_rng=7, max_batch=max_batch)
+    b = BatchedSketches(w["n_low"], w["n_high"], seed_rng=7, max_batch=max_batch, lanes_per_key=lpk)
     b.insert(w["keys"], w["offsets"])
     got = b.search(w["keys"], w["offsets"])
     b.sync()

@@ -69,7 +69,7 @@ def test_uniform_config1_full_size(gpu):
     assert sk.stats()["linked_buckets"] == 0
 
 
-@pytest.mark.parametrize("agg,route", [(1, 0), (2, 0), (3, 0), (3, 1), (3, 2)])
+@pytest.mark.parametrize("agg,route", [(1, 0), (2, 0), (3, 0), (3, 1), (3, 2), (3, 3)])
 def test_zipf_heavy_links(gpu, agg, route):
     sk, orc = make_pair(16381, 1 << 15, aggregate=agg, route=route)
     keys = data.zipf_keys(1 << 22, 1 << 18, 1.1, seed=5, perm_seed=77)
@@ -239,3 +239,43 @@ def test_mixed_config3_full_size(gpu):
     sk, orc = make_pair(8388593, 1 << 19)
     run_mixed(sk, orc, data.zipf_keys(1 << 28, 1 << 26, 0.8, seed=1000, perm_seed=99), 1 << 20, threads=8)
     sk.sync()
+
+
+@pytest.mark.parametrize("lpk", [4, 16, 32])
+@pytest.mark.parametrize("agg", [1, 3])
+def test_lanes_per_key_variants_bit_exact(gpu, lpk, agg):
+    # Every pass-1 width gives the oracle's tables and estimates on a stream that links
+    # thousands of buckets and repairs many chunks.
+    sk, orc = make_pair(65521, 1 << 14, lanes_per_key=lpk, aggregate=agg, max_batch=1 << 18)
+    keys = data.zipf_keys(1 << 21, 1 << 16, 1.1, seed=41, perm_seed=5)
+    q = data.rank_keys(5, 0, 1 << 16)
+    run_and_compare(sk, orc, keys, q)
+
+
+@pytest.mark.parametrize("ctas", [1, 2])
+def test_ctas_per_sm_bit_exact(gpu, ctas):
+    sk, orc = make_pair(65521, 1 << 14, lanes_per_key=4, ctas_per_sm=ctas, max_batch=1 << 18)
+    keys = data.zipf_keys(1 << 20, 1 << 16, 1.0, seed=43, perm_seed=6)
+    run_and_compare(sk, orc, keys, keys[:1 << 16])
+
+
+def test_autotune_picks_a_timed_setting_and_create_uses_it(gpu):
+    from qsketch_b200 import autotune
+    autotune.reset()
+    keys = data.zipf_keys(1 << 22, 1 << 20, 1.1, seed=47, perm_seed=8)
+    best, allc = autotune.autotune(524287, 1 << 15, keys, reps=2)
+    print("autotune best:", best, "of", len(allc))
+    assert len(allc) >= 10
+    assert best["insert_ms"] == min(c["insert_ms"] for c in allc)
+    assert autotune.lookup(524287) == best
+    assert autotune.lookup(300000) == best  # same size class (2^18 <= n < 2^19)
+    # a sketch of that class with knobs left at 0 uses the tuned setting: same results
+    tuned = qs.Sketch_GPU_Sub_Warp_Level(524287, 8, 1 << 15, 32, hash_seed=2654435769)
+    plain = qs.Sketch_GPU_Sub_Warp_Level(524287, 8, 1 << 15, 32, hash_seed=2654435769, lanes_per_key=8,
+                                         aggregate=3, route=1)
+    tuned.insert(keys)
+    plain.insert(keys)
+    q = keys[:1 << 18]
+    assert torch.equal(tuned.search(q), plain.search(q))
+    autotune.reset()
+    assert autotune.lookup(524287) is None
