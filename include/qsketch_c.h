@@ -91,9 +91,9 @@ typedef struct qs_params {
     /* Insert-kernel knobs; none changes any result.  When lanes_per_key, aggregate, route
      * and ctas_per_sm are all 0, qs_create takes them (and max_batch, if 0) from the
      * autotuner's entry for the sketch's size class (qs_autotune), else the defaults
-     * 8 / 3 / 1 / 0. */
-    uint32_t lanes_per_key;      /* lanes serving one key in pass 1: 4, 8 (one lane per
-                                    bucket word, the reference's sub-warp), 16 or 32 */
+     * 4 (8 with route 2) / 3 / 1 / 0. */
+    uint32_t lanes_per_key;      /* lanes serving one key in pass 1: 1, 2, 4, 8 (one lane
+                                    per bucket word, the reference's sub-warp), 16 or 32 */
     uint32_t aggregate;          /* 1 = off, 2 = warp, 3 = warp + block pre-aggregation
                                     of duplicate keys */
     uint32_t route;              /* insert routing between the levels: 1 = load each
@@ -299,7 +299,7 @@ qs_status qs_mlp_train(qs_learned *lk, const uint32_t *d_keys, const uint8_t *d_
                        uint32_t batch, float lr, float pos_weight, double *last_loss);
 
 /* ---- autotuner (no counterpart in the reference) -----------------------------------------
- * Times pass-1 knob settings (lanes per key, aggregation, routing, CTAs per SM, chunk size
+ * Times pass-1 knob settings (lanes per key 1-32, aggregation, routing, CTAs per SM, chunk size
  * max_batch; every setting gives identical results) on a scratch sketch built from `base`
  * over the caller's sample keys (device memory, inserted `reps` times after a clear), by a
  * coordinate search from the defaults: lanes per key, then aggregation, routing, CTAs per

@@ -1,7 +1,7 @@
 """The insert autotuner over the C ABI (qs_autotune* in include/qsketch_c.h).
 
 No counterpart in the reference, whose kernels have fixed launch shapes (<<<65536, 32>>>,
-device_sketch_v3.h:587).  Pass-1 knobs — lanes per key (4, 8, 16, 32 over the fixed 32 B
+device_sketch_v3.h:587).  Pass-1 knobs — lanes per key (1, 2, 4, 8, 16, 32 over the fixed 32 B
 bucket), duplicate-key aggregation, level routing, CTAs per SM and the chunk size — never
 change results, only speed; qs_autotune times them on a sample and records the fastest for
 the sketch's size class floor(log2(n_low)), which later sketches of that class use when

@@ -365,10 +365,11 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         qs_tune_config tc{};
         const bool tuned = p.lanes_per_key == 0 && p.aggregate == 0 && p.route == 0 && p.ctas_per_sm == 0 &&
                            tune_lookup(n_low, &tc);
-        const uint32_t lpk = tuned ? tc.lanes_per_key : (p.lanes_per_key ? p.lanes_per_key : 8u);
+        // default 4 lanes per key (measured fastest on every workload here), 8 for route 2
         const uint32_t route = tuned ? tc.route : (p.route ? p.route : 1u);
-        if (lpk != 4 && lpk != 8 && lpk != 16 && lpk != 32)
-            return bail(fail(QS_ERR_INVALID_ARG, "lanes_per_key must be 0, 4, 8, 16 or 32"));
+        const uint32_t lpk = tuned ? tc.lanes_per_key : (p.lanes_per_key ? p.lanes_per_key : route == 2 ? 8u : 4u);
+        if (lpk != 1 && lpk != 2 && lpk != 4 && lpk != 8 && lpk != 16 && lpk != 32)
+            return bail(fail(QS_ERR_INVALID_ARG, "lanes_per_key must be 0, 1, 2, 4, 8, 16 or 32"));
         if (route > 3) return bail(fail(QS_ERR_INVALID_ARG, "route out of [0, 3]"));
         if (route == 2 && lpk != 8) return bail(fail(QS_ERR_INVALID_ARG, "route 2 needs 8 lanes per key"));
         if (p.ctas_per_sm > 64) return bail(fail(QS_ERR_INVALID_ARG, "ctas_per_sm out of [0, 64]"));
@@ -422,6 +423,7 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         CKB(sk->alloc(&D.flag_list, cap), "alloc flag list");
         CKB(sk->alloc(&D.bitmap, (n_low + 31) / 32), "alloc bitmap");
         CKB(sk->alloc(&D.tile_counts, D.max_tiles), "alloc tile counts");
+        CKB(sk->alloc(&D.hits, (uint64_t)D.max_tiles * (REPAIR_TILE / 8)), "alloc hit bits");
         CKB(sk->alloc(&D.rec[0], B), "alloc records");
         CKB(sk->alloc(&D.rec[1], B), "alloc records");
         CKB(sk->alloc(&D.hist, (uint64_t)256 * D.max_tiles), "alloc histograms");
@@ -1634,7 +1636,7 @@ qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, u
         if (q == QS_OK && c.insert_ms < cur.insert_ms) cur = c;
         return q;
     };
-    for (uint32_t lpk : {4u, 16u, 32u}) {
+    for (uint32_t lpk : {4u, 2u, 1u, 16u, 32u}) {
         qs_tune_config c = cur;
         c.lanes_per_key = lpk;
         if ((s = consider(c)) != QS_OK) return cleanup(s);

@@ -8,13 +8,15 @@
 
 namespace qsb {
 
+constexpr int LPK_VARIANTS = 6;  // lanes per key 4, 8, 16, 32, 2, 1 (index order of lpk_index)
+
 struct MswsLaunch {
     int num_sms;
     int insert_grid;
     int repair_grid;
     int query_grid;
-    int ins_occ[3][4];       // resident pass-1 CTAs per SM by [aggregation][lanes-per-key index]
-    int lanes_per_key = 8;   // pass-1 sub-warp width: 4, 8, 16 or 32
+    int ins_occ[3][6];       // resident pass-1 CTAs per SM by [aggregation][lanes-per-key index]
+    int lanes_per_key = 8;   // pass-1 lanes per key: 1, 2, 4, 8, 16 or 32
     int ctas_per_sm = 0;     // pass-1 CTAs per SM, 0 = as many as fit
 };
 

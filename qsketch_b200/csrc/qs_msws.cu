@@ -125,13 +125,13 @@ __device__ __forceinline__ bool agg_insert(const InsShared& S, uint32_t key, uin
 // Sub-warp rounds over the staged entries of this warp: entry j = (target, mask, count,
 // kind).  LPK lanes serve one entry (32/LPK entries per round, LPK rounds for 32 entries);
 // lane w of a group owns bucket words w, w+LPK, ... (LPK = 8: one word per lane, the
-// reference's sub-warp mapping, device_sketch_v3.h:131-170; LPK = 4: two words per lane;
-// LPK = 16, 32: lanes past the eighth idle).  kind 0: low bucket `target`, each owned word
+// reference's sub-warp mapping, device_sketch_v3.h:131-170; LPK = 4, 2, 1: two, four or
+// all eight words per lane; LPK = 16, 32: lanes past the eighth idle).  kind 0: low bucket `target`, each owned word
 // gets its nibble of 8-bit counters with one returning atomic; kind 1: linked, the owning
 // lanes add to the selected high counters of id `target` (insert_high, :54-65, :111-129).
 template <int LPK>
 __device__ __forceinline__ void staged_rounds(const MswsDev& D, const uint4* st, int nact) {
-    static_assert(LPK == 4 || LPK == 8 || LPK == 16 || LPK == 32, "lanes per key");
+    static_assert(LPK == 1 || LPK == 2 || LPK == 4 || LPK == 8 || LPK == 16 || LPK == 32, "lanes per key");
     constexpr int KPR = 32 / LPK;                // entries per round
     constexpr int WPL = LPK >= 8 ? 1 : 8 / LPK;  // bucket words per lane
     const int lane = threadIdx.x & 31, sub = lane / LPK, w = lane % LPK;
@@ -677,6 +677,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     constexpr int NW = REPAIR_THREADS / 32;
     constexpr int PER = REPAIR_TILE / REPAIR_THREADS;  // 8 consecutive keys per thread
+    static_assert(PER == 8, "one hit byte per thread");
     const uint32_t ntk = (uint32_t)((n + REPAIR_TILE - 1) / REPAIR_TILE);
     const uint32_t nthreads = gridDim.x * REPAIR_THREADS;
     const uint32_t gtid = blockIdx.x * REPAIR_THREADS + tid;
@@ -708,17 +709,19 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         uint32_t c = 0;
         KeyHash<BATCH> kh;
         if (base < n) kh.start(B, c0 + base);
+        uint32_t hit = 0;
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
             const uint64_t i = base + j;
             if (i < n && !(D.skip && ((__ldg(D.skip + (i >> 5)) >> (i & 31)) & 1u))) {
                 uint32_t hv;
                 const uint32_t b = kh.bucket(D, B, c0 + i, __ldg(keys + i), hv);
-                c += flagged_slot(D, skey, sval, use_set, b) != NONE ? 1u : 0u;
+                if (flagged_slot(D, skey, sval, use_set, b) != NONE) hit |= 1u << j;
             }
         }
+        __stcg(D.hits + (base >> 3), (uint8_t)hit);  // PER == 8: one byte per thread
         uint32_t total;
-        block_exclusive_scan(c, &total);
+        block_exclusive_scan((uint32_t)__popc(hit), &total);
         if (tid == 0) __stcg(D.tile_counts + t, total);
     }
     if (!grid_barrier(ctl)) return;
@@ -733,29 +736,21 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     const uint32_t K = __ldcg(&ctl->n_records);
     // Phase 3: stable write of (slot, mask) records in array order.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
+        // only the keys phase 1 marked are hashed again
         const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
-        uint32_t slots[PER], hvs[PER];
-        uint32_t c = 0;
-        KeyHash<BATCH> kh;
-        if (base < n) kh.start(B, c0 + base);
-#pragma unroll
-        for (int j = 0; j < PER; ++j) {
-            const uint64_t i = base + j;
-            slots[j] = NONE;
-            hvs[j] = 0;
-            if (i < n && !(D.skip && ((__ldg(D.skip + (i >> 5)) >> (i & 31)) & 1u))) {
-                const uint32_t b = kh.bucket(D, B, c0 + i, __ldg(keys + i), hvs[j]);
-                slots[j] = flagged_slot(D, skey, sval, use_set, b);
-                c += slots[j] != NONE ? 1u : 0u;
-            }
-        }
+        const uint32_t hit = base < n ? __ldcg(D.hits + (base >> 3)) : 0u;
         uint32_t total;
-        uint32_t pos = block_exclusive_scan(c, &total) + __ldcg(D.tile_counts + t);
-#pragma unroll
-        for (int j = 0; j < PER; ++j) {
-            if (slots[j] != NONE) {
-                const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hvs[j]));
-                __stcg(D.rec[0] + pos, make_uint2(slots[j], mask));
+        uint32_t pos = block_exclusive_scan((uint32_t)__popc(hit), &total) + __ldcg(D.tile_counts + t);
+        if (hit) {
+            KeyHash<BATCH> kh;
+            kh.start(B, c0 + base);
+            for (uint32_t m = hit; m; m &= m - 1) {
+                const int j = __ffs(m) - 1;
+                uint32_t hv;
+                const uint32_t b = kh.bucket(D, B, c0 + base + j, __ldg(keys + base + j), hv);
+                const uint32_t slot = flagged_slot(D, skey, sval, use_set, b);
+                const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hv));
+                __stcg(D.rec[0] + pos, make_uint2(slot, mask));
                 ++pos;
             }
         }
@@ -1093,8 +1088,10 @@ __global__ void __launch_bounds__(QRY_THREADS) k_batch_query(const uint32_t* __r
 
 // ---- launchers ----------------------------------------------------------------------------
 
-// Pass-1 kernels by aggregation mode and lanes per key (4, 8, 16, 32).
-int lpk_index(int lpk) { return lpk == 4 ? 0 : lpk == 16 ? 2 : lpk == 32 ? 3 : 1; }
+// Pass-1 kernels by aggregation mode and lanes per key (1, 2, 4, 8, 16, 32).
+int lpk_index(int lpk) {
+    return lpk == 4 ? 0 : lpk == 16 ? 2 : lpk == 32 ? 3 : lpk == 2 ? 4 : lpk == 1 ? 5 : 1;
+}
 
 template <int AGG>
 const void* ins_fn(int li, bool batch) {
@@ -1102,6 +1099,8 @@ const void* ins_fn(int li, bool batch) {
         case 0: return batch ? (const void*)k_batch_insert<AGG, 4> : (const void*)k_msws_insert<AGG, 4>;
         case 2: return batch ? (const void*)k_batch_insert<AGG, 16> : (const void*)k_msws_insert<AGG, 16>;
         case 3: return batch ? (const void*)k_batch_insert<AGG, 32> : (const void*)k_msws_insert<AGG, 32>;
+        case 4: return batch ? (const void*)k_batch_insert<AGG, 2> : (const void*)k_msws_insert<AGG, 2>;
+        case 5: return batch ? (const void*)k_batch_insert<AGG, 1> : (const void*)k_msws_insert<AGG, 1>;
         default: return batch ? (const void*)k_batch_insert<AGG, 8> : (const void*)k_msws_insert<AGG, 8>;
     }
 }
@@ -1128,7 +1127,7 @@ cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
     // process: set it for the largest mask table (16384 words); the launch passes the actual size.
     const size_t ins_smem = msws_insert_smem(n_masks);
     for (int agg = 0; agg < 3; ++agg)
-        for (int li = 0; li < 4; ++li)
+        for (int li = 0; li < LPK_VARIANTS; ++li)
             for (int batch = 0; batch < 2; ++batch) {
                 const void* fn = ins_fn(agg, li, batch != 0);
                 e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -241,7 +241,7 @@ def test_mixed_config3_full_size(gpu):
     sk.sync()
 
 
-@pytest.mark.parametrize("lpk", [4, 16, 32])
+@pytest.mark.parametrize("lpk", [1, 2, 4, 16, 32])
 @pytest.mark.parametrize("agg", [1, 3])
 def test_lanes_per_key_variants_bit_exact(gpu, lpk, agg):
     # Every pass-1 width gives the oracle's tables and estimates on a stream that links
