@@ -516,6 +516,49 @@ __device__ __forceinline__ void tile_count(RadixSmem& rs, const uint2* src, uint
     __syncthreads();
 }
 
+// One stable counting pass over at most REPAIR_TILE records held in shared memory, by the
+// 8-bit digit at `shift` (warp w owns records [256w, 256w + 256), as in tile_count).
+__device__ __forceinline__ void smem_radix_pass(RadixSmem& rs, const uint2* src, uint2* dst, uint32_t K, int shift) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    constexpr int NW = REPAIR_THREADS / 32;
+    for (int d = threadIdx.x; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
+    __syncthreads();
+    for (int r = 0; r < 256 / 32; ++r) {
+        const uint32_t i = wid * 256 + r * 32 + lane;
+        const bool v = i < K;
+        const uint32_t d = v ? (src[i].x >> shift) & 0xffu : 256u + lane;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // digit d starts at the records of all smaller digits; within d, warp order keeps stability
+    uint32_t tot = 0;
+    if (threadIdx.x < 256)
+        for (int w = 0; w < NW; ++w) tot += rs.whist[w][threadIdx.x];
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(tot, &total);
+    if (threadIdx.x < 256)
+        for (int w = 0; w < NW; ++w) {
+            const uint32_t x = rs.whist[w][threadIdx.x];
+            rs.whist[w][threadIdx.x] = run;
+            run += x;
+        }
+    __syncthreads();
+    for (int r = 0; r < 256 / 32; ++r) {
+        const uint32_t i = wid * 256 + r * 32 + lane;
+        const bool v = i < K;
+        const uint2 rec = v ? src[i] : make_uint2(0, 0);
+        const uint32_t d = v ? (rec.x >> shift) & 0xffu : 256u + lane;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        if (v) dst[rs.whist[wid][d] + __popc(peers & lanemask_lt())] = rec;
+        __syncwarp();
+        if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+}
+
 // ---- per-bucket replay (one warp per flagged bucket; lane i keeps counter i) ------------
 // The chunk's keys of a flagged bucket, in array order, are replayed with the sequential
 // semantics of device_sketch_v3.h:88-191: the pre-chunk counters are restored (final word
@@ -761,7 +804,24 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     // Phase 4: stable LSD radix sort of the records by slot, 8 bits per pass.
     const int npass = radix_passes(F);
     const uint32_t ntr = (K + REPAIR_TILE - 1) / REPAIR_TILE;
-    for (int p = 0; p < npass; ++p) {
+    const uint2* sorted = D.rec[npass & 1];
+    if (ntr <= 1 && npass > 0) {
+        // One tile: block 0 sorts it in shared memory (the flagged-bucket set is no longer
+        // needed; its 64 KiB hold two tiles of records), the others wait at one barrier.
+        static_assert(2 * SET_SLOTS * 4 >= 2 * REPAIR_TILE * 8, "two record tiles fit the set's space");
+        if (blockIdx.x == 0) {
+            uint2* a = reinterpret_cast<uint2*>(s_set);
+            uint2* c = a + REPAIR_TILE;
+            for (uint32_t i = tid; i < K; i += REPAIR_THREADS) a[i] = __ldcg(D.rec[0] + i);
+            __syncthreads();
+            for (int p = 0; p < npass; ++p) smem_radix_pass(rs, (p & 1) ? c : a, (p & 1) ? a : c, K, 8 * p);
+            const uint2* res = (npass & 1) ? c : a;
+            for (uint32_t i = tid; i < K; i += REPAIR_THREADS) __stcg(D.rec[1] + i, res[i]);
+        }
+        sorted = D.rec[1];
+        if (!grid_barrier(ctl)) return;
+    }
+    for (int p = 0; p < npass && ntr > 1; ++p) {
         const uint2* src = D.rec[p & 1];
         uint2* dst = D.rec[(p + 1) & 1];
         const int shift = 8 * p;
@@ -807,7 +867,6 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         if (!grid_barrier(ctl)) return;
     }
     phase_mark(ctl, 3);
-    const uint2* sorted = D.rec[npass & 1];
 
     // Phase 5: segment starts, and per-counter totals of slots < long_cap; each block a
     // contiguous record range whose first and last slot accumulate in shared memory.
