@@ -161,29 +161,11 @@ def dist_setup(gpus):
 
 def init_ranks(args):
     """One process per GPU; returns (world, rank, local, barrier, max_over_ranks)."""
-    import datetime
+    from qsketch_b200.replicas import Ranks
 
-    import torch
-    import torch.distributed as dist
-
-    world, rank, local = dist_setup(args.gpus)
-    torch.cuda.set_device(local)
-    if world > 1:
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    return world, rank, local, barrier, max_over_ranks
+    dist_setup(args.gpus)
+    r = Ranks(backend="nccl")
+    return r.world, r.rank, r.local, r.barrier, r.max
 
 
 def run_ours(args, cfg):
