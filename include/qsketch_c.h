@@ -57,6 +57,12 @@ typedef enum qs_kind {
 #define QS_FLAG_COMPAT_V3 0x1u /* reproduce device_sketch_v3.h:187: the key that links a
                                   bucket adds its high increments at index (bit % 8)
                                   instead of at the bit's own counter */
+#define QS_FLAG_NO_CHUNK_RAMP 0x2u /* insert in chunks of max_batch from the first key.  By
+                                     default the chunks after a create or clear grow from
+                                     first_chunk keys (f, f, 2f, 4f, ... max_batch): the buckets of
+                                     heavy keys then link in a small first chunk instead of
+                                     sending all their occurrences of a large chunk through the
+                                     ordered replay.  Results never depend on the chunking. */
 
 /* Creation parameters.  Zero-initialise and set what you need; qs_params_default()
  * fills the reference defaults (lib/default.cu:39-54). */
@@ -100,6 +106,8 @@ typedef struct qs_params {
                                     bucket's index word first, 2 = read it with the counter
                                     atomic (8 lanes per key only), 3 = adaptive per tile */
     uint32_t ctas_per_sm;        /* pass-1 CTAs per SM, 0 = as many as fit */
+    uint64_t first_chunk;        /* first chunk of the ramp after a create or clear (multiple
+                                    of 32); 0 = 2^18, or the autotuner's choice */
 } qs_params;
 
 typedef struct qs_sketch qs_sketch;
@@ -300,16 +308,17 @@ qs_status qs_mlp_train(qs_learned *lk, const uint32_t *d_keys, const uint8_t *d_
 
 /* ---- autotuner (no counterpart in the reference) -----------------------------------------
  * Times pass-1 knob settings (lanes per key 1-32, aggregation, routing, CTAs per SM, chunk size
- * max_batch; every setting gives identical results) on a scratch sketch built from `base`
+ * max_batch, the chunk ramp after a clear; every setting gives identical results) on a scratch sketch built from `base`
  * over the caller's sample keys (device memory, inserted `reps` times after a clear), by a
  * coordinate search from the defaults: lanes per key, then aggregation, routing, CTAs per
- * SM, chunk size.  The fastest setting is returned in *best, recorded in a process-wide
+ * SM, chunk size, ramp.  The fastest setting is returned in *best, recorded in a process-wide
  * table for the size class floor(log2(n_low)) of `base`, and used by later qs_create calls
  * of that class whose knobs are all 0.  h_all (may be null) receives up to max_all of the
  * timed settings, *n_all how many were timed. */
 typedef struct qs_tune_config {
     uint32_t lanes_per_key, aggregate, route, ctas_per_sm;
     uint64_t max_batch;
+    uint64_t first_chunk; /* chunk-size ramp after a clear; 0 = no ramp */
     double insert_ms; /* mean time of one insert of the sample (pass 1 + ordered replay) */
 } qs_tune_config;
 

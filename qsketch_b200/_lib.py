@@ -21,6 +21,7 @@ QS_ERR_CAPACITY = 7
 QS_KIND_MSWS = 0
 QS_KIND_PLAIN_CM = 1
 QS_FLAG_COMPAT_V3 = 0x1
+QS_FLAG_NO_CHUNK_RAMP = 0x2
 
 
 class qs_params(ctypes.Structure):
@@ -46,6 +47,7 @@ class qs_params(ctypes.Structure):
         ("aggregate", ctypes.c_uint32),
         ("route", ctypes.c_uint32),
         ("ctas_per_sm", ctypes.c_uint32),
+        ("first_chunk", ctypes.c_uint64),
     ]
 
 
@@ -131,7 +133,8 @@ class qs_batch_params(ctypes.Structure):
 
 class qs_tune_config(ctypes.Structure):
     _fields_ = [("lanes_per_key", ctypes.c_uint32), ("aggregate", ctypes.c_uint32), ("route", ctypes.c_uint32),
-                ("ctas_per_sm", ctypes.c_uint32), ("max_batch", ctypes.c_uint64), ("insert_ms", ctypes.c_double)]
+                ("ctas_per_sm", ctypes.c_uint32), ("max_batch", ctypes.c_uint64), ("first_chunk", ctypes.c_uint64),
+                ("insert_ms", ctypes.c_double)]
 
 
 class qs_batch_info(ctypes.Structure):

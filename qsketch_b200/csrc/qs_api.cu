@@ -88,6 +88,8 @@ struct qs_sketch {
     int device = 0;
     uint32_t kind = 0;
     uint64_t max_batch = 0;
+    uint64_t fresh = 0;       // keys inserted since create / clear (drives the chunk-size ramp)
+    uint64_t ramp_first = 0;  // first chunk of the ramp, 0 = no ramp
     int agg = 1;
     std::vector<uint32_t> seeds;
     std::vector<uint32_t> masks;  // mask words
@@ -223,15 +225,22 @@ qs_status setup_io(qs_sketch* sk) {
 qs_status insert_device(qs_sketch* sk, const uint32_t* d_keys, size_t n, cudaStream_t st,
                         const uint32_t* skip = nullptr) {
     if (sk->kind == QS_KIND_MSWS) {
-        for (size_t off = 0; off < n; off += sk->max_batch) {
-            const uint64_t c = std::min<uint64_t>(sk->max_batch, n - off);
+        for (size_t off = 0; off < n;) {
+            uint64_t c = std::min<uint64_t>(sk->max_batch, n - off);
+            // after a create or clear the chunks grow geometrically from ramp_first keys, so
+            // the buckets of heavy keys link in a small first chunk (sizes stay multiples of 32)
+            if (sk->ramp_first && sk->fresh < sk->max_batch)
+                c = std::min<uint64_t>(c, std::max<uint64_t>(sk->ramp_first, sk->fresh));
+            off += c;
+            sk->fresh += c;
+            const uint64_t start = off - c;
             MswsDev D = sk->D;
-            D.skip = skip ? skip + off / 32 : nullptr;
+            D.skip = skip ? skip + start / 32 : nullptr;
             CK(sk->prof_begin(0, st), "profile");
-            CK(msws_insert_pass(d_keys + off, c, D, sk->L, sk->agg, st), "msws insert");
+            CK(msws_insert_pass(d_keys + start, c, D, sk->L, sk->agg, st), "msws insert");
             CK(sk->prof_end(0, st), "profile");
             CK(sk->prof_begin(1, st), "profile");
-            CK(msws_repair(d_keys + off, c, D, sk->L, st), "msws repair");
+            CK(msws_repair(d_keys + start, c, D, sk->L, st), "msws repair");
             CK(sk->prof_end(1, st), "profile");
         }
     } else {
@@ -338,6 +347,11 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
     sk->device = dev;
     sk->kind = p.kind;
     sk->max_batch = p.max_batch ? p.max_batch : (1ull << 22);
+    if (p.first_chunk & 31) {
+        delete sk;
+        return fail(QS_ERR_INVALID_ARG, "first_chunk must be a multiple of 32");
+    }
+    sk->ramp_first = (p.flags & QS_FLAG_NO_CHUNK_RAMP) ? 0 : (p.first_chunk ? p.first_chunk : (1ull << 18));
     if (sk->max_batch > (1ull << 30) || (sk->max_batch & 31)) {
         delete sk;
         return fail(QS_ERR_INVALID_ARG, "max_batch must be a multiple of 32 and at most 2^30");
@@ -376,6 +390,7 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         if (tuned) {
             sk->agg = (int)tc.aggregate - 1;
             if (!p.max_batch && tc.max_batch) sk->max_batch = tc.max_batch;
+            if (!p.first_chunk && !(p.flags & QS_FLAG_NO_CHUNK_RAMP)) sk->ramp_first = tc.first_chunk;
         }
         std::vector<uint8_t> bytes((size_t)H * 4);
         if (p.mask_table) {
@@ -560,6 +575,7 @@ qs_status qs_clear(qs_sketch* sk, void* stream) {
         CK(cudaMemsetAsync(sk->D.low, 0, sk->D.n_low * LOW_WORDS * 4, st), "clear low");
         CK(cudaMemsetAsync(sk->D.high, 0, sk->D.n_high * HIGH_WORDS * 4, st), "clear high");
         CK(cudaMemsetAsync(sk->D.bitmap, 0, (sk->D.n_low + 31) / 32 * 4, st), "clear bitmap");
+        sk->fresh = 0;
         return ctl_reset(sk, st);
     }
     CK(cudaMemsetAsync(sk->C.table, 0, sk->C.n * sk->C.rows * 4, st), "clear table");
@@ -1610,6 +1626,7 @@ qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, u
         sk->agg = (int)c.aggregate - 1;
         sk->D.route = c.route == 3 ? 0u : c.route;
         sk->max_batch = std::min(c.max_batch, alloc_mb);
+        sk->ramp_first = c.first_chunk;
         double tot = 0;
         for (uint32_t r = 0; r <= reps; ++r) {  // the first round warms up
             qs_status q = qs_clear(sk, st);
@@ -1628,7 +1645,7 @@ qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, u
         ++timed;
         return QS_OK;
     };
-    qs_tune_config cur{8u, 3u, 1u, 0u, std::min<uint64_t>(1ull << 22, mbs.back()), 0.0};
+    qs_tune_config cur{8u, 3u, 1u, 0u, std::min<uint64_t>(1ull << 22, mbs.back()), 1ull << 18, 0.0};
     s = run(cur);
     if (s != QS_OK) return cleanup(s);
     auto consider = [&](qs_tune_config c) -> qs_status {
@@ -1662,6 +1679,11 @@ qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, u
         if (mb == cur.max_batch) continue;
         qs_tune_config c = cur;
         c.max_batch = mb;
+        if ((s = consider(c)) != QS_OK) return cleanup(s);
+    }
+    for (uint64_t first : {0ull, 1ull << 20}) {
+        qs_tune_config c = cur;
+        c.first_chunk = first;
         if ((s = consider(c)) != QS_OK) return cleanup(s);
     }
     if (n_all) *n_all = timed;

@@ -22,8 +22,8 @@ import ctypes
 
 import numpy as np
 
-from ._lib import (QS_FLAG_COMPAT_V3, QS_KIND_MSWS, QS_KIND_PLAIN_CM, QsError, check, lib, qs_params,
-                   qs_profile, qs_stats)
+from ._lib import (QS_FLAG_COMPAT_V3, QS_FLAG_NO_CHUNK_RAMP, QS_KIND_MSWS, QS_KIND_PLAIN_CM, QsError, check, lib,
+                   qs_params, qs_profile, qs_stats)
 
 try:  # torch only supplies device memory and the current stream
     import torch
@@ -210,11 +210,11 @@ class Sketch_GPU_Sub_Warp_Level(Sketch):
     def __init__(self, n_low=0, m_low=8, n_high=1024, m_high=32, seed_sz=1, n_hash_mask_table=1021, *,
                  low_bytes=0, hash_mask_ones=3, hash_seed=0, seed_rng=1, mask_rng=1, mask_table=None,
                  compat_v3=False, max_batch=0, device=None, aggregate=0, lanes_per_key=0, route=0,
-                 ctas_per_sm=0):
+                 ctas_per_sm=0, chunk_ramp=True):
         p = qs_params()
         lib.qs_params_default(ctypes.byref(p))
         p.kind = QS_KIND_MSWS
-        p.flags = QS_FLAG_COMPAT_V3 if compat_v3 else 0
+        p.flags = (QS_FLAG_COMPAT_V3 if compat_v3 else 0) | (0 if chunk_ramp else QS_FLAG_NO_CHUNK_RAMP)
         p.n_low, p.low_bytes, p.m_low, p.m_high, p.n_high = n_low, low_bytes, m_low, m_high, n_high
         p.seed_sz, p.hash_mask_table_sz, p.hash_mask_ones = seed_sz, n_hash_mask_table, hash_mask_ones
         p.hash_seed, p.seed_rng, p.mask_rng = hash_seed, seed_rng, mask_rng

@@ -279,3 +279,14 @@ def test_autotune_picks_a_timed_setting_and_create_uses_it(gpu):
     assert torch.equal(tuned.search(q), plain.search(q))
     autotune.reset()
     assert autotune.lookup(524287) is None
+
+
+@pytest.mark.parametrize("ramp", [True, False])
+def test_chunk_ramp_on_and_off_bit_exact(gpu, ramp):
+    # After a clear the chunks grow from 2^18 keys (or not); both give the oracle's tables.
+    sk, orc = make_pair(131071, 1 << 14, max_batch=1 << 21, chunk_ramp=ramp)
+    keys = data.zipf_keys(3 << 20, 1 << 18, 1.2, seed=51, perm_seed=9)
+    run_and_compare(sk, orc, keys, data.rank_keys(9, 0, 1 << 16), pieces=[1000, (1 << 20) - 1000, 2 << 20])
+    sk.clear()
+    orc2 = make_pair(131071, 1 << 14)[1]
+    run_and_compare(sk, orc2, keys[:1 << 20], data.rank_keys(9, 0, 1 << 16))
