@@ -403,6 +403,7 @@ __global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* 
 
 constexpr int SET_CAP = 4096;    // flagged buckets looked up in a per-block shared-memory set
 constexpr int SET_SLOTS = 8192;  // open addressing, load factor <= 1/2
+constexpr uint32_t SCAN_CAP = SET_SLOTS;  // records replayed without a sort (2 * SET_SLOTS words)
 constexpr uint32_t NONE = 0xffffffffu;
 
 __device__ __forceinline__ int radix_passes(uint32_t F) {
@@ -510,49 +511,6 @@ __device__ __forceinline__ void tile_count(RadixSmem& rs, const uint2* src, uint
         const bool v = i < K;
         const uint32_t d = v ? (__ldcg(&src[i].x) >> shift) & 0xffu : 256u + lane;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
-        __syncwarp();
-    }
-    __syncthreads();
-}
-
-// One stable counting pass over at most REPAIR_TILE records held in shared memory, by the
-// 8-bit digit at `shift` (warp w owns records [256w, 256w + 256), as in tile_count).
-__device__ __forceinline__ void smem_radix_pass(RadixSmem& rs, const uint2* src, uint2* dst, uint32_t K, int shift) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    constexpr int NW = REPAIR_THREADS / 32;
-    for (int d = threadIdx.x; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
-    __syncthreads();
-    for (int r = 0; r < 256 / 32; ++r) {
-        const uint32_t i = wid * 256 + r * 32 + lane;
-        const bool v = i < K;
-        const uint32_t d = v ? (src[i].x >> shift) & 0xffu : 256u + lane;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
-        __syncwarp();
-    }
-    __syncthreads();
-    // digit d starts at the records of all smaller digits; within d, warp order keeps stability
-    uint32_t tot = 0;
-    if (threadIdx.x < 256)
-        for (int w = 0; w < NW; ++w) tot += rs.whist[w][threadIdx.x];
-    uint32_t total;
-    uint32_t run = block_exclusive_scan(tot, &total);
-    if (threadIdx.x < 256)
-        for (int w = 0; w < NW; ++w) {
-            const uint32_t x = rs.whist[w][threadIdx.x];
-            rs.whist[w][threadIdx.x] = run;
-            run += x;
-        }
-    __syncthreads();
-    for (int r = 0; r < 256 / 32; ++r) {
-        const uint32_t i = wid * 256 + r * 32 + lane;
-        const bool v = i < K;
-        const uint2 rec = v ? src[i] : make_uint2(0, 0);
-        const uint32_t d = v ? (rec.x >> shift) & 0xffu : 256u + lane;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        if (v) dst[rs.whist[wid][d] + __popc(peers & lanemask_lt())] = rec;
-        __syncwarp();
         if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
         __syncwarp();
     }
@@ -699,6 +657,49 @@ __device__ __forceinline__ void replay_slot(const MswsDev& D, const BatchDev& B,
     finish_bucket<BATCH>(D, B, b, L != NONE, L != NONE ? end - L : 0u, end - beg, T, P, cur, mL);
 }
 
+// Replay slot s straight from the chunk's records in array order (all K of them staged in
+// shared memory): steps of 32 records without one of this slot skip after one ballot.  The
+// slot's counter totals and record count come from the write phase (slots < long_cap).
+template <bool BATCH>
+__device__ __forceinline__ void replay_slot_scan(const MswsDev& D, const BatchDev& B, const uint2* srec, uint32_t s,
+                                                 uint32_t K) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t b = __ldcg(D.flag_list + s);
+    uint32_t T = 0, n_total = 0;
+    if (s < D.long_cap) {  // accumulated while the records were written
+        T = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane) : 0u;
+        n_total = __ldcg(D.seg_beg + s);
+    } else {
+        for (uint32_t g = 0; g < K; g += 32) {
+            const uint2 r = g + lane < K ? srec[g + lane] : make_uint2(NONE, 0u);
+            const bool hit = r.x == s;
+            const uint32_t hb = __ballot_sync(0xffffffffu, hit);
+            if (!hb) continue;
+            n_total += __popc(hb);
+            count_counters(hit ? r.y : 0u, T);
+        }
+    }
+    const uint32_t P = pre_counters(D.low + (uint64_t)b * LOW_WORDS, T);
+    uint32_t cur = P, mL = 0, before = 0;
+    bool found = false;
+    for (uint32_t g = 0; g < K; g += 32) {
+        const uint2 r = g + lane < K ? srec[g + lane] : make_uint2(NONE, 0u);
+        const bool hit = r.x == s;
+        const uint32_t hb = __ballot_sync(0xffffffffu, hit);
+        if (!hb) continue;
+        const uint32_t m = hit ? r.y : 0u;
+        const int j = link_step(m, cur);
+        if (j >= 0) {
+            found = true;
+            before += __popc(hb & ((1u << j) - 1u));
+            mL = __shfl_sync(0xffffffffu, m, j);
+            break;
+        }
+        before += __popc(hb);
+    }
+    finish_bucket<BATCH>(D, B, b, found, found ? n_total - before : 0u, n_total, T, P, cur, mL);
+}
+
 // BATCH: the keys are the window of a batch's flat key array that starts at flat index
 // B.win[0]; n is read from the window (the launch's own n is ignored).
 template <bool BATCH>
@@ -745,6 +746,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     }
     const uint32_t ntot = min(F, D.long_cap);
     for (uint32_t i = gtid; i < ntot * LOW_COUNTERS; i += nthreads) __stcg(D.totals + i, 0u);
+    for (uint32_t i = gtid; i < ntot; i += nthreads) __stcg(D.seg_beg + i, 0u);  // record counts (scan mode)
 
     // Phase 1: count keys of flagged buckets per tile of the chunk.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
@@ -777,6 +779,9 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 1);
     const uint32_t K = __ldcg(&ctl->n_records);
+    // Few records (K <= SCAN_CAP): the replay scans them unsorted, and the per-slot counter
+    // totals and record counts it needs are accumulated here with global atomics.
+    const bool scan_mode = K <= SCAN_CAP;
     // Phase 3: stable write of (slot, mask) records in array order.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
         // only the keys phase 1 marked are hashed again
@@ -795,33 +800,46 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
                 const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hv));
                 __stcg(D.rec[0] + pos, make_uint2(slot, mask));
                 ++pos;
+                if (scan_mode && slot < D.long_cap) {
+                    for (uint32_t mm = mask; mm; mm &= mm - 1)
+                        atomicAdd(D.totals + (uint64_t)slot * LOW_COUNTERS + (__ffs(mm) - 1), 1u);
+                    atomicAdd(D.seg_beg + slot, 1u);
+                }
             }
         }
     }
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 2);
 
+    // Few records: no sort.  Every block that replays a slot stages all K records in shared
+    // memory (the flagged-bucket set is no longer needed; its 64 KiB hold SCAN_CAP records)
+    // and each warp scans them for its slot in array order.
+    if (scan_mode) {
+        constexpr int NWB = REPAIR_THREADS / 32;
+        if (blockIdx.x * NWB < F) {
+            uint2* srec = reinterpret_cast<uint2*>(s_set);
+            for (uint32_t i = tid; i < K; i += REPAIR_THREADS) srec[i] = __ldcg(D.rec[0] + i);
+            __syncthreads();
+            for (uint32_t s = blockIdx.x * NWB + wid; s < F; s += gridDim.x * NWB)
+                replay_slot_scan<BATCH>(D, B, srec, s, K);
+        }
+        if (!grid_barrier(ctl)) return;
+        phase_mark(ctl, 5);
+        if (blockIdx.x == 0 && tid == 0) {
+            ctl->n_flagged = 0;
+            ctl->n_records = 0;
+            ctl->n_long = 0;
+            ctl->repairs += 1;
+            __threadfence();
+        }
+        return;
+    }
+
     // Phase 4: stable LSD radix sort of the records by slot, 8 bits per pass.
     const int npass = radix_passes(F);
     const uint32_t ntr = (K + REPAIR_TILE - 1) / REPAIR_TILE;
     const uint2* sorted = D.rec[npass & 1];
-    if (ntr <= 1 && npass > 0) {
-        // One tile: block 0 sorts it in shared memory (the flagged-bucket set is no longer
-        // needed; its 64 KiB hold two tiles of records), the others wait at one barrier.
-        static_assert(2 * SET_SLOTS * 4 >= 2 * REPAIR_TILE * 8, "two record tiles fit the set's space");
-        if (blockIdx.x == 0) {
-            uint2* a = reinterpret_cast<uint2*>(s_set);
-            uint2* c = a + REPAIR_TILE;
-            for (uint32_t i = tid; i < K; i += REPAIR_THREADS) a[i] = __ldcg(D.rec[0] + i);
-            __syncthreads();
-            for (int p = 0; p < npass; ++p) smem_radix_pass(rs, (p & 1) ? c : a, (p & 1) ? a : c, K, 8 * p);
-            const uint2* res = (npass & 1) ? c : a;
-            for (uint32_t i = tid; i < K; i += REPAIR_THREADS) __stcg(D.rec[1] + i, res[i]);
-        }
-        sorted = D.rec[1];
-        if (!grid_barrier(ctl)) return;
-    }
-    for (int p = 0; p < npass && ntr > 1; ++p) {
+    for (int p = 0; p < npass; ++p) {
         const uint2* src = D.rec[p & 1];
         uint2* dst = D.rec[(p + 1) & 1];
         const int shift = 8 * p;
