@@ -2,7 +2,7 @@
 """QSketch insert/query throughput on B200 — one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config zipf|uniform|mixed|learned|batched|zipf_prof]
+                    [--config zipf|uniform|mixed|learned|batched|zipf_prof|batched_prof]
 
 A step is one pass of the hot path over one batch of synthetic input: clear the sketch,
 insert the whole key stream, query the distinct keys.  The default workload is the
@@ -54,6 +54,11 @@ CONFIGS = {
     # n_low = prime <= bytes/32, high pool bytes/4; inserted and queried in one batch each
     "batched": dict(workload="512_streams_len_2^10..2^22_zipf0.6..1.4_2^20ranks_sketch32KB..16MB_pool_bytes/4",
                     kind=4, n_streams=512, n_keys=0, n_ranks=1 << 20, s=0.0, n_low=0, n_high=0, n_query=0),
+    # a smaller batch for Nsight Compute captures: 64 streams of 2^10..2^21 keys (key stream
+    # and tables still larger than L2)
+    "batched_prof": dict(workload="64_streams_len_2^10..2^21_zipf0.6..1.4_2^20ranks_sketch32KB..16MB_pool_bytes/4",
+                         kind=4, n_streams=64, max_len=1 << 21, n_keys=0, n_ranks=1 << 20, s=0.0, n_low=0, n_high=0,
+                         n_query=0),
     # a smaller skewed case for Nsight Compute captures (key stream still larger than L2)
     "zipf_prof": dict(workload="zipf1.1_2^25keys_2^22ranks_low16MB_high4MB_query2^22", kind=1, n_keys=1 << 25,
                       n_ranks=1 << 22, s=1.1, n_low=524287, n_high=1 << 15, n_query=1 << 22),
@@ -517,7 +522,7 @@ def run_learned(args, cfg):
 def run_batched(args, cfg):
     """512 uneven streams, each with its own sketch, in one batch (qs_batch_*).  A step is:
     clear every sketch, insert every stream, query every stream's keys.  Beside it: the same
-    streams through 512 separate sketches one call after another, and the latency of a small
+    streams through as many separate sketches one call after another, and the latency of a small
     serving batch eager vs replayed from a CUDA graph."""
     import torch
     import torch.distributed as dist
@@ -529,7 +534,7 @@ def run_batched(args, cfg):
     world, rank, local, barrier, max_over_ranks = init_ranks(args)
     stream = torch.cuda.current_stream()
     S = cfg["n_streams"]
-    w = data.uneven_streams(S, seed=1000 + rank, n_ranks=cfg["n_ranks"])
+    w = data.uneven_streams(S, seed=1000 + rank, n_ranks=cfg["n_ranks"], max_len=cfg.get("max_len", 1 << 22))
     keys, offs = w["keys"], w["offsets"]
     total = keys.numel()
     out = torch.empty(total, dtype=torch.uint32, device="cuda")
@@ -666,7 +671,7 @@ def run_batched(args, cfg):
             "insert_gkeys_per_s": round(world * total / (ins_ms * 1e6), 4),
             "query_gkeys_per_s": round(world * total / (q_ms * 1e6), 4),
             "alone": {"ms": round(alone_ms, 3), "gkeys_per_s": round(2 * total / (alone_ms * 1e6), 4),
-                      "note": "the same streams through 512 separate sketches, one insert + one query call each"},
+                      "note": "the same streams through %d separate sketches, one insert + one query call each" % S},
             "serving_batch": {"keys": int(sv_keys.numel()), "eager_ms": round(lat["eager"], 4),
                               "graph_ms": round(lat["graph"], 4), "graph_capture": int(graph_ok),
                               "note": "insert + query of the first 1024 keys of every stream, host wall time"},
