@@ -27,7 +27,11 @@ constexpr int INS_THREADS = 256;
 constexpr int INS_WARPS = INS_THREADS / 32;
 constexpr int INS_TILE = 2048;  // keys per TMA stage (8 KiB)
 constexpr int INS_STAGES = 3;
+constexpr int INS_MIN_CTAS = 4;  // resident pass-1 CTAs per SM the register budget is cut for (6 measured slower)
 constexpr int AGG_SLOTS = 1024; // per-CTA table merging the linked keys of a tile
+// mbarriers of the stages (+ one spare word), padded so the uint4 staging area that follows
+// the 4-byte tables stays 16-byte aligned for any stage count
+constexpr int INS_BAR_BYTES = (INS_STAGES * 8 + 8 + 15) & ~15;
 constexpr int AGG_PROBES = 32;
 constexpr uint32_t AGG_EMPTY = 0xffffffffu;
 
@@ -62,7 +66,7 @@ __device__ __forceinline__ InsShared ins_carve(uint8_t* smem, uint32_t n_masks) 
     S.keys = reinterpret_cast<uint32_t*>(p);
     p += INS_STAGES * INS_TILE * 4;
     S.bar = reinterpret_cast<uint64_t*>(p);
-    p += INS_STAGES * 8 + 8;
+    p += INS_BAR_BYTES;
     S.akey = reinterpret_cast<uint32_t*>(p);
     p += AGG_SLOTS * 4;
     S.acnt = reinterpret_cast<uint32_t*>(p);
@@ -78,8 +82,12 @@ __device__ __forceinline__ InsShared ins_carve(uint8_t* smem, uint32_t n_masks) 
     return S;
 }
 
+// the carve above: TMA stages 16-byte aligned, mbarriers 8-byte, the uint4 staging 16-byte
+static_assert((INS_STAGES * INS_TILE * 4) % 16 == 0, "stage bytes");
+static_assert((INS_STAGES * INS_TILE * 4 + INS_BAR_BYTES + 3 * AGG_SLOTS * 4) % 16 == 0, "uint4 staging alignment");
+
 size_t msws_insert_smem(uint32_t n_masks) {
-    return (size_t)INS_STAGES * INS_TILE * 4 + INS_STAGES * 8 + 8 + 3 * AGG_SLOTS * 4 + INS_WARPS * 32 * 16 + 16 +
+    return (size_t)INS_STAGES * INS_TILE * 4 + INS_BAR_BYTES + 3 * AGG_SLOTS * 4 + INS_WARPS * 32 * 16 + 16 +
            (size_t)n_masks * 4;
 }
 
@@ -300,7 +308,7 @@ __device__ __forceinline__ void drain_table(const MswsDev& D, const InsShared& S
 }
 
 template <int AGG, int LPK>
-__global__ void __launch_bounds__(INS_THREADS, 4) k_msws_insert(const uint32_t* __restrict__ keys, uint64_t n,
+__global__ void __launch_bounds__(INS_THREADS, INS_MIN_CTAS) k_msws_insert(const uint32_t* __restrict__ keys, uint64_t n,
                                                                 MswsDev D) {
     extern __shared__ __align__(128) uint8_t smem[];
     const InsShared S = ins_carve(smem, D.n_masks);
@@ -1081,7 +1089,7 @@ __device__ __forceinline__ uint32_t stream_of_item(const BatchDev& B, uint32_t i
 // all belong to one stream, so they hash with its descriptor and the tile's shared-memory
 // merge table never mixes sketches.  Everything after hashing is the single-sketch pass 1.
 template <int AGG, int LPK>
-__global__ void __launch_bounds__(INS_THREADS, 4) k_batch_insert(const uint32_t* __restrict__ keys, MswsDev D,
+__global__ void __launch_bounds__(INS_THREADS, INS_MIN_CTAS) k_batch_insert(const uint32_t* __restrict__ keys, MswsDev D,
                                                                  BatchDev B) {
     extern __shared__ __align__(128) uint8_t smem[];
     const InsShared S = ins_carve(smem, D.n_masks);
