@@ -759,7 +759,6 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     // Phase 1: count keys of flagged buckets per tile of the chunk.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
         const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
-        uint32_t c = 0;
         KeyHash<BATCH> kh;
         if (base < n) kh.start(B, c0 + base);
         uint32_t hit = 0;
