@@ -409,9 +409,11 @@ __global__ void __launch_bounds__(INS_THREADS, INS_MIN_CTAS) k_msws_insert(const
 
 // ---- ordered replay ---------------------------------------------------------------------
 
-constexpr int SET_CAP = 4096;    // flagged buckets looked up in a per-block shared-memory set
-constexpr int SET_SLOTS = 8192;  // open addressing, load factor <= 1/2
-constexpr uint32_t SCAN_CAP = SET_SLOTS;  // records replayed without a sort (2 * SET_SLOTS words)
+constexpr int SET_CAP = 8192;     // flagged buckets looked up in a per-block shared-memory set
+constexpr int SET_SLOTS = 16384;  // bucket ids only, open addressing, load factor <= 1/2 (64 KiB)
+constexpr int SET_BITS = 14;
+constexpr uint32_t SCAN_CAP = SET_SLOTS / 2;  // records replayed without a sort (the set's 64 KiB)
+static_assert((1 << SET_BITS) == SET_SLOTS, "set size");
 constexpr uint32_t NONE = 0xffffffffu;
 
 __device__ __forceinline__ int radix_passes(uint32_t F) {
@@ -420,20 +422,23 @@ __device__ __forceinline__ int radix_passes(uint32_t F) {
     return (bits + 7) / 8;
 }
 
-// Slot of bucket b if it was flagged in this chunk, else NONE.
-__device__ __forceinline__ uint32_t flagged_slot(const MswsDev& D, const uint32_t* skey, const uint32_t* sval,
-                                                 bool use_set, uint32_t b) {
+// Was bucket b flagged in this chunk?  The shared-memory set when it holds them all, else
+// the bitmap in global memory.
+__device__ __forceinline__ bool is_flagged(const MswsDev& D, const uint32_t* skey, bool use_set, uint32_t b) {
     if (use_set) {
-        const uint32_t h = (b * 0x9E3779B1u) >> 19;  // 13 bits
+        const uint32_t h = (b * 0x9E3779B1u) >> (32 - SET_BITS);
         for (int p = 0; p < SET_SLOTS; ++p) {
-            const uint32_t s = (h + p) & (SET_SLOTS - 1);
-            const uint32_t k = skey[s];
-            if (k == b) return sval[s];
-            if (k == NONE) return NONE;
+            const uint32_t k = skey[(h + p) & (SET_SLOTS - 1)];
+            if (k == b) return true;
+            if (k == NONE) return false;
         }
-        return NONE;
+        return false;
     }
-    if (!((__ldcg(D.bitmap + (b >> 5)) >> (b & 31)) & 1u)) return NONE;
+    return (__ldcg(D.bitmap + (b >> 5)) >> (b & 31)) & 1u;
+}
+
+// Slot of a flagged bucket: pass 1 left FLAG | slot in its index word.
+__device__ __forceinline__ uint32_t flagged_slot(const MswsDev& D, uint32_t b) {
     return __ldcg(D.low + (uint64_t)b * LOW_WORDS + 7) & ~FLAG;
 }
 
@@ -505,7 +510,7 @@ struct RadixSmem {
     uint32_t whist[REPAIR_THREADS / 32][256];
 };
 
-size_t msws_repair_smem() { return (size_t)2 * SET_SLOTS * 4; }
+size_t msws_repair_smem() { return (size_t)SET_SLOTS * 4; }
 
 // Stable ranking of a tile of REPAIR_TILE records by the 8-bit digit at `shift`: each of
 // the 16 warps owns 256 consecutive records; per-warp digit counts, then per digit an
@@ -718,7 +723,6 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     __shared__ uint32_t s_acc_slot[2];
     extern __shared__ __align__(16) uint32_t s_set[];
     uint32_t* skey = s_set;
-    uint32_t* sval = s_set + SET_SLOTS;
     Ctl* ctl = D.ctl;
     const uint32_t F = min(__ldcg(&ctl->n_flagged), D.flag_cap);
     if (F == 0) return;
@@ -741,14 +745,9 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         __syncthreads();
         for (uint32_t s = tid; s < F; s += REPAIR_THREADS) {
             const uint32_t b = __ldcg(D.flag_list + s);
-            uint32_t h = (b * 0x9E3779B1u) >> 19;
-            for (int p = 0; p < SET_SLOTS; ++p, ++h) {
-                const uint32_t x = h & (SET_SLOTS - 1);
-                if (atomicCAS(skey + x, NONE, b) == NONE) {
-                    sval[x] = s;
-                    break;
-                }
-            }
+            uint32_t h = (b * 0x9E3779B1u) >> (32 - SET_BITS);
+            for (int p = 0; p < SET_SLOTS; ++p, ++h)
+                if (atomicCAS(skey + (h & (SET_SLOTS - 1)), NONE, b) == NONE) break;
         }
         __syncthreads();
     }
@@ -768,7 +767,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             if (i < n && !(D.skip && ((__ldg(D.skip + (i >> 5)) >> (i & 31)) & 1u))) {
                 uint32_t hv;
                 const uint32_t b = kh.bucket(D, B, c0 + i, __ldg(keys + i), hv);
-                if (flagged_slot(D, skey, sval, use_set, b) != NONE) hit |= 1u << j;
+                if (is_flagged(D, skey, use_set, b)) hit |= 1u << j;
             }
         }
         __stcg(D.hits + (base >> 3), (uint8_t)hit);  // PER == 8: one byte per thread
@@ -803,7 +802,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
                 const int j = __ffs(m) - 1;
                 uint32_t hv;
                 const uint32_t b = kh.bucket(D, B, c0 + base + j, __ldg(keys + base + j), hv);
-                const uint32_t slot = flagged_slot(D, skey, sval, use_set, b);
+                const uint32_t slot = flagged_slot(D, b);
                 const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hv));
                 __stcg(D.rec[0] + pos, make_uint2(slot, mask));
                 ++pos;
