@@ -760,13 +760,24 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
         KeyHash<BATCH> kh;
         if (base < n) kh.start(B, c0 + base);
+        // the 8 keys: two 16-byte loads when whole and aligned (base is a multiple of 8, so
+        // the 8 skip bits lie in one word)
+        uint32_t k[PER];
+        if (base + PER <= n && !(reinterpret_cast<uintptr_t>(keys + base) & 15u)) {
+            const uint4 a = __ldg(reinterpret_cast<const uint4*>(keys + base));
+            const uint4 c = __ldg(reinterpret_cast<const uint4*>(keys + base) + 1);
+            k[0] = a.x, k[1] = a.y, k[2] = a.z, k[3] = a.w, k[4] = c.x, k[5] = c.y, k[6] = c.z, k[7] = c.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < PER; ++j) k[j] = base + j < n ? __ldg(keys + base + j) : 0u;
+        }
+        const uint32_t skip8 = (D.skip && base < n) ? (__ldg(D.skip + (base >> 5)) >> (base & 31)) & 0xffu : 0u;
         uint32_t hit = 0;
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
-            const uint64_t i = base + j;
-            if (i < n && !(D.skip && ((__ldg(D.skip + (i >> 5)) >> (i & 31)) & 1u))) {
+            if (base + j < n && !((skip8 >> j) & 1u)) {
                 uint32_t hv;
-                const uint32_t b = kh.bucket(D, B, c0 + i, __ldg(keys + i), hv);
+                const uint32_t b = kh.bucket(D, B, c0 + base + j, k[j], hv);
                 if (is_flagged(D, skey, use_set, b)) hit |= 1u << j;
             }
         }
