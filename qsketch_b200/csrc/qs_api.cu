@@ -441,7 +441,7 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         CKB(sk->alloc(&D.hits, (uint64_t)D.max_tiles * (REPAIR_TILE / 8)), "alloc hit bits");
         CKB(sk->alloc(&D.rec[0], B), "alloc records");
         CKB(sk->alloc(&D.rec[1], B), "alloc records");
-        CKB(sk->alloc(&D.hist, (uint64_t)256 * D.max_tiles), "alloc histograms");
+        CKB(sk->alloc(&D.hist, (uint64_t)256 * D.max_tiles + 256), "alloc histograms");  // + digit totals
         CKB(sk->alloc(&D.seg_beg, cap), "alloc segments");
         CKB(sk->alloc(&D.totals, (uint64_t)D.long_cap * LOW_COUNTERS), "alloc totals");
         CKB(cudaMemcpy(masks_d, sk->masks.data(), (size_t)H * 4, cudaMemcpyHostToDevice), "upload masks");
@@ -756,6 +756,8 @@ struct qs_learned {
     std::vector<void*> allocs;
     uint32_t* warm = nullptr;
     uint64_t warm_seen = 0;
+    std::vector<uint32_t> tkeys;    // host mirror of the exact table's keys (changed only by admission)
+    uint32_t tfill = 0;             // keys in the exact table
     uint32_t* d_sorted = nullptr;   // admission order upload buffer
     uint32_t* d_cand_est = nullptr; // sketch estimates of the chunk's candidates
     uint32_t admit_cap = 0;
@@ -779,6 +781,20 @@ struct qs_learned {
 };
 
 namespace {
+
+// Admit `order` (most deserving first) into the exact table: placement on the host mirror,
+// then the mirror and the fill are uploaded (stream-ordered, synchronised: the mirror is
+// the source of the copy).
+qs_status learned_admit(qs_learned* lk, const uint32_t* order, uint32_t count, cudaStream_t st) {
+    const uint32_t fill = table_admit_host(lk->tkeys.data(), lk->T.slots, order, count, lk->tfill, lk->T.max_fill);
+    if (fill == lk->tfill) return QS_OK;
+    lk->tfill = fill;
+    CK(cudaMemcpyAsync(lk->T.keys, lk->tkeys.data(), (size_t)lk->T.slots * 4, cudaMemcpyHostToDevice, st),
+       "table upload");
+    CK(cudaMemcpyAsync(lk->T.fill, &lk->tfill, 4, cudaMemcpyHostToDevice, st), "fill upload");
+    CK(cudaStreamSynchronize(st), "admit sync");
+    return QS_OK;
+}
 
 qs_status mlp_init_params(qs_learned* lk) {
     // He-uniform hidden layers, Glorot-uniform output, zero biases; deterministic in init_seed
@@ -846,15 +862,14 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     CKT(cudaMalloc(&d_set, (size_t)set_slots * 4), "train set");
     CKT(cudaMalloc(&d_distinct, W * 4 + 4), "train distinct");
     CKT(cudaMalloc(&d_cnt, 8), "train count");
-    CKT(distinct_keys(lk->warm, W, d_set, set_slots, d_distinct, d_cnt, st), "distinct");
-    uint32_t hc[2] = {0, 0};
-    CKT(cudaMemcpyAsync(hc, d_cnt, 8, cudaMemcpyDeviceToHost, st), "distinct count");
+    // the warm-up window's distinct keys in ascending order (a fixed order for training)
+    CKT(distinct_sorted(lk->warm, (uint32_t)W, d_set, d_distinct, d_cnt, st), "distinct");
+    uint32_t hc = 0;
+    CKT(cudaMemcpyAsync(&hc, d_cnt, 4, cudaMemcpyDeviceToHost, st), "distinct count");
     CKT(cudaStreamSynchronize(st), "distinct sync");
-    const uint64_t D = hc[0];
+    const uint64_t D = hc;
     std::vector<uint32_t> keys(D);
     CKT(cudaMemcpy(keys.data(), d_distinct, D * 4, cudaMemcpyDeviceToHost), "distinct copy");
-    std::sort(keys.begin(), keys.end());  // a fixed order, whatever the set's layout
-    CKT(cudaMemcpy(d_distinct, keys.data(), D * 4, cudaMemcpyHostToDevice), "distinct upload");
     // labels from the sketch's own estimates
     CKT(cudaMalloc(&d_est, D * 4 + 4), "train est");
     qs_status s = query_device(lk->sk, d_distinct, D, d_est, st);
@@ -873,28 +888,33 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     uint64_t npos = 0;
     for (uint64_t i = 0; i < D; ++i) npos += (lab[i] = est[i] >= thr ? 1 : 0);
     const float pw = std::min(lk->p.max_pos_weight, (float)(D - npos) / (float)std::max<uint64_t>(1, npos));
-    // epochs over a seeded shuffle of the examples
+    // epochs over a seeded order of the examples, drawn on the device per epoch
+    uint8_t* d_lab_sorted = nullptr;
     CKT(cudaMalloc(&d_lab, D + 4), "train labels");
     CKT(cudaMalloc(&d_perm_keys, D * 4 + 4), "train keys");
-    std::vector<uint32_t> perm(D), pk(D);
-    std::vector<uint8_t> pl(D);
-    for (uint64_t i = 0; i < D; ++i) perm[i] = (uint32_t)i;
-    std::mt19937 g(lk->p.init_seed ^ 0x5bd1e995u);
+    CKT(cudaMalloc(&d_lab_sorted, D + 4), "train labels");
+    {
+        const cudaError_t e = cudaMemcpy(d_lab_sorted, lab.data(), D, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(d_lab_sorted);
+            CKT(e, "train labels upload");
+        }
+    }
     double loss = 0.0, first = -1.0;
-    for (uint32_t ep = 0; ep < lk->p.epochs; ++ep) {
-        std::shuffle(perm.begin(), perm.end(), g);
-        for (uint64_t i = 0; i < D; ++i) {
-            pk[i] = keys[perm[i]];
-            pl[i] = lab[perm[i]];
+    for (uint32_t ep = 0; ep < lk->p.epochs && s == QS_OK; ++ep) {
+        const uint64_t seed = ((uint64_t)lk->p.init_seed << 32) ^ (0x5bd1e995ull * (ep + 1));
+        const cudaError_t e = permute_examples(d_distinct, d_lab_sorted, (uint32_t)D, seed, d_perm_keys, d_lab, st);
+        if (e != cudaSuccess) {
+            cudaFree(d_lab_sorted);
+            CKT(e, "permute examples");
         }
-        CKT(cudaMemcpy(d_perm_keys, pk.data(), D * 4, cudaMemcpyHostToDevice), "train keys upload");
-        CKT(cudaMemcpy(d_lab, pl.data(), D, cudaMemcpyHostToDevice), "train labels upload");
         s = mlp_train_pass(lk, d_perm_keys, d_lab, D, lk->p.batch, lk->p.lr, pw, &loss, st);
-        if (s != QS_OK) {
-            cleanup();
-            return s;
-        }
         if (first < 0) first = loss;
+    }
+    cudaFree(d_lab_sorted);
+    if (s != QS_OK) {
+        cleanup();
+        return s;
     }
     // predictions on the warm-up keys: admit the predicted heavy, most confident first
     CKT(cudaMalloc(&d_logit, D * 4 + 4), "train logits");
@@ -929,13 +949,13 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     std::vector<uint32_t> order(take);
     for (uint32_t i = 0; i < take; ++i) order[i] = heavy[i].second;
     if (take) {
-        CKT(cudaMemcpy(lk->d_sorted, order.data(), take * 4, cudaMemcpyHostToDevice), "admit upload");
-        CKT(table_admit(lk->T, lk->d_sorted, take, st), "admit");
+        s = learned_admit(lk, order.data(), take, st);
+        if (s != QS_OK) {
+            cleanup();
+            return s;
+        }
     }
-    uint32_t fill = 0;
-    CKT(cudaMemcpyAsync(&fill, lk->T.fill, 4, cudaMemcpyDeviceToHost, st), "fill");
-    CKT(cudaStreamSynchronize(st), "admit sync");
-    lk->table_full = fill >= lk->T.max_fill;
+    lk->table_full = lk->tfill >= lk->T.max_fill;
     cleanup();
 #undef CKT
     qs_learned_info& I = lk->info;
@@ -984,7 +1004,7 @@ qs_status qs_learned_create(const qs_learned_params* p, qs_learned** out) {
     *out = nullptr;
     if (p->table_slots < 64 || (p->table_slots & (p->table_slots - 1)))
         return fail(QS_ERR_INVALID_ARG, "table_slots must be a power of two >= 64");
-    if (p->warmup_keys == 0 || p->heavy_fraction <= 0 || p->heavy_fraction >= 1 || p->batch == 0 || p->epochs == 0)
+    if (p->warmup_keys == 0 || p->warmup_keys > (1ull << 30) || p->heavy_fraction <= 0 || p->heavy_fraction >= 1 || p->batch == 0 || p->epochs == 0)
         return fail(QS_ERR_INVALID_ARG, "learned params out of range");
     const uint64_t mlp_bytes = (uint64_t)MLP_BF16_PARAMS * 2 + (uint64_t)(MLP_PARAMS - MLP_BF16_PARAMS) * 4;
     const uint64_t table_bytes = (uint64_t)p->table_slots * 8;
@@ -1019,6 +1039,7 @@ qs_status qs_learned_create(const qs_learned_params* p, qs_learned** out) {
     T.slots = p->table_slots;
     T.max_fill = (uint32_t)std::max(1.0f, p->table_max_fill * (float)p->table_slots);
     CKB(lk->alloc(&T.keys, T.slots, 0xff), "table keys");
+    lk->tkeys.assign(T.slots, TBL_EMPTY);
     CKB(lk->alloc(&T.counts, T.slots), "table counts");
     CKB(lk->alloc(&T.fill, 1), "table fill");
     RouteDev& R = lk->R;
@@ -1133,16 +1154,14 @@ qs_status qs_learned_insert(qs_learned* lk, const uint32_t* d_keys, size_t n, vo
             std::sort(order.begin(), order.end());
             const uint32_t take = std::min<uint32_t>(ncand, lk->admit_cap);
             for (uint32_t i = 0; i < take; ++i) cand[i] = order[i].second;
-            CK(cudaMemcpy(lk->d_sorted, cand.data(), take * 4, cudaMemcpyHostToDevice), "admit upload");
-            uint32_t before = 0, after = 0;
-            CK(cudaMemcpy(&before, lk->T.fill, 4, cudaMemcpyDeviceToHost), "fill");
-            CK(table_admit(lk->T, lk->d_sorted, take, st), "admit");
-            CK(cudaMemcpyAsync(&after, lk->T.fill, 4, cudaMemcpyDeviceToHost, st), "fill");
+            const uint32_t before = lk->tfill;
+            s = learned_admit(lk, cand.data(), take, st);
+            if (s != QS_OK) return s;
             CK(cudaMemsetAsync(lk->R.cand_keys, 0xff, (size_t)lk->R.cand_slots * 4, st), "candidate reset");
             CK(cudaMemsetAsync(lk->R.n_cand, 0, 4, st), "candidate reset");
             CK(cudaStreamSynchronize(st), "admit sync");
-            lk->info.admitted_after_warmup += after - before;
-            lk->table_full = after >= lk->T.max_fill;
+            lk->info.admitted_after_warmup += lk->tfill - before;
+            lk->table_full = lk->tfill >= lk->T.max_fill;
         }
         off += c;
     }

@@ -106,10 +106,14 @@ struct RouteDev {
 
 cudaError_t route_chunk(const uint32_t* d_keys, uint64_t n, const TableDev& T, const RouteDev& R, cudaStream_t st);
 cudaError_t classify_misses(const MlpDev& M, const RouteDev& R, uint64_t max_misses, cudaStream_t st);
-cudaError_t table_admit(const TableDev& T, const uint32_t* d_sorted, uint32_t count, cudaStream_t st);
+uint32_t table_admit_host(uint32_t* keys, uint32_t slots, const uint32_t* order, uint32_t count, uint32_t fill,
+                          uint32_t max_fill);
 cudaError_t learned_query(const uint32_t* d_keys, uint64_t n, const TableDev& T, const MswsDev& D, const MswsLaunch& L,
                           uint32_t* d_out, cudaStream_t st);
-cudaError_t distinct_keys(const uint32_t* d_keys, uint64_t n, uint32_t* d_set, uint32_t set_slots, uint32_t* d_out,
-                          uint32_t* d_count, cudaStream_t st);
+cudaError_t distinct_sorted(const uint32_t* d_keys, uint32_t n, uint32_t* d_tmp, uint32_t* d_out, uint32_t* d_count,
+                            cudaStream_t st);
+// Training examples in a seeded order (a Feistel-network bijection of [0, n)).
+cudaError_t permute_examples(const uint32_t* d_keys, const uint8_t* d_labels, uint32_t n, uint64_t seed,
+                             uint32_t* d_okeys, uint8_t* d_olabels, cudaStream_t st);
 
 }  // namespace qsb

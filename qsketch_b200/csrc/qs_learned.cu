@@ -1,5 +1,8 @@
-// qs_learned.cu — routing of the learned heavy-hitter split: exact-table lookups, hit counting,
-// the per-chunk skip bitmap for the sketch, table admission, and distinct-key extraction.
+// qs_learned.cu — the learned heavy-hitter split's routing (exact-table lookups, hit counting,
+// the per-chunk skip bitmap for the sketch), host-side table admission, and the training set
+// (distinct warm-up keys, per-epoch example order).
+#include <cub/cub.cuh>
+
 #include "qs_device.cuh"
 #include "qs_kernels.h"
 
@@ -84,60 +87,34 @@ __global__ void __launch_bounds__(RT_THREADS) k_route(const uint32_t* __restrict
     }
 }
 
-// Admit keys into the exact table in the given order, one thread, so the result does not
-// depend on scheduling: a key takes the first free slot along its sector probe sequence
-// (the sequence table_find follows) while the table holds fewer than max_fill keys.
-__global__ void k_table_admit(TableDev T, const uint32_t* __restrict__ sorted, uint32_t count) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    uint32_t fill = *T.fill;
-    const uint32_t nsec = T.slots / TBL_SECTOR;
-    for (uint32_t j = 0; j < count && fill < T.max_fill; ++j) {
-        const uint32_t key = sorted[j];
+// Admission into the exact table, on the host over a mirror of the table's key array (the
+// device array changes only by admission): in the given order, a key takes the first free
+// slot along its sector probe sequence — the sequence table_find follows — while the table
+// holds fewer than max_fill keys.  Returns the new fill; the caller uploads the mirror.
+uint32_t table_admit_host(uint32_t* keys, uint32_t slots, const uint32_t* order, uint32_t count, uint32_t fill,
+                          uint32_t max_fill) {
+    const uint32_t nsec = slots / TBL_SECTOR;
+    for (uint32_t j = 0; j < count && fill < max_fill; ++j) {
+        const uint32_t key = order[j];
         if (key == TBL_EMPTY) continue;
         const uint32_t s0 = mix32(key) & (nsec - 1);
         bool done = false;
         for (int p = 0; p < TBL_SECTOR_PROBES && !done; ++p) {
-            uint32_t* sk = T.keys + (uint64_t)((s0 + p) & (nsec - 1)) * TBL_SECTOR;
+            uint32_t* sk = keys + (uint64_t)((s0 + p) & (nsec - 1)) * TBL_SECTOR;
             for (int q = 0; q < TBL_SECTOR && !done; ++q) {
                 if (sk[q] == key) {
                     done = true;
                 } else if (sk[q] == TBL_EMPTY) {
-                    sk[q] = key;
-                    T.counts[(sk - T.keys) + q] = 0;
+                    sk[q] = key;  // its count slot is still 0: slots are never vacated
                     ++fill;
                     done = true;
                 }
             }
         }
     }
-    *T.fill = fill;
+    return fill;
 }
 
-// Distinct keys: insert into an open-addressing set, then gather the occupied slots.
-__global__ void k_set_insert(const uint32_t* __restrict__ keys, uint64_t n, uint32_t* set, uint32_t slots,
-                             uint32_t* overflow) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t key = keys[i];
-        if (key == 0xffffffffu) continue;
-        uint32_t h = mix32(key) & (slots - 1);
-        bool ok = false;
-        for (uint32_t p = 0; p < 4096; ++p, h = (h + 1) & (slots - 1)) {
-            const uint32_t prev = atomicCAS(set + h, 0xffffffffu, key);
-            if (prev == 0xffffffffu || prev == key) {
-                ok = true;
-                break;
-            }
-        }
-        if (!ok) atomicAdd(overflow, 1u);
-    }
-}
-
-__global__ void k_set_gather(const uint32_t* __restrict__ set, uint32_t slots, uint32_t* out, uint32_t* count) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < slots; i += gridDim.x * blockDim.x) {
-        const uint32_t k = set[i];
-        if (k != 0xffffffffu) out[atomicAdd(count, 1u)] = k;
-    }
-}
 
 cudaError_t route_chunk(const uint32_t* d_keys, uint64_t n, const TableDev& T, const RouteDev& R, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
@@ -147,20 +124,69 @@ cudaError_t route_chunk(const uint32_t* d_keys, uint64_t n, const TableDev& T, c
     return cudaGetLastError();
 }
 
-cudaError_t table_admit(const TableDev& T, const uint32_t* d_sorted, uint32_t count, cudaStream_t st) {
-    if (count == 0) return cudaSuccess;
-    k_table_admit<<<1, 1, 0, st>>>(T, d_sorted, count);
+
+// A seeded bijection of [0, n): a 4-round Feistel network on 2h bits (4^h >= n), walked
+// until it lands below n (each step is itself a bijection of [0, 4^h), so the walk is one
+// of [0, n)).  Expected walk length <= 4.
+struct FeistelPerm {
+    uint32_t h, mask, n, k[4];
+    __device__ __forceinline__ uint32_t step(uint32_t x) const {
+        uint32_t l = x >> h, r = x & mask;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t t = l ^ (mix32(r ^ k[i]) & mask);
+            l = r;
+            r = t;
+        }
+        return (l << h) | r;
+    }
+    __device__ __forceinline__ uint32_t operator()(uint32_t i) const {
+        uint32_t x = step(i);
+        while (x >= n) x = step(x);
+        return x;
+    }
+};
+
+// Training examples of one epoch in a seeded order: out[i] = in[perm(i)].
+__global__ void k_permute_examples(const uint32_t* __restrict__ keys, const uint8_t* __restrict__ labels,
+                                   FeistelPerm P, uint32_t* __restrict__ okeys, uint8_t* __restrict__ olabels) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+        const uint32_t j = P(i);
+        okeys[i] = __ldg(keys + j);
+        olabels[i] = __ldg(labels + j);
+    }
+}
+
+cudaError_t permute_examples(const uint32_t* d_keys, const uint8_t* d_labels, uint32_t n, uint64_t seed,
+                             uint32_t* d_okeys, uint8_t* d_olabels, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    FeistelPerm P;
+    P.n = n;
+    P.h = 1;
+    while ((1ull << (2 * P.h)) < n) ++P.h;
+    P.mask = (1u << P.h) - 1u;
+    for (int i = 0; i < 4; ++i) P.k[i] = mix32((uint32_t)(seed >> (16 * (i & 1))) ^ (0x9E3779B9u * (i + 1)));
+    k_permute_examples<<<148 * 8, 256, 0, st>>>(d_keys, d_labels, P, d_okeys, d_olabels);
     return cudaGetLastError();
 }
 
-cudaError_t distinct_keys(const uint32_t* d_keys, uint64_t n, uint32_t* d_set, uint32_t set_slots, uint32_t* d_out,
-                          uint32_t* d_count, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(d_set, 0xff, (size_t)set_slots * 4, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, 8, st);
+// Distinct keys in ascending order: a device radix sort into d_tmp (n words), then unique into
+// d_out; *d_count (device) receives how many.  The scratch of the two passes is allocated here.
+cudaError_t distinct_sorted(const uint32_t* d_keys, uint32_t n, uint32_t* d_tmp, uint32_t* d_out, uint32_t* d_count,
+                            cudaStream_t st) {
+    size_t b1 = 0, b2 = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortKeys(nullptr, b1, d_keys, d_tmp, n, 0, 32, st);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Unique(nullptr, b2, d_tmp, d_out, d_count, n, st);
     if (e != cudaSuccess) return e;
-    k_set_insert<<<148 * 8, 256, 0, st>>>(d_keys, n, d_set, set_slots, d_count + 1);
-    k_set_gather<<<148 * 8, 256, 0, st>>>(d_set, set_slots, d_out, d_count);
-    return cudaGetLastError();
+    void* scratch = nullptr;
+    e = cudaMalloc(&scratch, std::max<size_t>(std::max(b1, b2), 16));
+    if (e != cudaSuccess) return e;
+    e = cub::DeviceRadixSort::SortKeys(scratch, b1, d_keys, d_tmp, n, 0, 32, st);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Unique(scratch, b2, d_tmp, d_out, d_count, n, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(scratch);
+    return e;
 }
+
 
 }  // namespace qsb
