@@ -719,6 +719,7 @@ template <bool BATCH>
 __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* __restrict__ keys, uint64_t n,
                                                                 MswsDev D, BatchDev B) {
     __shared__ RadixSmem rs;
+    __shared__ uint32_t s_dbase[256];  // radix pass: first output position of each digit
     __shared__ uint32_t s_acc[2][LOW_COUNTERS];
     __shared__ uint32_t s_acc_slot[2];
     extern __shared__ __align__(16) uint32_t s_set[];
@@ -870,12 +871,37 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             __syncthreads();
         }
         if (!grid_barrier(ctl)) return;
-        if (blockIdx.x == 0) block_scan_array(D.hist, 256u * ntr);
+        // one warp per digit scans its row of tile counts (exclusive, in place) and stores the
+        // digit's total; then every block forms the 256 digit bases itself
+        uint32_t* dtot = D.hist + 256ull * D.max_tiles;
+        for (uint32_t d = blockIdx.x * NW + wid; d < 256; d += gridDim.x * NW) {
+            uint32_t* row = D.hist + (uint64_t)d * ntr;
+            uint32_t run = 0;
+            for (uint32_t t0 = 0; t0 < ntr; t0 += 32) {
+                const uint32_t t = t0 + lane;
+                const uint32_t v = t < ntr ? __ldcg(row + t) : 0u;
+                uint32_t x = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o) x += y;
+                }
+                if (t < ntr) __stcg(row + t, run + x - v);
+                run += __shfl_sync(0xffffffffu, x, 31);
+            }
+            if (lane == 0) __stcg(dtot + d, run);
+        }
         if (!grid_barrier(ctl)) return;
+        {
+            uint32_t total;
+            const uint32_t ex = block_exclusive_scan(tid < 256 ? __ldcg(dtot + tid) : 0u, &total);
+            if (tid < 256) s_dbase[tid] = ex;
+            __syncthreads();
+        }
         for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {  // stable scatter
             tile_count(rs, src, K, t, shift);
             for (int d = tid; d < 256; d += REPAIR_THREADS) {
-                uint32_t run = __ldcg(D.hist + (uint64_t)d * ntr + t);
+                uint32_t run = s_dbase[d] + __ldcg(D.hist + (uint64_t)d * ntr + t);
                 for (int w = 0; w < NW; ++w) {
                     const uint32_t x = rs.whist[w][d];
                     rs.whist[w][d] = run;

@@ -36,7 +36,7 @@ constexpr uint64_t NA_OFF_FLAGS = NA_OFF_REC1 + na_align(NA_MAX_KEYS * 8);
 constexpr uint64_t NA_OFF_SEG = NA_OFF_FLAGS + na_align(NA_MAX_KEYS * 4);
 constexpr uint64_t NA_OFF_TILES = NA_OFF_SEG + na_align(NA_MAX_KEYS * 4);
 constexpr uint64_t NA_OFF_HIST = NA_OFF_TILES + na_align(NA_TILES * 4);
-constexpr uint64_t NA_OFF_TOTALS = NA_OFF_HIST + na_align(256 * NA_TILES * 4);
+constexpr uint64_t NA_OFF_TOTALS = NA_OFF_HIST + na_align(256 * NA_TILES * 4 + 256 * 4);  // + digit totals
 constexpr uint64_t NA_OFF_BITMAP = NA_OFF_TOTALS + na_align(NA_TOTAL_SLOTS * LOW_COUNTERS * 4);
 constexpr uint64_t NA_OFF_HITS = NA_OFF_BITMAP + na_align(NA_MAX_BUCKETS / 8);
 constexpr uint64_t NA_BYTES = NA_OFF_HITS + na_align(NA_MAX_KEYS / 8);
