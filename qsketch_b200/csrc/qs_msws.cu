@@ -269,9 +269,14 @@ __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& 
     const bool sat = c && w7 == SATURATED;
     if (sat) atomicAdd(S.misc + 0, c);
     if (linked) atomicAdd(S.misc + 1, c);
-    bool direct_high = linked;
-    if (AGG == AGG_BLOCK && linked && use_table) direct_high = !agg_insert(S, key, c, w7);
-    const bool act = (c && !linked && !sat) || direct_high;
+    bool direct_high = linked, tabled = false;
+    if (AGG == AGG_BLOCK && use_table) {
+        if (linked)
+            direct_high = !agg_insert(S, key, c, w7);
+        else if (c >= 2 && !sat)  // a key repeated within the warp: likely heavy, merge the tile's
+            tabled = agg_insert(S, key, c, 0u);
+    }
+    const bool act = (c && !linked && !sat && !tabled) || direct_high;
     const uint32_t am = __ballot_sync(0xffffffffu, act);
     if (act) st[__popc(am & lanemask_lt())] = make_uint4(direct_high ? w7 : b, m, c, direct_high ? 1u : 0u);
     __syncwarp();
@@ -279,28 +284,34 @@ __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& 
     __syncwarp();
 }
 
-// Merged linked keys of the tile: one red per selected high counter per distinct key (the
-// tile's keys share the hash multiplier `seed`).
+// Merged keys of the tile: per distinct key one add of its count, to the selected high
+// counters of a linked bucket (id != 0) or, with crossing detection, to the low bucket (id 0:
+// a key repeated within a warp whose bucket is not linked; a count above 255 carries into
+// the next byte, but it also crosses, so the bucket is flagged and the replay restores its
+// pre-chunk words by subtraction, exact mod 2^32).  The tile's keys are of one sketch:
+// multiplier `seed`, `fm_low.d` buckets from bucket `base`.
 template <int LPK>
-__device__ __forceinline__ void drain_table(const MswsDev& D, const InsShared& S, uint32_t seed) {
+__device__ __forceinline__ void drain_table(const MswsDev& D, const InsShared& S, uint32_t seed,
+                                            const FastMod& fm_low, uint32_t base) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint4* st = S.stage + wid * 32;
-    for (int base = wid * 32; base < AGG_SLOTS; base += INS_THREADS) {
-        const int s = base + lane;
+    for (int s0 = wid * 32; s0 < AGG_SLOTS; s0 += INS_THREADS) {
+        const int s = s0 + lane;
         const uint32_t k = S.akey[s];
         const bool has = k != AGG_EMPTY;
-        uint32_t m = 0, c = 0, id = 0;
+        uint32_t m = 0, c = 0, id = 0, b = 0;
         if (has) {
             const uint32_t hv = k * seed;
             m = S.masks[fast_mod(D.fm_mask, hv)];
             c = S.acnt[s];
             id = S.aid[s];
+            if (id == 0) b = base + fast_mod(fm_low, hv);
             S.akey[s] = AGG_EMPTY;
             S.acnt[s] = 0;
         }
         const uint32_t am = __ballot_sync(0xffffffffu, has);
         if (!am) continue;
-        if (has) st[__popc(am & lanemask_lt())] = make_uint4(id, m, c, 1u);
+        if (has) st[__popc(am & lanemask_lt())] = id ? make_uint4(id, m, c, 1u) : make_uint4(b, m, c, 0u);
         __syncwarp();
         staged_rounds<LPK>(D, st, __popc(am));
         __syncwarp();
@@ -395,7 +406,7 @@ __global__ void __launch_bounds__(INS_THREADS, INS_MIN_CTAS) k_msws_insert(const
             S.misc[1] = 0;
         }
         if (AGG == AGG_BLOCK) {
-            drain_table<LPK>(D, S, D.seed);
+            drain_table<LPK>(D, S, D.seed, D.fm_low, 0u);
             __syncthreads();
         }
         if (tid == 0 && i + INS_STAGES < my_tiles) {
@@ -1177,7 +1188,7 @@ __global__ void __launch_bounds__(INS_THREADS, INS_MIN_CTAS) k_batch_insert(cons
             if (D.route == 0) S.misc[2] = S.misc[1] * 16u < (uint32_t)cnt ? ROUTE_FUSED : ROUTE_PRELOAD;
             S.misc[1] = 0;
         }
-        if (AGG == AGG_BLOCK) drain_table<LPK>(D, S, seed);
+        if (AGG == AGG_BLOCK) drain_table<LPK>(D, S, seed, fm, base);
         __syncthreads();
     }
     if (tid == 0 && S.misc[0]) atomicAdd(&D.ctl->dropped, (unsigned long long)S.misc[0]);
