@@ -215,8 +215,9 @@ def run_ours(args, cfg):
     # timed region; no knob changes any result); the sketch below takes them from its table
     from qsketch_b200 import autotune
     autotune.reset()
-    tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], keys, reps=2,
-                                 hash_seed=SEED, mask_rng=1)
+    # (the mixed workload inserts one batch at a time: tune on one batch, not the whole stream)
+    sample = ins_views[0] if cfg["kind"] == 2 else keys
+    tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], sample, reps=3, hash_seed=SEED, mask_rng=1)
     sk = qs.Sketch_GPU_Sub_Warp_Level(cfg["n_low"], 8, cfg["n_high"], 32, hash_seed=SEED, mask_rng=1)
     n_ins, n_q = cfg["n_keys"], cfg["n_query"]
     if cfg["kind"] == 2:

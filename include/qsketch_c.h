@@ -265,8 +265,8 @@ typedef struct qs_learned_params {
     uint64_t warmup_keys;      /* default 2^24 */
     double heavy_fraction;     /* default 0.005 */
     uint32_t epochs;           /* default 4 */
-    uint32_t batch;            /* training batch, default 4096 */
-    float lr;                  /* Adam step, default 2e-3 */
+    uint32_t batch;            /* training batch, default 16384 */
+    float lr;                  /* Adam step, default 4e-3 */
     float max_pos_weight;      /* positive-class weight cap, default 64 */
     float eligible_recall;     /* the logit cut for table eligibility keeps this share of
                                   the labelled-heavy warm-up keys, default 0.95 */

@@ -943,9 +943,11 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
         fn += !pred && lab[i];
         if (pred) heavy.push_back({-(double)est[i], keys[i]});
     }
-    // the network decides who may enter the table; the sketch's own counts rank them
-    std::sort(heavy.begin(), heavy.end());
+    // the network decides who may enter the table; the sketch's own counts rank them (only the
+    // first max_fill of the order can enter, so only they are sorted; keys are distinct, so the
+    // order is total)
     const uint32_t take = (uint32_t)std::min<uint64_t>(heavy.size(), lk->T.max_fill);
+    std::partial_sort(heavy.begin(), heavy.begin() + take, heavy.end());
     std::vector<uint32_t> order(take);
     for (uint32_t i = 0; i < take; ++i) order[i] = heavy[i].second;
     if (take) {
@@ -988,8 +990,8 @@ void qs_learned_params_default(qs_learned_params* p) {
     p->warmup_keys = 1ull << 24;
     p->heavy_fraction = 0.005;
     p->epochs = 4;
-    p->batch = 4096;
-    p->lr = 2e-3f;
+    p->batch = 16384;  // 256 tiles of 64 examples: one backward launch fills the GPU
+    p->lr = 4e-3f;
     p->max_pos_weight = 64.0f;
     p->eligible_recall = 0.95f;
     p->seed_rng = 1;
