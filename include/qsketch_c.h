@@ -355,6 +355,10 @@ typedef struct qs_batch_params {
     uint32_t aggregate, route;    /* as qs_params */
     uint32_t lanes_per_key, ctas_per_sm; /* as qs_params */
     uint64_t max_batch;           /* keys per window (replay scratch), default 2^22 */
+    uint64_t first_chunk;         /* per-stream chunk ramp of qs_batch_insert: rounds over every
+                                     stream's keys [0, f), [f, 2f), [2f, 4f), ... (windows of at
+                                     most max_batch keys); 0 = 2^14; QS_FLAG_NO_CHUNK_RAMP in
+                                     flags: flat windows of max_batch keys */
     int32_t device;
 } qs_batch_params;
 

@@ -127,6 +127,7 @@ class qs_batch_params(ctypes.Structure):
         ("lanes_per_key", ctypes.c_uint32),
         ("ctas_per_sm", ctypes.c_uint32),
         ("max_batch", ctypes.c_uint64),
+        ("first_chunk", ctypes.c_uint64),
         ("device", ctypes.c_int32),
     ]
 

@@ -12,7 +12,7 @@ import ctypes
 import numpy as np
 import torch
 
-from ._lib import QS_FLAG_COMPAT_V3, QsError, check, lib, qs_batch_info, qs_batch_params
+from ._lib import QS_FLAG_COMPAT_V3, QS_FLAG_NO_CHUNK_RAMP, QsError, check, lib, qs_batch_info, qs_batch_params
 from .sketch import _ptr, _stream
 
 
@@ -28,7 +28,7 @@ class BatchedSketches:
 
     def __init__(self, n_low, n_high, *, hash_seeds=None, seed_rng=1, mask_rng=1, hash_mask_table_sz=1021,
                  hash_mask_ones=3, compat_v3=False, aggregate=0, route=0, lanes_per_key=0, ctas_per_sm=0,
-                 max_batch=0, device=None):
+                 max_batch=0, first_chunk=0, chunk_ramp=True, device=None):
         nl = np.ascontiguousarray(n_low, dtype=np.uint64)
         nh = np.ascontiguousarray(n_high, dtype=np.uint64)
         if nl.shape != nh.shape or nl.ndim != 1:
@@ -46,7 +46,8 @@ class BatchedSketches:
             p.hash_seeds = seeds.ctypes.data
         p.seed_rng, p.mask_rng = seed_rng, mask_rng
         p.hash_mask_table_sz, p.hash_mask_ones = hash_mask_table_sz, hash_mask_ones
-        p.flags = QS_FLAG_COMPAT_V3 if compat_v3 else 0
+        p.flags = (QS_FLAG_COMPAT_V3 if compat_v3 else 0) | (0 if chunk_ramp else QS_FLAG_NO_CHUNK_RAMP)
+        p.first_chunk = first_chunk
         p.aggregate, p.route = aggregate, route
         p.lanes_per_key, p.ctas_per_sm = lanes_per_key, ctas_per_sm
         if max_batch:

@@ -1266,23 +1266,32 @@ struct qs_batch {
         uint64_t max_total = 0;
     } g[2];  // 0 insert, 1 query
     int graph_ok = -1;  // -1 not tried, 1 works, 0 capture unsupported here
+    uint64_t ramp_first = 0;  // per-stream chunk ramp of eager inserts: first slice, 0 = none
     qs_batch_info info{};
 };
 
 namespace {
 
 // `timed`: bracket the launches with the arena sketch's profiling events (not while capturing).
-qs_status batch_insert_seq(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets, uint64_t c0, uint64_t c1,
+BatchWindow flat_window(uint64_t c0, uint64_t c1) {
+    BatchWindow W{};
+    W.c0 = c0;
+    W.c1 = c1;
+    W.flat = 1;
+    return W;
+}
+
+qs_status batch_insert_seq(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets, const BatchWindow& W,
                            bool strict, cudaStream_t st, bool timed = true) {
     qs_sketch* sk = b->sk;
     BatchDev B = b->B;
     B.key_off = d_offsets;
-    CK(batch_plan(B, sk->D.ctl, c0, c1, strict, st), "batch plan");
+    CK(batch_plan(B, sk->D.ctl, W, strict, st), "batch plan");
     if (timed) CK(sk->prof_begin(0, st), "profile");
     CK(batch_insert_pass(d_keys, sk->D, B, sk->L, sk->agg, st), "batch insert");
     if (timed) CK(sk->prof_end(0, st), "profile");
     if (timed) CK(sk->prof_begin(1, st), "profile");
-    CK(batch_repair(d_keys + c0, sk->D, B, sk->L, st), "batch repair");
+    CK(batch_repair(d_keys, sk->D, B, sk->L, st), "batch repair");
     if (timed) CK(sk->prof_end(1, st), "profile");
     b->info.launches += 3;
     return QS_OK;
@@ -1293,7 +1302,7 @@ qs_status batch_query_seq(qs_batch* b, const uint32_t* d_keys, const uint64_t* d
     qs_sketch* sk = b->sk;
     BatchDev B = b->B;
     B.key_off = d_offsets;
-    CK(batch_plan(B, sk->D.ctl, 0, total, false, st), "batch plan");
+    CK(batch_plan(B, sk->D.ctl, flat_window(0, total), false, st), "batch plan");
     if (timed) CK(sk->prof_begin(2, st), "profile");
     CK(batch_query(d_keys, d_counts, sk->D, B, sk->L, st), "batch query");
     if (timed) CK(sk->prof_end(2, st), "profile");
@@ -1427,6 +1436,7 @@ qs_status qs_batch_create(const qs_batch_params* p, qs_batch** out) {
     CKB(sk->alloc(&B.lo, S), "alloc windows");
     CKB(sk->alloc(&B.hi, S), "alloc windows");
     CKB(sk->alloc(&B.item_off, (uint64_t)S + 1), "alloc work items");
+    CKB(sk->alloc(&B.wpre, (uint64_t)S + 1), "alloc window prefix");
     CKB(sk->alloc(&B.win, 2), "alloc window");
     CKB(sk->alloc(&B.work, 1), "alloc work queue");
     CKB(sk->alloc(&B.next_id, S), "alloc allocators");
@@ -1434,6 +1444,8 @@ qs_status qs_batch_create(const qs_batch_params* p, qs_batch** out) {
     CKB(cudaMemcpy(d_desc, desc.data(), (size_t)S * sizeof(StreamDesc), cudaMemcpyHostToDevice), "upload descriptors");
     std::vector<uint32_t> first(S, FIRST_ID);
     CKB(cudaMemcpy(B.next_id, first.data(), (size_t)S * 4, cudaMemcpyHostToDevice), "init allocators");
+    if (p->first_chunk & 31) return bail(fail(QS_ERR_INVALID_ARG, "first_chunk must be a multiple of 32"));
+    b->ramp_first = (p->flags & QS_FLAG_NO_CHUNK_RAMP) ? 0 : (p->first_chunk ? p->first_chunk : (1ull << 14));
     b->info.n_streams = S;
     b->info.low_buckets = tl;
     b->info.high_buckets = th;
@@ -1472,9 +1484,64 @@ qs_status qs_batch_insert(qs_batch* b, const uint32_t* d_keys, const uint64_t* d
     DeviceGuard guard(b->sk->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const uint64_t mb = b->sk->max_batch;
-    for (uint64_t c0 = 0; c0 < total; c0 += mb) {
-        s = batch_insert_seq(b, d_keys, d_offsets, c0, std::min(total, c0 + mb), false, st);
-        if (s != QS_OK) return s;
+    const uint32_t S = b->S;
+    // Per-stream chunk ramp: rounds over every stream's keys [0, f), [f, 2f), [2f, 4f), ...
+    // counted from the stream's start, so the hot buckets of each stream link on its first
+    // keys instead of sending most of its keys through the ordered replay.  Each round is cut
+    // into windows of at most max_batch keys.  Needs the offsets on the host; when they are
+    // not valid (or there is no ramp) the flat windows below run and the plan latches the error.
+    std::vector<uint64_t> off;
+    if (b->ramp_first) {
+        off.resize((size_t)S + 1);
+        CK(cudaMemcpyAsync(off.data(), d_offsets, off.size() * 8, cudaMemcpyDeviceToHost, st), "offsets copy");
+        CK(cudaStreamSynchronize(st), "offsets sync");
+        bool ok = off[0] == 0 && off[S] == total;
+        for (uint32_t i = 0; ok && i < S; ++i) ok = off[i + 1] >= off[i];
+        if (!ok) off.clear();
+    }
+    if (off.empty()) {
+        for (uint64_t c0 = 0; c0 < total; c0 += mb) {
+            s = batch_insert_seq(b, d_keys, d_offsets, flat_window(c0, std::min(total, c0 + mb)), false, st);
+            if (s != QS_OK) return s;
+        }
+        ++b->info.inserts;
+        return QS_OK;
+    }
+    uint64_t longest = 0;
+    for (uint32_t i = 0; i < S; ++i) longest = std::max(longest, off[i + 1] - off[i]);
+    auto run = [&](uint32_t s_lo, uint32_t s_hi, uint64_t r0, uint64_t r1) -> qs_status {
+        BatchWindow W{};
+        W.s_lo = s_lo;
+        W.s_hi = s_hi;
+        W.rel_lo = r0;
+        W.rel_hi = r1;
+        W.flat = 0;
+        return batch_insert_seq(b, d_keys, d_offsets, W, false, st);
+    };
+    for (uint64_t r0 = 0, r1 = b->ramp_first; r0 < longest; r0 = r1, r1 = std::max(r1 * 2, r1 + 1)) {
+        uint64_t acc = 0;
+        uint32_t first = 0;
+        for (uint32_t i = 0; i <= S; ++i) {
+            const uint64_t len = i < S ? off[i + 1] - off[i] : 0;
+            const uint64_t part = i < S ? std::min(len, r1) - std::min(len, r0) : 0;
+            if (i == S || acc + part > mb) {  // close the window [first, i)
+                if (acc) {
+                    s = run(first, i, r0, r1);
+                    if (s != QS_OK) return s;
+                }
+                acc = 0;
+                first = i;
+            }
+            if (part > mb) {  // one stream's slice alone exceeds a window: split it
+                for (uint64_t a = r0; a < std::min(len, r1); a += mb) {
+                    s = run(i, i + 1, a, std::min(std::min(len, r1), a + mb));
+                    if (s != QS_OK) return s;
+                }
+                first = i + 1;
+                continue;
+            }
+            acc += part;
+        }
     }
     ++b->info.inserts;
     return QS_OK;
@@ -1503,9 +1570,11 @@ qs_status qs_batch_insert_graph(qs_batch* b, const uint32_t* d_keys, const uint6
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     bool ran = false;
     s = batch_graph(b, 0, d_keys, d_offsets, nullptr, max_total, st,
-                    [&](cudaStream_t cs) { return batch_insert_seq(b, d_keys, d_offsets, 0, max_total, true, cs, false); },
+                    [&](cudaStream_t cs) {
+                        return batch_insert_seq(b, d_keys, d_offsets, flat_window(0, max_total), true, cs, false);
+                    },
                     &ran);
-    if (s == QS_OK && !ran) s = batch_insert_seq(b, d_keys, d_offsets, 0, max_total, true, st);
+    if (s == QS_OK && !ran) s = batch_insert_seq(b, d_keys, d_offsets, flat_window(0, max_total), true, st);
     if (s == QS_OK) ++b->info.inserts;
     return s;
 }

@@ -109,14 +109,27 @@ struct StreamDesc {
 struct BatchDev {
     const StreamDesc* desc;   // [n_streams]
     const uint64_t* key_off;  // [n_streams + 1] caller's offsets: stream s = keys[off[s], off[s+1])
-    uint64_t* lo;             // [n_streams] window-clipped first key of each stream
-    uint64_t* hi;             // [n_streams] window-clipped end
+    uint64_t* lo;             // [n_streams] first flat key of each stream's slice in the window
+    uint64_t* hi;             // [n_streams] end of that slice
     uint32_t* item_off;       // [n_streams + 1] prefix of work items (key tiles) per stream
-    uint64_t* win;            // [2] the window [c0, c1) of the flat key array this call covers
+    uint32_t* wpre;           // [n_streams + 1] prefix of the slices' key counts: window key i of
+                              // stream s is flat key lo[s] + i - wpre[s]
+    uint64_t* win;            // [2] 0 and the window's key count
     uint32_t* work;           // work-queue head
     uint32_t* next_id;        // [n_streams] per-stream bump allocators (from FIRST_ID)
     uint32_t* status;         // [n_streams] latched ST_* bits per stream
     uint32_t n_streams;       // 0: not a batch
+    uint32_t pad;
+};
+
+// Which keys one batched launch sequence covers: flat mode, the keys [c0, c1) of the caller's
+// flat array; else, for the streams [s_lo, s_hi), each stream's keys [rel_lo, rel_hi) counted
+// from the stream's start (the per-stream chunk ramp).
+struct BatchWindow {
+    uint64_t c0, c1;
+    uint64_t rel_lo, rel_hi;
+    uint32_t s_lo, s_hi;
+    uint32_t flat;
     uint32_t pad;
 };
 

@@ -25,7 +25,7 @@ cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L);
 // Pass 1 (packed atomics + crossing detection) and the ordered repair of one chunk of at
 // most max_batch keys; the repair exits at once when nothing crossed.
 // Batched streams (StreamDesc / BatchDev in qs_common.cuh).
-cudaError_t batch_plan(const BatchDev& B, Ctl* ctl, uint64_t c0, uint64_t c1, bool strict, cudaStream_t st);
+cudaError_t batch_plan(const BatchDev& B, Ctl* ctl, const BatchWindow& W, bool strict, cudaStream_t st);
 cudaError_t batch_insert_pass(const uint32_t* d_keys, const MswsDev& D, const BatchDev& B, const MswsLaunch& L,
                               int agg, cudaStream_t st);
 cudaError_t batch_repair(const uint32_t* d_window, const MswsDev& D, const BatchDev& B, const MswsLaunch& L,

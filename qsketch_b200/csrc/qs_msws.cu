@@ -468,13 +468,13 @@ __device__ __forceinline__ void phase_mark(Ctl* ctl, int k) {
     }
 }
 
-// Batched streams: the stream of flat key index f (< key_off[n_streams]), i.e. the last s
-// with key_off[s] <= f, which is never an empty stream.
-__device__ __forceinline__ uint32_t stream_of_key(const BatchDev& B, uint64_t f) {
-    uint32_t lo = 0, hi = B.n_streams;  // key_off[lo] <= f < key_off[hi]
+// Batched streams: the stream of window key i (< wpre[n_streams]), i.e. the last s with
+// wpre[s] <= i, which is never an empty slice.
+__device__ __forceinline__ uint32_t stream_of_window_key(const BatchDev& B, uint32_t i) {
+    uint32_t lo = 0, hi = B.n_streams;  // wpre[lo] <= i < wpre[hi]
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(B.key_off + mid) <= f)
+        if (__ldg(B.wpre + mid) <= i)
             lo = mid;
         else
             hi = mid;
@@ -495,21 +495,30 @@ __device__ __forceinline__ uint32_t stream_of_bucket(const BatchDev& B, uint32_t
     return lo;
 }
 
-// Hashing of the repair's key passes: one sketch, or a stream cursor over flat key indices
-// that only moves forward (a thread walks consecutive keys).
+// The repair's key passes: one sketch whose chunk is `keys[0, n)`, or a batch window whose key
+// i lies in stream s at flat index lo[s] + i - wpre[s]; a thread walks window keys in
+// increasing order, so the stream cursor only moves forward.
 template <bool BATCH>
-struct KeyHash {
+struct KeyMap {
     uint32_t s = 0;
-    __device__ __forceinline__ void start(const BatchDev& B, uint64_t f) {
-        if (BATCH) s = stream_of_key(B, f);
+    __device__ __forceinline__ void start(const BatchDev& B, uint32_t i) {
+        if (BATCH) s = stream_of_window_key(B, i);
     }
-    __device__ __forceinline__ uint32_t bucket(const MswsDev& D, const BatchDev& B, uint64_t f, uint32_t key,
-                                               uint32_t& hv) {
+    __device__ __forceinline__ uint64_t flat(const BatchDev& B, uint32_t i) {
+        if (!BATCH) return i;
+        while (i >= __ldg(B.wpre + s + 1)) ++s;
+        return __ldg(B.lo + s) + (i - __ldg(B.wpre + s));
+    }
+    // window keys of the current stream end here (exclusive)
+    __device__ __forceinline__ uint32_t end(const BatchDev& B) const {
+        return BATCH ? __ldg(B.wpre + s + 1) : 0xffffffffu;
+    }
+    // bucket of a key of the current stream
+    __device__ __forceinline__ uint32_t bucket(const MswsDev& D, const BatchDev& B, uint32_t key, uint32_t& hv) const {
         if (!BATCH) {
             hv = key * D.seed;
             return fast_mod(D.fm_low, hv);
         }
-        while (f >= __ldg(B.key_off + s + 1)) ++s;
         const StreamDesc* sd = B.desc + s;
         hv = key * __ldg(&sd->seed);
         const FastMod fm{__ldg(&sd->fm_low.M), __ldg(&sd->fm_low.d), 0u};
@@ -724,8 +733,8 @@ __device__ __forceinline__ void replay_slot_scan(const MswsDev& D, const BatchDe
     finish_bucket<BATCH>(D, B, b, found, found ? n_total - before : 0u, n_total, T, P, cur, mL);
 }
 
-// BATCH: the keys are the window of a batch's flat key array that starts at flat index
-// B.win[0]; n is read from the window (the launch's own n is ignored).
+// BATCH: `keys` is the batch's flat key array and the chunk is the window the plan kernel
+// described (B.wpre, B.lo); n is read from the window (the launch's own n is ignored).
 template <bool BATCH>
 __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* __restrict__ keys, uint64_t n,
                                                                 MswsDev D, BatchDev B) {
@@ -739,8 +748,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     const uint32_t F = min(__ldcg(&ctl->n_flagged), D.flag_cap);
     if (F == 0) return;
     phase_mark(ctl, -1);
-    const uint64_t c0 = BATCH ? __ldcg(B.win) : 0ull;
-    if (BATCH) n = __ldcg(B.win + 1) - c0;
+    if (BATCH) n = __ldcg(B.win + 1);
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     constexpr int NW = REPAIR_THREADS / 32;
@@ -770,26 +778,36 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     // Phase 1: count keys of flagged buckets per tile of the chunk.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
         const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
-        KeyHash<BATCH> kh;
-        if (base < n) kh.start(B, c0 + base);
-        // the 8 keys: two 16-byte loads when whole and aligned (base is a multiple of 8, so
-        // the 8 skip bits lie in one word)
+        KeyMap<BATCH> km;
+        uint64_t f0 = 0;
+        if (base < n) {
+            km.start(B, (uint32_t)base);
+            f0 = km.flat(B, (uint32_t)base);
+        }
+        // the 8 keys: two 16-byte loads when they are whole, contiguous (one stream) and
+        // aligned (base is a multiple of 8, so the 8 skip bits lie in one word)
         uint32_t k[PER];
-        if (base + PER <= n && !(reinterpret_cast<uintptr_t>(keys + base) & 15u)) {
-            const uint4 a = __ldg(reinterpret_cast<const uint4*>(keys + base));
-            const uint4 c = __ldg(reinterpret_cast<const uint4*>(keys + base) + 1);
+        const bool whole = base + PER <= n && base + PER <= km.end(B);
+        if (whole && !(reinterpret_cast<uintptr_t>(keys + f0) & 15u)) {
+            const uint4 a = __ldg(reinterpret_cast<const uint4*>(keys + f0));
+            const uint4 c = __ldg(reinterpret_cast<const uint4*>(keys + f0) + 1);
             k[0] = a.x, k[1] = a.y, k[2] = a.z, k[3] = a.w, k[4] = c.x, k[5] = c.y, k[6] = c.z, k[7] = c.w;
-        } else {
+        } else if (whole) {
 #pragma unroll
-            for (int j = 0; j < PER; ++j) k[j] = base + j < n ? __ldg(keys + base + j) : 0u;
+            for (int j = 0; j < PER; ++j) k[j] = __ldg(keys + f0 + j);
+        } else {
+            KeyMap<BATCH> kl = km;
+#pragma unroll
+            for (int j = 0; j < PER; ++j) k[j] = base + j < n ? __ldg(keys + kl.flat(B, (uint32_t)(base + j))) : 0u;
         }
         const uint32_t skip8 = (D.skip && base < n) ? (__ldg(D.skip + (base >> 5)) >> (base & 31)) & 0xffu : 0u;
         uint32_t hit = 0;
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
             if (base + j < n && !((skip8 >> j) & 1u)) {
+                if (BATCH) km.flat(B, (uint32_t)(base + j));  // moves the cursor to key j's stream
                 uint32_t hv;
-                const uint32_t b = kh.bucket(D, B, c0 + base + j, k[j], hv);
+                const uint32_t b = km.bucket(D, B, k[j], hv);
                 if (is_flagged(D, skey, use_set, b)) hit |= 1u << j;
             }
         }
@@ -819,12 +837,13 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         uint32_t total;
         uint32_t pos = block_exclusive_scan((uint32_t)__popc(hit), &total) + __ldcg(D.tile_counts + t);
         if (hit) {
-            KeyHash<BATCH> kh;
-            kh.start(B, c0 + base);
+            KeyMap<BATCH> km;
+            km.start(B, (uint32_t)base);
             for (uint32_t m = hit; m; m &= m - 1) {
                 const int j = __ffs(m) - 1;
+                const uint64_t f = km.flat(B, (uint32_t)(base + j));
                 uint32_t hv;
-                const uint32_t b = kh.bucket(D, B, c0 + base + j, __ldg(keys + base + j), hv);
+                const uint32_t b = km.bucket(D, B, __ldg(keys + f), hv);
                 const uint32_t slot = flagged_slot(D, b);
                 const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hv));
                 __stcg(D.rec[0] + pos, make_uint2(slot, mask));
@@ -1086,35 +1105,51 @@ cudaError_t learned_query(const uint32_t* d_keys, uint64_t n, const TableDev& T,
 // are tiles of at most INS_TILE keys of one stream; every size is read on the device, so
 // the launch sequence can be recorded once in a CUDA graph and replayed on new contents.
 
-// One block: clip the streams to the window, count their tiles, prefix-sum the counts,
-// reset the work queue.  Offsets that are not non-decreasing from 0 latch ST_BAD_OFFSETS
-// and empty the window; strict mode latches ST_CAPACITY if the keys run past c1.
-__global__ void __launch_bounds__(1024) k_batch_plan(BatchDev B, uint64_t c0, uint64_t c1, uint32_t strict,
-                                                     Ctl* ctl) {
+// One block: each stream's slice of the window (flat mode: the stream clipped to [c0, c1);
+// else for streams in [s_lo, s_hi) its keys [rel_lo, rel_hi) from its start), its tile count
+// and the prefix sums of tiles and keys; reset the work queue.  Offsets that are not
+// non-decreasing from 0 latch ST_BAD_OFFSETS and empty the window; strict (flat) mode
+// latches ST_CAPACITY if the keys run past c1.
+__global__ void __launch_bounds__(1024) k_batch_plan(BatchDev B, BatchWindow W, uint32_t strict, Ctl* ctl) {
     const uint32_t S = B.n_streams;
     bool bad = false;
     for (uint32_t s = threadIdx.x; s < S; s += blockDim.x)
         bad |= __ldcg(B.key_off + s + 1) < __ldcg(B.key_off + s);
     bad = __syncthreads_or(bad) || __ldcg(B.key_off) != 0;
     const uint64_t total = __ldcg(B.key_off + S);
-    const uint64_t e = bad ? c0 : umin64(c1, total);
-    const uint64_t b0 = umin64(c0, e);
+    const uint64_t e = bad ? W.c0 : umin64(W.c1, total);
+    const uint64_t b0 = umin64(W.c0, e);
     for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
-        const uint64_t lo = umin64(e, max(__ldcg(B.key_off + s), b0));
-        const uint64_t hi = umin64(e, max(__ldcg(B.key_off + s + 1), lo));
+        const uint64_t o0 = __ldcg(B.key_off + s), o1 = __ldcg(B.key_off + s + 1);
+        uint64_t lo, hi;
+        if (bad) {
+            lo = hi = 0;
+        } else if (W.flat) {
+            lo = umin64(e, max(o0, b0));
+            hi = umin64(e, max(o1, lo));
+        } else if (s >= W.s_lo && s < W.s_hi) {
+            const uint64_t len = o1 - o0;
+            lo = o0 + umin64(W.rel_lo, len);
+            hi = o0 + umin64(W.rel_hi, len);
+        } else {
+            lo = hi = o0;
+        }
         B.lo[s] = lo;
         B.hi[s] = hi;
         B.item_off[s] = (uint32_t)((hi - lo + INS_TILE - 1) / INS_TILE);
+        B.wpre[s] = (uint32_t)(hi - lo);
     }
     __syncthreads();
     const uint32_t items = block_scan_array(B.item_off, S);
+    const uint32_t keys = block_scan_array(B.wpre, S);
     if (threadIdx.x == 0) {
         B.item_off[S] = items;
-        B.win[0] = b0;
-        B.win[1] = e;
+        B.wpre[S] = keys;
+        B.win[0] = 0;
+        B.win[1] = keys;
         *B.work = 0;
         if (bad) atomicOr(&ctl->status, ST_BAD_OFFSETS);
-        if (strict && !bad && total > c1) atomicOr(&ctl->status, ST_CAPACITY);
+        if (strict && !bad && total > W.c1) atomicOr(&ctl->status, ST_CAPACITY);
     }
 }
 
@@ -1328,8 +1363,8 @@ cudaError_t msws_repair(const uint32_t* d_keys, uint64_t n, const MswsDev& D, co
                                        args, msws_repair_smem(), st);
 }
 
-cudaError_t batch_plan(const BatchDev& B, Ctl* ctl, uint64_t c0, uint64_t c1, bool strict, cudaStream_t st) {
-    k_batch_plan<<<1, 1024, 0, st>>>(B, c0, c1, strict ? 1u : 0u, ctl);
+cudaError_t batch_plan(const BatchDev& B, Ctl* ctl, const BatchWindow& W, bool strict, cudaStream_t st) {
+    k_batch_plan<<<1, 1024, 0, st>>>(B, W, strict ? 1u : 0u, ctl);
     return cudaGetLastError();
 }
 
@@ -1343,7 +1378,7 @@ cudaError_t batch_insert_pass(const uint32_t* d_keys, const MswsDev& D, const Ba
     return cudaLaunchKernel(ins_fn(agg, li, true), dim3(ins_grid(L, agg, li)), dim3(INS_THREADS), args, smem, st);
 }
 
-// d_window: the caller's flat key array advanced to the window start c0.
+// d_keys: the caller's flat key array (the window is described by the plan).
 cudaError_t batch_repair(const uint32_t* d_window, const MswsDev& D, const BatchDev& B, const MswsLaunch& L,
                          cudaStream_t st) {
     MswsDev Dc = D;

@@ -45,10 +45,14 @@ def check_streams(b, w, got, streams=None):
         assert torch.equal(g, want), f"stream {s}: {(g != want).sum().item()} of {g.numel()} estimates differ"
 
 
-@pytest.mark.parametrize("max_batch,lpk", [(1 << 16, 8), (1 << 22, 8), (1 << 18, 4), (1 << 18, 16)])
-def test_batch_equals_each_stream_alone(gpu, max_batch, lpk):
+@pytest.mark.parametrize("max_batch,lpk,first", [(1 << 16, 8, 0), (1 << 22, 8, 0), (1 << 18, 4, 0), (1 << 18, 16, 0),
+                                                (1 << 14, 4, 1 << 10), (1 << 15, 4, 1 << 16), (1 << 22, 4, None)])
+def test_batch_equals_each_stream_alone(gpu, max_batch, lpk, first):
+    # first: the per-stream chunk ramp's first slice (0 = default, None = flat windows); small
+    # windows split rounds and single streams across windows
     w = workload(64, seed=3, max_len=1 << 17)
-    b = BatchedSketches(w["n_low"], w["n_high"], seed_rng=7, max_batch=max_batch, lanes_per_key=lpk)
+    b = BatchedSketches(w["n_low"], w["n_high"], seed_rng=7, max_batch=max_batch, lanes_per_key=lpk,
+                        first_chunk=first or 0, chunk_ramp=first is not None)
     b.insert(w["keys"], w["offsets"])
     got = b.search(w["keys"], w["offsets"])
     b.sync()
