@@ -222,8 +222,11 @@ qs_status setup_io(qs_sketch* sk) {
 
 // skip: optional bitmap over the keys (bit set = the key is not for this sketch); chunk
 // offsets are multiples of max_batch, itself a multiple of 32.
+// table (learned split, optional): pass 1 looks keys up in this exact table itself, counts the
+// hits there and marks them in `skipbuf` (max_batch / 32 words, cleared per chunk here) for the
+// replay.
 qs_status insert_device(qs_sketch* sk, const uint32_t* d_keys, size_t n, cudaStream_t st,
-                        const uint32_t* skip = nullptr) {
+                        const uint32_t* skip = nullptr, const TableDev* table = nullptr, uint32_t* skipbuf = nullptr) {
     if (sk->kind == QS_KIND_MSWS) {
         for (size_t off = 0; off < n;) {
             uint64_t c = std::min<uint64_t>(sk->max_batch, n - off);
@@ -236,8 +239,17 @@ qs_status insert_device(qs_sketch* sk, const uint32_t* d_keys, size_t n, cudaStr
             const uint64_t start = off - c;
             MswsDev D = sk->D;
             D.skip = skip ? skip + start / 32 : nullptr;
+            MswsDev D1 = D;
+            if (table) {
+                CK(cudaMemsetAsync(skipbuf, 0, (c + 31) / 32 * 4, st), "skip bits");
+                D1.tbl_keys = table->keys;
+                D1.tbl_counts = table->counts;
+                D1.tbl_slots = table->slots;
+                D1.skip_out = skipbuf;
+                D.skip = skipbuf;  // the replay leaves the table's keys out
+            }
             CK(sk->prof_begin(0, st), "profile");
-            CK(msws_insert_pass(d_keys + start, c, D, sk->L, sk->agg, st), "msws insert");
+            CK(msws_insert_pass(d_keys + start, c, D1, sk->L, sk->agg, st), "msws insert");
             CK(sk->prof_end(0, st), "profile");
             CK(sk->prof_begin(1, st), "profile");
             CK(msws_repair(d_keys + start, c, D, sk->L, st), "msws repair");
@@ -765,7 +777,11 @@ struct qs_learned {
     uint8_t* d_labels_tmp = nullptr;
     qs_learned_info info{};
     uint32_t adam_step = 0;
-    bool table_full = false;  // no admission possible: routing skips the classifier
+    bool table_full = false;  // (almost) no admission possible: routing skips the classifier
+
+    // Full for routing purposes once fewer than 1/1024 of the slots below max fill are left:
+    // classifying a whole chunk to fill the last few slots costs more than they can save.
+    bool nearly_full() const { return (uint64_t)(T.max_fill - std::min(tfill, T.max_fill)) * 1024 < T.slots; }
 
     template <class X>
     cudaError_t alloc(X** ptr, size_t count, int fill = 0) {
@@ -957,7 +973,7 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
             return s;
         }
     }
-    lk->table_full = lk->tfill >= lk->T.max_fill;
+    lk->table_full = lk->nearly_full();
     cleanup();
 #undef CKT
     qs_learned_info& I = lk->info;
@@ -1127,18 +1143,22 @@ qs_status qs_learned_insert(qs_learned* lk, const uint32_t* d_keys, size_t n, vo
             }
             continue;
         }
-        // route a chunk: table hits count exactly and are skipped by the sketch insert
-        uint64_t c = std::min<uint64_t>(n - off, lk->sk->max_batch);
-        CK(cudaMemsetAsync(lk->R.n_misses, 0, 4, st), "misses reset");
-        lk->R.collect = lk->table_full ? 0u : 1u;
-        CK(route_chunk(d_keys + off, c, lk->T, lk->R, st), "route");
-        if (!lk->table_full) CK(classify_misses(lk->M, lk->R, c, st), "classify");
-        qs_status s = insert_device(lk->sk, d_keys + off, c, st, lk->R.skip);
-        if (s != QS_OK) return s;
         if (lk->table_full) {
+            // nothing more to admit: pass 1 looks the keys up in the exact table itself
+            const uint64_t c = n - off;
+            qs_status s = insert_device(lk->sk, d_keys + off, c, st, nullptr, &lk->T, lk->R.skip);
+            if (s != QS_OK) return s;
             off += c;
             continue;
         }
+        // route a chunk: table hits count exactly and are skipped by the sketch insert
+        uint64_t c = std::min<uint64_t>(n - off, lk->sk->max_batch);
+        CK(cudaMemsetAsync(lk->R.n_misses, 0, 4, st), "misses reset");
+        lk->R.collect = 1u;
+        CK(route_chunk(d_keys + off, c, lk->T, lk->R, st), "route");
+        CK(classify_misses(lk->M, lk->R, c, st), "classify");
+        qs_status s = insert_device(lk->sk, d_keys + off, c, st, lk->R.skip);
+        if (s != QS_OK) return s;
         uint32_t ncand = 0;
         CK(cudaMemcpyAsync(&ncand, lk->R.n_cand, 4, cudaMemcpyDeviceToHost, st), "candidates");
         CK(cudaStreamSynchronize(st), "candidate sync");
@@ -1163,7 +1183,7 @@ qs_status qs_learned_insert(qs_learned* lk, const uint32_t* d_keys, size_t n, vo
             CK(cudaMemsetAsync(lk->R.n_cand, 0, 4, st), "candidate reset");
             CK(cudaStreamSynchronize(st), "admit sync");
             lk->info.admitted_after_warmup += lk->tfill - before;
-            lk->table_full = lk->tfill >= lk->T.max_fill;
+            lk->table_full = lk->nearly_full();
         }
         off += c;
     }

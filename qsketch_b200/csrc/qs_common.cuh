@@ -91,6 +91,12 @@ struct MswsDev {
     uint32_t route;          // 0 adaptive, 1 preload, 2 fused (pass-1 routing)
     const uint32_t* skip;    // optional: bit i set = key i of the chunk is not for this sketch
     uint32_t max_tiles;      // tiles of REPAIR_TILE elements in a chunk
+    // learned split, pass 1 only: keys found in this exact table count there instead of in
+    // the sketch, and pass 1 sets their bits in skip_out (null tbl_keys: no table)
+    const uint32_t* tbl_keys;
+    uint32_t* tbl_counts;
+    uint32_t* skip_out;
+    uint32_t tbl_slots;
 };
 
 // Batched streams: many per-stream MSWS sketches share one low-table arena and one high

@@ -34,6 +34,7 @@ constexpr int AGG_SLOTS = 1024; // per-CTA table merging the linked keys of a ti
 constexpr int INS_BAR_BYTES = (INS_STAGES * 8 + 8 + 15) & ~15;
 constexpr int AGG_PROBES = 32;
 constexpr uint32_t AGG_EMPTY = 0xffffffffu;
+constexpr uint32_t AGG_TBL = 0x80000000u;  // merge-table id tag: the key's exact-table slot
 
 // Aggregation modes (qs_params.aggregate): 1 none, 2 warp (equal keys of a warp merge),
 // 3 warp + block (linked keys of a whole tile merge in shared memory, so a heavy hitter
@@ -244,7 +245,32 @@ __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& 
                                              bool use_table, int route, uint64_t idx, uint32_t seed,
                                              const FastMod& fm_low, uint32_t base) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const bool valid = lane < cnt && !(D.skip && ((__ldg(D.skip + (idx >> 5)) >> (idx & 31)) & 1u));
+    bool valid = lane < cnt && !(D.skip && ((__ldg(D.skip + (idx >> 5)) >> (idx & 31)) & 1u));
+    if (D.tbl_keys) {  // learned split: a key in the exact table counts there, not in the sketch
+        const int ts = valid ? table_find(D.tbl_keys, D.tbl_slots, key) : -1;
+        const uint32_t hb = __ballot_sync(0xffffffffu, ts >= 0);
+        if (hb) {
+            // its skip bit (for the replay): two words per warp when the lanes hold
+            // consecutive key indices, else one atomic per hit
+            const uint64_t i0 = __shfl_sync(0xffffffffu, idx, 0), i31 = __shfl_sync(0xffffffffu, idx, 31);
+            if (i31 - i0 == 31) {
+                if (lane == 0) {
+                    atomicOr(D.skip_out + (i0 >> 5), hb << (i0 & 31));
+                    if (i0 & 31) atomicOr(D.skip_out + (i0 >> 5) + 1, hb >> (32 - (i0 & 31)));
+                }
+            } else if (ts >= 0) {
+                atomicOr(D.skip_out + (idx >> 5), 1u << (idx & 31));
+            }
+            // its count: equal slots of the warp merge, then the tile's through the merge table
+            const uint32_t peers = __match_any_sync(0xffffffffu, ts >= 0 ? (uint32_t)ts : 0xffffffffu) & hb;
+            if (ts >= 0 && lane == __ffs(peers) - 1) {
+                const uint32_t c = __popc(peers);
+                if (!(AGG == AGG_BLOCK && use_table && agg_insert(S, key, c, AGG_TBL | (uint32_t)ts)))
+                    atomicAdd(D.tbl_counts + ts, c);
+            }
+            valid = valid && ts < 0;
+        }
+    }
     const uint32_t hv = key * seed;  // hash_mul_add, device_hash_function.h:6-18
     const uint32_t b = base + fast_mod(fm_low, hv);
     const uint32_t m = S.masks[fast_mod(D.fm_mask, hv)];
@@ -298,7 +324,7 @@ __device__ __forceinline__ void drain_table(const MswsDev& D, const InsShared& S
     for (int s0 = wid * 32; s0 < AGG_SLOTS; s0 += INS_THREADS) {
         const int s = s0 + lane;
         const uint32_t k = S.akey[s];
-        const bool has = k != AGG_EMPTY;
+        bool has = k != AGG_EMPTY;
         uint32_t m = 0, c = 0, id = 0, b = 0;
         if (has) {
             const uint32_t hv = k * seed;
@@ -308,6 +334,10 @@ __device__ __forceinline__ void drain_table(const MswsDev& D, const InsShared& S
             if (id == 0) b = base + fast_mod(fm_low, hv);
             S.akey[s] = AGG_EMPTY;
             S.acnt[s] = 0;
+            if (id & AGG_TBL) {  // an exact-table key (learned split): its count goes there
+                atomicAdd(D.tbl_counts + (id & ~AGG_TBL), c);
+                has = false;
+            }
         }
         const uint32_t am = __ballot_sync(0xffffffffu, has);
         if (!am) continue;
