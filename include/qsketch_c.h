@@ -295,6 +295,9 @@ qs_status qs_learned_destroy(qs_learned *lk);
 qs_status qs_learned_insert(qs_learned *lk, const uint32_t *d_keys, size_t n, void *stream);
 qs_status qs_learned_query(qs_learned *lk, const uint32_t *d_keys, size_t n, uint32_t *d_counts, void *stream);
 qs_status qs_learned_get_info(qs_learned *lk, qs_learned_info *out);
+/* Debug access (tests, tooling): the exact table's slots (key 0xffffffff = free) and counts,
+ * table_slots entries each, and the sketch's hash multiplier (may be null). */
+qs_status qs_learned_get_table(qs_learned *lk, uint32_t *h_keys, uint32_t *h_counts, uint32_t *h_seed);
 /* The classifier alone (tests and tooling): fp32 parameters in the layout above. */
 qs_status qs_mlp_get_params(qs_learned *lk, float *h_params);
 qs_status qs_mlp_set_params(qs_learned *lk, const float *h_params);

@@ -205,6 +205,7 @@ SIGNATURES = {
     "qs_learned_insert": (_I, [_P, _P, _SZ, _P]),
     "qs_learned_query": (_I, [_P, _P, _SZ, _P, _P]),
     "qs_learned_get_info": (_I, [_P, ctypes.POINTER(qs_learned_info)]),
+    "qs_learned_get_table": (_I, [_P, _P, _P, ctypes.POINTER(_U32)]),
     "qs_mlp_get_params": (_I, [_P, _P]),
     "qs_mlp_set_params": (_I, [_P, _P]),
     "qs_mlp_forward": (_I, [_P, _P, _SZ, _P, _P]),

@@ -1212,6 +1212,16 @@ qs_status qs_learned_get_info(qs_learned* lk, qs_learned_info* out) {
     return QS_OK;
 }
 
+qs_status qs_learned_get_table(qs_learned* lk, uint32_t* h_keys, uint32_t* h_counts, uint32_t* h_seed) {
+    if (!lk || !h_keys || !h_counts) return fail(QS_ERR_INVALID_ARG, "null argument");
+    DeviceGuard guard(lk->device);
+    CK(cudaDeviceSynchronize(), "table sync");
+    CK(cudaMemcpy(h_keys, lk->T.keys, (size_t)lk->T.slots * 4, cudaMemcpyDeviceToHost), "table keys");
+    CK(cudaMemcpy(h_counts, lk->T.counts, (size_t)lk->T.slots * 4, cudaMemcpyDeviceToHost), "table counts");
+    if (h_seed) *h_seed = lk->sk->D.seed;
+    return QS_OK;
+}
+
 qs_status qs_mlp_get_params(qs_learned* lk, float* h) {
     if (!lk || !h) return fail(QS_ERR_INVALID_ARG, "null argument");
     DeviceGuard guard(lk->device);

@@ -56,6 +56,16 @@ class LearnedSketch:
         check(lib.qs_learned_get_info(self.handle, ctypes.byref(i)), "info")
         return {f: getattr(i, f) for f, _ in qs_learned_info._fields_}
 
+    def table(self):
+        """The exact table: (keys, counts) of its occupied slots, and the sketch's multiplier."""
+        n = self.info()["table_slots"]
+        k = np.zeros(n, np.uint32)
+        c = np.zeros(n, np.uint32)
+        seed = ctypes.c_uint32()
+        check(lib.qs_learned_get_table(self.handle, k.ctypes.data, c.ctypes.data, ctypes.byref(seed)), "table")
+        used = k != 0xffffffff
+        return k[used], c[used], seed.value
+
     # ---- the classifier alone -----------------------------------------------------------
     def mlp_params(self):
         out = np.zeros(QS_MLP_PARAMS, np.float32)

@@ -94,3 +94,40 @@ def test_learned_split_beats_plain_at_equal_bytes(gpu):
     # deterministic: the same stream and parameters give the same estimates
     lk2, _, _, _, _ = run_learned_vs_plain(1 << 22, 1 << 20, budget, 1 << 14)
     assert torch.equal(lk2.search(uniq), est_l)
+
+
+@pytest.mark.parametrize("max_batch", [1 << 18, 1 << 20])
+def test_split_is_exact_table_plus_sketch(gpu, max_batch):
+    # A table that training fills: every later key is looked up by pass 1 itself.  Then each
+    # table key's count is exactly its occurrences after the warm-up, and the sketch part is
+    # exactly a plain sketch (same size, multiplier and masks) fed the warm-up keys plus the
+    # later keys that are not in the table, in order.
+    import qsketch_b200 as qs
+    keys = data.class_keys(1 << 22, seed=17, perm_seed=19, n_class=1 << 12)
+    warm = 1 << 20
+    lk = LearnedSketch(budget_bytes=6 << 20, table_slots=1 << 12, warmup_keys=warm, hash_seed=2654435769,
+                       max_batch=max_batch, heavy_fraction=0.2, epochs=2)
+    lk.insert(keys)
+    info = lk.info()
+    max_fill = int(0.75 * 4096)
+    assert (max_fill - min(info["table_fill"], max_fill)) * 1024 < 4096, info  # (nearly) full at training
+    tkeys, tcounts, seed = lk.table()
+    assert tkeys.size == info["table_fill"] and seed == 2654435769
+    hk = keys.cpu().numpy()
+    rest = hk[warm:]
+    in_table = np.isin(rest, tkeys)
+    u, c = np.unique(rest[in_table], return_counts=True)
+    order = np.argsort(tkeys)
+    got_counts = dict(zip(tkeys[order].tolist(), tcounts[order].tolist()))
+    want_counts = dict(zip(u.tolist(), c.tolist()))
+    for k in tkeys.tolist():
+        assert got_counts[k] == want_counts.get(k, 0), k
+    plain = qs.Sketch_GPU_Sub_Warp_Level(info["n_low"], 8, info["n_high"], 32, hash_seed=seed)
+    plain.insert(keys[:warm])
+    plain.insert(torch.from_numpy(rest[~in_table].astype(np.int32)).cuda().view(torch.uint32))
+    q = torch.from_numpy(np.unique(hk).astype(np.int32)).cuda().view(torch.uint32)
+    est = lk.search(q).cpu().numpy().astype(np.int64)
+    sk = plain.search(q).cpu().numpy().astype(np.int64)
+    qk = q.cpu().numpy()
+    tbl = np.array([got_counts.get(k, 0) for k in qk.tolist()], np.int64)
+    assert np.array_equal(est, sk + tbl), f"{(est != sk + tbl).sum()} estimates differ"
