@@ -92,7 +92,7 @@ typedef struct qs_params {
     const uint8_t *mask_table;   /* optional host table of H*4 bytes (bits 0..27 only);
                                     overrides mask_rng */
     uint64_t max_batch;          /* keys per internal insert chunk (scratch sizing);
-                                    0 = 1<<22 */
+                                    a multiple of 32, at most 2^26; 0 = 1<<22 */
     int32_t device;              /* CUDA device ordinal; -1 = current */
     /* Insert-kernel knobs; none changes any result.  When lanes_per_key, aggregate, route
      * and ctas_per_sm are all 0, qs_create takes them (and max_batch, if 0) from the

@@ -364,9 +364,9 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         return fail(QS_ERR_INVALID_ARG, "first_chunk must be a multiple of 32");
     }
     sk->ramp_first = (p.flags & QS_FLAG_NO_CHUNK_RAMP) ? 0 : (p.first_chunk ? p.first_chunk : (1ull << 18));
-    if (sk->max_batch > (1ull << 30) || (sk->max_batch & 31)) {
+    if (sk->max_batch > (1ull << 26) || (sk->max_batch & 31)) {
         delete sk;
-        return fail(QS_ERR_INVALID_ARG, "max_batch must be a multiple of 32 and at most 2^30");
+        return fail(QS_ERR_INVALID_ARG, "max_batch must be a multiple of 32 and at most 2^26");
     }
     // aggregate: 1 none, 2 warp, 3 warp + block, 0 = default (3)
     if (p.aggregate > 3) {

@@ -125,6 +125,25 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
     return r;
 }
 
+// Exclusive scan in place of a shared-memory array a[0..len) by one block; returns the total
+// (all threads).  Each thread owns a contiguous run.
+__device__ __forceinline__ uint32_t block_scan_smem(uint32_t* a, uint32_t len) {
+    const uint32_t per = (len + blockDim.x - 1) / blockDim.x;
+    const uint32_t beg = min(len, threadIdx.x * per);
+    const uint32_t end = min(len, beg + per);
+    uint32_t sum = 0;
+    for (uint32_t i = beg; i < end; ++i) sum += a[i];
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(sum, &total);
+    for (uint32_t i = beg; i < end; ++i) {
+        const uint32_t t = a[i];
+        a[i] = run;
+        run += t;
+    }
+    __syncthreads();
+    return total;
+}
+
 // Exclusive scan in place of a global array a[0..len) by one block; returns the total.
 // a must be 16-byte aligned; each thread owns a run of a multiple of 4 entries.
 __device__ __forceinline__ uint32_t block_scan_array(uint32_t* a, uint32_t len) {

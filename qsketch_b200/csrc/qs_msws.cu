@@ -785,6 +785,13 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     constexpr int PER = REPAIR_TILE / REPAIR_THREADS;  // 8 consecutive keys per thread
     static_assert(PER == 8, "one hit byte per thread");
     const uint32_t ntk = (uint32_t)((n + REPAIR_TILE - 1) / REPAIR_TILE);
+    // the tile-count prefix of phase 2 lives in the set's SET_SLOTS words: chunks of at most
+    // SET_SLOTS tiles (2^26 keys; the host rejects larger max_batch); uniform, so every block
+    // leaves before any barrier
+    if (ntk > (uint32_t)SET_SLOTS) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->status, ST_CAPACITY);
+        return;
+    }
     const uint32_t nthreads = gridDim.x * REPAIR_THREADS;
     const uint32_t gtid = blockIdx.x * REPAIR_THREADS + tid;
 
@@ -848,14 +855,15 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     }
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 0);
-    // Phase 2: exclusive scan of the tile counts.
-    if (blockIdx.x == 0) {
-        const uint32_t K = block_scan_array(D.tile_counts, ntk);
-        if (tid == 0) __stcg(&ctl->n_records, K);
-    }
-    if (!grid_barrier(ctl)) return;
+    // Phase 2: every block scans the tile counts itself (exclusive, in shared memory — the
+    // flagged-bucket set is not needed after phase 1), which gives its tiles' record offsets
+    // and the record total K without another grid barrier.
+    uint32_t* spre = s_set;
+    for (uint32_t i = tid; i < ntk; i += REPAIR_THREADS) spre[i] = __ldcg(D.tile_counts + i);
+    __syncthreads();
+    const uint32_t K = block_scan_smem(spre, ntk);
+    if (blockIdx.x == 0 && tid == 0) __stcg(&ctl->n_records, K);
     phase_mark(ctl, 1);
-    const uint32_t K = __ldcg(&ctl->n_records);
     // Few records (K <= SCAN_CAP): the replay scans them unsorted, and the per-slot counter
     // totals and record counts it needs are accumulated here with global atomics.
     const bool scan_mode = K <= SCAN_CAP;
@@ -865,7 +873,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
         const uint32_t hit = base < n ? __ldcg(D.hits + (base >> 3)) : 0u;
         uint32_t total;
-        uint32_t pos = block_exclusive_scan((uint32_t)__popc(hit), &total) + __ldcg(D.tile_counts + t);
+        uint32_t pos = block_exclusive_scan((uint32_t)__popc(hit), &total) + spre[t];
         if (hit) {
             KeyMap<BATCH> km;
             km.start(B, (uint32_t)base);
