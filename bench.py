@@ -217,7 +217,8 @@ def run_ours(args, cfg):
     autotune.reset()
     # (the mixed workload inserts one batch at a time: tune on one batch, not the whole stream)
     sample = ins_views[0] if cfg["kind"] == 2 else keys
-    tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], sample, reps=3, hash_seed=SEED, mask_rng=1)
+    reps = max(3, min(20, (1 << 24) // sample.numel()))  # small samples: more repetitions against noise
+    tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], sample, reps=reps, hash_seed=SEED, mask_rng=1)
     sk = qs.Sketch_GPU_Sub_Warp_Level(cfg["n_low"], 8, cfg["n_high"], 32, hash_seed=SEED, mask_rng=1)
     n_ins, n_q = cfg["n_keys"], cfg["n_query"]
     if cfg["kind"] == 2:

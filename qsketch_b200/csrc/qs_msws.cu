@@ -450,11 +450,12 @@ __global__ void __launch_bounds__(INS_THREADS, INS_MIN_CTAS) k_msws_insert(const
 
 // ---- ordered replay ---------------------------------------------------------------------
 
-constexpr int SET_CAP = 8192;     // flagged buckets looked up in a per-block shared-memory set
-constexpr int SET_SLOTS = 16384;  // bucket ids only, open addressing, load factor <= 1/2 (64 KiB)
-constexpr int SET_BITS = 14;
-constexpr uint32_t SCAN_CAP = SET_SLOTS / 2;  // records replayed without a sort (the set's 64 KiB)
-static_assert((1 << SET_BITS) == SET_SLOTS, "set size");
+constexpr int SET_SLOTS = 16384;  // words of the repair's dynamic shared memory (64 KiB), reused by
+                                  // the phases: flag filter, tile prefix, staged records
+constexpr int BLOOM_BITS = 17;    // per-block filter of the flagged buckets: 2^17 bits (16 KiB)
+constexpr int BLOOM_WORDS = (1 << BLOOM_BITS) / 32;
+constexpr uint32_t SCAN_CAP = SET_SLOTS / 2;  // records replayed without a sort (64 KiB of uint2)
+static_assert(BLOOM_WORDS <= SET_SLOTS, "filter fits the shared space");
 constexpr uint32_t NONE = 0xffffffffu;
 
 __device__ __forceinline__ int radix_passes(uint32_t F) {
@@ -463,18 +464,14 @@ __device__ __forceinline__ int radix_passes(uint32_t F) {
     return (bits + 7) / 8;
 }
 
-// Was bucket b flagged in this chunk?  The shared-memory set when it holds them all, else
-// the bitmap in global memory.
-__device__ __forceinline__ bool is_flagged(const MswsDev& D, const uint32_t* skey, bool use_set, uint32_t b) {
-    if (use_set) {
-        const uint32_t h = (b * 0x9E3779B1u) >> (32 - SET_BITS);
-        for (int p = 0; p < SET_SLOTS; ++p) {
-            const uint32_t k = skey[(h + p) & (SET_SLOTS - 1)];
-            if (k == b) return true;
-            if (k == NONE) return false;
-        }
-        return false;
-    }
+// Was bucket b flagged in this chunk?  A per-block filter in shared memory (one bit per
+// hash of each flagged bucket) answers "no" for almost every key with one shared load; a
+// filter hit is confirmed in the bitmap of flagged buckets in global memory.
+__device__ __forceinline__ uint32_t bloom_bit(uint32_t b) { return (b * 0x9E3779B1u) >> (32 - BLOOM_BITS); }
+
+__device__ __forceinline__ bool is_flagged(const MswsDev& D, const uint32_t* sbloom, uint32_t b) {
+    const uint32_t h = bloom_bit(b);
+    if (!((sbloom[h >> 5] >> (h & 31)) & 1u)) return false;
     return (__ldcg(D.bitmap + (b >> 5)) >> (b & 31)) & 1u;
 }
 
@@ -773,7 +770,6 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     __shared__ uint32_t s_acc[2][LOW_COUNTERS];
     __shared__ uint32_t s_acc_slot[2];
     extern __shared__ __align__(16) uint32_t s_set[];
-    uint32_t* skey = s_set;
     Ctl* ctl = D.ctl;
     const uint32_t F = min(__ldcg(&ctl->n_flagged), D.flag_cap);
     if (F == 0) return;
@@ -785,7 +781,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     constexpr int PER = REPAIR_TILE / REPAIR_THREADS;  // 8 consecutive keys per thread
     static_assert(PER == 8, "one hit byte per thread");
     const uint32_t ntk = (uint32_t)((n + REPAIR_TILE - 1) / REPAIR_TILE);
-    // the tile-count prefix of phase 2 lives in the set's SET_SLOTS words: chunks of at most
+    // the tile-count prefix of phase 2 lives in the SET_SLOTS words of shared memory: chunks of at most
     // SET_SLOTS tiles (2^26 keys; the host rejects larger max_batch); uniform, so every block
     // leaves before any barrier
     if (ntk > (uint32_t)SET_SLOTS) {
@@ -795,19 +791,15 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     const uint32_t nthreads = gridDim.x * REPAIR_THREADS;
     const uint32_t gtid = blockIdx.x * REPAIR_THREADS + tid;
 
-    // Phase 0: the flagged buckets as a shared-memory set in every block; zero the totals.
-    const bool use_set = F <= (uint32_t)SET_CAP;
-    if (use_set) {
-        for (int i = tid; i < SET_SLOTS; i += REPAIR_THREADS) skey[i] = NONE;
-        __syncthreads();
-        for (uint32_t s = tid; s < F; s += REPAIR_THREADS) {
-            const uint32_t b = __ldcg(D.flag_list + s);
-            uint32_t h = (b * 0x9E3779B1u) >> (32 - SET_BITS);
-            for (int p = 0; p < SET_SLOTS; ++p, ++h)
-                if (atomicCAS(skey + (h & (SET_SLOTS - 1)), NONE, b) == NONE) break;
-        }
-        __syncthreads();
+    // Phase 0: the flagged buckets' filter in every block; zero the totals.
+    uint32_t* sbloom = s_set;
+    for (int i = tid; i < BLOOM_WORDS; i += REPAIR_THREADS) sbloom[i] = 0u;
+    __syncthreads();
+    for (uint32_t s = tid; s < F; s += REPAIR_THREADS) {
+        const uint32_t h = bloom_bit(__ldcg(D.flag_list + s));
+        atomicOr(sbloom + (h >> 5), 1u << (h & 31));
     }
+    __syncthreads();
     const uint32_t ntot = min(F, D.long_cap);
     for (uint32_t i = gtid; i < ntot * LOW_COUNTERS; i += nthreads) __stcg(D.totals + i, 0u);
     for (uint32_t i = gtid; i < ntot; i += nthreads) __stcg(D.seg_beg + i, 0u);  // record counts (scan mode)
@@ -845,7 +837,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
                 if (BATCH) km.flat(B, (uint32_t)(base + j));  // moves the cursor to key j's stream
                 uint32_t hv;
                 const uint32_t b = km.bucket(D, B, k[j], hv);
-                if (is_flagged(D, skey, use_set, b)) hit |= 1u << j;
+                if (is_flagged(D, sbloom, b)) hit |= 1u << j;
             }
         }
         __stcg(D.hits + (base >> 3), (uint8_t)hit);  // PER == 8: one byte per thread
@@ -856,7 +848,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 0);
     // Phase 2: every block scans the tile counts itself (exclusive, in shared memory — the
-    // flagged-bucket set is not needed after phase 1), which gives its tiles' record offsets
+    // flag filter is not needed after phase 1), which gives its tiles' record offsets
     // and the record total K without another grid barrier.
     uint32_t* spre = s_set;
     for (uint32_t i = tid; i < ntk; i += REPAIR_THREADS) spre[i] = __ldcg(D.tile_counts + i);
@@ -898,7 +890,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     phase_mark(ctl, 2);
 
     // Few records: no sort.  Every block that replays a slot stages all K records in shared
-    // memory (the flagged-bucket set is no longer needed; its 64 KiB hold SCAN_CAP records)
+    // memory (the flag filter is no longer needed; the 64 KiB hold SCAN_CAP records)
     // and each warp scans them for its slot in array order.
     if (scan_mode) {
         constexpr int NWB = REPAIR_THREADS / 32;
