@@ -215,10 +215,14 @@ def run_ours(args, cfg):
     # timed region; no knob changes any result); the sketch below takes them from its table
     from qsketch_b200 import autotune
     autotune.reset()
-    # (the mixed workload inserts one batch at a time: tune on one batch, not the whole stream)
-    sample = ins_views[0] if cfg["kind"] == 2 else keys
-    reps = max(3, min(20, (1 << 24) // sample.numel()))  # small samples: more repetitions against noise
-    tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], sample, reps=reps, hash_seed=SEED, mask_rng=1)
+    # (the mixed workload inserts one batch per call: tune on its first 16 batches inserted in
+    # chunks of one batch, so the tuner sees the real chunk size and a sketch that fills)
+    if cfg["kind"] == 2:
+        sample = torch.cat(ins_views[:16])
+        tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], sample, reps=3, hash_seed=SEED, mask_rng=1,
+                                     max_batch=(ni_b + 31) // 32 * 32)
+    else:
+        tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], keys, reps=3, hash_seed=SEED, mask_rng=1)
     sk = qs.Sketch_GPU_Sub_Warp_Level(cfg["n_low"], 8, cfg["n_high"], 32, hash_seed=SEED, mask_rng=1)
     n_ins, n_q = cfg["n_keys"], cfg["n_query"]
     if cfg["kind"] == 2:
@@ -353,7 +357,7 @@ def run_ours(args, cfg):
                        "l2": "key stream of %d MB per step > 126 MB L2" % (n_ins * 4 >> 20),
                        "parallelism": "independent sketch per GPU" if world > 1 else "single GPU",
                        "insert_knobs": {k: tuned[k] for k in ("lanes_per_key", "aggregate", "route", "ctas_per_sm",
-                                                              "max_batch", "first_chunk")}},
+                                                              "max_batch", "first_chunk", "keys_per_tile")}},
             "insert_gkeys_per_s": round(world * n_ins / (ins_ms * 1e6), 4),
             "query_gkeys_per_s": round(world * n_q / (q_ms * 1e6), 4),
             "avg_rel_error": rel, "mean_est_over_exact": ratio,

@@ -108,6 +108,9 @@ typedef struct qs_params {
     uint32_t ctas_per_sm;        /* pass-1 CTAs per SM, 0 = as many as fit */
     uint64_t first_chunk;        /* first chunk of the ramp after a create or clear (multiple
                                     of 32); 0 = 2^18, or the autotuner's choice */
+    uint32_t keys_per_tile;      /* pass-1 keys per CTA tile: 256, 512, 1024 or 2048 (0 =
+                                    2048, or the autotuner's choice); small chunks spread over
+                                    more CTAs with smaller tiles */
 } qs_params;
 
 typedef struct qs_sketch qs_sketch;
@@ -310,11 +313,14 @@ qs_status qs_mlp_train(qs_learned *lk, const uint32_t *d_keys, const uint8_t *d_
                        uint32_t batch, float lr, float pos_weight, double *last_loss);
 
 /* ---- autotuner (no counterpart in the reference) -----------------------------------------
- * Times pass-1 knob settings (lanes per key 1-32, aggregation, routing, CTAs per SM, chunk size
- * max_batch, the chunk ramp after a clear; every setting gives identical results) on a scratch sketch built from `base`
- * over the caller's sample keys (device memory, inserted `reps` times after a clear), by a
- * coordinate search from the defaults: lanes per key, then aggregation, routing, CTAs per
- * SM, chunk size, ramp.  The fastest setting is returned in *best, recorded in a process-wide
+ * Times pass-1 knob settings (lanes per key 1-32, keys per CTA tile, aggregation, routing,
+ * CTAs per SM, chunk size max_batch, the chunk ramp after a clear; every setting gives
+ * identical results) on a scratch sketch built from `base` over the caller's sample keys
+ * (device memory, inserted `reps` times after a clear), by a coordinate search from the
+ * defaults: lanes per key, then keys per tile, aggregation, routing, CTAs per SM, chunk size,
+ * ramp.  A caller that inserts in calls of a fixed size passes it as base->max_batch: the
+ * chunk size is then not searched, and the sample is inserted in chunks of that size.  The
+ * fastest setting is returned in *best, recorded in a process-wide
  * table for the size class floor(log2(n_low)) of `base`, and used by later qs_create calls
  * of that class whose knobs are all 0.  h_all (may be null) receives up to max_all of the
  * timed settings, *n_all how many were timed. */
@@ -322,6 +328,7 @@ typedef struct qs_tune_config {
     uint32_t lanes_per_key, aggregate, route, ctas_per_sm;
     uint64_t max_batch;
     uint64_t first_chunk; /* chunk-size ramp after a clear; 0 = no ramp */
+    uint32_t keys_per_tile, pad;
     double insert_ms; /* mean time of one insert of the sample (pass 1 + ordered replay) */
 } qs_tune_config;
 

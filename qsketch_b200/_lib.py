@@ -48,6 +48,7 @@ class qs_params(ctypes.Structure):
         ("route", ctypes.c_uint32),
         ("ctas_per_sm", ctypes.c_uint32),
         ("first_chunk", ctypes.c_uint64),
+        ("keys_per_tile", ctypes.c_uint32),
     ]
 
 
@@ -135,7 +136,7 @@ class qs_batch_params(ctypes.Structure):
 class qs_tune_config(ctypes.Structure):
     _fields_ = [("lanes_per_key", ctypes.c_uint32), ("aggregate", ctypes.c_uint32), ("route", ctypes.c_uint32),
                 ("ctas_per_sm", ctypes.c_uint32), ("max_batch", ctypes.c_uint64), ("first_chunk", ctypes.c_uint64),
-                ("insert_ms", ctypes.c_double)]
+                ("keys_per_tile", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("insert_ms", ctypes.c_double)]
 
 
 class qs_batch_info(ctypes.Structure):

@@ -390,7 +390,10 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         // insert knobs: explicit, else the autotuner's entry for this size class, else defaults
         qs_tune_config tc{};
         const bool tuned = p.lanes_per_key == 0 && p.aggregate == 0 && p.route == 0 && p.ctas_per_sm == 0 &&
-                           tune_lookup(n_low, &tc);
+                           p.keys_per_tile == 0 && tune_lookup(n_low, &tc);
+        const uint32_t tile = tuned && tc.keys_per_tile ? tc.keys_per_tile : (p.keys_per_tile ? p.keys_per_tile : 2048u);
+        if (tile != 256 && tile != 512 && tile != 1024 && tile != 2048)
+            return bail(fail(QS_ERR_INVALID_ARG, "keys_per_tile must be 0, 256, 512, 1024 or 2048"));
         // default 4 lanes per key (measured fastest on every workload here), 8 for route 2
         const uint32_t route = tuned ? tc.route : (p.route ? p.route : 1u);
         const uint32_t lpk = tuned ? tc.lanes_per_key : (p.lanes_per_key ? p.lanes_per_key : route == 2 ? 8u : 4u);
@@ -463,6 +466,7 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         e = msws_configure(dev, H, &sk->L);
         if (e != cudaSuccess) return bail(cuda_fail(e, "configure kernels"));
         sk->L.lanes_per_key = (int)lpk;
+        sk->L.tile_keys = (int)tile;
         sk->L.ctas_per_sm = tuned ? (int)tc.ctas_per_sm : (int)p.ctas_per_sm;
     } else {
         const uint32_t rows = p.m_low;
@@ -1711,10 +1715,18 @@ qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, u
     if (base->kind != QS_KIND_MSWS) return fail(QS_ERR_INVALID_ARG, "qs_autotune: MSWS sketches only");
     if (reinterpret_cast<uintptr_t>(d_keys) & 3u) return fail(QS_ERR_INVALID_ARG, "keys not 4-byte aligned");
     reps = std::max(1u, reps);
-    // chunk sizes worth trying: 2^20 .. 2^24, none far beyond the sample
+    // chunk sizes worth trying: 2^20 .. 2^24, none far beyond the sample; a caller that inserts
+    // in calls of a fixed size passes it as base->max_batch: that size is kept, and the sample
+    // is inserted in chunks of it (into a sketch that keeps its state from chunk to chunk)
     std::vector<uint64_t> mbs;
-    for (uint64_t mb = 1ull << 20; mb <= (1ull << 24); mb <<= 1)
-        if (mb <= std::max<uint64_t>(1ull << 20, 2 * (uint64_t)n)) mbs.push_back(mb);
+    if (base->max_batch) {
+        if ((base->max_batch & 31) || base->max_batch > (1ull << 26))
+            return fail(QS_ERR_INVALID_ARG, "qs_autotune: max_batch must be a multiple of 32, at most 2^26");
+        mbs.push_back(base->max_batch);
+    } else {
+        for (uint64_t mb = 1ull << 20; mb <= (1ull << 24); mb <<= 1)
+            if (mb <= std::max<uint64_t>(1ull << 20, 2 * (uint64_t)n)) mbs.push_back(mb);
+    }
     qs_params p = *base;
     p.lanes_per_key = 8;
     p.aggregate = 3;
@@ -1743,6 +1755,7 @@ qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, u
     auto run = [&](qs_tune_config& c) -> qs_status {
         sk->L.lanes_per_key = (int)c.lanes_per_key;
         sk->L.ctas_per_sm = (int)c.ctas_per_sm;
+        sk->L.tile_keys = (int)c.keys_per_tile;
         sk->agg = (int)c.aggregate - 1;
         sk->D.route = c.route == 3 ? 0u : c.route;
         sk->max_batch = std::min(c.max_batch, alloc_mb);
@@ -1765,7 +1778,8 @@ qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, u
         ++timed;
         return QS_OK;
     };
-    qs_tune_config cur{8u, 3u, 1u, 0u, std::min<uint64_t>(1ull << 22, mbs.back()), 1ull << 18, 0.0};
+    qs_tune_config cur{8u, 3u, 1u, 0u, base->max_batch ? mbs[0] : std::min<uint64_t>(1ull << 22, mbs.back()), 1ull << 18,
+                       2048u, 0u, 0.0};
     s = run(cur);
     if (s != QS_OK) return cleanup(s);
     auto consider = [&](qs_tune_config c) -> qs_status {
@@ -1776,6 +1790,11 @@ qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, u
     for (uint32_t lpk : {4u, 2u, 1u, 16u, 32u}) {
         qs_tune_config c = cur;
         c.lanes_per_key = lpk;
+        if ((s = consider(c)) != QS_OK) return cleanup(s);
+    }
+    for (uint32_t tile : {1024u, 512u, 256u}) {  // keys per CTA tile
+        qs_tune_config c = cur;
+        c.keys_per_tile = tile;
         if ((s = consider(c)) != QS_OK) return cleanup(s);
     }
     for (uint32_t agg : {1u, 2u, 3u}) {

@@ -97,6 +97,7 @@ struct MswsDev {
     uint32_t* tbl_counts;
     uint32_t* skip_out;
     uint32_t tbl_slots;
+    uint32_t ins_tile;       // pass-1 keys per tile (0: the stage size)
 };
 
 // Batched streams: many per-stream MSWS sketches share one low-table arena and one high

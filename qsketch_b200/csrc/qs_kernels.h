@@ -18,6 +18,7 @@ struct MswsLaunch {
     int ins_occ[3][6];       // resident pass-1 CTAs per SM by [aggregation][lanes-per-key index]
     int lanes_per_key = 8;   // pass-1 lanes per key: 1, 2, 4, 8, 16 or 32
     int ctas_per_sm = 0;     // pass-1 CTAs per SM, 0 = as many as fit
+    int tile_keys = 2048;    // pass-1 keys per tile: 256, 512, 1024 or 2048
 };
 
 size_t msws_insert_smem(uint32_t n_masks);

@@ -390,14 +390,17 @@ __global__ void __launch_bounds__(INS_THREADS, INS_MIN_CTAS) k_msws_insert(const
         insert_group<AGG, LPK>(D, S, k, (int)(head + tail), false, ROUTE_PRELOAD, idx, D.seed, D.fm_low, 0u);
     }
 
-    const uint64_t ntiles = (body_n + INS_TILE - 1) / INS_TILE;
+    // keys per tile (<= INS_TILE, a multiple of 4 so that every TMA copy stays 16-byte sized
+    // and aligned): small chunks take smaller tiles to spread over more CTAs
+    const uint64_t tile = (D.ins_tile && D.ins_tile <= (uint32_t)INS_TILE) ? (D.ins_tile & ~3u) : (uint64_t)INS_TILE;
+    const uint64_t ntiles = (body_n + tile - 1) / tile;
     const uint64_t my_tiles = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
     auto issue = [&](uint64_t i) {
         const int st = (int)(i % INS_STAGES);
         const uint64_t g = blockIdx.x + i * gridDim.x;
-        const uint64_t start = g * INS_TILE;
-        const uint32_t cnt = (uint32_t)umin64(INS_TILE, body_n - start);
+        const uint64_t start = g * tile;
+        const uint32_t cnt = (uint32_t)umin64(tile, body_n - start);
         mbar_arrive_expect_tx(&S.bar[st], cnt * 4u);
         tma_bulk_g2s(S.keys + st * INS_TILE, body + start, cnt * 4u, &S.bar[st]);
     };
@@ -421,14 +424,13 @@ __global__ void __launch_bounds__(INS_THREADS, INS_MIN_CTAS) k_msws_insert(const
         for (uint32_t it = 0; it < 64 && !mbar_try_wait(&S.bar[st], parity); ++it) {
         }
         const uint64_t g = blockIdx.x + i * gridDim.x;
-        const int cnt = (int)umin64(INS_TILE, body_n - g * INS_TILE);
+        const int cnt = (int)umin64(tile, body_n - g * tile);
         const uint32_t* tk = S.keys + st * INS_TILE;
         const int route = (int)S.misc[2];
         for (int base = wid * 32; base < cnt; base += INS_THREADS) {
             const int c = min(32, cnt - base);
             const uint32_t k = lane < c ? tk[base + lane] : 0u;
-            insert_group<AGG, LPK>(D, S, k, c, true, route, head + g * INS_TILE + base + lane, D.seed, D.fm_low,
-                                   0u);
+            insert_group<AGG, LPK>(D, S, k, c, true, route, head + g * tile + base + lane, D.seed, D.fm_low, 0u);
         }
         __syncthreads();
         if (tid == 0) {  // adaptive: the next tile is fused while under 1/16 of the keys are linked
@@ -1377,9 +1379,10 @@ cudaError_t msws_insert_pass(const uint32_t* d_keys, uint64_t n, const MswsDev& 
     if (n == 0) return cudaSuccess;
     const size_t smem = msws_insert_smem(D.n_masks);
     const int li = lpk_index(L.lanes_per_key);
-    const uint64_t tiles = (n + INS_TILE - 1) / INS_TILE;
-    const int grid = (int)std::min<uint64_t>((uint64_t)ins_grid(L, agg, li), std::max<uint64_t>(1ull, tiles));
     MswsDev Dc = D;
+    Dc.ins_tile = (L.tile_keys >= 256 && L.tile_keys <= INS_TILE) ? (uint32_t)L.tile_keys : (uint32_t)INS_TILE;
+    const uint64_t tiles = (n + Dc.ins_tile - 1) / Dc.ins_tile;
+    const int grid = (int)std::min<uint64_t>((uint64_t)ins_grid(L, agg, li), std::max<uint64_t>(1ull, tiles));
     void* args[] = {(void*)&d_keys, (void*)&n, (void*)&Dc};
     return cudaLaunchKernel(ins_fn(agg, li, false), dim3(grid), dim3(INS_THREADS), args, smem, st);
 }

@@ -252,6 +252,14 @@ def test_lanes_per_key_variants_bit_exact(gpu, lpk, agg):
     run_and_compare(sk, orc, keys, q)
 
 
+@pytest.mark.parametrize("tile", [256, 512, 1024])
+def test_keys_per_tile_bit_exact(gpu, tile):
+    # smaller CTA tiles (and an unaligned start, so the ragged keys take CTA 0's path)
+    sk, orc = make_pair(65521, 1 << 14, keys_per_tile=tile, max_batch=1 << 18)
+    keys = data.zipf_keys((1 << 20) + 7, 1 << 16, 1.1, seed=45, perm_seed=7)
+    run_and_compare(sk, orc, keys[3:], data.rank_keys(7, 0, 1 << 16))
+
+
 @pytest.mark.parametrize("ctas", [1, 2])
 def test_ctas_per_sm_bit_exact(gpu, ctas):
     sk, orc = make_pair(65521, 1 << 14, lanes_per_key=4, ctas_per_sm=ctas, max_batch=1 << 18)
@@ -279,6 +287,18 @@ def test_autotune_picks_a_timed_setting_and_create_uses_it(gpu):
     assert torch.equal(tuned.search(q), plain.search(q))
     autotune.reset()
     assert autotune.lookup(524287) is None
+
+
+def test_autotune_keeps_a_fixed_chunk_size(gpu):
+    # A caller that inserts in calls of one size passes it: only that chunk size is timed.
+    from qsketch_b200 import autotune
+    autotune.reset()
+    keys = data.zipf_keys(1 << 21, 1 << 18, 1.1, seed=53, perm_seed=3)
+    best, allc = autotune.autotune(65521, 1 << 13, keys, reps=1, max_batch=3 << 17)
+    assert {c["max_batch"] for c in allc} == {3 << 17}
+    with pytest.raises(qs.QsError):
+        autotune.autotune(65521, 1 << 13, keys, reps=1, max_batch=1000)
+    autotune.reset()
 
 
 @pytest.mark.parametrize("ramp", [True, False])
