@@ -244,8 +244,10 @@ qs_status qs_error_metrics(const uint32_t *d_est, const uint32_t *d_exact, size_
                            double *mean_rel_err, double *mean_ratio, void *stream);
 
 /* Roofline probes: time `kind` (0 random sub-warp sector red with 3 words per sector,
- * 1 random 32 B sector load, 2 streaming read) over a device buffer of `bytes`,
- * returning operations per second (sectors/s or bytes/s for kind 2). */
+ * 1 random 32 B sector load, 2 streaming read, 3 load + returning atomics, 4 returning
+ * atomics with the index word, 5 load + red) over a device buffer of `bytes`, returning
+ * operations per second (sectors/s or bytes/s for kind 2); kind 6 times `ops` grid-wide
+ * barriers of the ordered replay's form (`bytes` unused) and returns barriers/s. */
 qs_status qs_probe(uint32_t kind, uint64_t bytes, uint64_t ops, double *ops_per_s);
 
 /* ---- learned heavy-hitter split (no counterpart in the reference) ------------------------

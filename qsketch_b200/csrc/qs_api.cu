@@ -451,9 +451,7 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         D.masks = masks_d;
         CKB(sk->alloc(&D.ctl, 1), "alloc control");
         CKB(sk->alloc(&D.flag_list, cap), "alloc flag list");
-        CKB(sk->alloc(&D.bitmap, (n_low + 31) / 32), "alloc bitmap");
         CKB(sk->alloc(&D.tile_counts, D.max_tiles), "alloc tile counts");
-        CKB(sk->alloc(&D.hits, (uint64_t)D.max_tiles * (REPAIR_TILE / 8)), "alloc hit bits");
         CKB(sk->alloc(&D.rec[0], B), "alloc records");
         CKB(sk->alloc(&D.rec[1], B), "alloc records");
         CKB(sk->alloc(&D.hist, (uint64_t)256 * D.max_tiles + 256), "alloc histograms");  // + digit totals
@@ -590,7 +588,6 @@ qs_status qs_clear(qs_sketch* sk, void* stream) {
     if (sk->kind == QS_KIND_MSWS) {
         CK(cudaMemsetAsync(sk->D.low, 0, sk->D.n_low * LOW_WORDS * 4, st), "clear low");
         CK(cudaMemsetAsync(sk->D.high, 0, sk->D.n_high * HIGH_WORDS * 4, st), "clear high");
-        CK(cudaMemsetAsync(sk->D.bitmap, 0, (sk->D.n_low + 31) / 32 * 4, st), "clear bitmap");
         sk->fresh = 0;
         return ctl_reset(sk, st);
     }

@@ -265,7 +265,50 @@ __global__ void k_probe(uint32_t kind, uint32_t* buf, uint64_t nsec, uint64_t no
     if (acc == 0x9e3779b9u) sink[0] = acc;
 }
 
+// kind 6: `nops` grid-wide barriers of the replay kernel's form (bounded waits) in one
+// cooperative launch of 512-thread blocks, two per SM
+__global__ void __launch_bounds__(512) k_probe_barrier(Ctl* ctl, uint64_t nops) {
+    for (uint64_t i = 0; i < nops; ++i)
+        if (!grid_barrier(ctl)) return;
+}
+
+cudaError_t probe_barrier(uint64_t ops, double* ops_per_s) {
+    Ctl* ctl = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    int dev = 0, sms = 148, occ = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_probe_barrier, 512, 0);
+    if (e == cudaSuccess && occ < 1) e = cudaErrorInvalidConfiguration;
+    if (e == cudaSuccess) e = cudaMalloc(&ctl, sizeof(Ctl));
+    if (e == cudaSuccess) e = cudaMemset(ctl, 0, sizeof(Ctl));
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    const int grid = sms * std::min(occ, 2);
+    float best = 1e30f;
+    for (int r = 0; r < 4 && e == cudaSuccess; ++r) {
+        uint64_t n = r ? ops : 16;  // the first launch warms up
+        void* args[] = {&ctl, &n};
+        cudaEventRecord(a);
+        e = cudaLaunchCooperativeKernel((const void*)k_probe_barrier, dim3(grid), dim3(512), args, 0, nullptr);
+        cudaEventRecord(b);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+        if (r && ms > 0 && ms < best) best = ms;
+    }
+    Ctl h{};
+    if (e == cudaSuccess) e = cudaMemcpy(&h, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && (h.status & ST_TIMEOUT)) e = cudaErrorLaunchTimeout;
+    if (e == cudaSuccess) *ops_per_s = (double)ops / (best * 1e-3);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (ctl) cudaFree(ctl);
+    return e;
+}
+
 cudaError_t probe(uint32_t kind, uint64_t bytes, uint64_t ops, double* ops_per_s) {
+    if (kind == 6) return ops ? probe_barrier(ops, ops_per_s) : cudaErrorInvalidValue;
     if (kind > 5 || bytes < 64) return cudaErrorInvalidValue;
     uint32_t* buf = nullptr;
     uint32_t* sink = nullptr;

@@ -80,9 +80,7 @@ struct MswsDev {
     uint32_t flag_cap;       // capacity of flag_list / per-slot arrays
     // ordered-replay scratch
     uint32_t* flag_list;     // slot -> bucket
-    uint32_t* bitmap;        // 1 bit per bucket, set while the bucket is flagged
     uint32_t* tile_counts;   // per key tile of the chunk
-    uint8_t* hits;           // 1 bit per key of the chunk: its bucket was flagged (replay phase 1)
     uint2* rec[2];           // (slot, mask) records, ping-pong for the radix passes
     uint32_t* hist;          // 256 * max record tiles
     uint32_t* seg_beg;       // per slot: first record of its segment

@@ -101,9 +101,9 @@ __device__ __forceinline__ void flag_bucket(const MswsDev& D, uint32_t b) {
     const uint32_t slot = atomicAdd(&D.ctl->n_flagged, 1u);
     if (slot < D.flag_cap) {
         D.flag_list[slot] = b;
-        atomicOr(D.bitmap + (b >> 5), 1u << (b & 31));
         atomicExch(w7, FLAG | slot);
-    } else {
+    } else {  // cannot happen (a chunk flags at most one bucket per key); no slot to name
+        atomicExch(w7, 0xffffffffu);
         atomicOr(&D.ctl->status, ST_CAPACITY);
     }
 }
@@ -466,20 +466,16 @@ __device__ __forceinline__ int radix_passes(uint32_t F) {
     return (bits + 7) / 8;
 }
 
-// Was bucket b flagged in this chunk?  A per-block filter in shared memory (one bit per
-// hash of each flagged bucket) answers "no" for almost every key with one shared load; a
-// filter hit is confirmed in the bitmap of flagged buckets in global memory.
+// Slot of bucket b if it was flagged in this chunk, else NONE.  A per-block filter in shared
+// memory (one bit per hash of each flagged bucket) answers "no" for almost every key with one
+// shared load; a filter hit reads the bucket's index word, which pass 1 left at FLAG | slot.
 __device__ __forceinline__ uint32_t bloom_bit(uint32_t b) { return (b * 0x9E3779B1u) >> (32 - BLOOM_BITS); }
 
-__device__ __forceinline__ bool is_flagged(const MswsDev& D, const uint32_t* sbloom, uint32_t b) {
+__device__ __forceinline__ uint32_t flagged_slot(const MswsDev& D, const uint32_t* sbloom, uint32_t b, uint32_t F) {
     const uint32_t h = bloom_bit(b);
-    if (!((sbloom[h >> 5] >> (h & 31)) & 1u)) return false;
-    return (__ldcg(D.bitmap + (b >> 5)) >> (b & 31)) & 1u;
-}
-
-// Slot of a flagged bucket: pass 1 left FLAG | slot in its index word.
-__device__ __forceinline__ uint32_t flagged_slot(const MswsDev& D, uint32_t b) {
-    return __ldcg(D.low + (uint64_t)b * LOW_WORDS + 7) & ~FLAG;
+    if (!((sbloom[h >> 5] >> (h & 31)) & 1u)) return NONE;
+    const uint32_t w7 = __ldcg(D.low + (uint64_t)b * LOW_WORDS + 7);
+    return ((w7 & FLAG) && (w7 & ~FLAG) < F) ? (w7 & ~FLAG) : NONE;
 }
 
 __device__ __forceinline__ uint64_t globaltimer() {
@@ -561,17 +557,30 @@ struct RadixSmem {
 
 size_t msws_repair_smem() { return (size_t)SET_SLOTS * 4; }
 
-// Stable ranking of a tile of REPAIR_TILE records by the 8-bit digit at `shift`: each of
-// the 16 warps owns 256 consecutive records; per-warp digit counts, then per digit an
-// exclusive scan across warps (plus the tile's global offset when `base` is given).
-__device__ __forceinline__ void tile_count(RadixSmem& rs, const uint2* src, uint32_t K, uint32_t t, int shift) {
+// A tile of REPAIR_TILE records in registers: each of the 16 warps owns 256 consecutive
+// records, lane l of warp w holding records t*REPAIR_TILE + w*256 + r*32 + l (r < 8).  All
+// eight loads are issued before any is used, so a tile costs one L2 round trip.
+constexpr int TILE_ROUNDS = 256 / 32;
+__device__ __forceinline__ void tile_load(const uint2* src, uint32_t K, uint32_t t, uint2 (&rec)[TILE_ROUNDS]) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int r = 0; r < TILE_ROUNDS; ++r) {
+        const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
+        rec[r] = i < K ? __ldcg(&src[i]) : make_uint2(0u, 0u);
+    }
+}
+
+// Per-warp counts of the tile's records by the 8-bit digit at `shift`.
+__device__ __forceinline__ void tile_count(RadixSmem& rs, const uint2 (&rec)[TILE_ROUNDS], uint32_t K, uint32_t t,
+                                           int shift) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int d = threadIdx.x; d < 256 * (REPAIR_THREADS / 32); d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
     __syncthreads();
-    for (int r = 0; r < 256 / 32; ++r) {
+#pragma unroll
+    for (int r = 0; r < TILE_ROUNDS; ++r) {
         const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
         const bool v = i < K;
-        const uint32_t d = v ? (__ldcg(&src[i].x) >> shift) & 0xffu : 256u + lane;
+        const uint32_t d = v ? (rec[r].x >> shift) & 0xffu : 256u + lane;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
         __syncwarp();
@@ -685,7 +694,6 @@ __device__ __forceinline__ void finish_bucket(const MswsDev& D, const BatchDev& 
         __stcg(wp + 7, 0u);  // every key added to the low level; the words are final
     }
     if (lane == 0) {
-        atomicAnd(D.bitmap + (b >> 5), ~(1u << (b & 31)));
         atomicAdd(&ctl->repaired_buckets, 1ull);
         atomicAdd(&ctl->repaired_keys, (unsigned long long)n_total);
     }
@@ -762,6 +770,34 @@ __device__ __forceinline__ void replay_slot_scan(const MswsDev& D, const BatchDe
     finish_bucket<BATCH>(D, B, b, found, found ? n_total - before : 0u, n_total, T, P, cur, mL);
 }
 
+// The 8 keys of the chunk from position `base` (a multiple of 8) and their skip bits; km is
+// left at base's stream.  Two 16-byte loads when the keys are whole, contiguous (one
+// stream) and aligned; keys past n read as 0 (the caller skips them).
+template <bool BATCH>
+__device__ __forceinline__ void repair_tile_keys(const uint32_t* __restrict__ keys, uint64_t n, const MswsDev& D,
+                                                 const BatchDev& B, uint64_t base, uint32_t (&k)[8], uint32_t& skip8,
+                                                 KeyMap<BATCH>& km) {
+    uint64_t f0 = 0;
+    if (base < n) {
+        km.start(B, (uint32_t)base);
+        f0 = km.flat(B, (uint32_t)base);
+    }
+    const bool whole = base + 8 <= n && base + 8 <= km.end(B);
+    if (whole && !(reinterpret_cast<uintptr_t>(keys + f0) & 15u)) {
+        const uint4 a = __ldg(reinterpret_cast<const uint4*>(keys + f0));
+        const uint4 c = __ldg(reinterpret_cast<const uint4*>(keys + f0) + 1);
+        k[0] = a.x, k[1] = a.y, k[2] = a.z, k[3] = a.w, k[4] = c.x, k[5] = c.y, k[6] = c.z, k[7] = c.w;
+    } else if (whole) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) k[j] = __ldg(keys + f0 + j);
+    } else {
+        KeyMap<BATCH> kl = km;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) k[j] = base + j < n ? __ldg(keys + kl.flat(B, (uint32_t)(base + j))) : 0u;
+    }
+    skip8 = (D.skip && base < n) ? (__ldg(D.skip + (base >> 5)) >> (base & 31)) & 0xffu : 0u;
+}
+
 // BATCH: `keys` is the batch's flat key array and the chunk is the window the plan kernel
 // described (B.wpre, B.lo); n is read from the window (the launch's own n is ignored).
 template <bool BATCH>
@@ -806,46 +842,52 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     for (uint32_t i = gtid; i < ntot * LOW_COUNTERS; i += nthreads) __stcg(D.totals + i, 0u);
     for (uint32_t i = gtid; i < ntot; i += nthreads) __stcg(D.seg_beg + i, 0u);  // record counts (scan mode)
 
-    // Phase 1: count keys of flagged buckets per tile of the chunk.
+    // Phase 1: count keys of flagged buckets per tile of the chunk.  The next tile's keys
+    // are loaded before the current tile is tested, so their latency overlaps the hashing.
+    uint32_t k[PER], skip8 = 0;
+    KeyMap<BATCH> km;
+    if (blockIdx.x < ntk) repair_tile_keys<BATCH>(keys, n, D, B, (uint64_t)blockIdx.x * REPAIR_TILE + tid * PER, k, skip8, km);
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
         const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
-        KeyMap<BATCH> km;
-        uint64_t f0 = 0;
-        if (base < n) {
-            km.start(B, (uint32_t)base);
-            f0 = km.flat(B, (uint32_t)base);
-        }
-        // the 8 keys: two 16-byte loads when they are whole, contiguous (one stream) and
-        // aligned (base is a multiple of 8, so the 8 skip bits lie in one word)
-        uint32_t k[PER];
-        const bool whole = base + PER <= n && base + PER <= km.end(B);
-        if (whole && !(reinterpret_cast<uintptr_t>(keys + f0) & 15u)) {
-            const uint4 a = __ldg(reinterpret_cast<const uint4*>(keys + f0));
-            const uint4 c = __ldg(reinterpret_cast<const uint4*>(keys + f0) + 1);
-            k[0] = a.x, k[1] = a.y, k[2] = a.z, k[3] = a.w, k[4] = c.x, k[5] = c.y, k[6] = c.z, k[7] = c.w;
-        } else if (whole) {
-#pragma unroll
-            for (int j = 0; j < PER; ++j) k[j] = __ldg(keys + f0 + j);
-        } else {
-            KeyMap<BATCH> kl = km;
-#pragma unroll
-            for (int j = 0; j < PER; ++j) k[j] = base + j < n ? __ldg(keys + kl.flat(B, (uint32_t)(base + j))) : 0u;
-        }
-        const uint32_t skip8 = (D.skip && base < n) ? (__ldg(D.skip + (base >> 5)) >> (base & 31)) & 0xffu : 0u;
-        uint32_t hit = 0;
+        uint32_t kn[PER] = {}, skipn = 0;
+        KeyMap<BATCH> kmn;
+        if (t + gridDim.x < ntk)
+            repair_tile_keys<BATCH>(keys, n, D, B, base + (uint64_t)gridDim.x * REPAIR_TILE, kn, skipn, kmn);
+        uint32_t hit = 0, slot[PER];
+        KeyMap<BATCH> km0 = km;
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
+            slot[j] = NONE;
             if (base + j < n && !((skip8 >> j) & 1u)) {
                 if (BATCH) km.flat(B, (uint32_t)(base + j));  // moves the cursor to key j's stream
                 uint32_t hv;
                 const uint32_t b = km.bucket(D, B, k[j], hv);
-                if (is_flagged(D, sbloom, b)) hit |= 1u << j;
+                slot[j] = flagged_slot(D, sbloom, b, F);
+            }
+            if (slot[j] != NONE) hit |= 1u << j;
+        }
+        uint32_t total;
+        uint32_t pos = block_exclusive_scan((uint32_t)__popc(hit), &total);
+        if (tid == 0) __stcg(D.tile_counts + t, total);
+        // the hit keys' (slot, mask) records in array order, staged at the tile's own place
+        // in rec[1] (tile t's keys start at t * REPAIR_TILE < n, so the stage stays inside)
+        if (hit) {
+            uint2* stage = D.rec[1] + (uint64_t)t * REPAIR_TILE;
+#pragma unroll
+            for (int j = 0; j < PER; ++j) {
+                if ((hit >> j) & 1u) {
+                    if (BATCH) km0.flat(B, (uint32_t)(base + j));
+                    uint32_t hv;
+                    km0.bucket(D, B, k[j], hv);
+                    __stcg(stage + pos, make_uint2(slot[j], __ldg(D.masks + fast_mod(D.fm_mask, hv))));
+                    ++pos;
+                }
             }
         }
-        __stcg(D.hits + (base >> 3), (uint8_t)hit);  // PER == 8: one byte per thread
-        uint32_t total;
-        block_exclusive_scan((uint32_t)__popc(hit), &total);
-        if (tid == 0) __stcg(D.tile_counts + t, total);
+#pragma unroll
+        for (int j = 0; j < PER; ++j) k[j] = kn[j];
+        skip8 = skipn;
+        km = kmn;
     }
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 0);
@@ -861,30 +903,18 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     // Few records (K <= SCAN_CAP): the replay scans them unsorted, and the per-slot counter
     // totals and record counts it needs are accumulated here with global atomics.
     const bool scan_mode = K <= SCAN_CAP;
-    // Phase 3: stable write of (slot, mask) records in array order.
+    // Phase 3: the staged records of every tile move to their place in array order.
     for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
-        // only the keys phase 1 marked are hashed again
-        const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
-        const uint32_t hit = base < n ? __ldcg(D.hits + (base >> 3)) : 0u;
-        uint32_t total;
-        uint32_t pos = block_exclusive_scan((uint32_t)__popc(hit), &total) + spre[t];
-        if (hit) {
-            KeyMap<BATCH> km;
-            km.start(B, (uint32_t)base);
-            for (uint32_t m = hit; m; m &= m - 1) {
-                const int j = __ffs(m) - 1;
-                const uint64_t f = km.flat(B, (uint32_t)(base + j));
-                uint32_t hv;
-                const uint32_t b = km.bucket(D, B, __ldg(keys + f), hv);
-                const uint32_t slot = flagged_slot(D, b);
-                const uint32_t mask = __ldg(D.masks + fast_mod(D.fm_mask, hv));
-                __stcg(D.rec[0] + pos, make_uint2(slot, mask));
-                ++pos;
-                if (scan_mode && slot < D.long_cap) {
-                    for (uint32_t mm = mask; mm; mm &= mm - 1)
-                        atomicAdd(D.totals + (uint64_t)slot * LOW_COUNTERS + (__ffs(mm) - 1), 1u);
-                    atomicAdd(D.seg_beg + slot, 1u);
-                }
+        const uint32_t beg = spre[t];
+        const uint32_t cnt = (t + 1 < ntk ? spre[t + 1] : K) - beg;
+        const uint2* stage = D.rec[1] + (uint64_t)t * REPAIR_TILE;
+        for (uint32_t i = tid; i < cnt; i += REPAIR_THREADS) {
+            const uint2 r = __ldcg(stage + i);
+            __stcg(D.rec[0] + beg + i, r);
+            if (scan_mode && r.x < D.long_cap) {
+                for (uint32_t mm = r.y; mm; mm &= mm - 1)
+                    atomicAdd(D.totals + (uint64_t)r.x * LOW_COUNTERS + (__ffs(mm) - 1), 1u);
+                atomicAdd(D.seg_beg + r.x, 1u);
             }
         }
     }
@@ -924,7 +954,9 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         uint2* dst = D.rec[(p + 1) & 1];
         const int shift = 8 * p;
         for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {  // per-tile digit counts
-            tile_count(rs, src, K, t, shift);
+            uint2 rec[TILE_ROUNDS];
+            tile_load(src, K, t, rec);
+            tile_count(rs, rec, K, t, shift);
             for (int d = tid; d < 256; d += REPAIR_THREADS) {
                 uint32_t s = 0;
                 for (int w = 0; w < NW; ++w) s += rs.whist[w][d];
@@ -961,7 +993,9 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             __syncthreads();
         }
         for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {  // stable scatter
-            tile_count(rs, src, K, t, shift);
+            uint2 rec[TILE_ROUNDS];
+            tile_load(src, K, t, rec);
+            tile_count(rs, rec, K, t, shift);
             for (int d = tid; d < 256; d += REPAIR_THREADS) {
                 uint32_t run = s_dbase[d] + __ldcg(D.hist + (uint64_t)d * ntr + t);
                 for (int w = 0; w < NW; ++w) {
@@ -971,15 +1005,15 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
                 }
             }
             __syncthreads();
-            for (int r = 0; r < 256 / 32; ++r) {
+#pragma unroll
+            for (int r = 0; r < TILE_ROUNDS; ++r) {
                 const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
                 const bool v = i < K;
-                const uint2 rec = v ? __ldcg(&src[i]) : make_uint2(0, 0);
-                const uint32_t d = v ? (rec.x >> shift) & 0xffu : 256u + lane;
+                const uint32_t d = v ? (rec[r].x >> shift) & 0xffu : 256u + lane;
                 const uint32_t peers = __match_any_sync(0xffffffffu, d);
                 if (v) {
                     const uint32_t rank = rs.whist[wid][d] + __popc(peers & lanemask_lt());
-                    __stcg(dst + rank, rec);
+                    __stcg(dst + rank, rec[r]);
                 }
                 __syncwarp();
                 if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);

@@ -37,9 +37,7 @@ constexpr uint64_t NA_OFF_SEG = NA_OFF_FLAGS + na_align(NA_MAX_KEYS * 4);
 constexpr uint64_t NA_OFF_TILES = NA_OFF_SEG + na_align(NA_MAX_KEYS * 4);
 constexpr uint64_t NA_OFF_HIST = NA_OFF_TILES + na_align(NA_TILES * 4);
 constexpr uint64_t NA_OFF_TOTALS = NA_OFF_HIST + na_align(256 * NA_TILES * 4 + 256 * 4);  // + digit totals
-constexpr uint64_t NA_OFF_BITMAP = NA_OFF_TOTALS + na_align(NA_TOTAL_SLOTS * LOW_COUNTERS * 4);
-constexpr uint64_t NA_OFF_HITS = NA_OFF_BITMAP + na_align(NA_MAX_BUCKETS / 8);
-constexpr uint64_t NA_BYTES = NA_OFF_HITS + na_align(NA_MAX_KEYS / 8);
+constexpr uint64_t NA_BYTES = NA_OFF_TOTALS + na_align(NA_TOTAL_SLOTS * LOW_COUNTERS * 4);
 static_assert(NA_BYTES <= QS_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds the documented size");
 static_assert(sizeof(Ctl) <= QS_MSWS_STATE_BYTES, "control block exceeds the caller's state block");
 
@@ -151,16 +149,10 @@ extern "C" qs_status qs_msws_insert_noalloc(uint32_t* d_low, uint64_t n_low, uin
     D.tile_counts = reinterpret_cast<uint32_t*>(sc + NA_OFF_TILES);
     D.hist = reinterpret_cast<uint32_t*>(sc + NA_OFF_HIST);
     D.totals = reinterpret_cast<uint32_t*>(sc + NA_OFF_TOTALS);
-    D.bitmap = reinterpret_cast<uint32_t*>(sc + NA_OFF_BITMAP);
-    D.hits = sc + NA_OFF_HITS;
 
-    // The flag bitmap must start at zero; a previous call may have left bits behind if it
-    // was cut short.  The other scratch parts are written before they are read.
-    e = cudaMemsetAsync(D.bitmap, 0, ((n_low + 31) / 32) * 4, st);
-    if (e == cudaSuccess) {
-        k_noalloc_begin<<<1, 1, 0, st>>>(D.ctl);
-        e = cudaGetLastError();
-    }
+    // Every scratch part is written before it is read.
+    k_noalloc_begin<<<1, 1, 0, st>>>(D.ctl);
+    e = cudaGetLastError();
     if (e == cudaSuccess) e = msws_insert_pass(d_keys, n, D, nd->launch, 2, st);
     if (e == cudaSuccess) e = msws_repair(d_keys, n, D, nd->launch, st);
     if (e != cudaSuccess) {

@@ -210,7 +210,7 @@ class Sketch_GPU_Sub_Warp_Level(Sketch):
     def __init__(self, n_low=0, m_low=8, n_high=1024, m_high=32, seed_sz=1, n_hash_mask_table=1021, *,
                  low_bytes=0, hash_mask_ones=3, hash_seed=0, seed_rng=1, mask_rng=1, mask_table=None,
                  compat_v3=False, max_batch=0, device=None, aggregate=0, lanes_per_key=0, route=0,
-                 ctas_per_sm=0, chunk_ramp=True, keys_per_tile=0):
+                 ctas_per_sm=0, chunk_ramp=True, keys_per_tile=0, first_chunk=0):
         p = qs_params()
         lib.qs_params_default(ctypes.byref(p))
         p.kind = QS_KIND_MSWS
@@ -219,7 +219,7 @@ class Sketch_GPU_Sub_Warp_Level(Sketch):
         p.seed_sz, p.hash_mask_table_sz, p.hash_mask_ones = seed_sz, n_hash_mask_table, hash_mask_ones
         p.hash_seed, p.seed_rng, p.mask_rng = hash_seed, seed_rng, mask_rng
         p.max_batch, p.aggregate, p.lanes_per_key, p.route = max_batch, aggregate, lanes_per_key, route
-        p.ctas_per_sm, p.keys_per_tile = ctas_per_sm, keys_per_tile
+        p.ctas_per_sm, p.keys_per_tile, p.first_chunk = ctas_per_sm, keys_per_tile, first_chunk
         p.device = -1 if device is None else int(device)
         self._keep = None
         if mask_table is not None:
