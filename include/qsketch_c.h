@@ -198,8 +198,9 @@ typedef struct qs_profile {
     uint64_t insert_launches, repair_launches, query_launches;
     /* MSWS ordered repair, measured on the device (globaltimer) since the previous
      * qs_get_profile: invocations that found crossed buckets, and time per phase —
-     * 0 filter count, 1 tile scan, 2 filter write, 3 radix passes, 4-5 segments,
-     * 6 long-segment counts, 7 replay. */
+     * 0 flag test (and staging of the records), 1 tile scan, 2 record move, radix passes
+     * split into 6 tile digit counts, 7 digit scans and 3 scatters, 4 segments and
+     * totals, 5 replay. */
     uint64_t repairs_active;
     double repair_phase_ms[8];
 } qs_profile;

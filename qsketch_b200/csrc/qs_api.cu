@@ -1712,7 +1712,7 @@ qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, u
     if (base->kind != QS_KIND_MSWS) return fail(QS_ERR_INVALID_ARG, "qs_autotune: MSWS sketches only");
     if (reinterpret_cast<uintptr_t>(d_keys) & 3u) return fail(QS_ERR_INVALID_ARG, "keys not 4-byte aligned");
     reps = std::max(1u, reps);
-    // chunk sizes worth trying: 2^20 .. 2^24, none far beyond the sample; a caller that inserts
+    // chunk sizes worth trying: 2^20 .. 2^26, none far beyond the sample; a caller that inserts
     // in calls of a fixed size passes it as base->max_batch: that size is kept, and the sample
     // is inserted in chunks of it (into a sketch that keeps its state from chunk to chunk)
     std::vector<uint64_t> mbs;
@@ -1721,7 +1721,7 @@ qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, u
             return fail(QS_ERR_INVALID_ARG, "qs_autotune: max_batch must be a multiple of 32, at most 2^26");
         mbs.push_back(base->max_batch);
     } else {
-        for (uint64_t mb = 1ull << 20; mb <= (1ull << 24); mb <<= 1)
+        for (uint64_t mb = 1ull << 20; mb <= (1ull << 26); mb <<= 1)
             if (mb <= std::max<uint64_t>(1ull << 20, 2 * (uint64_t)n)) mbs.push_back(mb);
     }
     qs_params p = *base;

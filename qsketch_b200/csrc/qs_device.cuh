@@ -59,24 +59,33 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 // ---- grid barrier for cooperative launches (bounded) ---------------------------------
-// All blocks of the grid are co-resident (cudaLaunchCooperativeKernel).  Returns false
-// (and latches ST_TIMEOUT) if the other blocks do not arrive within the spin limit.
+// All blocks of the grid are co-resident (cudaLaunchCooperativeKernel).  Thread 0 of each
+// block reads the generation before the block arrives (it cannot advance earlier), fences
+// the block's writes and arrives with atomicInc, which wraps the counter to 0 on the last
+// arrival; the last block fences again and advances the generation, the others poll it
+// with acquire loads.  Returns false (and latches ST_TIMEOUT) if the other blocks do not
+// arrive within the spin limit.
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ bool grid_barrier(Ctl* ctl) {
     __shared__ int s_ok;
+    uint32_t gen = 0;
+    if (threadIdx.x == 0) gen = ld_acquire_gpu(&ctl->bar_gen);
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile uint32_t* genp = &ctl->bar_gen;
-        const uint32_t gen = *genp;
         __threadfence();
-        const uint32_t arrived = atomicAdd(&ctl->bar_count, 1u);
+        const uint32_t arrived = atomicInc(&ctl->bar_count, gridDim.x - 1);
         int ok = 1;
         if (arrived == gridDim.x - 1) {
-            atomicExch(&ctl->bar_count, 0u);
             __threadfence();
             atomicAdd(&ctl->bar_gen, 1u);
         } else {
             uint32_t it = 0;
-            while (*genp == gen) {
+            while (ld_acquire_gpu(&ctl->bar_gen) == gen) {
                 if (++it > SPIN_LIMIT) {
                     ok = 0;
                     atomicOr(&ctl->status, ST_TIMEOUT);
@@ -85,7 +94,6 @@ __device__ __forceinline__ bool grid_barrier(Ctl* ctl) {
                 if (it > 256) __nanosleep(64);
             }
         }
-        __threadfence();
         s_ok = ok;
     }
     __syncthreads();

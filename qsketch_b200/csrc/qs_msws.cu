@@ -117,6 +117,14 @@ __device__ __forceinline__ bool agg_insert(const InsShared& S, uint32_t key, uin
     const uint32_t h = (key * 0x9E3779B1u) >> 22;  // 10 bits
     for (int p = 0; p < AGG_PROBES; ++p) {
         const uint32_t s = (h + p) & (AGG_SLOTS - 1);
+        // a key already in the table (the common case for a heavy key) needs no CAS: a slot
+        // only goes from empty to a key within a tile
+        const uint32_t seen = reinterpret_cast<volatile uint32_t*>(S.akey)[s];
+        if (seen == key) {
+            atomicAdd(S.acnt + s, c);
+            return true;
+        }
+        if (seen != AGG_EMPTY) continue;
         const uint32_t prev = atomicCAS(S.akey + s, AGG_EMPTY, key);
         if (prev == AGG_EMPTY) {
             S.aid[s] = id;
@@ -285,16 +293,24 @@ __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& 
         const uint32_t am = __ballot_sync(0xffffffffu, c != 0);
         if (c) st[__popc(am & lanemask_lt())] = make_uint4(b, m, c, key);
         __syncwarp();
-        const uint32_t lk = staged_rounds_fused(D, S, st, __popc(am));
-        if (lk) atomicAdd(S.misc + 1, lk);
+        const uint32_t lk = __reduce_add_sync(0xffffffffu, staged_rounds_fused(D, S, st, __popc(am)));
+        if (lane == 0 && lk && D.route == 0) atomicAdd(S.misc + 1, lk);
         __syncwarp();
         return;
     }
     const uint32_t w7 = c ? __ldcg(D.low + (uint64_t)b * LOW_WORDS + 7) : 0u;
     const bool linked = c && is_linked(D, w7);
     const bool sat = c && w7 == SATURATED;
-    if (sat) atomicAdd(S.misc + 0, c);
-    if (linked) atomicAdd(S.misc + 1, c);
+    // the tile's dropped and linked keys: one shared atomic per warp (the linked count only
+    // feeds the adaptive routing)
+    if (__any_sync(0xffffffffu, sat)) {
+        const uint32_t ns = __reduce_add_sync(0xffffffffu, sat ? c : 0u);
+        if (lane == 0) atomicAdd(S.misc + 0, ns);
+    }
+    if (D.route == 0) {
+        const uint32_t nl = __reduce_add_sync(0xffffffffu, linked ? c : 0u);
+        if (lane == 0 && nl) atomicAdd(S.misc + 1, nl);
+    }
     bool direct_high = linked, tabled = false;
     if (AGG == AGG_BLOCK && use_table) {
         if (linked)
@@ -595,15 +611,21 @@ __device__ __forceinline__ void tile_count(RadixSmem& rs, const uint2 (&rec)[TIL
 // selected counter above LIMIT is found (the low->high switch of :160-190), the bucket is
 // linked there (atomic_malloc, :69-85) and that key and all later ones count high.
 
-// Lane c accumulates the occurrences of counter c among the 32 masks of the warp.
-__device__ __forceinline__ void count_counters(uint32_t m, uint32_t& T) {
+// Occurrences of counter c (lane c) among the 32 masks of the warp: seven warp sums of the
+// masks expanded to one byte per counter (a byte counts at most 32, so no carries).
+__device__ __forceinline__ uint32_t group_counts(uint32_t m) {
     const int lane = threadIdx.x & 31;
+    uint32_t mine = 0;
 #pragma unroll
-    for (int c = 0; c < LOW_COUNTERS; ++c) {
-        const uint32_t bal = __ballot_sync(0xffffffffu, (m >> c) & 1u);
-        if (lane == c) T += __popc(bal);
+    for (int w = 0; w < 7; ++w) {
+        const uint32_t t = __reduce_add_sync(0xffffffffu, expand_nibble((m >> (4 * w)) & 0xfu));
+        if ((lane >> 2) == w) mine = t;
     }
+    return lane < LOW_COUNTERS ? (mine >> (8 * (lane & 3))) & 0xffu : 0u;
 }
+
+// Lane c accumulates the occurrences of counter c among the 32 masks of the warp.
+__device__ __forceinline__ void count_counters(uint32_t m, uint32_t& T) { T += group_counts(m); }
 
 // Pre-chunk counter of lane i from the bucket's final words and the chunk totals T.
 __device__ __forceinline__ uint32_t pre_counters(const uint32_t* wp, uint32_t T) {
@@ -621,6 +643,13 @@ __device__ __forceinline__ uint32_t pre_counters(const uint32_t* wp, uint32_t T)
 // the records before it (all 32 when none triggers).
 __device__ __forceinline__ int link_step(uint32_t m, uint32_t& cur) {
     const int lane = threadIdx.x & 31;
+    // The last record with counter c sees cur + (occurrences - 1): when that stays within
+    // LIMIT for every counter, no record of the group switches.
+    const uint32_t tot = group_counts(m);
+    if (!__any_sync(0xffffffffu, tot && cur + tot > LIMIT + 1)) {
+        cur += tot;
+        return -1;
+    }
     const uint32_t lt = lanemask_lt();
     bool trig = false;
     uint32_t inc = 0;
@@ -715,13 +744,25 @@ __device__ __forceinline__ void replay_slot(const MswsDev& D, const BatchDev& B,
     }
     const uint32_t P = pre_counters(D.low + (uint64_t)b * LOW_WORDS, T);
     uint32_t cur = P, mL = 0, L = NONE;
-    for (uint32_t g = beg; g < end; g += 32) {
-        const uint32_t m = (g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u;
-        const int j = link_step(m, cur);
-        if (j >= 0) {
-            L = g + j;
-            mL = __shfl_sync(0xffffffffu, m, j);
-            break;
+    // four groups of 32 records loaded per step, so a long segment costs one L2 round trip
+    // per 128 records
+    constexpr int GR = 4;
+    for (uint32_t g0 = beg; g0 < end && L == NONE; g0 += 32 * GR) {
+        uint32_t mm[GR];
+#pragma unroll
+        for (int q = 0; q < GR; ++q) {
+            const uint32_t i = g0 + 32 * q + lane;
+            mm[q] = i < end ? __ldcg(&sorted[i].y) : 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < GR; ++q) {
+            if (L == NONE && g0 + 32 * q < end) {  // warp-uniform
+                const int j = link_step(mm[q], cur);
+                if (j >= 0) {
+                    L = g0 + 32 * q + j;
+                    mL = __shfl_sync(0xffffffffu, mm[q], j);
+                }
+            }
         }
     }
     finish_bucket<BATCH>(D, B, b, L != NONE, L != NONE ? end - L : 0u, end - beg, T, P, cur, mL);
@@ -965,6 +1006,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             __syncthreads();
         }
         if (!grid_barrier(ctl)) return;
+        phase_mark(ctl, 6);
         // one warp per digit scans its row of tile counts (exclusive, in place) and stores the
         // digit's total; then every block forms the 256 digit bases itself
         uint32_t* dtot = D.hist + 256ull * D.max_tiles;
@@ -986,6 +1028,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             if (lane == 0) __stcg(dtot + d, run);
         }
         if (!grid_barrier(ctl)) return;
+        phase_mark(ctl, 7);
         {
             uint32_t total;
             const uint32_t ex = block_exclusive_scan(tid < 256 ? __ldcg(dtot + tid) : 0u, &total);
@@ -1022,8 +1065,8 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             __syncthreads();
         }
         if (!grid_barrier(ctl)) return;
+        phase_mark(ctl, 3);
     }
-    phase_mark(ctl, 3);
 
     // Phase 5: segment starts, and per-counter totals of slots < long_cap; each block a
     // contiguous record range whose first and last slot accumulate in shared memory.
