@@ -198,11 +198,11 @@ typedef struct qs_profile {
     uint64_t insert_launches, repair_launches, query_launches;
     /* MSWS ordered repair, measured on the device (globaltimer) since the previous
      * qs_get_profile: invocations that found crossed buckets, and time per phase —
-     * 0 flag test (and staging of the records), 1 tile scan, 2 record move, radix passes
-     * split into 6 tile digit counts, 7 digit scans and 3 scatters, 4 segments and
-     * totals, 5 replay. */
+     * 8 filter build, 0 flag test (and staging of the records), 1 tile scan, 2 record
+     * move, radix passes split into 6 tile digit counts, 7 digit scans and 3 scatters,
+     * 4 segments and totals, 5 replay; 9-11 unused. */
     uint64_t repairs_active;
-    double repair_phase_ms[8];
+    double repair_phase_ms[12];
 } qs_profile;
 qs_status qs_set_profiling(qs_sketch *sk, int enable);
 qs_status qs_get_profile(qs_sketch *sk, qs_profile *out);

@@ -76,7 +76,7 @@ class qs_profile(ctypes.Structure):
         ("repair_launches", ctypes.c_uint64),
         ("query_launches", ctypes.c_uint64),
         ("repairs_active", ctypes.c_uint64),
-        ("repair_phase_ms", ctypes.c_double * 8),
+        ("repair_phase_ms", ctypes.c_double * 12),
     ]
 
 

@@ -655,7 +655,7 @@ qs_status qs_get_profile(qs_sketch* sk, qs_profile* out) {
         Ctl c;
         CK(cudaMemcpy(&c, sk->D.ctl, sizeof c, cudaMemcpyDeviceToHost), "read repair phases");
         out->repairs_active = c.repairs;
-        for (int k = 0; k < 8; ++k) out->repair_phase_ms[k] = (double)c.phase_ns[k] * 1e-6;
+        for (int k = 0; k < 12; ++k) out->repair_phase_ms[k] = (double)c.phase_ns[k] * 1e-6;
         CK(cudaMemset(&sk->D.ctl->repairs, 0, sizeof(unsigned long long) * 10), "reset repair phases");
     }
     return QS_OK;

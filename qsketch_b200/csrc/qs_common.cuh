@@ -61,7 +61,7 @@ struct Ctl {
     unsigned long long inserted;
     unsigned long long repairs;        // repair invocations that had flagged buckets
     unsigned long long phase_t;        // globaltimer at the last phase mark
-    unsigned long long phase_ns[8];    // accumulated time per repair phase
+    unsigned long long phase_ns[12];   // accumulated time per repair phase
 };
 
 // Everything a MSWS kernel needs, passed by value.

@@ -882,6 +882,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     const uint32_t ntot = min(F, D.long_cap);
     for (uint32_t i = gtid; i < ntot * LOW_COUNTERS; i += nthreads) __stcg(D.totals + i, 0u);
     for (uint32_t i = gtid; i < ntot; i += nthreads) __stcg(D.seg_beg + i, 0u);  // record counts (scan mode)
+    phase_mark(ctl, 8);
 
     // Phase 1: count keys of flagged buckets per tile of the chunk.  The next tile's keys
     // are loaded before the current tile is tested, so their latency overlaps the hashing.
@@ -990,20 +991,61 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     const int npass = radix_passes(F);
     const uint32_t ntr = (K + REPAIR_TILE - 1) / REPAIR_TILE;
     const uint2* sorted = D.rec[npass & 1];
+    // One tile per block (up to gridDim.x * REPAIR_TILE records): the count keeps the tile's
+    // records, each record's rank within its warp's run of its digit, and the per-warp digit
+    // offsets in shared memory, so the scatter needs neither a reload nor a recount.
+    const bool resident = ntr <= gridDim.x;
+    uint2* srec = reinterpret_cast<uint2*>(s_set);   // [REPAIR_TILE]
+    uint32_t* srank = s_set + 2 * REPAIR_TILE;        // [REPAIR_TILE]
+    static_assert(3 * REPAIR_TILE <= SET_SLOTS, "resident tile fits the shared space");
     for (int p = 0; p < npass; ++p) {
         const uint2* src = D.rec[p & 1];
         uint2* dst = D.rec[(p + 1) & 1];
         const int shift = 8 * p;
-        for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {  // per-tile digit counts
-            uint2 rec[TILE_ROUNDS];
-            tile_load(src, K, t, rec);
-            tile_count(rs, rec, K, t, shift);
-            for (int d = tid; d < 256; d += REPAIR_THREADS) {
-                uint32_t s = 0;
-                for (int w = 0; w < NW; ++w) s += rs.whist[w][d];
-                __stcg(D.hist + (uint64_t)d * ntr + t, s);
+        if (resident) {
+            if (blockIdx.x < ntr) {
+                const uint32_t t = blockIdx.x;
+                uint2 rec[TILE_ROUNDS];
+                tile_load(src, K, t, rec);
+                for (int d = tid; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
+                __syncthreads();
+#pragma unroll
+                for (int r = 0; r < TILE_ROUNDS; ++r) {
+                    const uint32_t li = wid * 256 + r * 32 + lane;
+                    const bool v = t * REPAIR_TILE + li < K;
+                    const uint32_t d = v ? (rec[r].x >> shift) & 0xffu : 256u + lane;
+                    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+                    const uint32_t before = v ? rs.whist[wid][d] : 0u;
+                    __syncwarp();
+                    if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] = before + __popc(peers);
+                    __syncwarp();
+                    srec[li] = rec[r];
+                    srank[li] = before + __popc(peers & lanemask_lt());
+                }
+                __syncthreads();
+                for (int d = tid; d < 256; d += REPAIR_THREADS) {  // per-warp offsets, tile total
+                    uint32_t run = 0;
+                    for (int w = 0; w < NW; ++w) {
+                        const uint32_t x = rs.whist[w][d];
+                        rs.whist[w][d] = run;
+                        run += x;
+                    }
+                    __stcg(D.hist + (uint64_t)d * ntr + t, run);
+                }
+                __syncthreads();
             }
-            __syncthreads();
+        } else {
+            for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {  // per-tile digit counts
+                uint2 rec[TILE_ROUNDS];
+                tile_load(src, K, t, rec);
+                tile_count(rs, rec, K, t, shift);
+                for (int d = tid; d < 256; d += REPAIR_THREADS) {
+                    uint32_t s = 0;
+                    for (int w = 0; w < NW; ++w) s += rs.whist[w][d];
+                    __stcg(D.hist + (uint64_t)d * ntr + t, s);
+                }
+                __syncthreads();
+            }
         }
         if (!grid_barrier(ctl)) return;
         phase_mark(ctl, 6);
@@ -1035,7 +1077,24 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             if (tid < 256) s_dbase[tid] = ex;
             __syncthreads();
         }
-        for (uint32_t t = blockIdx.x; t < ntr; t += gridDim.x) {  // stable scatter
+        if (resident) {
+            if (blockIdx.x < ntr) {
+                const uint32_t t = blockIdx.x;
+                for (int d = tid; d < 256; d += REPAIR_THREADS) s_dbase[d] += __ldcg(D.hist + (uint64_t)d * ntr + t);
+                __syncthreads();
+#pragma unroll
+                for (int r = 0; r < TILE_ROUNDS; ++r) {
+                    const uint32_t li = wid * 256 + r * 32 + lane;
+                    if (t * REPAIR_TILE + li < K) {
+                        const uint2 rec = srec[li];
+                        const uint32_t d = (rec.x >> shift) & 0xffu;
+                        __stcg(dst + s_dbase[d] + rs.whist[wid][d] + srank[li], rec);
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (uint32_t t = blockIdx.x; t < ntr && !resident; t += gridDim.x) {  // stable scatter
             uint2 rec[TILE_ROUNDS];
             tile_load(src, K, t, rec);
             tile_count(rs, rec, K, t, shift);
