@@ -472,6 +472,7 @@ constexpr int SET_SLOTS = 16384;  // words of the repair's dynamic shared memory
                                   // the phases: flag filter, tile prefix, staged records
 constexpr int BLOOM_BITS = 17;    // per-block filter of the flagged buckets: 2^17 bits (16 KiB)
 constexpr int BLOOM_WORDS = (1 << BLOOM_BITS) / 32;
+constexpr uint32_t TC_MAX = 128;  // tiles per block in the flag test (grids have >= 148 blocks)
 constexpr uint32_t SCAN_CAP = SET_SLOTS / 2;  // records replayed without a sort (64 KiB of uint2)
 static_assert(BLOOM_WORDS <= SET_SLOTS, "filter fits the shared space");
 constexpr uint32_t NONE = 0xffffffffu;
@@ -848,6 +849,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     __shared__ uint32_t s_dbase[256];  // radix pass: first output position of each digit
     __shared__ uint32_t s_acc[2][LOW_COUNTERS];
     __shared__ uint32_t s_acc_slot[2];
+    __shared__ uint32_t s_tc[TC_MAX];       // phase 1: counts of this block's tiles, by round
     extern __shared__ __align__(16) uint32_t s_set[];
     Ctl* ctl = D.ctl;
     const uint32_t F = min(__ldcg(&ctl->n_flagged), D.flag_cap);
@@ -863,7 +865,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     // the tile-count prefix of phase 2 lives in the SET_SLOTS words of shared memory: chunks of at most
     // SET_SLOTS tiles (2^26 keys; the host rejects larger max_batch); uniform, so every block
     // leaves before any barrier
-    if (ntk > (uint32_t)SET_SLOTS) {
+    if (ntk > (uint32_t)SET_SLOTS || ntk > TC_MAX * gridDim.x) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->status, ST_CAPACITY);
         return;
     }
@@ -874,22 +876,35 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     uint32_t* sbloom = s_set;
     for (int i = tid; i < BLOOM_WORDS; i += REPAIR_THREADS) sbloom[i] = 0u;
     __syncthreads();
-    for (uint32_t s = tid; s < F; s += REPAIR_THREADS) {
-        const uint32_t h = bloom_bit(__ldcg(D.flag_list + s));
-        atomicOr(sbloom + (h >> 5), 1u << (h & 31));
+    for (uint32_t s0 = tid; s0 < F; s0 += 8 * REPAIR_THREADS) {  // eight loads in flight
+        uint32_t fb[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) fb[u] = s0 + u * REPAIR_THREADS < F ? __ldcg(D.flag_list + s0 + u * REPAIR_THREADS) : NONE;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (fb[u] != NONE) {
+                const uint32_t h = bloom_bit(fb[u]);
+                atomicOr(sbloom + (h >> 5), 1u << (h & 31));
+            }
+        }
     }
+    for (int i = tid; i < TC_MAX; i += REPAIR_THREADS) s_tc[i] = 0u;
     __syncthreads();
     const uint32_t ntot = min(F, D.long_cap);
     for (uint32_t i = gtid; i < ntot * LOW_COUNTERS; i += nthreads) __stcg(D.totals + i, 0u);
     for (uint32_t i = gtid; i < ntot; i += nthreads) __stcg(D.seg_beg + i, 0u);  // record counts (scan mode)
     phase_mark(ctl, 8);
 
-    // Phase 1: count keys of flagged buckets per tile of the chunk.  The next tile's keys
-    // are loaded before the current tile is tested, so their latency overlaps the hashing.
+    // Phase 1: the keys of flagged buckets, per tile of the chunk.  Each warp owns 256
+    // consecutive keys of a tile (8 per lane) and stages their records at its own place, so
+    // no block-wide synchronisation happens per tile: the warp's record count goes to wcnt
+    // (the histogram buffer, unused until the radix passes) and into the tile's count in
+    // shared memory.  The next tile's keys are loaded before the current tile is tested.
+    uint32_t* wcnt = D.hist;  // [ntk][NW]
     uint32_t k[PER], skip8 = 0;
     KeyMap<BATCH> km;
     if (blockIdx.x < ntk) repair_tile_keys<BATCH>(keys, n, D, B, (uint64_t)blockIdx.x * REPAIR_TILE + tid * PER, k, skip8, km);
-    for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
+    for (uint32_t t = blockIdx.x, rk = 0; t < ntk; t += gridDim.x, ++rk) {
         const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
         uint32_t kn[PER] = {}, skipn = 0;
         KeyMap<BATCH> kmn;
@@ -908,13 +923,24 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             }
             if (slot[j] != NONE) hit |= 1u << j;
         }
-        uint32_t total;
-        uint32_t pos = block_exclusive_scan((uint32_t)__popc(hit), &total);
-        if (tid == 0) __stcg(D.tile_counts + t, total);
-        // the hit keys' (slot, mask) records in array order, staged at the tile's own place
-        // in rec[1] (tile t's keys start at t * REPAIR_TILE < n, so the stage stays inside)
+        const uint32_t hc = __popc(hit);
+        uint32_t x = hc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        uint32_t pos = x - hc;
+        const uint32_t wtot = __shfl_sync(0xffffffffu, x, 31);
+        if (lane == 0) {
+            __stcg(wcnt + (uint64_t)t * NW + wid, wtot);
+            if (wtot) atomicAdd(s_tc + rk, wtot);
+        }
+        // the hit keys' (slot, mask) records in array order, staged at the warp's own place
+        // in rec[1] (its keys start at t * REPAIR_TILE + wid * 256 < n, so the stage stays
+        // inside)
         if (hit) {
-            uint2* stage = D.rec[1] + (uint64_t)t * REPAIR_TILE;
+            uint2* stage = D.rec[1] + (uint64_t)t * REPAIR_TILE + wid * 256;
 #pragma unroll
             for (int j = 0; j < PER; ++j) {
                 if ((hit >> j) & 1u) {
@@ -931,6 +957,9 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         skip8 = skipn;
         km = kmn;
     }
+    __syncthreads();
+    for (uint32_t r = tid; blockIdx.x + r * gridDim.x < ntk; r += REPAIR_THREADS)
+        __stcg(D.tile_counts + blockIdx.x + r * gridDim.x, s_tc[r]);
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 0);
     // Phase 2: every block scans the tile counts itself (exclusive, in shared memory — the
@@ -945,13 +974,32 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     // Few records (K <= SCAN_CAP): the replay scans them unsorted, and the per-slot counter
     // totals and record counts it needs are accumulated here with global atomics.
     const bool scan_mode = K <= SCAN_CAP;
-    // Phase 3: the staged records of every tile move to their place in array order.
-    for (uint32_t t = blockIdx.x; t < ntk; t += gridDim.x) {
-        const uint32_t beg = spre[t];
-        const uint32_t cnt = (t + 1 < ntk ? spre[t + 1] : K) - beg;
+    // Phase 3: the staged records of every tile move to their place in array order, one warp
+    // per tile: the tile's 16 region counts, scanned in the warp, place record i of the tile
+    // in region r (the first whose running count exceeds i) at offset i - (counts before r).
+    for (uint32_t t = blockIdx.x * NW + wid; t < ntk; t += gridDim.x * NW) {
+        const uint32_t beg = spre[t], cnt = (t + 1 < ntk ? spre[t + 1] : K) - beg;
+        if (cnt == 0) continue;  // warp-uniform
+        const uint32_t v = lane < NW ? __ldcg(wcnt + (uint64_t)t * NW + lane) : 0u;
+        uint32_t x = v;  // inclusive running count over the regions
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
         const uint2* stage = D.rec[1] + (uint64_t)t * REPAIR_TILE;
-        for (uint32_t i = tid; i < cnt; i += REPAIR_THREADS) {
-            const uint2 r = __ldcg(stage + i);
+        for (uint32_t i0 = 0; i0 < cnt; i0 += 32) {  // warp-uniform trip count
+            const uint32_t i = i0 + lane;
+            uint32_t lo = 0, hi = NW - 1;  // region of record i: x[lo - 1] <= i < x[lo]
+#pragma unroll
+            for (int it = 0; it < 4; ++it) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (__shfl_sync(0xffffffffu, x, mid) > i) hi = mid;
+                else lo = mid + 1;
+            }
+            const uint32_t before = __shfl_sync(0xffffffffu, x - v, lo);
+            if (i >= cnt) continue;
+            const uint2 r = __ldcg(stage + lo * 256 + (i - before));
             __stcg(D.rec[0] + beg + i, r);
             if (scan_mode && r.x < D.long_cap) {
                 for (uint32_t mm = r.y; mm; mm &= mm - 1)
