@@ -1269,15 +1269,24 @@ __device__ __forceinline__ uint32_t msws_lookup(const MswsDev& D, const uint32_t
 __global__ void __launch_bounds__(QRY_THREADS) k_msws_query(const uint32_t* __restrict__ keys, uint64_t n,
                                                             uint32_t* __restrict__ out, MswsDev D) {
     extern __shared__ __align__(16) uint32_t s_masks[];
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t base = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t k[QRY_KPT], r[QRY_KPT];
+    // the first keys are loaded while the mask table is staged
+#pragma unroll
+    for (int j = 0; j < QRY_KPT; ++j) {
+        const uint64_t i = base + j * stride;
+        k[j] = i < n ? __ldcs(keys + i) : 0u;
+    }
     for (uint32_t i = threadIdx.x; i < D.n_masks; i += blockDim.x) s_masks[i] = __ldg(D.masks + i);
     __syncthreads();
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += stride * QRY_KPT) {
-        uint32_t k[QRY_KPT], r[QRY_KPT];
+    for (; base < n; base += stride * QRY_KPT) {
+        if (base != (uint64_t)blockIdx.x * blockDim.x + threadIdx.x) {
 #pragma unroll
-        for (int j = 0; j < QRY_KPT; ++j) {
-            const uint64_t i = base + j * stride;
-            k[j] = i < n ? __ldcs(keys + i) : 0u;
+            for (int j = 0; j < QRY_KPT; ++j) {
+                const uint64_t i = base + j * stride;
+                k[j] = i < n ? __ldcs(keys + i) : 0u;
+            }
         }
 #pragma unroll
         for (int j = 0; j < QRY_KPT; ++j) r[j] = msws_lookup(D, s_masks, k[j], D.seed, D.fm_low, 0u);
