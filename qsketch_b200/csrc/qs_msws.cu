@@ -510,6 +510,26 @@ __device__ __forceinline__ void phase_mark(Ctl* ctl, int k) {
     }
 }
 
+// End of a repair: the last block to finish (counted on the grid barrier's counter, which
+// wraps back to 0) resets the chunk's counters; no block waits for the others.
+__device__ __forceinline__ void finish_repair(Ctl* ctl) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicInc(&ctl->bar_count, gridDim.x - 1) == gridDim.x - 1) {
+            __threadfence();
+            const uint64_t now = globaltimer();
+            ctl->phase_ns[5] += now - ctl->phase_t;
+            ctl->phase_t = now;
+            ctl->n_flagged = 0;
+            ctl->n_records = 0;
+            ctl->n_long = 0;
+            ctl->repairs += 1;
+            __threadfence();
+        }
+    }
+}
+
 // Batched streams: the stream of window key i (< wpre[n_streams]), i.e. the last s with
 // wpre[s] <= i, which is never an empty slice.
 __device__ __forceinline__ uint32_t stream_of_window_key(const BatchDev& B, uint32_t i) {
@@ -1023,15 +1043,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             for (uint32_t s = blockIdx.x * NWB + wid; s < F; s += gridDim.x * NWB)
                 replay_slot_scan<BATCH>(D, B, srec, s, K);
         }
-        if (!grid_barrier(ctl)) return;
-        phase_mark(ctl, 5);
-        if (blockIdx.x == 0 && tid == 0) {
-            ctl->n_flagged = 0;
-            ctl->n_records = 0;
-            ctl->n_long = 0;
-            ctl->repairs += 1;
-            __threadfence();
-        }
+        finish_repair(ctl);
         return;
     }
 
@@ -1223,15 +1235,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
 
     // Phase 6: replay each flagged bucket in array order, one warp per slot.
     for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) replay_slot<BATCH>(D, B, sorted, s, F, K, true);
-    if (!grid_barrier(ctl)) return;
-    phase_mark(ctl, 5);
-    if (blockIdx.x == 0 && tid == 0) {
-        ctl->n_flagged = 0;
-        ctl->n_records = 0;
-        ctl->n_long = 0;
-        ctl->repairs += 1;
-        __threadfence();
-    }
+    finish_repair(ctl);
 }
 
 // ---- query ----------------------------------------------------------------------------

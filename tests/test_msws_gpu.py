@@ -320,3 +320,15 @@ def test_roofline_probes_report_rates(gpu):
     assert data.probe(6, 64, 1000) > 1e4  # barriers per second
     with pytest.raises(qs.QsError):
         data.probe(7, 64 << 20)
+
+
+def test_replay_with_more_records_than_resident_tiles(gpu):
+    # One 2^23-key chunk over 2^17 distinct keys into 65521 buckets: about 128 keys per bucket,
+    # so most buckets cross and nearly every key becomes a replay record (K > 296 x 4096): the
+    # radix passes take the multi-tile-per-block path; the tables must still equal the oracle's.
+    sk, orc = make_pair(65521, 1 << 16, max_batch=1 << 23, chunk_ramp=False)
+    distinct = data.uniform_keys(1 << 17, seed=71)
+    idx = torch.randint(0, 1 << 17, (1 << 23,), generator=torch.Generator().manual_seed(5)).cuda()
+    keys = distinct.view(torch.int32)[idx].view(torch.uint32).contiguous()
+    run_and_compare(sk, orc, keys, distinct)
+    assert sk.stats()["repaired_keys"] > 296 * 4096
