@@ -139,6 +139,14 @@ __device__ __forceinline__ bool agg_insert(const InsShared& S, uint32_t key, uin
     return false;
 }
 
+// Does a selected byte (nibble bit k selects byte k) of the pre-add word `old` reach CROSS
+// once c is added: byte + c >= CROSS, i.e. byte >= CROSS - c, four bytes at a time.
+__device__ __forceinline__ bool crosses(uint32_t old, uint32_t nib, uint32_t c) {
+    if (!nib) return false;
+    if (c >= CROSS) return true;
+    return (__vcmpgeu4(old, (CROSS - c) * 0x01010101u) & (expand_nibble(nib) * 0xffu)) != 0u;
+}
+
 // Sub-warp rounds over the staged entries of this warp: entry j = (target, mask, count,
 // kind).  LPK lanes serve one entry (32/LPK entries per round, LPK rounds for 32 entries);
 // lane w of a group owns bucket words w, w+LPK, ... (LPK = 8: one word per lane, the
@@ -169,9 +177,14 @@ __device__ __forceinline__ void staged_rounds(const MswsDev& D, const uint4* st,
                 if (nib) olds[r][h] = atomicAdd(D.low + (uint64_t)e.x * LOW_WORDS + ww, expand_nibble(nib) * e.z);
             }
         } else {
+            // lane w of the group adds to the selected counters number w, w + LPK, ...
             uint32_t* hb = D.high + (uint64_t)(e.x - START) * HIGH_WORDS;
-            const int pc = __popc(e.y);
-            for (int k = w; k < pc; k += LPK) atomicAdd(hb + __fns(e.y, 0, k + 1), e.z);
+            uint32_t mm = e.y;
+            for (int k = 0; k < w && mm; ++k) mm &= mm - 1;
+            while (mm) {
+                atomicAdd(hb + (__ffs(mm) - 1), e.z);
+                for (int k = 0; k < LPK && mm; ++k) mm &= mm - 1;
+            }
         }
     }
 #pragma unroll
@@ -186,9 +199,7 @@ __device__ __forceinline__ void staged_rounds(const MswsDev& D, const uint4* st,
             for (int h = 0; h < WPL; ++h) {
                 const int ww = w + h * LPK;
                 const uint32_t nib = (ww < 7) ? (e.y >> (4 * ww)) & 0xfu : 0u;
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if (((nib >> k) & 1u) && ((olds[r][h] >> (8 * k)) & 0xffu) + e.z >= CROSS) cross = true;
+                cross |= crosses(olds[r][h], nib, e.z);
             }
         }
         const uint32_t bal = __ballot_sync(0xffffffffu, cross);
@@ -227,11 +238,7 @@ __device__ __forceinline__ uint32_t staged_rounds_fused(const MswsDev& D, const 
         const uint32_t nib = (w < 7) ? (e.y >> (4 * w)) & 0xfu : 0u;
         if ((linked || sat) && nib) atomicAdd(D.low + (uint64_t)e.x * LOW_WORDS + w, 0u - expand_nibble(nib) * e.z);
         bool cross = false;
-        if (ve && !linked && !sat && nib) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (((nib >> k) & 1u) && ((olds[r] >> (8 * k)) & 0xffu) + e.z >= CROSS) cross = true;
-        }
+        if (ve && !linked && !sat) cross = crosses(olds[r], nib, e.z);
         const uint32_t bal = __ballot_sync(0xffffffffu, cross);
         if (w == 0) {
             if ((bal >> (sub * 8)) & 0xffu) flag_bucket(D, e.x);
