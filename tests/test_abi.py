@@ -116,6 +116,16 @@ def test_autotune_table_empty_and_bad_arguments():
     autotune.reset()
     assert autotune.lookup(1 << 20) is None
     assert _lib.lib.qs_autotune(None, None, 0, 1, None, None, 0, None) == _lib.QS_ERR_INVALID_ARG
+    # a fixed chunk size must be a multiple of 32 and at most 2^26; rejected before any device
+    # work (the key pointer is never dereferenced)
+    p = _lib.qs_params()
+    _lib.lib.qs_params_default(ctypes.byref(p))
+    p.n_low = 1021
+    best = _lib.qs_tune_config()
+    for mb in (1000, 1 << 27):
+        p.max_batch = mb
+        assert _lib.lib.qs_autotune(ctypes.byref(p), ctypes.c_void_p(256), 1024, 1, ctypes.byref(best), None, 0,
+                                    None) == _lib.QS_ERR_INVALID_ARG
 
 
 def test_knob_validation_happens_before_any_device_work():
