@@ -8,8 +8,8 @@
 // passes 128 its result depends on the schedule.  Here a chunk of keys is applied in two
 // steps whose result equals the one-key-at-a-time order of the array:
 //   1. k_msws_insert: every key of an unlinked bucket adds its packed 8-bit increments
-//      with returning 32-bit atomics (a sub-warp of 8 lanes per key, lane w on word w, as
-//      in the reference).  A bucket's result is independent of order iff no selected
+//      with returning 32-bit atomics (a group of 1-32 lanes per key; 8 lanes, lane w on
+//      word w, is the reference's sub-warp).  A bucket's result is independent of order iff no selected
 //      counter ends the chunk above 129; a key whose atomic saw old + add >= 130 proves
 //      the opposite and flags the bucket (word 7 := FLAG | slot).  Keys of linked buckets
 //      add to the high bucket (commutative).
