@@ -97,14 +97,14 @@ typedef struct qs_params {
     /* Insert-kernel knobs; none changes any result.  When lanes_per_key, aggregate, route
      * and ctas_per_sm are all 0, qs_create takes them (and max_batch, if 0) from the
      * autotuner's entry for the sketch's size class (qs_autotune), else the defaults
-     * 4 (8 with route 2) / 3 / 1 / 0. */
+     * 4 / 3 / 1 / 0. */
     uint32_t lanes_per_key;      /* lanes serving one key in pass 1: 1, 2, 4, 8 (one lane
                                     per bucket word, the reference's sub-warp), 16 or 32 */
     uint32_t aggregate;          /* 1 = off, 2 = warp, 3 = warp + block pre-aggregation
                                     of duplicate keys */
     uint32_t route;              /* insert routing between the levels: 1 = load each
                                     bucket's index word first, 2 = read it with the counter
-                                    atomic (8 lanes per key only), 3 = adaptive per tile */
+                                    atomic (at most 8 lanes per key), 3 = adaptive per tile */
     uint32_t ctas_per_sm;        /* pass-1 CTAs per SM, 0 = as many as fit */
     uint64_t first_chunk;        /* first chunk of the ramp after a create or clear (multiple
                                     of 32); 0 = 2^18, or the autotuner's choice */

@@ -394,13 +394,13 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         const uint32_t tile = tuned && tc.keys_per_tile ? tc.keys_per_tile : (p.keys_per_tile ? p.keys_per_tile : 2048u);
         if (tile != 256 && tile != 512 && tile != 1024 && tile != 2048)
             return bail(fail(QS_ERR_INVALID_ARG, "keys_per_tile must be 0, 256, 512, 1024 or 2048"));
-        // default 4 lanes per key (measured fastest on every workload here), 8 for route 2
+        // default 4 lanes per key (measured fastest on every workload here)
         const uint32_t route = tuned ? tc.route : (p.route ? p.route : 1u);
-        const uint32_t lpk = tuned ? tc.lanes_per_key : (p.lanes_per_key ? p.lanes_per_key : route == 2 ? 8u : 4u);
+        const uint32_t lpk = tuned ? tc.lanes_per_key : (p.lanes_per_key ? p.lanes_per_key : 4u);
         if (lpk != 1 && lpk != 2 && lpk != 4 && lpk != 8 && lpk != 16 && lpk != 32)
             return bail(fail(QS_ERR_INVALID_ARG, "lanes_per_key must be 0, 1, 2, 4, 8, 16 or 32"));
         if (route > 3) return bail(fail(QS_ERR_INVALID_ARG, "route out of [0, 3]"));
-        if (route == 2 && lpk != 8) return bail(fail(QS_ERR_INVALID_ARG, "route 2 needs 8 lanes per key"));
+        if (route == 2 && lpk > 8) return bail(fail(QS_ERR_INVALID_ARG, "route 2 needs at most 8 lanes per key"));
         if (p.ctas_per_sm > 64) return bail(fail(QS_ERR_INVALID_ARG, "ctas_per_sm out of [0, 64]"));
         if (tuned) {
             sk->agg = (int)tc.aggregate - 1;
@@ -1801,7 +1801,7 @@ qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, u
         if ((s = consider(c)) != QS_OK) return cleanup(s);
     }
     for (uint32_t route : {2u, 3u}) {
-        if (route == 2 && cur.lanes_per_key != 8) continue;
+        if (route == 2 && cur.lanes_per_key > 8) continue;
         qs_tune_config c = cur;
         c.route = route;
         if ((s = consider(c)) != QS_OK) return cleanup(s);

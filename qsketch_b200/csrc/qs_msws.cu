@@ -208,40 +208,58 @@ __device__ __forceinline__ void staged_rounds(const MswsDev& D, const uint4* st,
     }
 }
 
-// ROUTE_FUSED rounds: entry j = (bucket, mask, count, key).  Returns the linked count.
+// ROUTE_FUSED rounds (1, 2, 4 or 8 lanes per key): entry j = (bucket, mask, count, key).
+// The lane that owns word 7 adds 0 to it in the same instruction that adds the counters, so
+// the bucket's index word comes back with the old counter words; a key whose bucket turns
+// out linked or saturated takes its low increments back (u32 addition is invertible).
+// Returns the linked count.
+template <int LPK>
 __device__ __forceinline__ uint32_t staged_rounds_fused(const MswsDev& D, const InsShared& S, const uint4* st,
                                                         int nact) {
-    const int lane = threadIdx.x & 31, sub = lane >> 3, w = lane & 7;
-    uint32_t olds[8];
+    static_assert(LPK == 1 || LPK == 2 || LPK == 4 || LPK == 8, "fused rounds: at most 8 lanes per key");
+    constexpr int KPR = 32 / LPK, WPL = 8 / LPK;
+    constexpr int W7_LANE = 7 % LPK, W7_H = 7 / LPK;  // the owner of word 7 and its slot
+    const int lane = threadIdx.x & 31, sub = lane / LPK, w = lane % LPK;
+    uint32_t olds[LPK][WPL];
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        olds[r] = 0;
-        if (r * 4 >= nact) continue;  // warp-uniform
-        const int j = r * 4 + sub;
+    for (int r = 0; r < LPK; ++r) {
+#pragma unroll
+        for (int h = 0; h < WPL; ++h) olds[r][h] = 0;
+        if (r * KPR >= nact) continue;  // warp-uniform
+        const int j = r * KPR + sub;
         if (j >= nact) continue;
         const uint4 e = st[j];
-        const uint32_t nib = (w < 7) ? (e.y >> (4 * w)) & 0xfu : 0u;
-        if (nib || w == 7)
-            olds[r] = atomicAdd(D.low + (uint64_t)e.x * LOW_WORDS + w, w == 7 ? 0u : expand_nibble(nib) * e.z);
+#pragma unroll
+        for (int h = 0; h < WPL; ++h) {
+            const int ww = w + h * LPK;
+            const uint32_t nib = (ww < 7) ? (e.y >> (4 * ww)) & 0xfu : 0u;
+            if (nib || ww == 7)
+                olds[r][h] = atomicAdd(D.low + (uint64_t)e.x * LOW_WORDS + ww, ww == 7 ? 0u : expand_nibble(nib) * e.z);
+        }
     }
     uint32_t linked_keys = 0;
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        if (r * 4 >= nact) continue;  // warp-uniform
-        const int j = r * 4 + sub;
+    for (int r = 0; r < LPK; ++r) {
+        if (r * KPR >= nact) continue;  // warp-uniform
+        const int j = r * KPR + sub;
         const bool ve = j < nact;
         uint4 e = make_uint4(0, 0, 0, 0);
         if (ve) e = st[j];
-        const uint32_t ptr = __shfl_sync(0xffffffffu, olds[r], (lane & ~7) | 7);
+        const uint32_t ptr = __shfl_sync(0xffffffffu, olds[r][W7_H], sub * LPK + W7_LANE);
         const bool linked = ve && is_linked(D, ptr);
         const bool sat = ve && ptr == SATURATED;
-        const uint32_t nib = (w < 7) ? (e.y >> (4 * w)) & 0xfu : 0u;
-        if ((linked || sat) && nib) atomicAdd(D.low + (uint64_t)e.x * LOW_WORDS + w, 0u - expand_nibble(nib) * e.z);
         bool cross = false;
-        if (ve && !linked && !sat) cross = crosses(olds[r], nib, e.z);
+#pragma unroll
+        for (int h = 0; h < WPL; ++h) {
+            const int ww = w + h * LPK;
+            const uint32_t nib = (ww < 7) ? (e.y >> (4 * ww)) & 0xfu : 0u;
+            if ((linked || sat) && nib) atomicAdd(D.low + (uint64_t)e.x * LOW_WORDS + ww, 0u - expand_nibble(nib) * e.z);
+            if (ve && !linked && !sat) cross |= crosses(olds[r][h], nib, e.z);
+        }
         const uint32_t bal = __ballot_sync(0xffffffffu, cross);
+        const uint32_t grp = (bal >> (sub * LPK)) & ((1u << LPK) - 1u);
         if (w == 0) {
-            if ((bal >> (sub * 8)) & 0xffu) flag_bucket(D, e.x);
+            if (grp) flag_bucket(D, e.x);
             if (sat) atomicAdd(S.misc + 0, e.z);
             if (linked) {  // rare in this mode: count high directly
                 uint32_t* hb = D.high + (uint64_t)(ptr - START) * HIGH_WORDS;
@@ -296,11 +314,11 @@ __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& 
         c = (valid && lane == __ffs(peers) - 1) ? (uint32_t)__popc(peers) : 0u;
     }
     uint4* st = S.stage + wid * 32;
-    if (LPK == 8 && route == ROUTE_FUSED) {  // the fused form exists for 8 lanes per key
+    if (LPK <= 8 && route == ROUTE_FUSED) {  // the fused form exists for up to 8 lanes per key
         const uint32_t am = __ballot_sync(0xffffffffu, c != 0);
         if (c) st[__popc(am & lanemask_lt())] = make_uint4(b, m, c, key);
         __syncwarp();
-        const uint32_t lk = __reduce_add_sync(0xffffffffu, staged_rounds_fused(D, S, st, __popc(am)));
+        const uint32_t lk = __reduce_add_sync(0xffffffffu, staged_rounds_fused<(LPK <= 8 ? LPK : 8)>(D, S, st, __popc(am)));
         if (lane == 0 && lk && D.route == 0) atomicAdd(S.misc + 1, lk);
         __syncwarp();
         return;

@@ -79,6 +79,16 @@ def test_zipf_heavy_links(gpu, agg, route):
     assert st["linked_buckets"] > 100 and st["repaired_buckets"] == st["linked_buckets"]
 
 
+@pytest.mark.parametrize("lpk", [1, 2, 4, 8])
+def test_fused_routing_every_group_width(gpu, lpk):
+    # fused routing (the index word read by the counter atomic) with 1, 2, 4 or 8 lanes per
+    # key: linked keys take their low increments back; tables equal the oracle's
+    sk, orc = make_pair(16381, 1 << 15, aggregate=3, route=2, lanes_per_key=lpk, max_batch=1 << 19)
+    keys = data.zipf_keys(1 << 21, 1 << 18, 1.1, seed=15, perm_seed=71)
+    run_and_compare(sk, orc, keys, data.rank_keys(71, 0, 1 << 18))
+    assert sk.stats()["linked_buckets"] > 100
+
+
 def test_zipf_many_chunks_and_uneven_calls(gpu):
     sk, orc = make_pair(8191, 1 << 14, max_batch=1 << 16)
     keys = data.zipf_keys(3 * (1 << 18) + 77, 1 << 16, 1.2, seed=9, perm_seed=3)
