@@ -494,7 +494,8 @@ __global__ void __launch_bounds__(INS_THREADS, INS_MIN_CTAS) k_msws_insert(const
 // ---- ordered replay ---------------------------------------------------------------------
 
 constexpr int SET_SLOTS = 16384;  // words of the repair's dynamic shared memory (64 KiB), reused by
-                                  // the phases: flag filter, tile prefix, staged records
+                                  // the phases: flag filter, tile prefix, a resident radix tile,
+                                  // the records of a sort-free replay
 constexpr int BLOOM_BITS = 17;    // per-block filter of the flagged buckets: 2^17 bits (16 KiB)
 constexpr int BLOOM_WORDS = (1 << BLOOM_BITS) / 32;
 constexpr uint32_t TC_MAX = 128;  // tiles per block in the flag test (grids have >= 148 blocks)
@@ -905,7 +906,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     constexpr int NW = REPAIR_THREADS / 32;
     constexpr int PER = REPAIR_TILE / REPAIR_THREADS;  // 8 consecutive keys per thread
-    static_assert(PER == 8, "one hit byte per thread");
+    static_assert(PER == 8, "8 keys per thread: two 16-byte loads, one byte of skip bits");
     const uint32_t ntk = (uint32_t)((n + REPAIR_TILE - 1) / REPAIR_TILE);
     // the tile-count prefix of phase 2 lives in the SET_SLOTS words of shared memory: chunks of at most
     // SET_SLOTS tiles (2^26 keys; the host rejects larger max_batch); uniform, so every block
