@@ -222,7 +222,9 @@ def run_ours(args, cfg):
         tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], sample, reps=3, hash_seed=SEED, mask_rng=1,
                                      max_batch=(ni_b + 31) // 32 * 32)
     else:
-        tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], keys, reps=3, hash_seed=SEED, mask_rng=1)
+        # (whole-stream samples take a few ms each: 8 repetitions per setting keep the
+        # search's picks from following run-to-run noise of a few percent)
+        tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], keys, reps=8, hash_seed=SEED, mask_rng=1)
     sk = qs.Sketch_GPU_Sub_Warp_Level(cfg["n_low"], 8, cfg["n_high"], 32, hash_seed=SEED, mask_rng=1)
     n_ins, n_q = cfg["n_keys"], cfg["n_query"]
     if cfg["kind"] == 2:
