@@ -499,6 +499,9 @@ constexpr int SET_SLOTS = 16384;  // words of the repair's dynamic shared memory
 constexpr int BLOOM_BITS = 17;    // per-block filter of the flagged buckets: 2^17 bits (16 KiB)
 constexpr int BLOOM_WORDS = (1 << BLOOM_BITS) / 32;
 constexpr uint32_t TC_MAX = 128;  // tiles per block in the flag test (grids have >= 148 blocks)
+constexpr uint32_t SEMI_TILES = 4;  // radix tiles per block kept as offsets and ranks
+static_assert(SEMI_TILES * (REPAIR_THREADS / 32) * 256 * 2 + SEMI_TILES * REPAIR_TILE <= SET_SLOTS * 4,
+              "the offsets and ranks of SEMI_TILES tiles fit the shared space");
 constexpr uint32_t SCAN_CAP = SET_SLOTS / 2;  // records replayed without a sort (64 KiB of uint2)
 static_assert(BLOOM_WORDS <= SET_SLOTS, "filter fits the shared space");
 constexpr uint32_t NONE = 0xffffffffu;
@@ -893,6 +896,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
                                                                 MswsDev D, BatchDev B) {
     __shared__ RadixSmem rs;
     __shared__ uint32_t s_dbase[256];  // radix pass: first output position of each digit
+    __shared__ uint32_t s_acc_base[256];  // radix pass, several tiles per block: a tile's digit bases
     __shared__ uint32_t s_acc[2][LOW_COUNTERS];
     __shared__ uint32_t s_acc_slot[2];
     __shared__ uint32_t s_tc[TC_MAX];       // phase 1: counts of this block's tiles, by round
@@ -1084,6 +1088,13 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     uint2* srec = reinterpret_cast<uint2*>(s_set);   // [REPAIR_TILE]
     uint32_t* srank = s_set + 2 * REPAIR_TILE;        // [REPAIR_TILE]
     static_assert(3 * REPAIR_TILE <= SET_SLOTS, "resident tile fits the shared space");
+    // Up to SEMI_TILES tiles per block: the count keeps, per tile, the per-warp digit offsets
+    // (u16: below REPAIR_TILE) and each record's in-warp rank (u8: a warp holds 256 records);
+    // the scatter reloads the records but does not recount them.
+    const uint32_t tiles_here = blockIdx.x < ntr ? (ntr - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const bool semi = !resident && ntr <= SEMI_TILES * gridDim.x;
+    uint16_t* swoff = reinterpret_cast<uint16_t*>(s_set);                                    // [q][NW][256]
+    uint8_t* srank8 = reinterpret_cast<uint8_t*>(s_set) + SEMI_TILES * NW * 256 * 2;        // [q][REPAIR_TILE]
     for (int p = 0; p < npass; ++p) {
         const uint2* src = D.rec[p & 1];
         uint2* dst = D.rec[(p + 1) & 1];
@@ -1114,6 +1125,37 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
                     for (int w = 0; w < NW; ++w) {
                         const uint32_t x = rs.whist[w][d];
                         rs.whist[w][d] = run;
+                        run += x;
+                    }
+                    __stcg(D.hist + (uint64_t)d * ntr + t, run);
+                }
+                __syncthreads();
+            }
+        } else if (semi) {
+            for (uint32_t q = 0; q < tiles_here; ++q) {
+                const uint32_t t = blockIdx.x + q * gridDim.x;
+                uint2 rec[TILE_ROUNDS];
+                tile_load(src, K, t, rec);
+                for (int d = tid; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
+                __syncthreads();
+#pragma unroll
+                for (int r = 0; r < TILE_ROUNDS; ++r) {
+                    const uint32_t li = wid * 256 + r * 32 + lane;
+                    const bool v = t * REPAIR_TILE + li < K;
+                    const uint32_t d = v ? (rec[r].x >> shift) & 0xffu : 256u + lane;
+                    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+                    const uint32_t before = v ? rs.whist[wid][d] : 0u;
+                    __syncwarp();
+                    if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] = before + __popc(peers);
+                    __syncwarp();
+                    srank8[q * REPAIR_TILE + li] = (uint8_t)(before + __popc(peers & lanemask_lt()));
+                }
+                __syncthreads();
+                for (int d = tid; d < 256; d += REPAIR_THREADS) {  // per-warp offsets, tile total
+                    uint32_t run = 0;
+                    for (int w = 0; w < NW; ++w) {
+                        const uint32_t x = rs.whist[w][d];
+                        swoff[(q * NW + w) * 256 + d] = (uint16_t)run;
                         run += x;
                     }
                     __stcg(D.hist + (uint64_t)d * ntr + t, run);
@@ -1180,7 +1222,26 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
                 __syncthreads();
             }
         }
-        for (uint32_t t = blockIdx.x; t < ntr && !resident; t += gridDim.x) {  // stable scatter
+        if (semi) {
+            for (uint32_t q = 0; q < tiles_here; ++q) {
+                const uint32_t t = blockIdx.x + q * gridDim.x;
+                uint2 rec[TILE_ROUNDS];
+                tile_load(src, K, t, rec);
+                uint32_t* sbase = s_acc_base;  // this tile's first position of each digit
+                for (int d = tid; d < 256; d += REPAIR_THREADS) sbase[d] = s_dbase[d] + __ldcg(D.hist + (uint64_t)d * ntr + t);
+                __syncthreads();
+#pragma unroll
+                for (int r = 0; r < TILE_ROUNDS; ++r) {
+                    const uint32_t li = wid * 256 + r * 32 + lane;
+                    if (t * REPAIR_TILE + li < K) {
+                        const uint32_t d = (rec[r].x >> shift) & 0xffu;
+                        __stcg(dst + sbase[d] + swoff[(q * NW + wid) * 256 + d] + srank8[q * REPAIR_TILE + li], rec[r]);
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (uint32_t t = blockIdx.x; t < ntr && !resident && !semi; t += gridDim.x) {  // stable scatter
             uint2 rec[TILE_ROUNDS];
             tile_load(src, K, t, rec);
             tile_count(rs, rec, K, t, shift);

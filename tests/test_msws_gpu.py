@@ -342,3 +342,15 @@ def test_replay_with_more_records_than_resident_tiles(gpu):
     keys = distinct.view(torch.int32)[idx].view(torch.uint32).contiguous()
     run_and_compare(sk, orc, keys, distinct)
     assert sk.stats()["repaired_keys"] > 296 * 4096
+
+
+def test_replay_with_two_to_four_radix_tiles_per_block(gpu):
+    # 2^22 distinct keys into 2039 buckets in one chunk: every bucket crosses, so nearly all
+    # 4M keys become replay records (more than one and at most four 4096-record tiles per
+    # block of the 296-block grid): the radix keeps per-tile offsets and ranks, reloads the
+    # records for the scatter; the tables must equal the oracle's
+    sk, orc = make_pair(2039, 1 << 12, max_batch=1 << 22, chunk_ramp=False)
+    keys = data.uniform_keys(1 << 22, seed=73)
+    run_and_compare(sk, orc, keys, keys[:1 << 16])
+    rk = sk.stats()["repaired_keys"]
+    assert 296 * 4096 < rk <= 4 * 296 * 4096, rk
