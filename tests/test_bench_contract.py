@@ -25,3 +25,19 @@ def test_reference_arm_unavailable_line():
 def test_warmup_below_three_is_refused():
     r = run("--warmup", "2")
     assert r.returncode != 0 and "warmup" in r.stderr
+
+
+def test_reference_arm_under_torchrun_prints_once():
+    # two ranks launched the way the driver launches N > 1: rank 0 prints the line, the other
+    # rank exits 0 without work
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+                        "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
+                        "--impl", "reference", "--config", "batched", "--gpus", "2", "--steps", "1", "--warmup", "3"],
+                       capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1 and lines[0]["impl"] == "reference"
