@@ -415,7 +415,7 @@ qs_sketch *qs_batch_arena(qs_batch *b);
  * start-up, say) and may not call cudaMalloc/cudaFree while serving — those calls
  * synchronise the device and fragment the arena.  The caller keeps the sketch in its own
  * memory and passes it in: the low table (n_low*8 u32, 32-byte aligned), the high pool
- * (n_high*32 u32), a state block of QS_MSWS_STATE_BYTES, and the device mask words
+ * (n_high*32 u32), a state block of QS_MSWS_STATE_BYTES (16-byte aligned), and the device mask words
  * (n_masks u32, bits 0..27, e.g. from qs_generate_hashmask).  A new sketch is all three
  * zero-filled.  The call allocates nothing: the ordered replay's scratch is a fixed
  * QS_NOALLOC_SCRATCH_BYTES array inside the library, which every GPU that loads the library
@@ -435,6 +435,8 @@ qs_sketch *qs_batch_arena(qs_batch *b);
 #define QS_NOALLOC_MAX_BUCKETS (1ull << 26)
 #define QS_NOALLOC_SCRATCH_BYTES (16u << 20)
 #define QS_MSWS_STATE_BYTES 256u
+#define QS_MSWS_STATE_ALIGN 16u /* d_state alignment (it holds 64-bit counters); else
+                                   QS_ERR_INVALID_ARG */
 qs_status qs_msws_insert_noalloc(uint32_t *d_low, uint64_t n_low, uint32_t *d_high, uint64_t n_high,
                                  void *d_state, const uint32_t *d_masks, uint32_t n_masks,
                                  uint32_t hash_seed, uint32_t flags, const uint32_t *d_keys, size_t n,

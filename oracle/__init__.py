@@ -163,4 +163,46 @@ def ref_lib():
     r.ref_find_greatest_prime.argtypes = [ctypes.c_ulonglong]
     r.ref_find_greatest_prime.restype = ctypes.c_ulonglong
     r.ref_exact_counts.argtypes = [P, SZ, P, SZ, P]
+    if hasattr(r, "ref_msws_gpu"):
+        r.ref_msws_gpu.argtypes = [ctypes.c_uint, ctypes.c_uint, SZ, SZ, P, SZ, P, SZ, P, P, P, P]
+        r.ref_cm_gpu.argtypes = [ctypes.c_uint, SZ, SZ, P, SZ, P, SZ, P, P, P]
     return r
+
+
+def ref_msws_gpu(seed_rng, mask_rng, n_low, n_high, keys, queries, with_low=False):
+    """The reference's own Sketch_GPU_Sub_Warp_Level kernels on the current GPU
+    (device_sketch_v3.h:526-634), engines reseeded.  Returns (estimates, seed, mask table, low
+    table or None); raises ValueError for inputs the reference kernel is not defined on (a
+    warp share that is not a multiple of 4 keys, or a low counter that would pass 128)."""
+    r = ref_lib()
+    if r is None or not hasattr(r, "ref_msws_gpu"):
+        raise RuntimeError("oracle/_ref/libqsref.so with the reference's sketch kernels is not built")
+    k, q = _u32(keys), _u32(queries)
+    out = np.zeros(q.size, np.uint32)
+    low = np.zeros(n_low * 8, np.uint32) if with_low else None
+    seed = np.zeros(1, np.uint32)
+    masks = np.zeros(1021 * 4, np.uint8)
+    rc = r.ref_msws_gpu(seed_rng, mask_rng, n_low, n_high, k.ctypes.data, k.size, q.ctypes.data, q.size,
+                        out.ctypes.data, low.ctypes.data if with_low else None, seed.ctypes.data, masks.ctypes.data)
+    if rc == -1:
+        raise ValueError("input outside the reference kernel's defined range")
+    if rc != 0:
+        raise RuntimeError(f"reference MSWS run failed: CUDA error {rc}")
+    return out, int(seed[0]), masks, low
+
+
+def ref_cm_gpu(seed_rng, n, m, keys, queries, with_table=False):
+    """The reference's own Sketch_GPU_Thread kernels on the current GPU (device_sketch_v0.h:105-191),
+    seed engine reseeded.  Returns (estimates, seeds, table or None)."""
+    r = ref_lib()
+    if r is None or not hasattr(r, "ref_cm_gpu"):
+        raise RuntimeError("oracle/_ref/libqsref.so with the reference's sketch kernels is not built")
+    k, q = _u32(keys), _u32(queries)
+    out = np.zeros(q.size, np.uint32)
+    tab = np.zeros(n * m, np.uint32) if with_table else None
+    seeds = np.zeros(m, np.uint32)
+    rc = r.ref_cm_gpu(seed_rng, n, m, k.ctypes.data, k.size, q.ctypes.data, q.size, out.ctypes.data,
+                      tab.ctypes.data if with_table else None, seeds.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"reference count-min run failed: status {rc}")
+    return out, seeds, tab

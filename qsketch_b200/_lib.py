@@ -217,6 +217,7 @@ SIGNATURES = {
 QS_NOALLOC_MAX_KEYS = 1 << 18
 QS_NOALLOC_MAX_BUCKETS = 1 << 26
 QS_MSWS_STATE_BYTES = 256
+QS_MSWS_STATE_ALIGN = 16
 
 
 def _load():

@@ -58,6 +58,7 @@ __global__ void k_noalloc_begin(Ctl* st) {
 struct NaDevice {
     bool ready = false;
     unsigned char* scratch = nullptr;
+    uint32_t n_masks = 0;  // mask-table size the launch geometry below was computed for
     MswsLaunch launch{};
 };
 
@@ -65,9 +66,12 @@ constexpr int NA_MAX_DEVICES = 64;
 NaDevice na_devices[NA_MAX_DEVICES];
 std::mutex na_mutex;
 
-// Once per device, with that device current: resolve the scratch array's device address and
-// the launch geometry.  Runs on the first call on each device.
-static qs_status na_setup(int dev, NaDevice** out, char* err, size_t errlen) {
+// Once per device, with that device current: resolve the scratch array's device address.
+// The launch geometry (pass-1 occupancy depends on the shared-memory copy of the mask table)
+// is recomputed whenever the mask-table size differs from the previous call's; that is
+// host-side work only.  The caller gets a copy of the geometry, taken under the lock.
+static qs_status na_setup(int dev, uint32_t n_masks, unsigned char** scratch, MswsLaunch* launch, char* err,
+                          size_t errlen) {
     std::lock_guard<std::mutex> lk(na_mutex);
     NaDevice& d = na_devices[dev];
     if (!d.ready) {
@@ -77,15 +81,20 @@ static qs_status na_setup(int dev, NaDevice** out, char* err, size_t errlen) {
             snprintf(err, errlen, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
             return e == cudaErrorNoKernelImageForDevice ? QS_ERR_NO_DEVICE : QS_ERR_CUDA;
         }
-        e = msws_configure(dev, 1021, &d.launch);  // grid sized for the default mask table
-        if (e != cudaSuccess) {
-            snprintf(err, errlen, "kernel configuration: %s", cudaGetErrorString(e));
-            return QS_ERR_CUDA;
-        }
         d.scratch = static_cast<unsigned char*>(p);
         d.ready = true;
     }
-    *out = &d;
+    if (d.n_masks != n_masks) {
+        cudaError_t e = msws_configure(dev, n_masks, &d.launch);
+        if (e != cudaSuccess) {
+            d.n_masks = 0;
+            snprintf(err, errlen, "kernel configuration: %s", cudaGetErrorString(e));
+            return QS_ERR_CUDA;
+        }
+        d.n_masks = n_masks;
+    }
+    *scratch = d.scratch;
+    *launch = d.launch;
     return QS_OK;
 }
 
@@ -111,8 +120,11 @@ extern "C" qs_status qs_msws_insert_noalloc(uint32_t* d_low, uint64_t n_low, uin
         return set_last_error(err), QS_ERR_CAPACITY;
     }
     if ((reinterpret_cast<uintptr_t>(d_keys) | reinterpret_cast<uintptr_t>(d_low) |
-         reinterpret_cast<uintptr_t>(d_high) | reinterpret_cast<uintptr_t>(d_state)) & 3u)
+         reinterpret_cast<uintptr_t>(d_high) | reinterpret_cast<uintptr_t>(d_masks)) & 3u)
         return set_last_error("qs_msws_insert_noalloc: pointers must be 4-byte aligned"), QS_ERR_INVALID_ARG;
+    // The state block holds 64-bit counters updated with 64-bit atomics.
+    if (reinterpret_cast<uintptr_t>(d_state) & (QS_MSWS_STATE_ALIGN - 1))
+        return set_last_error("qs_msws_insert_noalloc: the state block must be 16-byte aligned"), QS_ERR_INVALID_ARG;
     if (reinterpret_cast<uintptr_t>(d_low) & 31u)
         return set_last_error("qs_msws_insert_noalloc: the low table must be 32-byte aligned"), QS_ERR_INVALID_ARG;
     if (n == 0) return QS_OK;
@@ -120,8 +132,9 @@ extern "C" qs_status qs_msws_insert_noalloc(uint32_t* d_low, uint64_t n_low, uin
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES)
         return set_last_error("qs_msws_insert_noalloc: no current CUDA device"), QS_ERR_NO_DEVICE;
-    NaDevice* nd = nullptr;
-    qs_status s = na_setup(dev, &nd, err, sizeof err);
+    unsigned char* sc = nullptr;
+    MswsLaunch launch{};
+    qs_status s = na_setup(dev, n_masks, &sc, &launch, err, sizeof err);
     if (s != QS_OK) return set_last_error(err), s;
 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -141,7 +154,6 @@ extern "C" qs_status qs_msws_insert_noalloc(uint32_t* d_low, uint64_t n_low, uin
     D.flag_cap = (uint32_t)std::min<uint64_t>(n_low, NA_MAX_KEYS);
     D.max_tiles = (uint32_t)NA_TILES;
     D.long_cap = (uint32_t)std::min<uint64_t>(D.flag_cap, NA_TOTAL_SLOTS);
-    unsigned char* sc = nd->scratch;
     D.rec[0] = reinterpret_cast<uint2*>(sc + NA_OFF_REC0);
     D.rec[1] = reinterpret_cast<uint2*>(sc + NA_OFF_REC1);
     D.flag_list = reinterpret_cast<uint32_t*>(sc + NA_OFF_FLAGS);
@@ -153,8 +165,8 @@ extern "C" qs_status qs_msws_insert_noalloc(uint32_t* d_low, uint64_t n_low, uin
     // Every scratch part is written before it is read.
     k_noalloc_begin<<<1, 1, 0, st>>>(D.ctl);
     e = cudaGetLastError();
-    if (e == cudaSuccess) e = msws_insert_pass(d_keys, n, D, nd->launch, 2, st);
-    if (e == cudaSuccess) e = msws_repair(d_keys, n, D, nd->launch, st);
+    if (e == cudaSuccess) e = msws_insert_pass(d_keys, n, D, launch, 2, st);
+    if (e == cudaSuccess) e = msws_repair(d_keys, n, D, launch, st);
     if (e != cudaSuccess) {
         snprintf(err, sizeof err, "qs_msws_insert_noalloc: %s", cudaGetErrorString(e));
         return set_last_error(err), QS_ERR_CUDA;
