@@ -122,6 +122,24 @@ class BatchedSketches:
         check(lib.qs_batch_get_info(self.handle, ctypes.byref(i)), "info")
         return {f: getattr(i, f) for f, _ in qs_batch_info._fields_}
 
+    def stream_tables(self, s):
+        """Stream s's low table (n_low[s]*8 words) and high pool (n_high[s]*32 words), copied out
+        of the arena, with the stream's own high ids in word 7 (as a sketch of its own holds
+        them)."""
+        arena = lib.qs_batch_arena(self.handle)
+        nl, nh = ctypes.c_uint64(), ctypes.c_uint64()
+        m = ctypes.c_uint32()
+        check(lib.qs_get_info(arena, ctypes.byref(nl), ctypes.byref(nh), ctypes.byref(m), None, None), "info")
+        low = np.zeros(nl.value * 8, np.uint32)
+        high = np.zeros(nh.value * 32, np.uint32)
+        check(lib.qs_get_tables(arena, low.ctypes.data, high.ctypes.data), "tables")
+        lb, hb = int(self.n_low[:s].sum()), int(self.n_high[:s].sum())
+        sl = low[lb * 8:(lb + int(self.n_low[s])) * 8].copy()
+        sh = high[hb * 32:(hb + int(self.n_high[s])) * 32].copy()
+        w7 = sl[7::8]
+        w7[w7 > 1024] -= np.uint32(hb)
+        return sl, sh
+
     def set_profiling(self, enable=True):
         check(lib.qs_set_profiling(lib.qs_batch_arena(self.handle), 1 if enable else 0), "set_profiling")
 

@@ -457,6 +457,12 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         CKB(sk->alloc(&D.hist, (uint64_t)256 * D.max_tiles + 256), "alloc histograms");  // + digit totals
         CKB(sk->alloc(&D.seg_beg, cap), "alloc segments");
         CKB(sk->alloc(&D.totals, (uint64_t)D.long_cap * LOW_COUNTERS), "alloc totals");
+        CKB(sk->alloc(&D.rpos[0], B), "alloc record positions");
+        CKB(sk->alloc(&D.rpos[1], B), "alloc record positions");
+        CKB(sk->alloc(&D.sw, cap), "alloc link order");
+        CKB(sk->alloc(&D.sw_base, cap), "alloc link order");
+        CKB(sk->alloc(&D.sw_bits, (B + 31) / 32), "alloc link order");
+        CKB(sk->alloc(&D.sw_cnt, (B + SW_BLOCK - 1) / SW_BLOCK), "alloc link order");
         CKB(cudaMemcpy(masks_d, sk->masks.data(), (size_t)H * 4, cudaMemcpyHostToDevice), "upload masks");
         qs_status s = ctl_reset(sk, 0);
         if (s != QS_OK) return bail(s);
@@ -656,7 +662,7 @@ qs_status qs_get_profile(qs_sketch* sk, qs_profile* out) {
         CK(cudaMemcpy(&c, sk->D.ctl, sizeof c, cudaMemcpyDeviceToHost), "read repair phases");
         out->repairs_active = c.repairs;
         for (int k = 0; k < 12; ++k) out->repair_phase_ms[k] = (double)c.phase_ns[k] * 1e-6;
-        CK(cudaMemset(&sk->D.ctl->repairs, 0, sizeof(unsigned long long) * 10), "reset repair phases");
+        CK(cudaMemset(&sk->D.ctl->repairs, 0, sizeof(Ctl) - offsetof(Ctl, repairs)), "reset repair phases");
     }
     return QS_OK;
 }
@@ -1472,6 +1478,7 @@ qs_status qs_batch_create(const qs_batch_params* p, qs_batch** out) {
     CKB(sk->alloc(&B.work, 1), "alloc work queue");
     CKB(sk->alloc(&B.next_id, S), "alloc allocators");
     CKB(sk->alloc(&B.status, S), "alloc stream status");
+    CKB(sk->alloc(&B.first, S), "alloc link ranks");
     CKB(cudaMemcpy(d_desc, desc.data(), (size_t)S * sizeof(StreamDesc), cudaMemcpyHostToDevice), "upload descriptors");
     std::vector<uint32_t> first(S, FIRST_ID);
     CKB(cudaMemcpy(B.next_id, first.data(), (size_t)S * 4, cudaMemcpyHostToDevice), "init allocators");
@@ -1638,6 +1645,8 @@ qs_status qs_batch_clear(qs_batch* b, void* stream) {
     std::vector<uint32_t> first(b->S, FIRST_ID);
     CK(cudaMemcpyAsync(b->B.next_id, first.data(), (size_t)b->S * 4, cudaMemcpyHostToDevice, st), "reset allocators");
     CK(cudaMemsetAsync(b->B.status, 0, (size_t)b->S * 4, st), "reset stream status");
+    // the clear restarts the control block's link generation, which tags these
+    CK(cudaMemsetAsync(b->B.first, 0, (size_t)b->S * 8, st), "reset link ranks");
     CK(cudaStreamSynchronize(st), "clear sync");  // the host vector above must outlive the copy
     return QS_OK;
 }

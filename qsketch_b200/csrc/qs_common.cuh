@@ -54,7 +54,8 @@ struct Ctl {
     uint32_t n_long;       // slots whose segment needed a grid-wide count
     uint32_t bar_count;    // grid barrier
     uint32_t bar_gen;
-    uint32_t pad0;
+    uint32_t link_gen;     // repairs that linked buckets since the create/clear (never reset
+                           // otherwise): tags the per-stream link ranks of batched streams
     unsigned long long dropped;
     unsigned long long repaired_buckets;
     unsigned long long repaired_keys;
@@ -96,7 +97,17 @@ struct MswsDev {
     uint32_t* skip_out;
     uint32_t tbl_slots;
     uint32_t ins_tile;       // pass-1 keys per tile (0: the stage size)
+    // Link order.  One-key-at-a-time insertion hands out high ids in the array order of the
+    // keys that switch buckets to the high level; the ordered replay does the same:
+    uint32_t* rpos[2];       // per record: its position in array order, carried through the
+                             // radix passes beside rec[]
+    uint2* sw;               // per slot: the switch key's position (then its rank) or NONE, and
+                             // the bucket's keys at or after the switch
+    uint32_t* sw_base;       // per slot, batched streams: the stream's allocator before the repair
+    uint32_t* sw_bits;       // one bit per record position: a bucket switches there
+    uint32_t* sw_cnt;        // switches per SW_BLOCK positions
 };
+constexpr uint32_t SW_BLOCK = 4096;  // positions per switch count (128 bit words)
 
 // Batched streams: many per-stream MSWS sketches share one low-table arena and one high
 // pool arena.  A stream's sketch is the bucket range [low_base, low_base + fm_low.d) of the
@@ -123,6 +134,8 @@ struct BatchDev {
     uint32_t* work;           // work-queue head
     uint32_t* next_id;        // [n_streams] per-stream bump allocators (from FIRST_ID)
     uint32_t* status;         // [n_streams] latched ST_* bits per stream
+    unsigned long long* first;// [n_streams] (repair generation << 32) | ~(lowest rank of the
+                              // stream's links in that repair): ranks within each stream
     uint32_t n_streams;       // 0: not a batch
     uint32_t pad;
 };

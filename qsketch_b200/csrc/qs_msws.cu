@@ -554,6 +554,7 @@ __device__ __forceinline__ void finish_repair(Ctl* ctl) {
             ctl->n_records = 0;
             ctl->n_long = 0;
             ctl->repairs += 1;
+            ctl->link_gen += 1;
             __threadfence();
         }
     }
@@ -633,6 +634,18 @@ __device__ __forceinline__ void tile_load(const uint2* src, uint32_t K, uint32_t
     for (int r = 0; r < TILE_ROUNDS; ++r) {
         const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
         rec[r] = i < K ? __ldcg(&src[i]) : make_uint2(0u, 0u);
+    }
+}
+
+// The array-order positions of a tile's records, in the layout of tile_load (psrc null: the
+// records are still in array order, so a record's position is its index).
+__device__ __forceinline__ void tile_load_pos(const uint32_t* psrc, uint32_t K, uint32_t t,
+                                              uint32_t (&pos)[TILE_ROUNDS]) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int r = 0; r < TILE_ROUNDS; ++r) {
+        const uint32_t i = t * REPAIR_TILE + wid * 256 + r * 32 + lane;
+        pos[r] = psrc ? (i < K ? __ldcg(psrc + i) : 0u) : i;
     }
 }
 
@@ -725,75 +738,56 @@ __device__ __forceinline__ int link_step(uint32_t m, uint32_t& cur) {
     return j;
 }
 
-// Final words of bucket b.  found: a key switched it to the high level; n_after: keys at
-// or after that key; n_total: the bucket's keys in the chunk; mL: the switching key's mask.
-template <bool BATCH>
-__device__ __forceinline__ void finish_bucket(const MswsDev& D, const BatchDev& B, uint32_t b, bool found,
-                                              uint32_t n_after, uint32_t n_total, uint32_t T, uint32_t P,
-                                              uint32_t cur, uint32_t mL) {
-    Ctl* ctl = D.ctl;
+// Where the replay of one flagged bucket ended (per lane c: counter c).
+struct ReplayOut {
+    bool found;        // a key switched the bucket to the high level
+    uint32_t L;        // that key's record: index into the records the replay read
+    uint32_t n_after;  // the bucket's keys at or after the switch
+    uint32_t n_total;  // the bucket's keys in the chunk
+    uint32_t T;        // the chunk's increments of counter c
+    uint32_t P;        // counter c before the chunk
+    uint32_t cur;      // counter c when the switch happens (final low value)
+    uint32_t mL;       // the switching key's mask
+};
+
+// Increments of high counter `lane` in the new high bucket: the switching key's and all
+// later keys'.
+__device__ __forceinline__ uint32_t high_increments(const MswsDev& D, const ReplayOut& o) {
     const int lane = threadIdx.x & 31;
-    uint32_t* wp = D.low + (uint64_t)b * LOW_WORDS;
-    if (found) {
-        uint32_t H = T - (cur - P);  // increments of the switching key and all later keys
-        if (D.compat_v3) {          // device_sketch_v3.h:187: the switching key lands on bit % 8
-            if (lane < LOW_COUNTERS && ((mL >> lane) & 1u)) H -= 1u;
-            if (lane < 8) H += __popc(mL & (0x01010101u << lane));
-        }
-        uint32_t id = 0;
-        bool ok;
-        if (BATCH) {  // the stream's own allocator and pool bound; the id is global
-            uint32_t own = 0, s = 0;
-            if (lane == 0) {
-                s = stream_of_bucket(B, b);
-                own = atomicAdd(B.next_id + s, 1u);
-            }
-            own = __shfl_sync(0xffffffffu, own, 0);
-            s = __shfl_sync(0xffffffffu, s, 0);
-            ok = (uint64_t)(own - START) < __ldg(&B.desc[s].n_high);
-            id = own + __ldg(&B.desc[s].high_base);
-            if (!ok && lane == 0) atomicOr(B.status + s, ST_POOL_FULL);
-        } else {
-            if (lane == 0) id = atomicAdd(&ctl->next_id, 1u);
-            id = __shfl_sync(0xffffffffu, id, 0);
-            ok = (uint64_t)(id - START) < D.n_high;
-        }
-        if (ok) {
-            __stcg(D.high + (uint64_t)(id - START) * HIGH_WORDS + lane, H);
-        } else if (lane == 0) {
-            atomicOr(&ctl->status, ST_POOL_FULL);
-            atomicAdd(&ctl->dropped, (unsigned long long)n_after);
-        }
-        uint32_t word = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) word |= __shfl_sync(0xffffffffu, cur, (4 * (lane & 7) + k) & 31) << (8 * k);
-        if (lane < 7) __stcg(wp + lane, word);
-        if (lane == 7) __stcg(wp + 7, ok ? id : SATURATED);
-    } else if (lane == 7) {
-        __stcg(wp + 7, 0u);  // every key added to the low level; the words are final
+    uint32_t H = o.T - (o.cur - o.P);
+    if (D.compat_v3) {  // device_sketch_v3.h:187: the switching key lands on bit % 8
+        if (lane < LOW_COUNTERS && ((o.mL >> lane) & 1u)) H -= 1u;
+        if (lane < 8) H += __popc(o.mL & (0x01010101u << lane));
     }
-    if (lane == 0) {
-        atomicAdd(&ctl->repaired_buckets, 1ull);
-        atomicAdd(&ctl->repaired_keys, (unsigned long long)n_total);
-    }
+    return H;
 }
 
-// Replay slot s from its segment of the slot-sorted records.
-template <bool BATCH>
-__device__ __forceinline__ void replay_slot(const MswsDev& D, const BatchDev& B, const uint2* sorted, uint32_t s,
-                                            uint32_t F, uint32_t K, bool use_totals) {
+// The low counters at the switch, packed back into words 0..6 of bucket b.
+__device__ __forceinline__ void write_low_words(const MswsDev& D, uint32_t b, uint32_t cur) {
     const int lane = threadIdx.x & 31;
-    const uint32_t b = __ldcg(D.flag_list + s);
+    uint32_t word = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) word |= __shfl_sync(0xffffffffu, cur, (4 * (lane & 7) + k) & 31) << (8 * k);
+    if (lane < 7) __stcg(D.low + (uint64_t)b * LOW_WORDS + lane, word);
+}
+
+// Replay slot s from its segment of the slot-sorted records (no writes).
+__device__ __forceinline__ ReplayOut replay_sorted(const MswsDev& D, const uint2* sorted, uint32_t s, uint32_t F,
+                                                  uint32_t K, uint32_t b) {
+    const int lane = threadIdx.x & 31;
     const uint32_t beg = __ldcg(D.seg_beg + s);
     const uint32_t end = (s + 1 < F) ? __ldcg(D.seg_beg + s + 1) : K;
-    uint32_t T = 0;
-    if (use_totals && s < D.long_cap) {
-        T = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane) : 0u;
+    ReplayOut o;
+    o.T = 0;
+    if (s < D.long_cap) {
+        o.T = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane) : 0u;
     } else {
-        for (uint32_t g = beg; g < end; g += 32) count_counters((g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u, T);
+        for (uint32_t g = beg; g < end; g += 32) count_counters((g + lane < end) ? __ldcg(&sorted[g + lane].y) : 0u, o.T);
     }
-    const uint32_t P = pre_counters(D.low + (uint64_t)b * LOW_WORDS, T);
-    uint32_t cur = P, mL = 0, L = NONE;
+    o.P = pre_counters(D.low + (uint64_t)b * LOW_WORDS, o.T);
+    o.cur = o.P;
+    o.mL = 0;
+    uint32_t L = NONE;
     // four groups of 32 records loaded per step, so a long segment costs one L2 round trip
     // per 128 records
     constexpr int GR = 4;
@@ -807,58 +801,127 @@ __device__ __forceinline__ void replay_slot(const MswsDev& D, const BatchDev& B,
 #pragma unroll
         for (int q = 0; q < GR; ++q) {
             if (L == NONE && g0 + 32 * q < end) {  // warp-uniform
-                const int j = link_step(mm[q], cur);
+                const int j = link_step(mm[q], o.cur);
                 if (j >= 0) {
                     L = g0 + 32 * q + j;
-                    mL = __shfl_sync(0xffffffffu, mm[q], j);
+                    o.mL = __shfl_sync(0xffffffffu, mm[q], j);
                 }
             }
         }
     }
-    finish_bucket<BATCH>(D, B, b, L != NONE, L != NONE ? end - L : 0u, end - beg, T, P, cur, mL);
+    o.found = L != NONE;
+    o.L = L;
+    o.n_after = o.found ? end - L : 0u;
+    o.n_total = end - beg;
+    return o;
 }
 
 // Replay slot s straight from the chunk's records in array order (all K of them staged in
-// shared memory): steps of 32 records without one of this slot skip after one ballot.  The
-// slot's counter totals and record count come from the write phase (slots < long_cap).
-template <bool BATCH>
-__device__ __forceinline__ void replay_slot_scan(const MswsDev& D, const BatchDev& B, const uint2* srec, uint32_t s,
-                                                 uint32_t K) {
+// shared memory; no writes): steps of 32 records without one of this slot skip after one
+// ballot.  The slot's counter totals and record count come from the write phase (slots <
+// long_cap).
+__device__ __forceinline__ ReplayOut replay_scan(const MswsDev& D, const uint2* srec, uint32_t s, uint32_t K,
+                                                uint32_t b) {
     const int lane = threadIdx.x & 31;
-    const uint32_t b = __ldcg(D.flag_list + s);
-    uint32_t T = 0, n_total = 0;
+    ReplayOut o;
+    o.T = 0;
+    o.n_total = 0;
     if (s < D.long_cap) {  // accumulated while the records were written
-        T = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane) : 0u;
-        n_total = __ldcg(D.seg_beg + s);
+        o.T = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane) : 0u;
+        o.n_total = __ldcg(D.seg_beg + s);
     } else {
         for (uint32_t g = 0; g < K; g += 32) {
             const uint2 r = g + lane < K ? srec[g + lane] : make_uint2(NONE, 0u);
             const bool hit = r.x == s;
             const uint32_t hb = __ballot_sync(0xffffffffu, hit);
             if (!hb) continue;
-            n_total += __popc(hb);
-            count_counters(hit ? r.y : 0u, T);
+            o.n_total += __popc(hb);
+            count_counters(hit ? r.y : 0u, o.T);
         }
     }
-    const uint32_t P = pre_counters(D.low + (uint64_t)b * LOW_WORDS, T);
-    uint32_t cur = P, mL = 0, before = 0;
-    bool found = false;
+    o.P = pre_counters(D.low + (uint64_t)b * LOW_WORDS, o.T);
+    o.cur = o.P;
+    o.mL = 0;
+    o.found = false;
+    o.L = NONE;
+    uint32_t before = 0;
     for (uint32_t g = 0; g < K; g += 32) {
         const uint2 r = g + lane < K ? srec[g + lane] : make_uint2(NONE, 0u);
         const bool hit = r.x == s;
         const uint32_t hb = __ballot_sync(0xffffffffu, hit);
         if (!hb) continue;
         const uint32_t m = hit ? r.y : 0u;
-        const int j = link_step(m, cur);
+        const int j = link_step(m, o.cur);
         if (j >= 0) {
-            found = true;
+            o.found = true;
+            o.L = g + j;
             before += __popc(hb & ((1u << j) - 1u));
-            mL = __shfl_sync(0xffffffffu, m, j);
+            o.mL = __shfl_sync(0xffffffffu, m, j);
             break;
         }
         before += __popc(hb);
     }
-    finish_bucket<BATCH>(D, B, b, found, found ? n_total - before : 0u, n_total, T, P, cur, mL);
+    o.n_after = o.found ? o.n_total - before : 0u;
+    return o;
+}
+
+// After the replay of slot s (bucket b): a bucket that did not switch is final (word 7 back
+// to 0).  One that switched records its switch position `pos` (array order of the chunk's
+// records) for the link order; when its slot has a totals row (s < long_cap) the low words
+// are written now and the high increments wait in that row, otherwise the bucket is replayed
+// again once its high id is known.
+__device__ __forceinline__ void settle_bucket(const MswsDev& D, uint32_t s, uint32_t b, const ReplayOut& o,
+                                              uint32_t pos) {
+    const int lane = threadIdx.x & 31;
+    if (o.found) {
+        if (s < D.long_cap) {
+            const uint32_t H = high_increments(D, o);
+            if (lane < LOW_COUNTERS) __stcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane, H);
+            write_low_words(D, b, o.cur);
+        }
+        if (lane == 0) {
+            __stcg(D.sw + s, make_uint2(pos, o.n_after));
+            atomicOr(D.sw_bits + (pos >> 5), 1u << (pos & 31));
+            atomicAdd(D.sw_cnt + pos / SW_BLOCK, 1u);
+        }
+    } else {
+        if (lane == 0) __stcg(D.sw + s, make_uint2(NONE, 0u));
+        if (lane == 7) __stcg(D.low + (uint64_t)b * LOW_WORDS + 7, 0u);  // every key added low
+    }
+    if (lane == 0) {
+        atomicAdd(&D.ctl->repaired_buckets, 1ull);
+        atomicAdd(&D.ctl->repaired_keys, (unsigned long long)o.n_total);
+    }
+}
+
+// Link bucket b to high id `id` (global; ok: inside the pool) with high increments H, or
+// saturate it when the pool has run out (its n_after keys are dropped).
+__device__ __forceinline__ void link_bucket(const MswsDev& D, uint32_t b, uint32_t id, bool ok, uint32_t H,
+                                            uint32_t n_after) {
+    const int lane = threadIdx.x & 31;
+    if (ok) {
+        __stcg(D.high + (uint64_t)(id - START) * HIGH_WORDS + lane, H);
+    } else if (lane == 0) {
+        atomicOr(&D.ctl->status, ST_POOL_FULL);
+        atomicAdd(&D.ctl->dropped, (unsigned long long)n_after);
+    }
+    if (lane == 7) __stcg(D.low + (uint64_t)b * LOW_WORDS + 7, ok ? id : SATURATED);
+}
+
+// Rank of switch position p among all switch positions of the chunk (the result in every
+// lane): the exclusive prefix `spre` of the per-SW_BLOCK counts, plus the set bits before p
+// in its block of 128 words.
+__device__ __forceinline__ uint32_t switch_rank(const MswsDev& D, const uint32_t* spre, uint32_t p) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t q = p / SW_BLOCK, w = p >> 5;
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < (int)(SW_BLOCK / 32 / 32); ++k) {
+        const uint32_t wi = q * (SW_BLOCK / 32) + k * 32 + lane;
+        if (wi < w) c += __popc(__ldcg(D.sw_bits + wi));
+    }
+    if (lane == 0) c += __popc(__ldcg(D.sw_bits + w) & ((1u << (p & 31)) - 1u));
+    return spre[q] + __reduce_add_sync(0xffffffffu, c);
 }
 
 // The 8 keys of the chunk from position `base` (a multiple of 8) and their skip bits; km is
@@ -889,10 +952,97 @@ __device__ __forceinline__ void repair_tile_keys(const uint32_t* __restrict__ ke
     skip8 = (D.skip && base < n) ? (__ldg(D.skip + (base >> 5)) >> (base & 31)) & 0xffu : 0u;
 }
 
+// Link a bucket that switched: its high increments wait in its totals row, or (no row) the
+// bucket is replayed again by `rerun` now that its id is known.
+template <typename Rerun>
+__device__ __forceinline__ void finish_link(const MswsDev& D, uint32_t s, uint32_t b, uint32_t id, bool ok,
+                                            uint32_t n_after, Rerun& rerun) {
+    const int lane = threadIdx.x & 31;
+    uint32_t H;
+    if (s < D.long_cap) {
+        H = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane) : 0u;
+    } else {
+        const ReplayOut o = rerun(s, b);
+        write_low_words(D, b, o.cur);
+        H = high_increments(D, o);
+        n_after = o.n_after;
+    }
+    link_bucket(D, b, id, ok, H, n_after);
+}
+
+// The link order of the chunk's switched buckets.  A bucket's rank is the number of switch
+// positions before its own (array order of the records), so the r-th switching key of the
+// chunk gets id next_id + r, as one-key-at-a-time insertion hands them out
+// (atomic_malloc, device_sketch_v3.h:69-85); once the pool is used up the remaining buckets
+// saturate.  Batched streams rank within their stream (each has its own allocator): the
+// stream's lowest rank in this repair is found with a generation-tagged atomicMax, then a
+// second pass links.  one_block: every slot lives in block 0 and only it runs this.
+// Returns false when a grid barrier timed out.
+template <bool BATCH, typename Rerun>
+__device__ __forceinline__ bool link_phase(const MswsDev& D, const BatchDev& B, uint32_t F, uint32_t K,
+                                           uint32_t base_id, unsigned long long gen, bool one_block, Rerun rerun,
+                                           uint32_t* s_small, uint32_t* s_big) {
+    Ctl* ctl = D.ctl;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    constexpr int NW = REPAIR_THREADS / 32;
+    const uint32_t nq = (K + SW_BLOCK - 1) / SW_BLOCK;  // K <= 2^26: at most 16384 counts
+    uint32_t* spre = nq <= 64 ? s_small : s_big;        // the sort-free replay (K <= SCAN_CAP) keeps
+                                                        // its records in s_big
+    for (uint32_t i = tid; i < nq; i += REPAIR_THREADS) spre[i] = __ldcg(D.sw_cnt + i);
+    __syncthreads();
+    const uint32_t nfound = block_scan_smem(spre, nq);
+    for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) {
+        const uint2 w = __ldcg(D.sw + s);
+        if (w.x == NONE) continue;  // warp-uniform
+        const uint32_t b = __ldcg(D.flag_list + s);
+        const uint32_t rank = switch_rank(D, spre, w.x);
+        if (!BATCH) {
+            const uint32_t id = base_id + rank;
+            finish_link(D, s, b, id, (uint64_t)(id - START) < D.n_high, w.y, rerun);
+        } else if (lane == 0) {
+            const uint32_t st = stream_of_bucket(B, b);
+            atomicMax(B.first + st, (gen << 32) | (unsigned long long)(~rank));
+            __stcg(D.sw_base + s, __ldcg(B.next_id + st));
+            __stcg(D.sw + s, make_uint2(rank, w.y));
+        }
+    }
+    if (!BATCH) {
+        if (blockIdx.x == 0 && tid == 0) {  // the allocator stops at the pool's end, as the oracle's
+            const unsigned long long nid = min((unsigned long long)base_id + nfound, (unsigned long long)START + D.n_high);
+            if (nid > base_id) ctl->next_id = (uint32_t)nid;
+        }
+        return true;
+    }
+    if (one_block)
+        __syncthreads();
+    else if (!grid_barrier(ctl))
+        return false;
+    for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) {
+        const uint2 w = __ldcg(D.sw + s);
+        if (w.x == NONE) continue;
+        const uint32_t b = __ldcg(D.flag_list + s);
+        uint32_t st = 0, own = 0;
+        if (lane == 0) {
+            st = stream_of_bucket(B, b);
+            own = __ldcg(D.sw_base + s) + (w.x - ~(uint32_t)__ldcg(B.first + st));
+        }
+        st = __shfl_sync(0xffffffffu, st, 0);
+        own = __shfl_sync(0xffffffffu, own, 0);
+        const uint32_t nh = __ldg(&B.desc[st].n_high);
+        const bool ok = (uint64_t)(own - START) < nh;
+        finish_link(D, s, b, own + __ldg(&B.desc[st].high_base), ok, w.y, rerun);
+        if (lane == 0) {
+            atomicMax(B.next_id + st, (uint32_t)min((unsigned long long)own + 1ull, (unsigned long long)START + nh));
+            if (!ok) atomicOr(B.status + st, ST_POOL_FULL);
+        }
+    }
+    return true;
+}
+
 // BATCH: `keys` is the batch's flat key array and the chunk is the window the plan kernel
 // described (B.wpre, B.lo); n is read from the window (the launch's own n is ignored).
 template <bool BATCH>
-__global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* __restrict__ keys, uint64_t n,
+__global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_t* __restrict__ keys, uint64_t n,
                                                                 MswsDev D, BatchDev B) {
     __shared__ RadixSmem rs;
     __shared__ uint32_t s_dbase[256];  // radix pass: first output position of each digit
@@ -900,10 +1050,14 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     __shared__ uint32_t s_acc[2][LOW_COUNTERS];
     __shared__ uint32_t s_acc_slot[2];
     __shared__ uint32_t s_tc[TC_MAX];       // phase 1: counts of this block's tiles, by round
+    __shared__ uint32_t s_swpre[64];        // link order: prefix of the switch counts (small chunks)
     extern __shared__ __align__(16) uint32_t s_set[];
     Ctl* ctl = D.ctl;
     const uint32_t F = min(__ldcg(&ctl->n_flagged), D.flag_cap);
     if (F == 0) return;
+    // Read before the first grid barrier; only the link phase, after it, writes them.
+    const uint32_t base_id = __ldcg(&ctl->next_id);
+    const unsigned long long gen = (unsigned long long)__ldcg(&ctl->link_gen) + 1ull;
     phase_mark(ctl, -1);
     if (BATCH) n = __ldcg(B.win + 1);
 
@@ -1024,6 +1178,11 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     // Few records (K <= SCAN_CAP): the replay scans them unsorted, and the per-slot counter
     // totals and record counts it needs are accumulated here with global atomics.
     const bool scan_mode = K <= SCAN_CAP;
+    {  // the link order's switch bits and counts: positions lie below K
+        const uint32_t nsw = (K + 31) >> 5, nswc = (K + SW_BLOCK - 1) / SW_BLOCK;
+        for (uint32_t i = gtid; i < nsw; i += nthreads) __stcg(D.sw_bits + i, 0u);
+        for (uint32_t i = gtid; i < nswc; i += nthreads) __stcg(D.sw_cnt + i, 0u);
+    }
     // Phase 3: the staged records of every tile move to their place in array order, one warp
     // per tile: the tile's 16 region counts, scanned in the warp, place record i of the tile
     // in region r (the first whose running count exceeds i) at offset i - (counts before r).
@@ -1064,15 +1223,32 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     // Few records: no sort.  Every block that replays a slot stages all K records in shared
     // memory (the flag filter is no longer needed; the 64 KiB hold SCAN_CAP records)
     // and each warp scans them for its slot in array order.
+    // The switch position of a record is its index here (array order).
+    const bool one_block = F <= (uint32_t)NW;  // every slot in block 0: no grid barrier to link
     if (scan_mode) {
-        constexpr int NWB = REPAIR_THREADS / 32;
-        if (blockIdx.x * NWB < F) {
-            uint2* srec = reinterpret_cast<uint2*>(s_set);
+        uint2* srec = reinterpret_cast<uint2*>(s_set);
+        if (blockIdx.x * NW < F) {
             for (uint32_t i = tid; i < K; i += REPAIR_THREADS) srec[i] = __ldcg(D.rec[0] + i);
             __syncthreads();
-            for (uint32_t s = blockIdx.x * NWB + wid; s < F; s += gridDim.x * NWB)
-                replay_slot_scan<BATCH>(D, B, srec, s, K);
+            for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) {
+                const uint32_t b = __ldcg(D.flag_list + s);
+                const ReplayOut o = replay_scan(D, srec, s, K, b);
+                settle_bucket(D, s, b, o, o.L);
+            }
         }
+        phase_mark(ctl, 5);
+        if (one_block) {
+            if (blockIdx.x != 0) {
+                finish_repair(ctl);
+                return;
+            }
+            __syncthreads();
+        } else if (!grid_barrier(ctl)) {
+            return;
+        }
+        auto rerun = [&](uint32_t s, uint32_t b) { return replay_scan(D, srec, s, K, b); };
+        if (!link_phase<BATCH>(D, B, F, K, base_id, gen, one_block, rerun, s_swpre, s_set)) return;
+        phase_mark(ctl, 9);
         finish_repair(ctl);
         return;
     }
@@ -1087,7 +1263,8 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     const bool resident = ntr <= gridDim.x;
     uint2* srec = reinterpret_cast<uint2*>(s_set);   // [REPAIR_TILE]
     uint32_t* srank = s_set + 2 * REPAIR_TILE;        // [REPAIR_TILE]
-    static_assert(3 * REPAIR_TILE <= SET_SLOTS, "resident tile fits the shared space");
+    uint32_t* spos = s_set + 3 * REPAIR_TILE;         // [REPAIR_TILE] the records' array-order positions
+    static_assert(4 * REPAIR_TILE <= SET_SLOTS, "resident tile fits the shared space");
     // Up to SEMI_TILES tiles per block: the count keeps, per tile, the per-warp digit offsets
     // (u16: below REPAIR_TILE) and each record's in-warp rank (u8: a warp holds 256 records);
     // the scatter reloads the records but does not recount them.
@@ -1098,12 +1275,17 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     for (int p = 0; p < npass; ++p) {
         const uint2* src = D.rec[p & 1];
         uint2* dst = D.rec[(p + 1) & 1];
+        // record positions in array order: the identity before the first pass
+        const uint32_t* psrc = p ? D.rpos[p & 1] : nullptr;
+        uint32_t* pdst = D.rpos[(p + 1) & 1];
         const int shift = 8 * p;
         if (resident) {
             if (blockIdx.x < ntr) {
                 const uint32_t t = blockIdx.x;
                 uint2 rec[TILE_ROUNDS];
+                uint32_t pos[TILE_ROUNDS];
                 tile_load(src, K, t, rec);
+                tile_load_pos(psrc, K, t, pos);
                 for (int d = tid; d < 256 * NW; d += REPAIR_THREADS) (&rs.whist[0][0])[d] = 0;
                 __syncthreads();
 #pragma unroll
@@ -1118,6 +1300,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
                     __syncwarp();
                     srec[li] = rec[r];
                     srank[li] = before + __popc(peers & lanemask_lt());
+                    spos[li] = pos[r];
                 }
                 __syncthreads();
                 for (int d = tid; d < 256; d += REPAIR_THREADS) {  // per-warp offsets, tile total
@@ -1216,7 +1399,9 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
                     if (t * REPAIR_TILE + li < K) {
                         const uint2 rec = srec[li];
                         const uint32_t d = (rec.x >> shift) & 0xffu;
-                        __stcg(dst + s_dbase[d] + rs.whist[wid][d] + srank[li], rec);
+                        const uint32_t to = s_dbase[d] + rs.whist[wid][d] + srank[li];
+                        __stcg(dst + to, rec);
+                        __stcg(pdst + to, spos[li]);
                     }
                 }
                 __syncthreads();
@@ -1226,7 +1411,9 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
             for (uint32_t q = 0; q < tiles_here; ++q) {
                 const uint32_t t = blockIdx.x + q * gridDim.x;
                 uint2 rec[TILE_ROUNDS];
+                uint32_t pos[TILE_ROUNDS];
                 tile_load(src, K, t, rec);
+                tile_load_pos(psrc, K, t, pos);
                 uint32_t* sbase = s_acc_base;  // this tile's first position of each digit
                 for (int d = tid; d < 256; d += REPAIR_THREADS) sbase[d] = s_dbase[d] + __ldcg(D.hist + (uint64_t)d * ntr + t);
                 __syncthreads();
@@ -1235,7 +1422,9 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
                     const uint32_t li = wid * 256 + r * 32 + lane;
                     if (t * REPAIR_TILE + li < K) {
                         const uint32_t d = (rec[r].x >> shift) & 0xffu;
-                        __stcg(dst + sbase[d] + swoff[(q * NW + wid) * 256 + d] + srank8[q * REPAIR_TILE + li], rec[r]);
+                        const uint32_t to = sbase[d] + swoff[(q * NW + wid) * 256 + d] + srank8[q * REPAIR_TILE + li];
+                        __stcg(dst + to, rec[r]);
+                        __stcg(pdst + to, pos[r]);
                     }
                 }
                 __syncthreads();
@@ -1243,7 +1432,9 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
         }
         for (uint32_t t = blockIdx.x; t < ntr && !resident && !semi; t += gridDim.x) {  // stable scatter
             uint2 rec[TILE_ROUNDS];
+            uint32_t pos[TILE_ROUNDS];
             tile_load(src, K, t, rec);
+            tile_load_pos(psrc, K, t, pos);
             tile_count(rs, rec, K, t, shift);
             for (int d = tid; d < 256; d += REPAIR_THREADS) {
                 uint32_t run = s_dbase[d] + __ldcg(D.hist + (uint64_t)d * ntr + t);
@@ -1263,6 +1454,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
                 if (v) {
                     const uint32_t rank = rs.whist[wid][d] + __popc(peers & lanemask_lt());
                     __stcg(dst + rank, rec[r]);
+                    __stcg(pdst + rank, pos[r]);
                 }
                 __syncwarp();
                 if (v && lane == __ffs(peers) - 1) rs.whist[wid][d] += __popc(peers);
@@ -1320,8 +1512,28 @@ __global__ void __launch_bounds__(REPAIR_THREADS) k_msws_repair(const uint32_t* 
     if (!grid_barrier(ctl)) return;
     phase_mark(ctl, 4);
 
-    // Phase 6: replay each flagged bucket in array order, one warp per slot.
-    for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) replay_slot<BATCH>(D, B, sorted, s, F, K, true);
+    // Phase 6: replay each flagged bucket in array order, one warp per slot; then link the
+    // switched buckets in the array order of their switching keys (the records' positions
+    // before the sort travelled through the radix passes in rpos).
+    const uint32_t* fpos = npass ? D.rpos[npass & 1] : nullptr;
+    for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) {
+        const uint32_t b = __ldcg(D.flag_list + s);
+        const ReplayOut o = replay_sorted(D, sorted, s, F, K, b);
+        settle_bucket(D, s, b, o, o.found ? (fpos ? __ldcg(fpos + o.L) : o.L) : 0u);
+    }
+    phase_mark(ctl, 5);
+    if (one_block) {
+        if (blockIdx.x != 0) {
+            finish_repair(ctl);
+            return;
+        }
+        __syncthreads();
+    } else if (!grid_barrier(ctl)) {
+        return;
+    }
+    auto rerun = [&](uint32_t s, uint32_t b) { return replay_sorted(D, sorted, s, F, K, b); };
+    if (!link_phase<BATCH>(D, B, F, K, base_id, gen, one_block, rerun, s_swpre, s_set)) return;
+    phase_mark(ctl, 9);
     finish_repair(ctl);
 }
 

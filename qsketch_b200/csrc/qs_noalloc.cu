@@ -37,7 +37,13 @@ constexpr uint64_t NA_OFF_SEG = NA_OFF_FLAGS + na_align(NA_MAX_KEYS * 4);
 constexpr uint64_t NA_OFF_TILES = NA_OFF_SEG + na_align(NA_MAX_KEYS * 4);
 constexpr uint64_t NA_OFF_HIST = NA_OFF_TILES + na_align(NA_TILES * 4);
 constexpr uint64_t NA_OFF_TOTALS = NA_OFF_HIST + na_align(256 * NA_TILES * 4 + 256 * 4);  // + digit totals
-constexpr uint64_t NA_BYTES = NA_OFF_TOTALS + na_align(NA_TOTAL_SLOTS * LOW_COUNTERS * 4);
+constexpr uint64_t NA_OFF_RPOS0 = NA_OFF_TOTALS + na_align(NA_TOTAL_SLOTS * LOW_COUNTERS * 4);
+constexpr uint64_t NA_OFF_RPOS1 = NA_OFF_RPOS0 + na_align(NA_MAX_KEYS * 4);
+constexpr uint64_t NA_OFF_SW = NA_OFF_RPOS1 + na_align(NA_MAX_KEYS * 4);
+constexpr uint64_t NA_OFF_SWBASE = NA_OFF_SW + na_align(NA_MAX_KEYS * 8);
+constexpr uint64_t NA_OFF_SWBITS = NA_OFF_SWBASE + na_align(NA_MAX_KEYS * 4);
+constexpr uint64_t NA_OFF_SWCNT = NA_OFF_SWBITS + na_align(NA_MAX_KEYS / 8);
+constexpr uint64_t NA_BYTES = NA_OFF_SWCNT + na_align(NA_MAX_KEYS / SW_BLOCK * 4 + 4);
 static_assert(NA_BYTES <= QS_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds the documented size");
 static_assert(sizeof(Ctl) <= QS_MSWS_STATE_BYTES, "control block exceeds the caller's state block");
 
@@ -161,6 +167,12 @@ extern "C" qs_status qs_msws_insert_noalloc(uint32_t* d_low, uint64_t n_low, uin
     D.tile_counts = reinterpret_cast<uint32_t*>(sc + NA_OFF_TILES);
     D.hist = reinterpret_cast<uint32_t*>(sc + NA_OFF_HIST);
     D.totals = reinterpret_cast<uint32_t*>(sc + NA_OFF_TOTALS);
+    D.rpos[0] = reinterpret_cast<uint32_t*>(sc + NA_OFF_RPOS0);
+    D.rpos[1] = reinterpret_cast<uint32_t*>(sc + NA_OFF_RPOS1);
+    D.sw = reinterpret_cast<uint2*>(sc + NA_OFF_SW);
+    D.sw_base = reinterpret_cast<uint32_t*>(sc + NA_OFF_SWBASE);
+    D.sw_bits = reinterpret_cast<uint32_t*>(sc + NA_OFF_SWBITS);
+    D.sw_cnt = reinterpret_cast<uint32_t*>(sc + NA_OFF_SWCNT);
 
     // Every scratch part is written before it is read.
     k_noalloc_begin<<<1, 1, 0, st>>>(D.ctl);

@@ -24,25 +24,36 @@ def workload(n_streams, seed, max_len, n_ranks=1 << 12, max_bytes=1 << 20):
     return w
 
 
-def alone(w, s, seed, **kw):
-    sk = qs.Sketch_GPU_Sub_Warp_Level(int(w["n_low"][s]), 8, int(w["n_high"][s]), 32, hash_seed=int(seed),
-                                      mask_rng=1, **kw)
+def alone(w, s, seed, queries=None, **kw):
+    """Stream s inserted alone into a sketch of its own: estimates (of its keys, or of
+    `queries`), status and tables."""
     lo, hi = int(w["offsets"][s]), int(w["offsets"][s + 1])
+    mb = min(1 << 22, max(32, (hi - lo + 31) // 32 * 32))  # results do not depend on the chunk size
+    sk = qs.Sketch_GPU_Sub_Warp_Level(int(w["n_low"][s]), 8, int(w["n_high"][s]), 32, hash_seed=int(seed),
+                                      mask_rng=1, max_batch=mb, **kw)
     sk.insert(w["keys"][lo:hi])
-    out = sk.search(w["keys"][lo:hi])
+    out = sk.search(w["keys"][lo:hi] if queries is None else queries)
     st = sk.status()
+    tables = sk.tables()
     sk.close()
-    return out, st
+    return out, st, tables
 
 
-def check_streams(b, w, got, streams=None):
+def check_streams(b, w, got, streams=None, tables=True):
+    """Every stream's estimates, pool status and low and high tables (all streams, or those in
+    the set `tables`) equal those of the stream inserted alone — pool exhaustion included."""
     seeds = b.seeds()
     off = w["offsets"].cpu().numpy()
+    sst = b.stream_status()
     for s in (range(b.n_streams) if streams is None else streams):
-        want, st = alone(w, s, seeds[s])
-        assert st == _lib.QS_OK
+        want, st, (low, high) = alone(w, s, seeds[s])
+        assert (st == _lib.QS_ERR_POOL_FULL) == bool(sst[s] & 1), f"stream {s}: pool status differs"
         g = got[off[s]:off[s + 1]]
         assert torch.equal(g, want), f"stream {s}: {(g != want).sum().item()} of {g.numel()} estimates differ"
+        if tables is True or (tables and s in tables):
+            bl, bh = b.stream_tables(s)
+            assert np.array_equal(bl, low), f"stream {s}: low table differs"
+            assert np.array_equal(bh, high), f"stream {s}: high pool differs"
 
 
 @pytest.mark.parametrize("max_batch,lpk,first", [(1 << 16, 8, 0), (1 << 22, 8, 0), (1 << 18, 4, 0), (1 << 18, 16, 0),
@@ -192,4 +203,20 @@ def test_batch_pool_exhaustion_is_per_stream(gpu):
     assert st[1] & 1 and not (st[[0, 2, 3]] & 1).any(), st
     assert b.info()["streams_pool_full"] == 1
     w2 = {"keys": keys, "offsets": offs, "n_low": w["n_low"], "n_high": nh}
-    check_streams(b, w2, got, streams=[0, 2, 3])
+    check_streams(b, w2, got)  # the exhausted stream too: its links follow its own array order
+
+
+def test_batch_uneven_streams_full_size(gpu):
+    """The batched configuration at full size: 512 streams, lengths log-uniform in [2^10, 2^22]
+    (~2.6e8 keys), per-stream Zipf s ~ U[0.6, 1.4] over 2^20 ranks, sketches log-uniform in
+    [32 KB, 16 MB] with pools of bytes/4, so dozens of small sketches run out of high buckets.
+    Every stream's estimates and pool status equal the stream inserted alone; tables are
+    compared for every 8th stream and for every stream whose pool ran out."""
+    w = data.uneven_streams(512, seed=1)
+    b = BatchedSketches(w["n_low"], w["n_high"], seed_rng=7, lanes_per_key=4)
+    b.insert(w["keys"], w["offsets"])
+    got = b.search(w["keys"], w["offsets"])
+    assert b.status() == _lib.QS_ERR_POOL_FULL
+    full = np.nonzero(b.stream_status() & 1)[0]
+    assert full.size > 10, "the workload is meant to exhaust some pools"
+    check_streams(b, w, got, tables=set(range(0, 512, 8)) | set(full.tolist()))

@@ -1,8 +1,8 @@
 """GPU parity of the MSWS insert/query path against the sequential CPU oracle.
 
-Every comparison is bit-exact: the per-key query vector, the low table's counter words,
-which buckets are linked, and each linked bucket's high counters (high ids themselves may
-differ: allocation order is free)."""
+Every comparison is bit-exact: the per-key query vector and both tables word for word — low
+counter words, the high id in word 7 (ids are handed out in the array order of the keys that
+switch buckets, as the sequential insert does) and the high pool — and the allocator."""
 import numpy as np
 import pytest
 import torch
@@ -24,16 +24,15 @@ def make_pair(n_low, n_high, seed=2654435769, mask_rng=1, compat=False, **kw):
 def assert_same_tables(sk, orc):
     low, high = sk.tables()
     gl, ol = low.reshape(-1, 8), orc.low.reshape(-1, 8)
+    assert (gl[:, 7] & 0x80000000 == 0).all(), "a bucket is still flagged"
     assert np.array_equal(gl[:, :7], ol[:, :7]), "low counter words differ"
-    gp, op = gl[:, 7], ol[:, 7]
-    assert np.array_equal(gp > 1024, op > 1024), "linked buckets differ"
-    assert np.array_equal(gp == oracle.SATURATED, op == oracle.SATURATED)
-    linked = np.nonzero(op > 1024)[0]
-    if linked.size:
-        gh = high.reshape(-1, 32)[gp[linked] - 1024]
-        oh = orc.high.reshape(-1, 32)[op[linked] - 1024]
-        assert np.array_equal(gh, oh), "high buckets differ"
-    assert (gp & 0x80000000 == 0).all(), "a bucket is still flagged"
+    bad = np.nonzero(gl[:, 7] != ol[:, 7])[0]
+    assert bad.size == 0, f"word 7 (high id) differs at {bad.size} buckets, first {bad[:4]}: " \
+                          f"{gl[bad[:4], 7]} vs {ol[bad[:4], 7]}"
+    assert np.array_equal(high, orc.high), "high pools differ"
+    st = sk.stats()
+    assert st["next_level_id"] == orc.next_id, (st["next_level_id"], orc.next_id)
+    assert st["dropped_keys"] == orc.dropped
 
 
 def run_and_compare(sk, orc, keys_d, queries_d, pieces=None):
@@ -163,6 +162,28 @@ def test_unaligned_and_tiny_inputs(gpu):
     assert_same_tables(sk, orc)
 
 
+@pytest.mark.parametrize("n_high,max_batch,n_ranks", [
+    (8, 1 << 22, 1 << 12),     # few crossed buckets per chunk: one block links them
+    (40, 1 << 22, 1 << 12),    # more than one block's warps of crossed buckets: grid-wide link order
+    (1000, 1 << 16, 1 << 14),  # 2^16-key chunks: the pool runs out after several of them
+    (600, 1 << 20, 1 << 16),   # hundreds of crossed buckets per chunk (sorted replay), pool runs out
+])
+def test_pool_exhaustion_matches_the_oracle(gpu, n_high, max_batch, n_ranks):
+    """Which buckets still get a high bucket when the pool runs out is decided by the array
+    order of their switching keys, as in the sequential insert: estimates, both tables, the
+    allocator and the dropped-key count equal the oracle's."""
+    sk, orc = make_pair(16381, n_high, max_batch=max_batch)
+    keys = data.zipf_keys(1 << 21, n_ranks, 1.1, seed=12, perm_seed=13)
+    q = data.rank_keys(13, 0, n_ranks)
+    sk.insert(keys)
+    got = sk.search(q).cpu().numpy()
+    assert sk.status() == _lib.QS_ERR_POOL_FULL
+    orc.insert(keys.cpu().numpy())
+    assert orc.pool_full
+    assert np.array_equal(got, orc.query(q.cpu().numpy()))
+    assert_same_tables(sk, orc)
+
+
 def test_pool_exhaustion_is_reported(gpu):
     sk, orc = make_pair(4093, 8)
     keys = data.zipf_keys(1 << 20, 1 << 12, 1.2, seed=1, perm_seed=2)
@@ -174,6 +195,7 @@ def test_pool_exhaustion_is_reported(gpu):
     assert st["linked_buckets"] == 7 and st["dropped_keys"] > 0
     orc.insert(keys.cpu().numpy())
     assert orc.pool_full and orc.next_id == 1024 + 8
+    assert_same_tables(sk, orc)
     sk.reset_status()
     assert sk.status() == _lib.QS_OK
 

@@ -54,7 +54,7 @@ def assert_three_equal(got_ref, want, got, what):
 def test_msws_uniform_2_24_pinned_by_reference_kernels(gpu, ref):
     """The uniform configuration at full size: 2^24 keys, n_low = 262139, query every key."""
     keys = data.uniform_keys(1 << 24, seed=1).cpu().numpy()
-    got_ref, want, got, low_ref, low_orc, low = three_way_msws(keys, keys, N_LOW_CFG1, 1024, 7, 3)
+    got_ref, want, got, low_ref, low_orc, low, _ = three_way_msws(keys, keys, N_LOW_CFG1, 1024, 7, 3)
     assert_three_equal(got_ref, want, got, "uniform 2^24")
     assert np.array_equal(low_ref, low_orc), "low tables: oracle vs reference kernel"
     assert np.array_equal(low, low_orc), "low tables: libqsketch vs oracle"
@@ -68,7 +68,7 @@ def test_msws_repeated_keys_pinned_by_reference_kernels(gpu, ref):
     rng = np.random.default_rng(5)
     distinct = np.unique(rng.integers(0, 2 ** 32, 1 << 21, dtype=np.uint64).astype(np.uint32))[:1 << 20]
     keys = rng.permutation(np.repeat(distinct, 16)).astype(np.uint32)
-    got_ref, want, got, low_ref, low_orc, low = three_way_msws(keys, distinct, N_LOW_CFG1, 1024, 7, 3)
+    got_ref, want, got, low_ref, low_orc, low, _ = three_way_msws(keys, distinct, N_LOW_CFG1, 1024, 7, 3)
     assert_three_equal(got_ref, want, got, "repeated keys")
     assert np.array_equal(low_ref, low_orc) and np.array_equal(low, low_orc)
     assert low_orc.reshape(-1, 8)[:, :7].copy().view(np.uint8).max() > 96

@@ -49,10 +49,12 @@ def run_both(masks, n_masks, n_low, n_high, batches, compat_v3=False):
         ref.insert(keys)
         torch.cuda.synchronize()
         ref.sync()
-        got = canonical(low.cpu().numpy(), high.cpu().numpy())
-        want = canonical(*ref.tables())
-        for g, w in zip(got, want):
+        got_low, got_high = low.cpu().numpy(), high.cpu().numpy()
+        want_low, want_high = ref.tables()
+        for g, w in zip(canonical(got_low, got_high), canonical(want_low, want_high)):
             assert np.array_equal(g, w)
+        # high ids follow the array order of the switching keys on both paths: word for word
+        assert np.array_equal(got_low, want_low) and np.array_equal(got_high, want_high)
         after = ref.stats()["repaired_buckets"]
         replayed.append(after - before)
         before = after
