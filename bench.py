@@ -2,7 +2,7 @@
 """QSketch insert/query throughput on B200 — one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config zipf|uniform|mixed|learned|batched|zipf_prof|batched_prof]
+                    [--config zipf|uniform|mixed|cm|learned|batched|zipf_prof|batched_prof]
 
 A step is one pass of the hot path over one batch of synthetic input: clear the sketch,
 insert the whole key stream, query the distinct keys.  The default workload is the
@@ -10,12 +10,16 @@ Zipf-skewed stream (2^27 keys, Zipf s=1.1 over 2^24 ranks, 64 MB low table, 16 M
 pool, query the 2^24 distinct keys); `--config uniform` is the 2^24-key uniform case,
 `--config mixed` the HBM-bound interleaved insert/query stream, `--config learned` the
 learned heavy-hitter split against the plain sketch at equal bytes (relative error of both,
-throughput with and without the warm-up/training phase), and `--config batched` 512 uneven
-streams with one sketch each, inserted and queried as one batch.
-For N > 1 (torchrun, one process per GPU) every rank runs its own sketch over its own
-seeded stream: the path has no data exchange, so this is weak scaling with no collective
-on the data path.  `--impl reference` times the CPU restatement of the reference path
-(oracle/, bucket-partitioned threads) on the host cores, rank 0 only.
+throughput with and without the warm-up/training phase), `--config batched` 512 uneven
+streams with one sketch each, inserted and queried as one batch, and `--config cm` the plain
+count-min (the in-GPU baseline) on the uniform stream at the uniform configuration's bytes,
+with the MSWS sketch of those bytes timed beside it.
+For N > 1 (one process per GPU; without torchrun's environment, `--gpus N` starts the N
+ranks itself) every rank runs its own sketch over its own seeded stream: the path has no
+data exchange, so this is weak scaling with no collective on the data path.
+`--impl reference` times the CPU restatement of the reference path (oracle/, one pass that
+partitions the keys by bucket over all host threads, then each thread applies its part in
+array order) on the host cores, rank 0 only, over the same key stream as the GPU arm.
 """
 import argparse
 import json
@@ -59,11 +63,16 @@ CONFIGS = {
     "batched_prof": dict(workload="64_streams_len_2^10..2^21_zipf0.6..1.4_2^20ranks_sketch32KB..16MB_pool_bytes/4",
                          kind=4, n_streams=64, max_len=1 << 21, n_keys=0, n_ranks=1 << 20, s=0.0, n_low=0, n_high=0,
                          n_query=0),
+    # plain count-min (device_sketch_v0.h), m = 3 rows, n = find_greatest_prime(8 MB / 4 / 3):
+    # the uniform configuration's 2^24 keys at (no more than) its 8 MB, queried for every key
+    "cm": dict(workload="countmin_m3_n524287_uniform_2^24keys_query2^24", kind=5, n_keys=1 << 24, n_ranks=0,
+               s=0.0, n_low=524287, rows=3, n_high=0, n_query=1 << 24),
     # a smaller skewed case for Nsight Compute captures (key stream still larger than L2)
     "zipf_prof": dict(workload="zipf1.1_2^25keys_2^22ranks_low16MB_high4MB_query2^22", kind=1, n_keys=1 << 25,
                       n_ranks=1 << 22, s=1.1, n_low=524287, n_high=1 << 15, n_query=1 << 22),
 }
 INSERT_BYTES_PER_KEY = 68  # 4 B key + 32 B bucket sector read + 32 B write-back
+L2_BYTES = 126 << 20      # B200 L2: tables above this live in HBM
 QUERY_BYTES_PER_KEY = 40   # 4 B key + 32 B bucket sector + 4 B result
 
 
@@ -74,6 +83,55 @@ def peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def traffic_per_unit(config, kernel):
+    """DRAM bytes per key of `kernel` from one ncu capture (profiles/traffic.json), or None."""
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(tfile):
+        return None
+    with open(tfile) as f:
+        k = json.load(f).get(f"{config}:{kernel}")
+    return k["dram_bytes_per_unit"] if k else None
+
+
+# Three distinct counters of 28, four to a 32-bit word: the expected number of distinct words
+# a key's increments touch is 3 P(all apart) + 2 P(one pair shares) + 1 P(all share).
+MSWS_WORD_OPS_PER_KEY = 3 * (24 / 27) * (20 / 26) + 2 * (1 - (24 / 27) * (20 / 26) - (3 / 27) * (2 / 26)) + \
+    (3 / 27) * (2 / 26)
+
+
+def l2_atomic_roofline(probes, units_per_s, word_ops_per_unit, kernel, what):
+    """Roofline against the L2's atomic units.  Their ceiling is a rate of 32-bit word
+    operations: the random-sector probes reach about the same word rate whether each sector
+    takes 3 words from 3 lanes (kind 0) or 1 word from every lane (kind 7), while their sector
+    rates differ threefold.  achieved = units/s x word operations per unit; the sector view
+    (one sector per unit against the best sector rate) is given beside it."""
+    if not probes:
+        return {"bound": "l2_atomic", "kernel": kernel, "achieved": None, "peak": None, "frac": None}
+    word_rates = {"red_3word_subwarp": 3 * probes["red_3word_subwarp"],
+                  "red_1word_per_lane": probes["red_1word_per_lane"]}
+    peak = max(word_rates.values())
+    sect = max(probes.values())
+    ach = units_per_s * word_ops_per_unit
+    return {"bound": "l2_atomic", "kernel": kernel, "achieved": round(ach / 1e9, 3), "peak": round(peak / 1e9, 3),
+            "unit": "G atomic word-ops/s", "frac": round(ach / peak, 4),
+            "peak_source": "live probes on a table of this size (qs_probe kind 0: 3 words per random sector from "
+                           "a sub-warp of 8; kind 7: one word per lane, every lane its own random sector), "
+                           "G word-ops/s: " + ", ".join(f"{k} {v / 1e9:.2f}" for k, v in word_rates.items()),
+            "word_ops_per_unit": round(word_ops_per_unit, 4), "units_per_s": round(units_per_s / 1e9, 4),
+            "units": what,
+            "sector_view": {"achieved_gsectors": round(units_per_s / 1e9, 3), "peak_gsectors": round(sect / 1e9, 3),
+                            "frac": round(units_per_s / sect, 4),
+                            "note": "one 32 B bucket sector per unit against the best probe sector rate"}}
+
+
+def atomic_probes(table_bytes):
+    """Random-sector red rates (sectors/s) on a table of `table_bytes`: 3 words per sector from
+    a sub-warp of 8 lanes (kind 0), and one word per lane, every lane its own sector (kind 7)."""
+    from qsketch_b200 import data
+    return {"red_3word_subwarp": data.probe(0, table_bytes, 1 << 26),
+            "red_1word_per_lane": data.probe(7, table_bytes, 1 << 26)}
 
 
 class Clocks:
@@ -184,6 +242,8 @@ def run_ours(args, cfg):
         return run_learned(args, cfg)
     if cfg["kind"] == 4:
         return run_batched(args, cfg)
+    if cfg["kind"] == 5:
+        return run_cm(args, cfg)
     world, rank, local, barrier, max_over_ranks = init_ranks(args)
 
     stream = torch.cuda.current_stream()
@@ -211,20 +271,36 @@ def run_ours(args, cfg):
         queries = torch.cat(q_views)
         cfg = dict(cfg, n_query=queries.numel())
     out = torch.empty(cfg["n_query"], dtype=torch.uint32, device="cuda")
-    # the library's autotuner picks the pass-1 knobs on the stream itself (outside the
-    # timed region; no knob changes any result); the sketch below takes them from its table
+    # the library's autotuner picks the pass-1 knobs (outside the timed region; no knob changes
+    # any result) on another stream of the same configuration — another seed — so the setting
+    # is not fitted to the timed data; the sketch below takes them from its table
     from qsketch_b200 import autotune
     autotune.reset()
-    # (the mixed workload inserts one batch per call: tune on its first 16 batches inserted in
-    # chunks of one batch, so the tuner sees the real chunk size and a sketch that fills)
-    if cfg["kind"] == 2:
-        sample = torch.cat(ins_views[:16])
+    if not args.autotune:
+        tune_keys = None
+    elif cfg["kind"] == 1:
+        tune_keys = data.zipf_keys(cfg["n_keys"], cfg["n_ranks"], cfg["s"], seed=seed + 7777,
+                                   perm_seed=perm_seed + 7777)
+    elif cfg["kind"] == 2:
+        tune_keys = data.zipf_keys(16 * cfg["batch"], cfg["n_ranks"], cfg["s"], seed=seed + 7777,
+                                   perm_seed=perm_seed + 7777)
+    else:
+        tune_keys = data.uniform_keys(cfg["n_keys"], seed=seed + 7777)
+    # (the mixed workload inserts one batch per call: tune on 16 batches' inserts in chunks of
+    # one batch, so the tuner sees the real chunk size and a sketch that fills)
+    if tune_keys is None:
+        tuned = {k: 0 for k in ("lanes_per_key", "aggregate", "route", "ctas_per_sm", "max_batch", "first_chunk",
+                                "keys_per_tile")}
+    elif cfg["kind"] == 2:
+        sample = torch.cat([tune_keys[b * cfg["batch"]:b * cfg["batch"] + ni_b] for b in range(16)])
         tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], sample, reps=3, hash_seed=SEED, mask_rng=1,
                                      max_batch=(ni_b + 31) // 32 * 32)
+        del sample
     else:
         # (whole-stream samples take a few ms each: 8 repetitions per setting keep the
         # search's picks from following run-to-run noise of a few percent)
-        tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], keys, reps=8, hash_seed=SEED, mask_rng=1)
+        tuned, _ = autotune.autotune(cfg["n_low"], cfg["n_high"], tune_keys, reps=8, hash_seed=SEED, mask_rng=1)
+    del tune_keys
     sk = qs.Sketch_GPU_Sub_Warp_Level(cfg["n_low"], 8, cfg["n_high"], 32, hash_seed=SEED, mask_rng=1)
     n_ins, n_q = cfg["n_keys"], cfg["n_query"]
     if cfg["kind"] == 2:
@@ -303,19 +379,32 @@ def run_ours(args, cfg):
     per_launch_units = units / max(1, launches_k)
     avg_ms = ms_k / max(1, launches_k)
     achieved = per_launch_units * bpu / (avg_ms * 1e-3) / 1e9
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tfile):
-        with open(tfile) as f:
-            tj = json.load(f)
-        k = tj.get(f"{args.config}:{dom}")
-        if k:
-            traffic = k["dram_bytes_per_unit"] * per_launch_units
-    atomic_peak = data.probe(0, max(64 << 20, cfg["n_low"] * 32), 1 << 26) if rank == 0 else None
+    dram_per_key = traffic_per_unit(args.config, dom)
+    table_bytes = cfg["n_low"] * 32 + cfg["n_high"] * 128
+    # the L2 atomic ceiling: the best of the random-sector red probes on a table of this size
+    probes = atomic_probes(max(64 << 20, cfg["n_low"] * 32)) if rank == 0 else {}
     if cfg["kind"] == 2:  # inserts and queries interleave: split their rates by kernel time
         ins_ms = prof["insert_ms"] + prof["repair_ms"]
         q_ms = prof["query_ms"]
+    insert_step_ms = prof["insert_ms"] + prof["repair_ms"]  # pass 1 + ordered replay of the step
+    keys_per_s = n_ins / (insert_step_ms * 1e-3)
+    hbm_line = {"bound": "hbm", "kernel": "k_msws_insert" if dom == "insert" else "k_msws_query",
+                "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "traffic": dram_per_key * per_launch_units if dram_per_key else None, "peak_source": peak_kind,
+                "bytes_per_unit": bpu, "units_per_launch": per_launch_units, "avg_launch_ms": round(avg_ms, 5)}
+    if table_bytes > L2_BYTES:  # the tables live in HBM: bucket sectors cost DRAM traffic
+        roofline = hbm_line
+    else:  # L2-resident tables: the L2's atomic units bound the insert
+        roofline = l2_atomic_roofline(probes, keys_per_s, MSWS_WORD_OPS_PER_KEY,
+                                      "k_msws_insert + k_msws_repair (pass 1 + ordered replay)",
+                                      "each key adds 1 to 3 of its bucket's 28 packed 8-bit counters: "
+                                      f"{MSWS_WORD_OPS_PER_KEY:.4f} 32-bit words on average (the expected number "
+                                      "of distinct words holding 3 distinct counters of 28, 4 per word)")
+        roofline.update({"traffic": round(dram_per_key * n_ins) if dram_per_key else None,
+                         "traffic_unit": "DRAM bytes per step of the insert kernels (ncu dram__bytes per key x keys)",
+                         "algorithmic_dram_bytes": n_ins * 4, "insert_ms_per_step": round(insert_step_ms, 4)})
     ins_rate = per_launch_units / (avg_ms * 1e-3) if dom == "insert" else n_ins / (prof["insert_ms"] * 1e-3)
+    atomic_peak = probes.get("red_3word_subwarp")
 
     # end to end through the host-buffer C ABI calls: pinned keys in, counts out
     hk = keys.cpu().pin_memory()
@@ -369,15 +458,13 @@ def run_ours(args, cfg):
                     "h2d_bytes_per_step": (n_ins + n_q) * 4, "d2h_bytes_per_step": n_q * 4,
                     "ms_per_step": round(e2e_ms, 3), "api": "qs_insert_host + qs_query_host"},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k_msws_insert" if dom == "insert" else "k_msws_query",
-                         "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                         "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_source": peak_kind,
-                         "bytes_per_unit": bpu, "units_per_launch": per_launch_units,
-                         "avg_launch_ms": round(avg_ms, 5)},
-            "atomic_roofline": {"kernel": "k_msws_insert", "achieved_gsectors": round(ins_rate / 1e9, 3),
-                                "peak_gsectors": round(atomic_peak / 1e9, 3) if atomic_peak else None,
-                                "frac": round(ins_rate / atomic_peak, 4) if atomic_peak else None,
-                                "probe": "random 32 B sectors, 3 red.add.u32 words per sector, sub-warp of 8"},
+            "roofline": roofline,
+            "hbm_roofline": hbm_line,
+            "pass1_atomic_roofline": {"kernel": "k_msws_insert alone", "achieved_gsectors": round(ins_rate / 1e9, 3),
+                                      "peak_gsectors": round(atomic_peak / 1e9, 3) if atomic_peak else None,
+                                      "frac": round(ins_rate / atomic_peak, 4) if atomic_peak else None,
+                                      "probe": "random 32 B sectors, 3 red.add.u32 words per sector, sub-warp "
+                                               "of 8"},
             "kernel_ms_per_step": {"insert": round(prof["insert_ms"], 4), "repair": round(prof["repair_ms"], 4),
                                    "query": round(prof["query_ms"], 4)},
             "clocks": clk.summary(),
@@ -386,6 +473,126 @@ def run_ours(args, cfg):
             line["cpu_baseline"] = cpu_baseline(cfg, keys.cpu().numpy(), queries.cpu().numpy())
         print(json.dumps(line), flush=True)
     sk.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_cm(args, cfg):
+    """Plain count-min (Sketch_GPU_Thread, device_sketch_v0.h:105-191), the in-GPU baseline: a
+    step is clear + insert the 2^24 uniform keys + query every key.  Beside it, the MSWS sketch
+    of the uniform configuration (8 MB low table) runs the same step, for the count-min vs
+    MSWS comparison the reference publishes."""
+    import torch
+    import torch.distributed as dist
+
+    import qsketch_b200 as qs
+    from qsketch_b200 import data
+
+    world, rank, local, barrier, max_over_ranks = init_ranks(args)
+    stream = torch.cuda.current_stream()
+    n, rows = cfg["n_keys"], cfg["rows"]
+    keys = data.uniform_keys(n, seed=1000 + rank)
+    out = torch.empty(n, dtype=torch.uint32, device="cuda")
+    out_m = torch.empty_like(out)
+    cm = qs.Sketch_GPU_Thread(cfg["n_low"], rows, seed_rng=1 + rank)
+    ms_cfg = CONFIGS["uniform"]
+    msws = qs.Sketch_GPU_Sub_Warp_Level(ms_cfg["n_low"], 8, ms_cfg["n_high"], 32, hash_seed=SEED, mask_rng=1)
+
+    def step(sk, ev=None):
+        sk.clear()
+        if ev:
+            ev[0].record(stream)
+        sk.insert(keys)
+        if ev:
+            ev[1].record(stream)
+        sk.search(keys, counts=out if sk is cm else out_m)
+        if ev:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step(cm)
+        step(msws)
+    torch.cuda.synchronize()
+    cm.profile()
+    K = args.steps
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    mevs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for i in range(K):
+            step(cm, evs[i])
+        t1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms_per_step = max_over_ranks(t0.elapsed_time(t1)) / K
+    ins_ms = max_over_ranks(sum(e[0].elapsed_time(e[1]) for e in evs) / K)
+    q_ms = max_over_ranks(sum(e[1].elapsed_time(e[2]) for e in evs) / K)
+    launches = cm.profile()
+    launches = launches["insert_launches"] + launches["query_launches"]
+    for i in range(K):  # the MSWS sketch of the uniform configuration, same keys, same step
+        step(msws, mevs[i])
+    torch.cuda.synchronize()
+    m_ins = sum(e[0].elapsed_time(e[1]) for e in mevs) / K
+    m_q = sum(e[1].elapsed_time(e[2]) for e in mevs) / K
+    probes = atomic_probes(max(64 << 20, cfg["n_low"] * rows * 4)) if rank == 0 else {}
+
+    hk = keys.cpu().pin_memory()
+    ho = torch.empty(n, dtype=torch.uint32).pin_memory()
+    e2e_steps = max(1, min(K, 5))
+
+    def e2e_step():
+        cm.clear()
+        cm.insert_host(hk)
+        cm.search_host(hk, ho)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    w0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks((time.perf_counter() - w0) * 1e3 / e2e_steps)
+    assert torch.equal(ho.cuda(), out), "host-buffer count-min estimates differ from the device path"
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(world * 2 * n / (ms_per_step * 1e6), 4), "unit": "Gkeys/s",
+            "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic: seeded xorshift64* uniform u32 keys",
+            "config": {"workload": cfg["workload"], "n_keys": n, "n_query": n, "n": cfg["n_low"], "rows": rows,
+                       "table_bytes": cfg["n_low"] * rows * 4,
+                       "l2": "key stream of %d MB per step > 126 MB L2" % (n * 4 >> 20),
+                       "parallelism": "independent sketch per GPU" if world > 1 else "single GPU"},
+            "insert_gkeys_per_s": round(world * n / (ins_ms * 1e6), 4),
+            "query_gkeys_per_s": round(world * n / (q_ms * 1e6), 4),
+            "msws_same_keys": {"workload": ms_cfg["workload"],
+                               "insert_gkeys_per_s": round(n / (m_ins * 1e6), 4),
+                               "query_gkeys_per_s": round(n / (m_q * 1e6), 4),
+                               "value": round(2 * n / ((m_ins + m_q) * 1e6), 4),
+                               "note": "MSWS at 8 MB low + 8 MB high on the same keys; the reference's own "
+                                       "count-min vs MSWS insert ratio is 0.42 vs 1.22 Gkeys/s on an RTX 2080 Ti "
+                                       "(doc/data/qsketch/perf_2080ti_1.0.dat)"},
+            "e2e": {"value": round(world * 2 * n / (e2e_ms * 1e6), 4), "unit": "Gkeys/s",
+                    "h2d_bytes_per_step": 2 * n * 4, "d2h_bytes_per_step": n * 4,
+                    "ms_per_step": round(e2e_ms, 3), "api": "qs_insert_host + qs_query_host"},
+            "gpu_launches": int(launches),
+            "roofline": dict(l2_atomic_roofline(probes, n / (ins_ms * 1e-3), rows, "k_cm_insert",
+                                                f"each key adds 1 to one 32-bit counter in each of the {rows} rows"),
+                             traffic=(round(traffic_per_unit("cm", "insert") * n)
+                                      if traffic_per_unit("cm", "insert") else None),
+                             traffic_unit="DRAM bytes per insert launch (ncu dram__bytes per key x keys)",
+                             algorithmic_dram_bytes=n * 4),
+            "clocks": clk.summary(),
+        }
+        if args.cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(cfg, keys.cpu().numpy(), keys.cpu().numpy())
+        print(json.dumps(line), flush=True)
+    cm.close()
+    msws.close()
     if world > 1:
         dist.destroy_process_group()
 
@@ -714,37 +921,101 @@ def host_zipf_keys(n, n_ranks, s, seed):
         np.uint32(2654435761) ^ np.uint32(0x5bd1e995)
 
 
-def oracle_step(cfg, keys, queries, threads):
-    import oracle
-    masks = oracle.generate_hashmask(1)
-    s = oracle.Msws(cfg["n_low"], cfg["n_high"], SEED, masks)
-    t0 = time.perf_counter()
-    s.insert(keys, threads=threads)
-    t1 = time.perf_counter()
+def cpu_baseline(cfg, keys, queries):
+    """The CPU path (the oracle, all host threads) on a bounded prefix of this run's own
+    stream: about 10-30 s of CPU work."""
+    threads = os.cpu_count() or 1
+    ni = min(keys.size, 1 << 25)
+    if cfg["kind"] == 2:
+        ni -= ni % cfg["batch"]
+        q = None
+    else:
+        q = queries[:min(queries.size, 1 << 22)]
+    ti, tq, n_ins, n_q = reference_step(cfg, keys[:ni], q, threads)
+    return {"value": round((n_ins + n_q) / (ti + tq) / 1e9, 5), "unit": "Gkeys/s", "cores": threads, "kind": "port",
+            "sample": f"first {ni} keys of this run's stream ({n_ins} inserted, {n_q} queried) into a sketch of the "
+                      "same size (oracle/oracle.cpp, keys partitioned by bucket over the threads, array order per "
+                      "bucket)",
+            "insert_gkeys_per_s": round(n_ins / ti / 1e9, 5), "query_gkeys_per_s": round(n_q / tq / 1e9, 5)}
+
+
+def reference_inputs(cfg):
+    """The GPU arm's rank-0 key stream (same generator, seeds and sizes) as host arrays.  On a
+    machine with a GPU it is generated once by libqsketch's generator and copied to the host
+    (input preparation, outside any timing; the timed work is the CPU path alone).  Without a
+    GPU a numpy stand-in of the same shape is used, and the line says it is not the same
+    stream.  Returns (keys, queries, same_stream)."""
+    kind = cfg["kind"]
+    try:
+        import torch
+        gpu = torch.cuda.is_available()
+    except Exception:  # pragma: no cover
+        gpu = False
+    if gpu:
+        from qsketch_b200 import data
+        if kind in (1, 2):
+            keys = data.zipf_keys(cfg["n_keys"], cfg["n_ranks"], cfg["s"], seed=1000, perm_seed=99).cpu().numpy()
+            queries = data.rank_keys(99, 0, cfg["n_query"]).cpu().numpy() if kind == 1 else None
+        else:
+            keys = data.uniform_keys(cfg["n_keys"], seed=1000).cpu().numpy()
+            queries = keys[:cfg["n_query"]]
+        return keys, queries, True
+    if kind in (1, 2):
+        keys, distinct = host_zipf_keys(cfg["n_keys"], cfg["n_ranks"], cfg["s"], 1000)
+        queries = distinct[:cfg["n_query"]] if kind == 1 else None
+    else:
+        keys = np.random.default_rng(1000).integers(0, 1 << 32, cfg["n_keys"], dtype=np.uint64).astype(np.uint32)
+        queries = keys[:cfg["n_query"]]
+    return keys, queries, False
+
+
+def threaded_query(sketch, queries, threads):
+    """Query with `threads` host threads over contiguous parts (ctypes releases the GIL)."""
     parts = np.array_split(queries, threads)
     outs = [None] * threads
 
     def q(i):
-        outs[i] = s.query(parts[i])
+        outs[i] = sketch.query(parts[i])
 
     th = [threading.Thread(target=q, args=(i,)) for i in range(threads)]
     for t in th:
         t.start()
     for t in th:
         t.join()
+    return np.concatenate(outs)
+
+
+def reference_step(cfg, keys, queries, threads):
+    """One step of the CPU path on a fresh sketch; returns (insert s, query s, keys inserted,
+    keys queried)."""
+    import oracle
+    kind = cfg["kind"]
+    if kind == 5:
+        sk = oracle.CountMin(cfg["n_low"], oracle.draw_seeds(1, cfg["rows"]))
+    else:
+        sk = oracle.Msws(cfg["n_low"], cfg["n_high"], SEED, oracle.generate_hashmask(1))
+    ti = tq = 0.0
+    if kind == 2:  # per batch: insert its first 90 %, then query the rest
+        B = cfg["batch"]
+        ni_b = int(B * cfg["insert_frac"])
+        n_ins = n_q = 0
+        for b0 in range(0, keys.size - B + 1, B):
+            t0 = time.perf_counter()
+            sk.insert(keys[b0:b0 + ni_b], threads=threads)
+            t1 = time.perf_counter()
+            threaded_query(sk, keys[b0 + ni_b:b0 + B], threads)
+            t2 = time.perf_counter()
+            ti += t1 - t0
+            tq += t2 - t1
+            n_ins += ni_b
+            n_q += B - ni_b
+        return ti, tq, n_ins, n_q
+    t0 = time.perf_counter()
+    sk.insert(keys, threads=threads)
+    t1 = time.perf_counter()
+    threaded_query(sk, queries, threads)
     t2 = time.perf_counter()
-    return t1 - t0, t2 - t1
-
-
-def cpu_baseline(cfg, keys, queries):
-    threads = os.cpu_count() or 1
-    ni = min(keys.size, 1 << 25)
-    nq = min(queries.size, 1 << 22)
-    ti, tq = oracle_step(cfg, keys[:ni], queries[:nq], threads)
-    return {"value": round((ni + nq) / (ti + tq) / 1e9, 5), "unit": "Gkeys/s", "cores": threads, "kind": "port",
-            "sample": f"first {ni} keys inserted + {nq} queries of the same stream and sketch size "
-                      "(oracle/oracle.cpp, bucket-partitioned threads, array order per bucket)",
-            "insert_gkeys_per_s": round(ni / ti / 1e9, 5), "query_gkeys_per_s": round(nq / tq / 1e9, 5)}
+    return t1 - t0, t2 - t1, keys.size, queries.size
 
 
 def run_reference(args, cfg):
@@ -754,37 +1025,53 @@ def run_reference(args, cfg):
     if cfg["kind"] in (3, 4):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned heavy-hitter split "
                           "and no batched multi-sketch path; its plain path is timed under --config zipf, "
-                          "uniform and mixed"}), flush=True)
+                          "uniform, mixed and cm"}), flush=True)
         return
     threads = os.cpu_count() or 1
-    ni = min(cfg["n_keys"], 1 << 24)
-    nq = min(cfg["n_query"], 1 << 21)
-    if cfg["kind"] == 1:
-        keys, distinct = host_zipf_keys(ni, cfg["n_ranks"], cfg["s"], 1000)
-        queries = distinct[:nq]
-    else:
-        keys = np.random.default_rng(1000).integers(0, 1 << 32, ni, dtype=np.uint64).astype(np.uint32)
-        queries = keys[:nq]
+    keys, queries, same = reference_inputs(cfg)
     for _ in range(args.warmup):
-        oracle_step(cfg, keys, queries, threads)
-    tot = 0.0
+        reference_step(cfg, keys, queries, threads)
+    tot, ti_s, tq_s = 0.0, 0.0, 0.0
     for _ in range(args.steps):
-        ti, tq = oracle_step(cfg, keys, queries, threads)
+        ti, tq, ni, nq = reference_step(cfg, keys, queries, threads)
         tot += ti + tq
+        ti_s += ti
+        tq_s += tq
     ms = tot * 1e3 / args.steps
     v = (ni + nq) / (ms * 1e6)
-    sample = (f"per step: clear + insert {ni} keys + query {nq} keys of the {cfg['workload']} stream; "
-              "CPU restatement of the reference path (oracle/oracle.cpp), bucket-partitioned threads")
+    path = ("count-min (oracle/oracle.cpp or_cm_insert_mt, relaxed atomic adds)" if cfg["kind"] == 5 else
+            "MSWS (oracle/oracle.cpp or_msws_insert_mt: one pass partitions the keys by bucket, then each "
+            "thread applies its part in array order)")
+    sample = (f"per step: a fresh sketch, insert {ni} keys, query {nq} keys of the {cfg['workload']} stream "
+              f"(the whole workload); CPU restatement of the reference path, {path}, queries split over the "
+              "threads")
     print(json.dumps({
         "metric": METRIC, "value": round(v, 5), "unit": "Gkeys/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic (numpy inverse-CDF Zipf / uniform)",
-        "config": {"workload": cfg["workload"], "n_low": cfg["n_low"], "n_high": cfg["n_high"]},
+        "vs_baseline": None, "dtype": "u32",
+        "data": ("synthetic: the GPU arm's rank-0 stream (libqsketch's seeded generator), copied to the host"
+                 if same else "synthetic: numpy stand-in of the stream's shape (no GPU to generate the same one)"),
+        "config": {"workload": cfg["workload"], "n_keys": int(ni), "n_query": int(nq), "n_low": cfg["n_low"],
+                   "n_high": cfg["n_high"], "same_config": bool(same)},
         "impl": "reference",
+        "insert_gkeys_per_s": round(ni * args.steps / ti_s / 1e9, 5),
+        "query_gkeys_per_s": round(nq * args.steps / tq_s / 1e9, 5),
         "cpu_baseline": {"value": round(v, 5), "unit": "Gkeys/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": round(v, 5), "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+def relaunch_ranks(n):
+    """`--gpus N` outside torchrun: start the N ranks (one process per GPU) through
+    torch.distributed.run on this node and wait for them."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
 
 
 def main():
@@ -795,10 +1082,14 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="zipf")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="the library's default insert knobs instead of the autotuner's (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     cfg = CONFIGS[args.config]
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch_ranks(args.gpus))
     if args.impl == "reference":
         run_reference(args, cfg)
     else:

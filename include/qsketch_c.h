@@ -200,7 +200,8 @@ typedef struct qs_profile {
      * qs_get_profile: invocations that found crossed buckets, and time per phase —
      * 8 filter build, 0 flag test (and staging of the records), 1 tile scan, 2 record
      * move, radix passes split into 6 tile digit counts, 7 digit scans and 3 scatters,
-     * 4 segments and totals, 5 replay; 9-11 unused. */
+     * 4 segments and totals, 5 replay, 9 link order (ranks, high buckets written);
+     * 10-11 unused.  qs_clear resets them too. */
     uint64_t repairs_active;
     double repair_phase_ms[12];
 } qs_profile;
@@ -246,9 +247,10 @@ qs_status qs_error_metrics(const uint32_t *d_est, const uint32_t *d_exact, size_
 
 /* Roofline probes: time `kind` (0 random sub-warp sector red with 3 words per sector,
  * 1 random 32 B sector load, 2 streaming read, 3 load + returning atomics, 4 returning
- * atomics with the index word, 5 load + red) over a device buffer of `bytes`, returning
- * operations per second (sectors/s or bytes/s for kind 2); kind 6 times `ops` grid-wide
- * barriers of the ordered replay's form (`bytes` unused) and returns barriers/s. */
+ * atomics with the index word, 5 load + red, 7 one red.add.u32 per lane, every lane its own
+ * random sector) over a device buffer of `bytes`, returning operations per second (sectors/s,
+ * or bytes/s for kind 2); kind 6 times `ops` grid-wide barriers of the ordered replay's form
+ * (`bytes` unused) and returns barriers/s. */
 qs_status qs_probe(uint32_t kind, uint64_t bytes, uint64_t ops, double *ops_per_s);
 
 /* ---- learned heavy-hitter split (no counterpart in the reference) ------------------------

@@ -5,8 +5,10 @@ package, as the checker.  It wraps oracle/liboracle.so (built from oracle.cpp by
 oracle/Makefile) and, when present, oracle/_ref/libqsref.so built from the reference's own
 library sources.  Parity status: the oracle's mask generator, seed draw, prime table and
 exact counter are pinned bit-for-bit against the reference's code (tests/golden/); the MSWS
-insert/query restatement is pinned by hand-worked known-answer cases derived from
-device_sketch_v3.h (the reference ships no golden vectors for it).
+and count-min insert/query restatements are pinned against the reference's own sketch
+kernels run on a GPU (tests/test_ref_pin_gpu.py, on inputs where the reference's result does
+not depend on the thread schedule) and by hand-worked known-answer cases derived from
+device_sketch_v3.h for the order-dependent part (the reference ships no golden vectors).
 """
 import ctypes
 import os
@@ -39,6 +41,7 @@ def _load():
         "or_msws_insert_mt": (None, [P, P, U64, ctypes.c_int]),
         "or_msws_query": (None, [P, P, U64, P]),
         "or_cm_insert": (None, [P, U64, U32, P, P, U64]),
+        "or_cm_insert_mt": (None, [P, U64, U32, P, P, U64, ctypes.c_int]),
         "or_cm_query": (None, [P, U64, U32, P, P, U64, P]),
         "or_exact_counts": (None, [P, U64, P, U64, P]),
         "or_error_metrics": (None, [P, P, U64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
@@ -126,9 +129,13 @@ class CountMin:
         self.m = self.seeds.size
         self.table = np.zeros(n * self.m, np.uint32)
 
-    def insert(self, keys):
+    def insert(self, keys, threads=1):
         k = _u32(keys)
-        lib.or_cm_insert(self.table.ctypes.data, self.n, self.m, self.seeds.ctypes.data, k.ctypes.data, k.size)
+        if threads > 1:
+            lib.or_cm_insert_mt(self.table.ctypes.data, self.n, self.m, self.seeds.ctypes.data, k.ctypes.data,
+                                k.size, threads)
+        else:
+            lib.or_cm_insert(self.table.ctypes.data, self.n, self.m, self.seeds.ctypes.data, k.ctypes.data, k.size)
 
     def query(self, keys):
         k = _u32(keys)

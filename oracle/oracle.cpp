@@ -25,8 +25,9 @@
 // Decisions where the reference is racy or unbounded (identical in the GPU path):
 //   * the high pool is bounded: a link needs (id - 1024) < n_high; when it is full the
 //     bucket becomes SATURATED (word 7 = 2): its keys are dropped and counted, its query
-//     is the frozen low minimum.  Which buckets saturate depends on the global order of
-//     allocation, so results under exhaustion are only compared through the status.
+//     is the frozen low minimum.  Ids go out in the array order of the keys that switch
+//     buckets, so which buckets saturate is defined by the key order (the GPU path hands
+//     them out in the same order).
 //   * compat_v3 = 1 reproduces device_sketch_v3.h:187 (the linking key's high increments
 //     land on index bit % 8); compat_v3 = 0 uses the bit's own index, as the later
 //     device_sketch_v32.h:175 and the paper's Algorithm 4 do.
@@ -156,27 +157,64 @@ void or_msws_insert(or_msws* s, const uint32_t* keys, uint64_t n) {
     for (uint64_t i = 0; i < n; ++i) msws_insert_one(s, keys[i], nullptr);
 }
 
-// Bucket-partitioned parallel insert: thread t applies, in stream order, the keys whose
-// bucket satisfies b % T == t.  Per-bucket order is the stream order, so the result equals
-// the sequential one (high ids differ; query results do not unless the pool runs out).
+// Bucket-partitioned parallel insert, one pass over the keys: T threads each take a
+// contiguous block of the keys and count them by partition (bucket % T); after a prefix over
+// (partition, block) they scatter their keys into per-partition lists, which keep array
+// order; then thread t applies partition t's list.  Per-bucket order is the array order, so
+// the tables equal the sequential ones except for the high ids (allocation interleaves
+// across threads) and, once the pool runs out, which buckets get one.
 void or_msws_insert_mt(or_msws* s, const uint32_t* keys, uint64_t n, int threads) {
-    if (threads <= 1) { or_msws_insert(s, keys, n); return; }
-    std::atomic<uint32_t> next(s->next_id);
-    std::vector<or_msws> local(threads, *s);
-    std::vector<std::thread> th;
-    for (int t = 0; t < threads; ++t) {
-        th.emplace_back([&, t] {
-            or_msws* ls = &local[t];
-            ls->dropped = 0;
-            ls->pool_full = 0;
-            for (uint64_t i = 0; i < n; ++i) {
-                const uint32_t hv = keys[i] * s->seed;
-                if ((hv % s->n_low) % (uint64_t)threads != (uint64_t)t) continue;
-                msws_insert_one(ls, keys[i], &next);
-            }
-        });
+    if (threads <= 1 || n < (1u << 16)) { or_msws_insert(s, keys, n); return; }
+    const uint32_t T = (uint32_t)threads;
+    auto part = [&](uint32_t k) { return (uint32_t)((uint64_t)(uint32_t)(k * s->seed) % s->n_low % T); };
+    std::vector<uint64_t> cnt((size_t)T * T, 0);  // [block][partition]
+    std::vector<uint32_t> list(n);
+    auto block = [&](uint32_t b, uint64_t& lo, uint64_t& hi) { lo = n * b / T; hi = n * (b + 1) / T; };
+    {
+        std::vector<std::thread> th;
+        for (uint32_t b = 0; b < T; ++b)
+            th.emplace_back([&, b] {
+                uint64_t lo, hi;
+                block(b, lo, hi);
+                uint64_t* c = &cnt[(size_t)b * T];
+                for (uint64_t i = lo; i < hi; ++i) ++c[part(keys[i])];
+            });
+        for (auto& x : th) x.join();
     }
-    for (auto& x : th) x.join();
+    std::vector<uint64_t> off((size_t)T * T), pbeg(T + 1, 0);  // off[block][partition]
+    uint64_t run = 0;
+    for (uint32_t p = 0; p < T; ++p) {
+        pbeg[p] = run;
+        for (uint32_t b = 0; b < T; ++b) {
+            off[(size_t)b * T + p] = run;
+            run += cnt[(size_t)b * T + p];
+        }
+    }
+    pbeg[T] = run;
+    {
+        std::vector<std::thread> th;
+        for (uint32_t b = 0; b < T; ++b)
+            th.emplace_back([&, b] {
+                uint64_t lo, hi;
+                block(b, lo, hi);
+                uint64_t* o = &off[(size_t)b * T];
+                for (uint64_t i = lo; i < hi; ++i) list[o[part(keys[i])]++] = keys[i];
+            });
+        for (auto& x : th) x.join();
+    }
+    std::atomic<uint32_t> next(s->next_id);
+    std::vector<or_msws> local(T, *s);
+    {
+        std::vector<std::thread> th;
+        for (uint32_t t = 0; t < T; ++t)
+            th.emplace_back([&, t] {
+                or_msws* ls = &local[t];
+                ls->dropped = 0;
+                ls->pool_full = 0;
+                for (uint64_t i = pbeg[t]; i < pbeg[t + 1]; ++i) msws_insert_one(ls, list[i], &next);
+            });
+        for (auto& x : th) x.join();
+    }
     uint32_t nid = next.load();
     uint64_t cap = START + s->n_high;
     s->next_id = nid > cap ? (uint32_t)cap : nid;
@@ -208,6 +246,22 @@ void or_cm_insert(uint32_t* table, uint64_t n, uint32_t m, const uint32_t* seeds
                   uint64_t nk) {
     for (uint64_t i = 0; i < nk; ++i)
         for (uint32_t j = 0; j < m; ++j) table[j * n + (uint32_t)(keys[i] * seeds[j]) % n] += 1;
+}
+
+// The same with T threads over contiguous blocks of the keys, relaxed atomic increments (the
+// additions commute, so the table equals the sequential one).
+void or_cm_insert_mt(uint32_t* table, uint64_t n, uint32_t m, const uint32_t* seeds, const uint32_t* keys,
+                     uint64_t nk, int threads) {
+    if (threads <= 1) { or_cm_insert(table, n, m, seeds, keys, nk); return; }
+    std::vector<std::thread> th;
+    for (int b = 0; b < threads; ++b)
+        th.emplace_back([=] {
+            const uint64_t lo = nk * b / threads, hi = nk * (b + 1) / threads;
+            for (uint64_t i = lo; i < hi; ++i)
+                for (uint32_t j = 0; j < m; ++j)
+                    __atomic_fetch_add(&table[j * n + (uint32_t)(keys[i] * seeds[j]) % n], 1u, __ATOMIC_RELAXED);
+        });
+    for (auto& x : th) x.join();
 }
 
 void or_cm_query(const uint32_t* table, uint64_t n, uint32_t m, const uint32_t* seeds, const uint32_t* keys,

@@ -250,6 +250,10 @@ __global__ void k_probe(uint32_t kind, uint32_t* buf, uint64_t nsec, uint64_t no
                 const uint32_t v = __ldcg(buf + s * 8 + 7);
                 if (w < 3 && v != 0xdeadbeefu) acc += atomicAdd(buf + s * 8 + word, 1u);
             }
+        } else if (kind == 7) {  // every lane its own random sector, one red per lane
+            const uint32_t h = probe_mix((uint32_t)i);
+            const uint64_t s = ((uint64_t)h * nsec) >> 32;
+            atomicAdd(buf + s * 8 + (h >> 29), 1u);
         } else if (kind == 1) {
             const uint32_t h = probe_mix((uint32_t)i);
             const uint64_t s = ((uint64_t)h * nsec) >> 32;
@@ -309,7 +313,7 @@ cudaError_t probe_barrier(uint64_t ops, double* ops_per_s) {
 
 cudaError_t probe(uint32_t kind, uint64_t bytes, uint64_t ops, double* ops_per_s) {
     if (kind == 6) return ops ? probe_barrier(ops, ops_per_s) : cudaErrorInvalidValue;
-    if (kind > 5 || bytes < 64) return cudaErrorInvalidValue;
+    if (kind > 7 || kind == 6 || bytes < 64) return cudaErrorInvalidValue;
     uint32_t* buf = nullptr;
     uint32_t* sink = nullptr;
     cudaEvent_t a = nullptr, b = nullptr;
@@ -320,7 +324,7 @@ cudaError_t probe(uint32_t kind, uint64_t bytes, uint64_t ops, double* ops_per_s
     if (e == cudaSuccess) e = cudaEventCreate(&b);
     const uint64_t nsec = bytes / 32;
     if (kind == 2) ops = nsec * 2 * 4;  // four passes of 16 B loads
-    const uint64_t thread_ops = (kind == 0 || kind >= 3) ? ops * 8 : ops;
+    const uint64_t thread_ops = (kind == 0 || (kind >= 3 && kind <= 5)) ? ops * 8 : ops;  // 8 lanes per sector
     float best = 1e30f;
     if (e == cudaSuccess) {
         int dev = 0, sms = 148;

@@ -41,3 +41,19 @@ def test_reference_arm_under_torchrun_prints_once():
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
     assert len(lines) == 1 and lines[0]["impl"] == "reference"
+
+
+def test_gpus_flag_without_torchrun_starts_the_ranks():
+    # `--gpus 2` outside torchrun starts two ranks itself; rank 0 prints one line for 2 GPUs
+    r = run("--impl", "reference", "--config", "uniform", "--gpus", "2", "--steps", "1", "--warmup", "3")
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1 and lines[0]["n_gpus"] == 2 and lines[0]["impl"] == "reference"
+    assert lines[0]["config"]["n_keys"] == 1 << 24 and lines[0]["config"]["n_query"] == 1 << 24
+
+
+def test_reference_arm_count_min():
+    r = run("--impl", "reference", "--config", "cm", "--steps", "1", "--warmup", "3")
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["cpu_baseline"]["cores"] >= 1
