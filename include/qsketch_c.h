@@ -253,6 +253,16 @@ qs_status qs_error_metrics(const uint32_t *d_est, const uint32_t *d_exact, size_
  * (`bytes` unused) and returns barriers/s. */
 qs_status qs_probe(uint32_t kind, uint64_t bytes, uint64_t ops, double *ops_per_s);
 
+/* Failure paths, for tests (no counterpart in the reference):
+ * qs_probe kind 8 launches one grid-wide barrier that block 0 never reaches, with every
+ * other block's wait bounded by `ops` polls (~128 ns each, at most the ~1 s of the sketch
+ * kernels' waits): it returns QS_ERR_TIMEOUT when the waits give up, as they must, and the
+ * context stays usable.
+ * qs_test_fail_allocations(k) makes the library's (k+1)-th device allocation from now on fail
+ * as if the device were out of memory (qs_create then returns QS_ERR_OOM and frees what it
+ * had allocated); -1 turns it off.  One failure per call. */
+void qs_test_fail_allocations(int32_t after);
+
 /* ---- learned heavy-hitter split (no counterpart in the reference) ------------------------
  * An MLP 32 -> 128 -> 128 -> 1 over the key's bits (BF16 weights, FP32 accumulation on the
  * tensor cores, weighted binary cross-entropy, Adam) decides which keys are heavy.  The

@@ -182,6 +182,7 @@ SIGNATURES = {
     "qs_rank_histogram": (_I, [_P, _SZ, _P, _U64, _P]),
     "qs_error_metrics": (_I, [_P, _P, _SZ, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _P]),
     "qs_probe": (_I, [_U32, _U64, _U64, ctypes.POINTER(ctypes.c_double)]),
+    "qs_test_fail_allocations": (None, [ctypes.c_int32]),
     "qs_msws_insert_noalloc": (_I, [_P, _U64, _P, _U64, _P, _P, _U32, _U32, _U32, _P, _SZ, _P]),
     "qs_autotune": (_I, [ctypes.POINTER(qs_params), _P, _SZ, _U32, ctypes.POINTER(qs_tune_config), _P, _U32,
                          ctypes.POINTER(_U32)]),

@@ -1,6 +1,7 @@
 // qs_api.cu — the C ABI (include/qsketch_c.h): sketch construction, host-side table
 // preparation (seeds, hash masks, prime sizing) and the stream-ordered launch sequence.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -62,6 +63,10 @@ const uint64_t kPrimes[] = {402653171, 268435399, 201326557, 134217689, 10066329
                             6143,      4093,      3067,      2039,      1531,      1021,     761,      509,
                             383,       251,       191,       127,       89,        61,       47,       31,
                             23,        13,        11,        7,         5,         3,        2};
+
+// Allocation-failure injection (qs_test_fail_allocations): the allocation after this many
+// more fails as if the device were out of memory; -1 = off.
+std::atomic<int32_t> g_fail_alloc_after{-1};
 
 // Autotuner table: the fastest pass-1 setting per size class floor(log2(n_low)).
 std::mutex g_tune_mu;
@@ -132,6 +137,10 @@ struct qs_sketch {
     cudaError_t alloc(T** ptr, size_t count) {
         void* v = nullptr;
         const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+        if (g_fail_alloc_after.load() >= 0 && g_fail_alloc_after.fetch_sub(1) == 0) {
+            g_fail_alloc_after.store(-1);
+            return cudaErrorMemoryAllocation;  // injected (qs_test_fail_allocations)
+        }
         cudaError_t e = cudaMalloc(&v, bytes);
         if (e != cudaSuccess) return e;
         allocs.push_back(v);
@@ -756,9 +765,14 @@ qs_status qs_error_metrics(const uint32_t* d_est, const uint32_t* d_exact, size_
 
 qs_status qs_probe(uint32_t kind, uint64_t bytes, uint64_t ops, double* ops_per_s) {
     if (!ops_per_s) return fail(QS_ERR_INVALID_ARG, "probe: null output");
-    CK(probe(kind, bytes, ops, ops_per_s), "probe");
+    const cudaError_t e = probe(kind, bytes, ops, ops_per_s);
+    if (e == cudaErrorLaunchTimeout && (kind == 6 || kind == 8))
+        return fail(QS_ERR_TIMEOUT, "probe: a bounded grid-barrier wait gave up");
+    CK(e, "probe");
     return QS_OK;
 }
+
+void qs_test_fail_allocations(int32_t after) { g_fail_alloc_after.store(after); }
 
 }  // extern "C"
 

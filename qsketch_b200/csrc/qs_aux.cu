@@ -276,6 +276,38 @@ __global__ void __launch_bounds__(512) k_probe_barrier(Ctl* ctl, uint64_t nops) 
         if (!grid_barrier(ctl)) return;
 }
 
+// kind 8 (failure path): one barrier that block 0 never reaches, waited for at most `limit`
+// polls; every other block gives up, latches ST_TIMEOUT and returns.
+__global__ void __launch_bounds__(512) k_probe_barrier_absent(Ctl* ctl, uint32_t limit) {
+    if (blockIdx.x == 0) return;
+    grid_barrier(ctl, limit);
+}
+
+// Launch kind 8 and report its latched status: cudaErrorLaunchTimeout when the waits gave up
+// (the expected outcome), cudaSuccess if they did not.
+cudaError_t probe_barrier_timeout(uint64_t limit) {
+    Ctl* ctl = nullptr;
+    int dev = 0, sms = 148, occ = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_probe_barrier_absent, 512, 0);
+    if (e == cudaSuccess && occ < 1) e = cudaErrorInvalidConfiguration;
+    if (e == cudaSuccess) e = cudaMalloc(&ctl, sizeof(Ctl));
+    if (e == cudaSuccess) e = cudaMemset(ctl, 0, sizeof(Ctl));
+    uint32_t lim = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(limit, 1), SPIN_LIMIT);
+    if (e == cudaSuccess) {
+        void* args[] = {&ctl, &lim};
+        e = cudaLaunchCooperativeKernel((const void*)k_probe_barrier_absent, dim3(sms * std::min(occ, 2)), dim3(512),
+                                        args, 0, nullptr);
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    Ctl h{};
+    if (e == cudaSuccess) e = cudaMemcpy(&h, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && (h.status & ST_TIMEOUT)) e = cudaErrorLaunchTimeout;
+    if (ctl) cudaFree(ctl);
+    return e;
+}
+
 cudaError_t probe_barrier(uint64_t ops, double* ops_per_s) {
     Ctl* ctl = nullptr;
     cudaEvent_t a = nullptr, b = nullptr;
@@ -313,6 +345,10 @@ cudaError_t probe_barrier(uint64_t ops, double* ops_per_s) {
 
 cudaError_t probe(uint32_t kind, uint64_t bytes, uint64_t ops, double* ops_per_s) {
     if (kind == 6) return ops ? probe_barrier(ops, ops_per_s) : cudaErrorInvalidValue;
+    if (kind == 8) {
+        *ops_per_s = 0.0;
+        return probe_barrier_timeout(ops);
+    }
     if (kind > 7 || kind == 6 || bytes < 64) return cudaErrorInvalidValue;
     uint32_t* buf = nullptr;
     uint32_t* sink = nullptr;

@@ -71,7 +71,7 @@ __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
     return v;
 }
 
-__device__ __forceinline__ bool grid_barrier(Ctl* ctl) {
+__device__ __forceinline__ bool grid_barrier(Ctl* ctl, uint32_t limit = SPIN_LIMIT) {
     __shared__ int s_ok;
     uint32_t gen = 0;
     if (threadIdx.x == 0) gen = ld_acquire_gpu(&ctl->bar_gen);
@@ -86,7 +86,7 @@ __device__ __forceinline__ bool grid_barrier(Ctl* ctl) {
         } else {
             uint32_t it = 0;
             while (ld_acquire_gpu(&ctl->bar_gen) == gen) {
-                if (++it > SPIN_LIMIT) {
+                if (++it > limit) {
                     ok = 0;
                     atomicOr(&ctl->status, ST_TIMEOUT);
                     break;

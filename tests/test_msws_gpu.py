@@ -347,11 +347,11 @@ def test_chunk_ramp_on_and_off_bit_exact(gpu, ramp):
 def test_roofline_probes_report_rates(gpu):
     # The bench's denominators: random-sector atomics, loads, a streaming read and the replay's
     # grid barrier all return positive rates; invalid kinds are refused.
-    for kind in (0, 1, 2, 3, 4, 5):
+    for kind in (0, 1, 2, 3, 4, 5, 7):
         assert data.probe(kind, 64 << 20, 1 << 22) > 0
     assert data.probe(6, 64, 1000) > 1e4  # barriers per second
     with pytest.raises(qs.QsError):
-        data.probe(7, 64 << 20)
+        data.probe(9, 64 << 20)
 
 
 def test_replay_with_more_records_than_resident_tiles(gpu):
