@@ -244,6 +244,8 @@ def run_ours(args, cfg):
         return run_batched(args, cfg)
     if cfg["kind"] == 5:
         return run_cm(args, cfg)
+    if args.shard:
+        return run_sharded(args, cfg)
     world, rank, local, barrier, max_over_ranks = init_ranks(args)
 
     stream = torch.cuda.current_stream()
@@ -473,6 +475,87 @@ def run_ours(args, cfg):
             line["cpu_baseline"] = cpu_baseline(cfg, keys.cpu().numpy(), queries.cpu().numpy())
         print(json.dumps(line), flush=True)
     sk.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_sharded(args, cfg):
+    """`--shard`: one sketch sharded by bucket over the N ranks (qsketch_b200/sharded.py),
+    strong scaling: the configuration's stream is split into N consecutive parts, rank r
+    inserting part r and querying part r of the distinct keys; every insert and query routes
+    the keys to their owner shards with an all-to-all (NCCL).  The estimates equal one sketch
+    fed the whole stream in order."""
+    import torch
+    import torch.distributed as dist
+
+    from qsketch_b200 import data
+    from qsketch_b200.sharded import ShardedSketch
+
+    if cfg["kind"] not in (0, 1):
+        raise SystemExit("--shard runs the zipf, zipf_prof and uniform configurations")
+    world, rank, local, barrier, max_over_ranks = init_ranks(args)
+    stream = torch.cuda.current_stream()
+    n, nq = cfg["n_keys"], cfg["n_query"]
+    lo, hi = n * rank // world, n * (rank + 1) // world
+    qlo, qhi = nq * rank // world, nq * (rank + 1) // world
+    if cfg["kind"] == 1:
+        keys = data.zipf_keys(n, cfg["n_ranks"], cfg["s"], seed=1000, perm_seed=99)[lo:hi].clone()
+        queries = data.rank_keys(99, qlo, qhi - qlo)
+    else:
+        keys = data.uniform_keys(n, seed=1000)[lo:hi].clone()
+        queries = keys[qlo - lo:qhi - lo].clone() if qhi <= hi else data.uniform_keys(n, seed=1000)[qlo:qhi].clone()
+    torch.cuda.empty_cache()
+    ss = ShardedSketch(cfg["n_low"], cfg["n_high"], hash_seed=SEED, mask_rng=1)
+
+    def step():
+        ss.local.clear()
+        ss.insert(keys)
+        return ss.search(queries)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for _ in range(args.steps):
+            out = step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms_per_step = max_over_ranks(t0.elapsed_time(t1)) / args.steps
+    hk, hq = keys.cpu().pin_memory(), queries.cpu().pin_memory()
+    ho = torch.empty(queries.numel(), dtype=torch.uint32).pin_memory()
+    dk, dq = torch.empty_like(keys), torch.empty_like(queries)
+    ss.local.clear()
+    torch.cuda.synchronize()
+    barrier()
+    w0 = time.perf_counter()
+    dk.copy_(hk, non_blocking=True)
+    ss.insert(dk)
+    dq.copy_(hq, non_blocking=True)
+    ho.copy_(ss.search(dq), non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks((time.perf_counter() - w0) * 1e3)
+    assert torch.equal(ho.cuda(), out), "host-buffer estimates differ from the device path"
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": round((n + nq) / (ms_per_step * 1e6), 4), "unit": "Gkeys/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic: the configuration's seeded stream, split into one consecutive part per rank",
+            "config": {"workload": cfg["workload"], "n_keys": n, "n_query": nq, "n_low": cfg["n_low"],
+                       "n_high_per_shard": cfg["n_high"], "parallelism": f"bucket-sharded over {world} GPU(s), "
+                       "keys routed by one all-to-all per insert and two per query (NCCL)"},
+            "e2e": {"value": round((n + nq) / (e2e_ms * 1e6), 4), "unit": "Gkeys/s",
+                    "h2d_bytes_per_step": (n + nq) * 4, "d2h_bytes_per_step": nq * 4, "ms_per_step": round(e2e_ms, 3),
+                    "api": "ShardedSketch.insert + search"},
+            "gpu_launches": None,
+            "clocks": clk.summary(),
+        }), flush=True)
+    ss.local.close()
     if world > 1:
         dist.destroy_process_group()
 
@@ -1082,6 +1165,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="zipf")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--shard", action="store_true",
+                    help="one sketch sharded by bucket over the N GPUs (strong scaling) instead of N replicas")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="the library's default insert knobs instead of the autotuner's (profiling runs)")
     args = ap.parse_args()

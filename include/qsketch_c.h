@@ -419,6 +419,24 @@ qs_status qs_batch_get_info(qs_batch *b, qs_batch_info *out);
  * (eager calls are timed per launch: insert = pass 1, repair, query); owned by the batch. */
 qs_sketch *qs_batch_arena(qs_batch *b);
 
+/* ---- bucket-sharded sketch across GPUs: routing (no counterpart in the reference) --------
+ * A key's whole MSWS state is one low bucket and the high bucket it may link to
+ * (device_sketch_v3.h:228, :119, :185), so a sketch shards by bucket: bucket b = hv % n_low
+ * (hv = key * hash_seed) belongs to shard floor(b * n_shards / n_low), n_shards contiguous
+ * ranges.  qs_shard_partition reorders a device batch by owner shard, stably (each
+ * shard's keys keep their array order), writes each shard's key count to d_shard_counts
+ * (device, n_shards u32) and, if d_perm is not null, each output key's index in the batch;
+ * d_scratch holds qs_shard_scratch_words(n, n_shards) u32.  The parts go to their owners with
+ * one all-to-all (qsketch_b200/sharded.py); estimates come back the same way and
+ * qs_shard_unpartition puts them at their array positions (d_out[d_perm[i]] = d_in[i]).
+ * n_shards <= 32. */
+size_t qs_shard_scratch_words(size_t n, uint32_t n_shards);
+qs_status qs_shard_partition(const uint32_t *d_keys, size_t n, uint32_t hash_seed, uint64_t n_low,
+                             uint32_t n_shards, uint32_t *d_out, uint32_t *d_perm, uint32_t *d_scratch,
+                             uint32_t *d_shard_counts, void *stream);
+qs_status qs_shard_unpartition(const uint32_t *d_in, const uint32_t *d_perm, size_t n, uint32_t *d_out,
+                               void *stream);
+
 /* ---- MSWS insert for callers that cannot allocate device memory ------------------------
  * No counterpart in the reference: its classes allocate their own tables
  * (device_sketch.h:83-114) and the harness allocates key buffers per batch.

@@ -183,6 +183,9 @@ SIGNATURES = {
     "qs_error_metrics": (_I, [_P, _P, _SZ, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _P]),
     "qs_probe": (_I, [_U32, _U64, _U64, ctypes.POINTER(ctypes.c_double)]),
     "qs_test_fail_allocations": (None, [ctypes.c_int32]),
+    "qs_shard_scratch_words": (_SZ, [_SZ, _U32]),
+    "qs_shard_partition": (_I, [_P, _SZ, _U32, _U64, _U32, _P, _P, _P, _P, _P]),
+    "qs_shard_unpartition": (_I, [_P, _P, _SZ, _P, _P]),
     "qs_msws_insert_noalloc": (_I, [_P, _U64, _P, _U64, _P, _P, _U32, _U32, _U32, _P, _SZ, _P]),
     "qs_autotune": (_I, [ctypes.POINTER(qs_params), _P, _SZ, _U32, ctypes.POINTER(qs_tune_config), _P, _U32,
                          ctypes.POINTER(_U32)]),
