@@ -173,6 +173,20 @@ qs_status qs_insert(qs_sketch *sk, const uint32_t *d_keys, size_t n, void *strea
 qs_status qs_query(qs_sketch *sk, const uint32_t *d_keys, size_t n, uint32_t *d_counts,
                    void *stream);
 
+/* REMOVE (no code in the reference; its paper defines deletion as the insertion with a
+ * subtraction, doc/main.tex:232).  d_keys: device pointer to n uint32 keys, one occurrence of
+ * each taken out.  MSWS: where the key's bucket is linked, its selected high counters lose
+ * one, else its selected 8-bit low counters lose one, each floored at 0; a saturated bucket
+ * drops the removal (counted in dropped_keys).  Removals never link or unlink a bucket, so
+ * the result of a call does not depend on the order of its keys, and a call is ordered after
+ * and before the sketch's other calls on the stream.  Count-min: each row's counter loses
+ * one, floored at 0.  A removal of a key that was never inserted lowers the estimates of the
+ * keys sharing its counters (as in any count-min with deletions); and for MSWS, one whose
+ * earlier occurrences were counted in the low level before its bucket linked lowers the high
+ * counters instead.  Contended counters are updated by compare-and-swap loops bounded to
+ * 2^22 tries (QS_ERR_TIMEOUT if one gives up). */
+qs_status qs_remove(qs_sketch *sk, const uint32_t *d_keys, size_t n, void *stream);
+
 /* Host-buffer variants: keys / counts in host memory (pinned or pageable).  The copies
  * run chunked and overlapped with the kernels on internal streams; the call returns
  * when the results are in h_counts (query) or the keys are consumed (insert). */

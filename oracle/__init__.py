@@ -40,6 +40,8 @@ def _load():
         "or_msws_insert": (None, [P, P, U64]),
         "or_msws_insert_mt": (None, [P, P, U64, ctypes.c_int]),
         "or_msws_query": (None, [P, P, U64, P]),
+        "or_msws_remove": (None, [P, P, U64]),
+        "or_cm_remove": (None, [P, U64, U32, P, P, U64]),
         "or_cm_insert": (None, [P, U64, U32, P, P, U64]),
         "or_cm_insert_mt": (None, [P, U64, U32, P, P, U64, ctypes.c_int]),
         "or_cm_query": (None, [P, U64, U32, P, P, U64, P]),
@@ -107,6 +109,10 @@ class Msws:
         lib.or_msws_query(ctypes.byref(self.s), k.ctypes.data, k.size, out.ctypes.data)
         return out
 
+    def remove(self, keys):
+        k = _u32(keys)
+        lib.or_msws_remove(ctypes.byref(self.s), k.ctypes.data, k.size)
+
     @property
     def next_id(self):
         return self.s.next_id
@@ -136,6 +142,10 @@ class CountMin:
                                 k.size, threads)
         else:
             lib.or_cm_insert(self.table.ctypes.data, self.n, self.m, self.seeds.ctypes.data, k.ctypes.data, k.size)
+
+    def remove(self, keys):
+        k = _u32(keys)
+        lib.or_cm_remove(self.table.ctypes.data, self.n, self.m, self.seeds.ctypes.data, k.ctypes.data, k.size)
 
     def query(self, keys):
         k = _u32(keys)

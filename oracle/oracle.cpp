@@ -221,6 +221,44 @@ void or_msws_insert_mt(or_msws* s, const uint32_t* keys, uint64_t n, int threads
     for (auto& ls : local) { s->dropped += ls.dropped; s->pool_full |= ls.pool_full; }
 }
 
+// REMOVE (no code in the reference; the paper defines deletion as insertion with a
+// subtraction, doc/main.tex:232): per key in array order, the bucket's level decides where
+// the key's selected counters lose one, each floored at 0 — the high counters when the bucket
+// is linked, else the low 8-bit counters; a saturated bucket drops the removal (counted).
+// Removals never link or unlink a bucket, so within one remove call the result per counter
+// is max(0, value - removals) whatever the order.
+void or_msws_remove(or_msws* s, const uint32_t* keys, uint64_t n) {
+    for (uint64_t k = 0; k < n; ++k) {
+        const uint32_t hv = keys[k] * s->seed;
+        const uint64_t b = hv % s->n_low;
+        const uint32_t mask = s->masks[hv % s->n_masks];
+        uint32_t* w = s->low + b * W;
+        const uint32_t ptr = w[7];
+        if (ptr == SATURATED) { ++s->dropped; continue; }
+        if (ptr > START) {
+            uint32_t* h = s->high + (uint64_t)(ptr - START) * HW;
+            for (uint32_t m = mask; m; m &= m - 1) {
+                uint32_t& c = h[__builtin_ctz(m)];
+                if (c) --c;
+            }
+            continue;
+        }
+        for (uint32_t m = mask; m; m &= m - 1) {
+            const int i = __builtin_ctz(m);
+            if (low_byte(w, i)) w[i >> 2] -= 1u << (8 * (i & 3));
+        }
+    }
+}
+
+// Count-min REMOVE: each row's counter loses one, floored at 0.
+void or_cm_remove(uint32_t* table, uint64_t n, uint32_t m, const uint32_t* seeds, const uint32_t* keys, uint64_t nk) {
+    for (uint64_t i = 0; i < nk; ++i)
+        for (uint32_t j = 0; j < m; ++j) {
+            uint32_t& c = table[j * n + (uint32_t)(keys[i] * seeds[j]) % n];
+            if (c) --c;
+        }
+}
+
 void or_msws_query(const or_msws* s, const uint32_t* keys, uint64_t n, uint32_t* out) {
     for (uint64_t k = 0; k < n; ++k) {
         const uint32_t hv = keys[k] * s->seed;

@@ -165,6 +165,7 @@ SIGNATURES = {
     "qs_create": (_I, [ctypes.POINTER(qs_params), ctypes.POINTER(_P)]),
     "qs_destroy": (_I, [_P]),
     "qs_insert": (_I, [_P, _P, _SZ, _P]),
+    "qs_remove": (_I, [_P, _P, _SZ, _P]),
     "qs_query": (_I, [_P, _P, _SZ, _P, _P]),
     "qs_insert_host": (_I, [_P, _P, _SZ]),
     "qs_query_host": (_I, [_P, _P, _SZ, _P]),

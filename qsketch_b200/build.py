@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libqsketch.so")
 SOURCES = ["qs_msws.cu", "qs_cm.cu", "qs_aux.cu", "qs_api.cu", "qs_noalloc.cu", "qs_mlp.cu", "qs_learned.cu",
-           "qs_shard.cu"]
+           "qs_shard.cu", "qs_remove.cu"]
 HEADERS = ["qs_common.cuh", "qs_device.cuh", "qs_kernels.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

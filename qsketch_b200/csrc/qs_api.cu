@@ -195,7 +195,7 @@ void draw_seeds(uint32_t rng_seed, size_t count, uint32_t* out) {
 
 qs_status check_status_word(qs_sketch* sk) {
     Ctl c;
-    if (sk->kind != QS_KIND_MSWS) return QS_OK;
+    if (!sk->D.ctl) return QS_OK;
     cudaError_t e = cudaMemcpy(&c, sk->D.ctl, sizeof c, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "read status");
     if (c.status & ST_TIMEOUT) return fail(QS_ERR_TIMEOUT, "a bounded device wait timed out");
@@ -497,6 +497,7 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         C.rows = rows;
         for (uint32_t j = 0; j < rows; ++j) C.seeds[j] = sk->seeds[j];
         CKB(sk->alloc(&C.table, n * rows), "alloc cm table");
+        CKB(sk->alloc(&sk->D.ctl, 1), "alloc control");  // status word (bounded remove loops)
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         sk->cm_grid = sms * 8;
@@ -535,6 +536,20 @@ qs_status qs_insert(qs_sketch* sk, const uint32_t* d_keys, size_t n, void* strea
     if ((reinterpret_cast<uintptr_t>(d_keys) & 3u) != 0) return fail(QS_ERR_INVALID_ARG, "keys not 4-byte aligned");
     DeviceGuard guard(sk->device);
     return insert_device(sk, d_keys, n, static_cast<cudaStream_t>(stream));
+}
+
+qs_status qs_remove(qs_sketch* sk, const uint32_t* d_keys, size_t n, void* stream) {
+    if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
+    if (n == 0) return QS_OK;
+    if (!d_keys) return fail(QS_ERR_INVALID_ARG, "null keys");
+    if ((reinterpret_cast<uintptr_t>(d_keys) & 3u) != 0) return fail(QS_ERR_INVALID_ARG, "keys not 4-byte aligned");
+    DeviceGuard guard(sk->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (sk->kind == QS_KIND_MSWS)
+        CK(msws_remove(d_keys, n, sk->D, sk->L, st), "msws remove");
+    else
+        CK(cm_remove(d_keys, n, sk->C, sk->cm_grid, sk->D.ctl ? &sk->D.ctl->status : nullptr, st), "cm remove");
+    return QS_OK;
 }
 
 qs_status qs_query(qs_sketch* sk, const uint32_t* d_keys, size_t n, uint32_t* d_counts, void* stream) {
@@ -678,7 +693,7 @@ qs_status qs_get_profile(qs_sketch* sk, qs_profile* out) {
 
 qs_status qs_reset_status(qs_sketch* sk) {
     if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
-    if (sk->kind != QS_KIND_MSWS) return QS_OK;
+    if (!sk->D.ctl) return QS_OK;
     DeviceGuard guard(sk->device);
     CK(cudaDeviceSynchronize(), "sync");
     CK(cudaMemset(&sk->D.ctl->status, 0, 4), "reset status");

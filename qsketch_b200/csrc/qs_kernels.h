@@ -40,6 +40,10 @@ cudaError_t msws_query(const uint32_t* d_keys, uint64_t n, uint32_t* d_out, cons
                        cudaStream_t st);
 
 cudaError_t cm_insert(const uint32_t* d_keys, uint64_t n, const CmDev& D, int agg, int grid, cudaStream_t st);
+// REMOVE (qs_remove.cu): one occurrence of each key out, counters floored at 0.
+cudaError_t msws_remove(const uint32_t* d_keys, uint64_t n, const MswsDev& D, const MswsLaunch& L, cudaStream_t st);
+cudaError_t cm_remove(const uint32_t* d_keys, uint64_t n, const CmDev& D, int grid, uint32_t* d_status,
+                      cudaStream_t st);
 cudaError_t cm_query(const uint32_t* d_keys, uint64_t n, uint32_t* d_out, const CmDev& D, int grid, cudaStream_t st);
 
 cudaError_t gen_keys(uint32_t kind, uint64_t seed, uint64_t n_ranks, double s, uint64_t perm_seed, uint32_t* d_keys,

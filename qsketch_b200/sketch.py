@@ -106,6 +106,14 @@ class Sketch:
         check(lib.qs_insert(self.handle, _ptr(keys, "keys"), n, _stream(stream)), "insert")
         return 0
 
+    def remove(self, keys, keys_sz=None, stream=None):
+        """Take one occurrence of each key out (qs_remove: counters floored at 0)."""
+        n = _numel(keys) if keys_sz is None else int(keys_sz)
+        if n is None:
+            raise ValueError("keys_sz is required with a raw pointer")
+        check(lib.qs_remove(self.handle, _ptr(keys, "keys"), n, _stream(stream)), "remove")
+        return 0
+
     def search(self, keys, keys_sz=None, counts=None, stream=None):
         n = _numel(keys) if keys_sz is None else int(keys_sz)
         if n is None:

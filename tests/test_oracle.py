@@ -150,3 +150,59 @@ def test_count_min_kat():
     assert list(cm.table[:7]) == [2, 2, 0, 0, 0, 0, 0]
     assert list(cm.table[7:]) == [2, 0, 0, 2, 0, 0, 0]
     assert list(cm.query([0, 1, 2])) == [2, 2, 0]
+
+
+# ---- REMOVE (deletion as the insertion with a subtraction, doc/main.tex:232) -------------
+
+def test_kat_remove_low_level_floors_at_zero():
+    s = one_bucket()
+    s.insert(np.zeros(5, np.uint32))
+    s.remove(np.zeros(2, np.uint32))
+    assert s.query([0])[0] == 3 and s.low[0] == 3 | 3 << 8 | 3 << 16
+    s.remove(np.zeros(10, np.uint32))  # more removals than insertions: counters stop at 0
+    assert s.query([0])[0] == 0 and s.low[0] == 0
+
+
+def test_kat_remove_linked_bucket_takes_from_the_high_level():
+    s = one_bucket()
+    s.insert(np.zeros(200, np.uint32))  # links at the 130th key: low 129, high 71
+    s.remove(np.zeros(20, np.uint32))
+    assert s.low[0] == 129 | 129 << 8 | 129 << 16 and list(s.high[32:35]) == [51] * 3
+    assert s.query([0])[0] == 180
+    s.remove(np.zeros(100, np.uint32))  # the high counters floor at 0, the low ones stay
+    assert list(s.high[32:35]) == [0] * 3 and s.query([0])[0] == 129 and s.low[7] == 1025
+
+
+def test_kat_remove_in_a_saturated_bucket_is_dropped():
+    s = oracle.Msws(2, 2, 1, MASKS)
+    s.insert(np.r_[np.zeros(131, np.uint32), np.full(140, 3, np.uint32)])
+    d = s.dropped
+    low = s.low.copy()
+    s.remove(np.full(7, 3, np.uint32))
+    assert s.dropped == d + 7 and np.array_equal(s.low, low)
+
+
+def test_remove_within_a_call_is_order_independent():
+    rng = np.random.default_rng(5)
+    masks = oracle.generate_hashmask(3)
+    keys = (rng.zipf(1.3, 200000) % 20000).astype(np.uint32) * np.uint32(2654435761)
+    rem = (rng.zipf(1.3, 150000) % 30000).astype(np.uint32) * np.uint32(2654435761)
+    a, b = (oracle.Msws(1021, 1024, 2654435769, masks) for _ in range(2))
+    for s, r in ((a, rem), (b, rng.permutation(rem))):
+        s.insert(keys)
+        s.remove(r)
+    assert np.array_equal(a.low, b.low) and np.array_equal(a.high, b.high)
+    assert (a.low.reshape(-1, 8)[:, 7] > 1024).any()
+
+
+def test_count_min_remove_floors_at_zero():
+    seeds, n = [3, 5, 7], 101
+    cm = oracle.CountMin(n, seeds)
+    cm.insert(np.array([1, 1, 2], np.uint32))
+    cm.remove(np.array([1, 9, 9], np.uint32))
+    want = np.zeros(3 * n, np.int64)
+    for k, d in ((1, 1), (1, 1), (2, 1), (1, -1), (9, -1), (9, -1)):  # device_sketch_v0.h:48-52
+        for j, sd in enumerate(seeds):
+            c = j * n + (k * sd % (1 << 32)) % n
+            want[c] = max(0, want[c] + d)
+    assert np.array_equal(cm.table, want.astype(np.uint32)) and cm.query([1])[0] == 1
