@@ -230,10 +230,30 @@ qs_status qs_get_info(qs_sketch *sk, uint64_t *n_low, uint64_t *n_high, uint32_t
                       uint32_t *seeds_out /* m_low for CM, 1 for MSWS; may be null */,
                       uint8_t *mask_table_out /* H*4 bytes; may be null */);
 
+/* The creation parameters as the sketch holds them (seeds and mask_table come back null;
+ * hash_seed is the first seed in use, n_low the bucket count, hash_mask_table_sz the mask
+ * count, max_batch and device the values in effect). */
+qs_status qs_get_params(qs_sketch *sk, qs_params *out);
+
 /* Copy the device tables to host buffers (debug / oracle comparison):
  * low: n_low*m_low words (MSWS: word 7 of each bucket is the high index),
  * high: n_high*m_high words (null to skip). */
 qs_status qs_get_tables(qs_sketch *sk, uint32_t *h_low, uint32_t *h_high);
+
+/* Snapshots: a sketch's whole state — parameters, seeds, mask table, low table, high pool,
+ * allocator, latched status and dropped count — as one byte string (version 1: a 96-byte
+ * header, the seeds, the mask words, the tables, a 64-bit FNV-1a checksum; little-endian).
+ * The reference declares read_file / write_file (include/qsketch.h:70-71) but never defines
+ * them; qs_save / qs_load write and read such a snapshot as a file.  A loaded sketch answers
+ * every query as the saved one did and continues exactly as it would have; it is created on
+ * `device` (-1 = current) with the default insert knobs.  qs_snapshot_load refuses (with
+ * QS_ERR_INVALID_ARG, before any device work) a buffer whose header, size or checksum does not
+ * hold.  The sketch must not be in use on any stream while it is saved. */
+qs_status qs_snapshot_bytes(qs_sketch *sk, uint64_t *bytes);
+qs_status qs_snapshot_save(qs_sketch *sk, void *h_buf, uint64_t buf_bytes);
+qs_status qs_snapshot_load(const void *h_buf, uint64_t bytes, int32_t device, qs_sketch **out);
+qs_status qs_save(qs_sketch *sk, const char *path);
+qs_status qs_load(const char *path, int32_t device, qs_sketch **out);
 
 /* Synthetic key streams (bench / tests), written to device memory on `stream`.
  * kind 0: uniform u32 from a seeded xorshift64 stream;

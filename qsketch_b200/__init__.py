@@ -5,7 +5,7 @@ reference's host interface (qsketch::Sketch, Sketch_GPU_Sub_Warp_Level, Sketch_G
 """
 from ._lib import LIB_PATH, QsError, check, lib  # noqa: F401  (raises ImportError if unbuilt)
 from .sketch import (Sketch, Sketch_GPU_Sub_Warp_Level, Sketch_GPU_Thread, draw_seeds,  # noqa: F401
-                     find_greatest_prime, generate_hashmask, number_of_buckets)
+                     find_greatest_prime, from_snapshot, generate_hashmask, load, number_of_buckets)
 
 __all__ = ["Sketch", "Sketch_GPU_Sub_Warp_Level", "Sketch_GPU_Thread", "find_greatest_prime",
-           "number_of_buckets", "generate_hashmask", "draw_seeds", "QsError", "LIB_PATH"]
+           "number_of_buckets", "generate_hashmask", "draw_seeds", "load", "from_snapshot", "QsError", "LIB_PATH"]

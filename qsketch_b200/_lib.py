@@ -166,6 +166,12 @@ SIGNATURES = {
     "qs_destroy": (_I, [_P]),
     "qs_insert": (_I, [_P, _P, _SZ, _P]),
     "qs_remove": (_I, [_P, _P, _SZ, _P]),
+    "qs_get_params": (_I, [_P, ctypes.POINTER(qs_params)]),
+    "qs_snapshot_bytes": (_I, [_P, ctypes.POINTER(_U64)]),
+    "qs_snapshot_save": (_I, [_P, _P, _U64]),
+    "qs_snapshot_load": (_I, [_P, _U64, ctypes.c_int32, ctypes.POINTER(_P)]),
+    "qs_save": (_I, [_P, ctypes.c_char_p]),
+    "qs_load": (_I, [ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(_P)]),
     "qs_query": (_I, [_P, _P, _SZ, _P, _P]),
     "qs_insert_host": (_I, [_P, _P, _SZ]),
     "qs_query_host": (_I, [_P, _P, _SZ, _P]),

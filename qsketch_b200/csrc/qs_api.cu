@@ -717,6 +717,19 @@ qs_status qs_get_info(qs_sketch* sk, uint64_t* n_low, uint64_t* n_high, uint32_t
     return QS_OK;
 }
 
+qs_status qs_get_params(qs_sketch* sk, qs_params* out) {
+    if (!sk || !out) return fail(QS_ERR_INVALID_ARG, "qs_get_params: null argument");
+    *out = sk->p;
+    out->seeds = nullptr;       // the caller's arrays are not kept
+    out->mask_table = nullptr;
+    out->hash_seed = sk->seeds.empty() ? 0u : sk->seeds[0];
+    out->n_low = sk->kind == QS_KIND_MSWS ? sk->D.n_low : sk->C.n;
+    out->hash_mask_table_sz = (uint32_t)sk->masks.size();
+    out->max_batch = sk->max_batch;
+    out->device = sk->device;
+    return QS_OK;
+}
+
 qs_status qs_get_tables(qs_sketch* sk, uint32_t* h_low, uint32_t* h_high) {
     if (!sk) return fail(QS_ERR_INVALID_ARG, "null sketch");
     DeviceGuard guard(sk->device);
@@ -728,6 +741,181 @@ qs_status qs_get_tables(qs_sketch* sk, uint32_t* h_low, uint32_t* h_high) {
         CK(cudaMemcpy(h_low, sk->C.table, sk->C.n * sk->C.rows * 4, cudaMemcpyDeviceToHost), "copy table");
     }
     return QS_OK;
+}
+
+// ---- snapshots (the reference declares read_file / write_file, include/qsketch.h:70-71, and
+// never defines them) -----------------------------------------------------------------------
+// Layout, little-endian: SnapHeader, then the seeds (u32), the mask words (u32), the low table
+// and (MSWS) the high pool, then a 64-bit FNV-1a checksum of everything before it.
+struct SnapHeader {
+    char magic[8];  // "QSKSNAP" + NUL
+    uint32_t version, kind;
+    uint64_t n_low, n_high;
+    uint32_t m_low, m_high, n_seeds, n_masks;
+    uint32_t hash_mask_ones, flags, next_level_id, status_bits;
+    uint64_t dropped_keys, payload_bytes, reserved[2];
+};
+static_assert(sizeof(SnapHeader) == 96, "snapshot header layout");
+constexpr char SNAP_MAGIC[8] = {'Q', 'S', 'K', 'S', 'N', 'A', 'P', 0};
+
+static uint64_t fnv1a64(const unsigned char* p, uint64_t n, uint64_t h = 0xcbf29ce484222325ull) {
+    for (uint64_t i = 0; i < n; ++i) h = (h ^ p[i]) * 0x100000001b3ull;
+    return h;
+}
+
+static uint64_t snap_table_words(const qs_sketch* sk, uint64_t* low_words, uint64_t* high_words) {
+    *low_words = sk->kind == QS_KIND_MSWS ? sk->D.n_low * LOW_WORDS : sk->C.n * sk->C.rows;
+    *high_words = sk->kind == QS_KIND_MSWS ? sk->D.n_high * HIGH_WORDS : 0;
+    return *low_words + *high_words;
+}
+
+qs_status qs_snapshot_bytes(qs_sketch* sk, uint64_t* bytes) {
+    if (!sk || !bytes) return fail(QS_ERR_INVALID_ARG, "qs_snapshot_bytes: null argument");
+    uint64_t lw, hw;
+    const uint64_t tw = snap_table_words(sk, &lw, &hw);
+    *bytes = sizeof(SnapHeader) + 4 * (sk->seeds.size() + sk->masks.size() + tw) + 8;
+    return QS_OK;
+}
+
+qs_status qs_snapshot_save(qs_sketch* sk, void* h_buf, uint64_t buf_bytes) {
+    uint64_t need = 0;
+    qs_status st = qs_snapshot_bytes(sk, &need);
+    if (st != QS_OK) return st;
+    if (!h_buf || buf_bytes < need) return fail(QS_ERR_INVALID_ARG, "qs_snapshot_save: buffer of %llu bytes needed",
+                                                (unsigned long long)need);
+    DeviceGuard guard(sk->device);
+    CK(cudaDeviceSynchronize(), "snapshot sync");
+    SnapHeader h{};
+    std::memcpy(h.magic, SNAP_MAGIC, 8);
+    h.version = 1;
+    h.kind = sk->kind;
+    uint64_t lw, hw;
+    snap_table_words(sk, &lw, &hw);
+    if (sk->kind == QS_KIND_MSWS) {
+        Ctl c;
+        CK(cudaMemcpy(&c, sk->D.ctl, sizeof c, cudaMemcpyDeviceToHost), "read control block");
+        h.n_low = sk->D.n_low;
+        h.n_high = sk->D.n_high;
+        h.m_low = LOW_WORDS;
+        h.m_high = HIGH_WORDS;
+        h.next_level_id = c.next_id;
+        h.status_bits = c.status;
+        h.dropped_keys = c.dropped;
+        h.hash_mask_ones = sk->p.hash_mask_ones;
+        h.flags = sk->D.compat_v3 ? QS_FLAG_COMPAT_V3 : 0u;
+    } else {
+        h.n_low = sk->C.n;
+        h.m_low = sk->C.rows;
+    }
+    h.n_seeds = (uint32_t)sk->seeds.size();
+    h.n_masks = (uint32_t)sk->masks.size();
+    h.payload_bytes = need - sizeof h - 8;
+    unsigned char* out = static_cast<unsigned char*>(h_buf);
+    std::memcpy(out, &h, sizeof h);
+    unsigned char* q = out + sizeof h;
+    std::memcpy(q, sk->seeds.data(), 4 * sk->seeds.size());
+    q += 4 * sk->seeds.size();
+    std::memcpy(q, sk->masks.data(), 4 * sk->masks.size());
+    q += 4 * sk->masks.size();
+    CK(cudaMemcpy(q, sk->kind == QS_KIND_MSWS ? sk->D.low : sk->C.table, lw * 4, cudaMemcpyDeviceToHost), "copy low");
+    q += lw * 4;
+    if (hw) CK(cudaMemcpy(q, sk->D.high, hw * 4, cudaMemcpyDeviceToHost), "copy high");
+    q += hw * 4;
+    const uint64_t sum = fnv1a64(out, (uint64_t)(q - out));
+    std::memcpy(q, &sum, 8);
+    return QS_OK;
+}
+
+qs_status qs_snapshot_load(const void* h_buf, uint64_t bytes, int32_t device, qs_sketch** out) {
+    if (!h_buf || !out) return fail(QS_ERR_INVALID_ARG, "qs_snapshot_load: null argument");
+    *out = nullptr;
+    const unsigned char* in = static_cast<const unsigned char*>(h_buf);
+    SnapHeader h;
+    if (bytes < sizeof h + 8) return fail(QS_ERR_INVALID_ARG, "snapshot: %llu bytes is too short",
+                                          (unsigned long long)bytes);
+    std::memcpy(&h, in, sizeof h);
+    if (std::memcmp(h.magic, SNAP_MAGIC, 8) != 0 || h.version != 1)
+        return fail(QS_ERR_INVALID_ARG, "snapshot: not a version-1 QSketch snapshot");
+    const bool msws = h.kind == QS_KIND_MSWS;
+    if ((!msws && h.kind != QS_KIND_PLAIN_CM) || (msws && (h.m_low != LOW_WORDS || h.m_high != HIGH_WORDS)) ||
+        h.n_low == 0 || h.n_seeds == 0 || h.n_seeds > MAX_CM_ROWS || (msws && h.n_masks == 0))
+        return fail(QS_ERR_INVALID_ARG, "snapshot: inconsistent header");
+    const uint64_t lw = h.n_low * h.m_low, hw = msws ? h.n_high * h.m_high : 0;
+    const uint64_t payload = 4 * ((uint64_t)h.n_seeds + h.n_masks + lw + hw);
+    if (h.payload_bytes != payload || bytes < sizeof h + payload + 8)
+        return fail(QS_ERR_INVALID_ARG, "snapshot: size does not match its header");
+    uint64_t sum;
+    std::memcpy(&sum, in + sizeof h + payload, 8);
+    if (fnv1a64(in, sizeof h + payload) != sum) return fail(QS_ERR_INVALID_ARG, "snapshot: checksum mismatch");
+    const unsigned char* q = in + sizeof h;
+    std::vector<uint32_t> seeds(h.n_seeds), masks(h.n_masks);
+    std::memcpy(seeds.data(), q, 4 * seeds.size());
+    q += 4 * seeds.size();
+    std::memcpy(masks.data(), q, 4 * masks.size());
+    q += 4 * masks.size();
+    qs_params p;
+    qs_params_default(&p);
+    p.kind = h.kind;
+    p.flags = h.flags & QS_FLAG_COMPAT_V3;
+    p.n_low = h.n_low;
+    p.m_low = h.m_low;
+    p.m_high = msws ? h.m_high : 32;
+    p.n_high = msws ? h.n_high : 1024;
+    p.hash_mask_table_sz = msws ? h.n_masks : 1021;
+    p.hash_mask_ones = msws ? h.hash_mask_ones : 3;
+    p.seeds = seeds.data();
+    p.mask_table = msws ? reinterpret_cast<const uint8_t*>(masks.data()) : nullptr;
+    p.device = device;
+    qs_sketch* sk = nullptr;
+    qs_status st = qs_create(&p, &sk);
+    if (st != QS_OK) return st;
+    DeviceGuard guard(sk->device);
+    cudaError_t e = cudaMemcpy(msws ? sk->D.low : sk->C.table, q, lw * 4, cudaMemcpyHostToDevice);
+    q += lw * 4;
+    if (e == cudaSuccess && hw) e = cudaMemcpy(sk->D.high, q, hw * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && msws) {
+        Ctl c;
+        e = cudaMemcpy(&c, sk->D.ctl, sizeof c, cudaMemcpyDeviceToHost);
+        c.next_id = h.next_level_id;
+        c.status = h.status_bits;
+        c.dropped = h.dropped_keys;
+        if (e == cudaSuccess) e = cudaMemcpy(sk->D.ctl, &c, sizeof c, cudaMemcpyHostToDevice);
+        sk->fresh = sk->max_batch;  // a warm sketch: no chunk ramp
+    }
+    if (e != cudaSuccess) {
+        qs_destroy(sk);
+        return cuda_fail(e, "snapshot upload");
+    }
+    *out = sk;
+    return QS_OK;
+}
+
+qs_status qs_save(qs_sketch* sk, const char* path) {
+    if (!path) return fail(QS_ERR_INVALID_ARG, "qs_save: null path");
+    uint64_t n = 0;
+    qs_status st = qs_snapshot_bytes(sk, &n);
+    if (st != QS_OK) return st;
+    std::vector<unsigned char> buf(n);
+    st = qs_snapshot_save(sk, buf.data(), n);
+    if (st != QS_OK) return st;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(QS_ERR_INVALID_ARG, "qs_save: cannot open %s", path);
+    const size_t w = std::fwrite(buf.data(), 1, n, f);
+    const int c = std::fclose(f);
+    if (w != n || c != 0) return fail(QS_ERR_INVALID_ARG, "qs_save: short write to %s", path);
+    return QS_OK;
+}
+
+qs_status qs_load(const char* path, int32_t device, qs_sketch** out) {
+    if (!path || !out) return fail(QS_ERR_INVALID_ARG, "qs_load: null argument");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(QS_ERR_INVALID_ARG, "qs_load: cannot open %s", path);
+    std::vector<unsigned char> buf;
+    unsigned char tmp[1 << 16];
+    size_t r;
+    while ((r = std::fread(tmp, 1, sizeof tmp, f)) > 0) buf.insert(buf.end(), tmp, tmp + r);
+    std::fclose(f);
+    return qs_snapshot_load(buf.data(), buf.size(), device, out);
 }
 
 qs_status qs_gen_keys(uint32_t kind, uint64_t seed, uint64_t n_ranks, double s, uint64_t perm_seed, uint32_t* d_keys,

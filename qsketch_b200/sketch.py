@@ -19,6 +19,7 @@ table from /dev/urandom (include/tool/tool.h:192-204); here they come from `seed
 and `mask_rng` (or explicit `hash_seed` / `mask_table`), so runs are reproducible.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -184,6 +185,18 @@ class Sketch:
               "tables")
         return low, high
 
+    def snapshot(self):
+        """The sketch's whole state as bytes (qs_snapshot_save)."""
+        n = ctypes.c_uint64()
+        check(lib.qs_snapshot_bytes(self.handle, ctypes.byref(n)), "snapshot")
+        buf = ctypes.create_string_buffer(n.value)
+        check(lib.qs_snapshot_save(self.handle, buf, n.value), "snapshot")
+        return buf.raw
+
+    def save(self, path):
+        """write_file (include/qsketch.h:70-71): the snapshot as a file (qs_save)."""
+        check(lib.qs_save(self.handle, os.fsencode(str(path))), "save")
+
     def close(self):
         if self._handle:
             lib.qs_destroy(self._handle)
@@ -200,6 +213,31 @@ class Sketch:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def _adopt(h):
+    """A Python object over a qs_sketch handle made by qs_load / qs_snapshot_load."""
+    p = qs_params()
+    check(lib.qs_get_params(h, ctypes.byref(p)), "params")
+    obj = object.__new__(Sketch_GPU_Thread if p.kind == QS_KIND_PLAIN_CM else Sketch_GPU_Sub_Warp_Level)
+    obj._handle = h
+    obj._keep = None
+    obj._n_masks = 0 if p.kind == QS_KIND_PLAIN_CM else p.hash_mask_table_sz
+    return obj
+
+
+def load(path, device=None):
+    """read_file (include/qsketch.h:70-71): a sketch from a snapshot file (qs_load)."""
+    h = ctypes.c_void_p()
+    check(lib.qs_load(os.fsencode(str(path)), -1 if device is None else int(device), ctypes.byref(h)), "load")
+    return _adopt(h)
+
+
+def from_snapshot(data, device=None):
+    """A sketch from snapshot bytes (qs_snapshot_load)."""
+    h = ctypes.c_void_p()
+    check(lib.qs_snapshot_load(data, len(data), -1 if device is None else int(device), ctypes.byref(h)), "load")
+    return _adopt(h)
 
 
 def _host(x):

@@ -136,3 +136,14 @@ def test_knob_validation_happens_before_any_device_work():
     p.n_low, p.lanes_per_key = 1021, 12
     h = ctypes.c_void_p()
     assert _lib.lib.qs_create(ctypes.byref(p), ctypes.byref(h)) != _lib.QS_OK
+
+
+def test_snapshot_load_refuses_bad_input_without_a_device(tmp_path):
+    # header, size and checksum checks run on the host before any device work
+    import ctypes
+    h = ctypes.c_void_p()
+    bogus = tmp_path / "bogus.qsk"
+    bogus.write_bytes(b"QSKSNAP\0" + bytes(200))
+    assert _lib.lib.qs_load(str(bogus).encode(), -1, ctypes.byref(h)) == _lib.QS_ERR_INVALID_ARG
+    assert _lib.lib.qs_load(str(tmp_path / "missing.qsk").encode(), -1, ctypes.byref(h)) == _lib.QS_ERR_INVALID_ARG
+    assert _lib.lib.qs_snapshot_load(b"short", 5, -1, ctypes.byref(h)) == _lib.QS_ERR_INVALID_ARG
