@@ -775,6 +775,17 @@ def run_learned(args, cfg):
     e2e_ms = max_over_ranks((time.perf_counter() - w0) * 1e3)
     lk2.close()
 
+    # diagnostic bound: the stream's true heaviest keys (exact counts) admitted before the first
+    # key, no training — what any classifier could gain with this table
+    order = torch.argsort(exact.to(torch.int64), descending=True)[:int(0.75 * cfg["table_slots"])]
+    top = uniq.view(torch.int32)[order].cpu().numpy().view(np.uint32)
+    lo = LearnedSketch(**params)
+    lo.admit_keys(top)
+    lo.insert(keys)
+    out_o = lo.search(uniq)
+    re_o, _ = data.error_metrics(out_o, exact)
+    lo.close()
+
     rest_keys = n - warm
     achieved = rest_keys * INSERT_BYTES_PER_KEY / (rest_ms * 1e-3) / 1e9
     hbm, peak_kind = peaks()
@@ -789,12 +800,17 @@ def run_learned(args, cfg):
                        "l2": "key stream of %d MB per step > 126 MB L2" % (n * 4 >> 20),
                        "parallelism": "independent sketch per GPU" if world > 1 else "single GPU"},
             "avg_rel_error": re_l, "avg_rel_error_plain": re_p, "re_ratio_learned_over_plain": re_l / re_p,
+            "avg_rel_error_true_top_admitted": re_o, "re_ratio_true_top_over_plain": re_o / re_p,
             "mean_est_over_exact": ratio_l, "mean_est_over_exact_plain": ratio_p,
             "learned": {"warmup_and_train_ms": round(warm_ms, 3), "routed_insert_ms": round(rest_ms, 3),
                         "routed_insert_gkeys_per_s": round(world * rest_keys / (rest_ms * 1e6), 4),
                         "whole_stream_insert_gkeys_per_s": round(world * n / ((warm_ms + rest_ms) * 1e6), 4),
                         "query_gkeys_per_s": round(world * n_q / (lq_ms * 1e6), 4),
                         "train_ms": round(info["train_ms"], 2), "table_fill": info["table_fill"],
+                        "train_examples": info["train_examples"], "adam_steps": info["steps"],
+                        "warmup_replayed": info["warmup_replayed"],
+                        "train_phase_ms": dict(zip(["distinct", "labels_and_set", "epochs", "admission", "replay"],
+                                                   [round(x, 2) for x in info["train_phase_ms"]])),
                         "train_precision": info["train_precision"], "train_recall": info["train_recall"],
                         "sketch_bytes": info["sketch_bytes"], "table_bytes": info["table_bytes"],
                         "mlp_bytes": info["mlp_bytes"]},

@@ -326,6 +326,12 @@ typedef struct qs_learned_params {
     uint32_t seed_rng, mask_rng, init_seed;
     uint64_t max_batch;        /* keys per routing chunk, default 2^22 */
     int32_t device;
+    uint32_t neg_per_pos;      /* training set: every labelled-heavy warm-up key and a seeded
+                                  sample of this many light keys per heavy one (0 = 16) */
+    uint32_t replay_warmup;    /* 1 (default): after admission the sketch is cleared and the
+                                  warm-up window inserted again through the router, so the
+                                  admitted keys' warm-up occurrences count in the table and never
+                                  link buckets; 2 = keep the warm-up counts in the sketch */
 } qs_learned_params;
 
 typedef struct qs_learned qs_learned;
@@ -337,11 +343,20 @@ typedef struct qs_learned_info {
     uint32_t threshold, trained, epochs, steps;
     float pos_weight, loss_first, loss_last, train_precision, train_recall, logit_threshold;
     double train_ms;
+    uint64_t warmup_replayed;  /* 1 when the warm-up window went through the router again */
+    double train_phase_ms[5];  /* distinct warm-up keys; labels and training set; Adam epochs;
+                                  classification and admission; replay of the warm-up window */
 } qs_learned_info;
 
 #define QS_MLP_PARAMS 20865u /* W1[128x32] | W2[128x128] | b1[128] | b2[128] | w3[128] | b3 */
 
 void qs_learned_params_default(qs_learned_params *p);
+/* Diagnostic admission: admit h_keys (host, in the order given, up to the table's max fill)
+ * into the exact table and end the warm-up without training, so every later key is routed
+ * (table keys count there; no other key is admitted later).
+ * With the workload's true heaviest keys this bounds what any classifier could gain with this
+ * table; call before the first insert. */
+qs_status qs_learned_admit_keys(qs_learned *lk, const uint32_t *h_keys, size_t n);
 qs_status qs_learned_create(const qs_learned_params *p, qs_learned **out);
 qs_status qs_learned_destroy(qs_learned *lk);
 qs_status qs_learned_insert(qs_learned *lk, const uint32_t *d_keys, size_t n, void *stream);

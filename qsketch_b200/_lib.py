@@ -98,6 +98,8 @@ class qs_learned_params(ctypes.Structure):
         ("init_seed", ctypes.c_uint32),
         ("max_batch", ctypes.c_uint64),
         ("device", ctypes.c_int32),
+        ("neg_per_pos", ctypes.c_uint32),
+        ("replay_warmup", ctypes.c_uint32),
     ]
 
 
@@ -108,7 +110,8 @@ class qs_learned_info(ctypes.Structure):
         [(n, ctypes.c_uint32) for n in ("threshold", "trained", "epochs", "steps")] + \
         [(n, ctypes.c_float) for n in ("pos_weight", "loss_first", "loss_last", "train_precision", "train_recall",
                                        "logit_threshold")] + \
-        [("train_ms", ctypes.c_double)]
+        [("train_ms", ctypes.c_double), ("warmup_replayed", ctypes.c_uint64),
+         ("train_phase_ms", ctypes.c_double * 5)]
 
 
 class qs_batch_params(ctypes.Structure):
@@ -212,6 +215,7 @@ SIGNATURES = {
     "qs_batch_get_info": (_I, [_P, ctypes.POINTER(qs_batch_info)]),
     "qs_batch_arena": (_P, [_P]),
     "qs_learned_params_default": (None, [ctypes.POINTER(qs_learned_params)]),
+    "qs_learned_admit_keys": (_I, [_P, _P, _SZ]),
     "qs_learned_create": (_I, [ctypes.POINTER(qs_learned_params), ctypes.POINTER(_P)]),
     "qs_learned_destroy": (_I, [_P]),
     "qs_learned_insert": (_I, [_P, _P, _SZ, _P]),

@@ -1108,6 +1108,7 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     CKT(cudaMemcpyAsync(&hc, d_cnt, 4, cudaMemcpyDeviceToHost, st), "distinct count");
     CKT(cudaStreamSynchronize(st), "distinct sync");
     const uint64_t D = hc;
+    const auto t_distinct = std::chrono::steady_clock::now();
     std::vector<uint32_t> keys(D);
     CKT(cudaMemcpy(keys.data(), d_distinct, D * 4, cudaMemcpyDeviceToHost), "distinct copy");
     // labels from the sketch's own estimates
@@ -1127,35 +1128,63 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     std::vector<uint8_t> lab(D);
     uint64_t npos = 0;
     for (uint64_t i = 0; i < D; ++i) npos += (lab[i] = est[i] >= thr ? 1 : 0);
-    const float pw = std::min(lk->p.max_pos_weight, (float)(D - npos) / (float)std::max<uint64_t>(1, npos));
+    // the training set: every labelled-heavy key and a seeded sample of neg_per_pos light keys
+    // per heavy one (a key is in the sample when its hash falls below the sampling rate), in
+    // ascending key order
+    const uint32_t npp = lk->p.neg_per_pos ? lk->p.neg_per_pos : 16u;
+    const double rate = std::min(1.0, (double)npp * (double)npos / (double)std::max<uint64_t>(1, D - npos));
+    const uint64_t cut = (uint64_t)(rate * 4294967296.0);
+    std::vector<uint32_t> tkeys;
+    std::vector<uint8_t> tlab;
+    tkeys.reserve(npos + (uint64_t)(rate * (double)(D - npos)) + 16);
+    uint64_t nneg = 0;
+    for (uint64_t i = 0; i < D; ++i) {
+        uint32_t h = keys[i] ^ lk->p.init_seed;  // murmur3 finaliser: a seeded, key-only sample
+        h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
+        if (lab[i] || (uint64_t)h < cut) {
+            tkeys.push_back(keys[i]);
+            tlab.push_back(lab[i]);
+            nneg += !lab[i];
+        }
+    }
+    const uint64_t TN = tkeys.size();
+    const auto t_labels = std::chrono::steady_clock::now();
+    const float pw = std::min(lk->p.max_pos_weight, (float)nneg / (float)std::max<uint64_t>(1, npos));
     // epochs over a seeded order of the examples, drawn on the device per epoch
     uint8_t* d_lab_sorted = nullptr;
-    CKT(cudaMalloc(&d_lab, D + 4), "train labels");
-    CKT(cudaMalloc(&d_perm_keys, D * 4 + 4), "train keys");
-    CKT(cudaMalloc(&d_lab_sorted, D + 4), "train labels");
+    uint32_t* d_train = nullptr;
+    CKT(cudaMalloc(&d_lab, TN + 4), "train labels");
+    CKT(cudaMalloc(&d_perm_keys, TN * 4 + 4), "train keys");
+    CKT(cudaMalloc(&d_lab_sorted, TN + 4), "train labels");
+    CKT(cudaMalloc(&d_train, TN * 4 + 4), "train set");
     {
-        const cudaError_t e = cudaMemcpy(d_lab_sorted, lab.data(), D, cudaMemcpyHostToDevice);
+        cudaError_t e = cudaMemcpy(d_lab_sorted, tlab.data(), TN, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(d_train, tkeys.data(), TN * 4, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) {
             cudaFree(d_lab_sorted);
-            CKT(e, "train labels upload");
+            cudaFree(d_train);
+            CKT(e, "train set upload");
         }
     }
     double loss = 0.0, first = -1.0;
     for (uint32_t ep = 0; ep < lk->p.epochs && s == QS_OK; ++ep) {
         const uint64_t seed = ((uint64_t)lk->p.init_seed << 32) ^ (0x5bd1e995ull * (ep + 1));
-        const cudaError_t e = permute_examples(d_distinct, d_lab_sorted, (uint32_t)D, seed, d_perm_keys, d_lab, st);
+        const cudaError_t e = permute_examples(d_train, d_lab_sorted, (uint32_t)TN, seed, d_perm_keys, d_lab, st);
         if (e != cudaSuccess) {
             cudaFree(d_lab_sorted);
+            cudaFree(d_train);
             CKT(e, "permute examples");
         }
-        s = mlp_train_pass(lk, d_perm_keys, d_lab, D, lk->p.batch, lk->p.lr, pw, &loss, st);
+        s = mlp_train_pass(lk, d_perm_keys, d_lab, TN, lk->p.batch, lk->p.lr, pw, &loss, st);
         if (first < 0) first = loss;
     }
     cudaFree(d_lab_sorted);
+    cudaFree(d_train);
     if (s != QS_OK) {
         cleanup();
         return s;
     }
+    const auto t_epochs = std::chrono::steady_clock::now();
     // predictions on the warm-up keys: admit the predicted heavy, most confident first
     CKT(cudaMalloc(&d_logit, D * 4 + 4), "train logits");
     CKT(mlp_forward(d_distinct, D, lk->M, d_logit, st), "train forward");
@@ -1175,19 +1204,21 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     }
     lk->R.z_threshold = zthr;
     uint64_t tp = 0, fp = 0, fn = 0;
-    std::vector<std::pair<double, uint32_t>> heavy;
+    std::vector<std::pair<int64_t, uint32_t>> heavy;
+    heavy.reserve(D / 8);
     for (uint64_t i = 0; i < D; ++i) {
         const bool pred = z[i] >= zthr;
         tp += pred && lab[i];
         fp += pred && !lab[i];
         fn += !pred && lab[i];
-        if (pred) heavy.push_back({-(double)est[i], keys[i]});
+        if (pred) heavy.push_back({-(int64_t)est[i], keys[i]});
     }
     // the network decides who may enter the table; the sketch's own counts rank them (only the
     // first max_fill of the order can enter, so only they are sorted; keys are distinct, so the
     // order is total)
     const uint32_t take = (uint32_t)std::min<uint64_t>(heavy.size(), lk->T.max_fill);
-    std::partial_sort(heavy.begin(), heavy.begin() + take, heavy.end());
+    if (take < heavy.size()) std::nth_element(heavy.begin(), heavy.begin() + take, heavy.end());
+    std::sort(heavy.begin(), heavy.begin() + take);
     std::vector<uint32_t> order(take);
     for (uint32_t i = 0; i < take; ++i) order[i] = heavy[i].second;
     if (take) {
@@ -1202,7 +1233,7 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
 #undef CKT
     qs_learned_info& I = lk->info;
     I.trained = 1;
-    I.train_examples = D;
+    I.train_examples = TN;
     I.train_positives = npos;
     I.threshold = thr;
     I.pos_weight = pw;
@@ -1213,13 +1244,59 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     I.logit_threshold = zthr;
     I.epochs = lk->p.epochs;
     I.steps = lk->adam_step;
-    I.train_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    const auto t_end = std::chrono::steady_clock::now();
+    auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+        return std::chrono::duration<double, std::milli>(b - a).count();
+    };
+    I.train_ms = ms(t0, t_end);
+    I.train_phase_ms[0] = ms(t0, t_distinct);
+    I.train_phase_ms[1] = ms(t_distinct, t_labels);
+    I.train_phase_ms[2] = ms(t_labels, t_epochs);
+    I.train_phase_ms[3] = ms(t_epochs, t_end);
+    return QS_OK;
+}
+
+// The warm-up window again, now through the router: the sketch is cleared, admitted keys
+// count exactly in the table and are left out of the sketch, every other key is inserted.  The
+// heavy keys' warm-up occurrences then never link (and freeze) the buckets they share with
+// light keys.  No classification here: admission already used the whole window.
+qs_status learned_replay_warmup(qs_learned* lk, cudaStream_t st) {
+    const auto t0 = std::chrono::steady_clock::now();
+    qs_status s = qs_clear(lk->sk, st);
+    if (s != QS_OK) return s;
+    CK(cudaMemsetAsync(lk->T.counts, 0, (size_t)lk->T.slots * 4, st), "table counts reset");
+    const uint64_t W = lk->warm_seen;
+    for (uint64_t off = 0; off < W;) {
+        const uint64_t c = std::min<uint64_t>(W - off, lk->sk->max_batch);
+        lk->R.collect = 0u;
+        CK(route_chunk(lk->warm + off, c, lk->T, lk->R, st), "route warm-up");
+        s = insert_device(lk->sk, lk->warm + off, c, st, lk->R.skip);
+        if (s != QS_OK) return s;
+        off += c;
+    }
+    lk->info.warmup_replayed = 1;
+    CK(cudaStreamSynchronize(st), "replay sync");
+    lk->info.train_phase_ms[4] =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return QS_OK;
 }
 
 }  // namespace
 
 extern "C" {
+
+qs_status qs_learned_admit_keys(qs_learned* lk, const uint32_t* h_keys, size_t n) {
+    if (!lk || (!h_keys && n)) return fail(QS_ERR_INVALID_ARG, "qs_learned_admit_keys: null argument");
+    if (lk->warm_seen) return fail(QS_ERR_INVALID_ARG, "qs_learned_admit_keys: call before the first insert");
+    DeviceGuard guard(lk->device);
+    const uint32_t take = (uint32_t)std::min<uint64_t>(n, lk->T.max_fill);
+    qs_status s = take ? learned_admit(lk, h_keys, take, 0) : QS_OK;
+    if (s != QS_OK) return s;
+    lk->warm_seen = lk->p.warmup_keys;  // no warm-up, no training: route from the first key
+    lk->table_full = true;              // and no further admission (the network is untrained)
+    lk->info.trained = 0;
+    return QS_OK;
+}
 
 void qs_learned_params_default(qs_learned_params* p) {
     if (!p) return;
@@ -1237,6 +1314,8 @@ void qs_learned_params_default(qs_learned_params* p) {
     p->seed_rng = 1;
     p->mask_rng = 1;
     p->init_seed = 1;
+    p->neg_per_pos = 16;
+    p->replay_warmup = 1;
     p->max_batch = 1ull << 22;
     p->device = -1;
 }
@@ -1363,6 +1442,7 @@ qs_status qs_learned_insert(qs_learned* lk, const uint32_t* d_keys, size_t n, vo
             off += take;
             if (lk->warm_seen == lk->p.warmup_keys) {
                 s = learned_train(lk, st);
+                if (s == QS_OK && lk->p.replay_warmup != 2) s = learned_replay_warmup(lk, st);
                 if (s != QS_OK) return s;
             }
             continue;

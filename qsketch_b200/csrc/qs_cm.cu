@@ -32,17 +32,35 @@ __global__ void __launch_bounds__(CM_THREADS) k_cm_insert(const uint32_t* __rest
     }
 }
 
+// CM_QPT keys per thread in flight: every row's counter of all of them is loaded before any
+// is used, so a thread waits one L2 round trip per CM_QPT keys instead of per key.
+constexpr int CM_QPT = 4;
+
 __global__ void __launch_bounds__(CM_THREADS) k_cm_query(const uint32_t* __restrict__ keys, uint64_t n,
                                                          uint32_t* __restrict__ out, CmDev D) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t key = __ldcs(keys + i);
-        uint32_t c = 0xffffffffu;
-        for (uint32_t j = 0; j < D.rows; ++j) {
-            const uint32_t col = fast_mod(D.fm, key * D.seeds[j]);
-            c = min(c, __ldg(D.table + (uint64_t)j * D.n + col));
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += stride * CM_QPT) {
+        uint32_t key[CM_QPT], c[CM_QPT];
+#pragma unroll
+        for (int q = 0; q < CM_QPT; ++q) {
+            const uint64_t i = base + q * stride;
+            key[q] = i < n ? __ldcs(keys + i) : 0u;
+            c[q] = 0xffffffffu;
         }
-        __stcs(out + i, c);
+        for (uint32_t j = 0; j < D.rows; ++j) {
+            const uint32_t sd = D.seeds[j];
+            const uint32_t* row = D.table + (uint64_t)j * D.n;
+            uint32_t v[CM_QPT];
+#pragma unroll
+            for (int q = 0; q < CM_QPT; ++q) v[q] = __ldg(row + fast_mod(D.fm, key[q] * sd));
+#pragma unroll
+            for (int q = 0; q < CM_QPT; ++q) c[q] = min(c[q], v[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < CM_QPT; ++q) {
+            const uint64_t i = base + q * stride;
+            if (i < n) __stcs(out + i, c[q]);
+        }
     }
 }
 
@@ -59,7 +77,7 @@ cudaError_t cm_insert(const uint32_t* d_keys, uint64_t n, const CmDev& D, int ag
 
 cudaError_t cm_query(const uint32_t* d_keys, uint64_t n, uint32_t* d_out, const CmDev& D, int grid, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
-    const uint64_t want = (n + CM_THREADS - 1) / CM_THREADS;
+    const uint64_t want = (n + (uint64_t)CM_THREADS * CM_QPT - 1) / ((uint64_t)CM_THREADS * CM_QPT);
     const int g = (int)std::min<uint64_t>((uint64_t)grid, std::max<uint64_t>(1, want));
     k_cm_query<<<g, CM_THREADS, 0, st>>>(d_keys, n, d_out, D);
     return cudaGetLastError();

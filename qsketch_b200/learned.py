@@ -51,10 +51,18 @@ class LearnedSketch:
 
     query = search
 
+    def admit_keys(self, keys):
+        """Diagnostic admission (qs_learned_admit_keys): these host keys enter the exact table in
+        order, up to its max fill, and the warm-up ends without training."""
+        k = np.ascontiguousarray(np.asarray(keys, np.uint32))
+        check(lib.qs_learned_admit_keys(self.handle, k.ctypes.data, k.size), "admit_keys")
+
     def info(self):
         i = qs_learned_info()
         check(lib.qs_learned_get_info(self.handle, ctypes.byref(i)), "info")
-        return {f: getattr(i, f) for f, _ in qs_learned_info._fields_}
+        d = {f: getattr(i, f) for f, _ in qs_learned_info._fields_}
+        d["train_phase_ms"] = list(d["train_phase_ms"])
+        return d
 
     def table(self):
         """The exact table: (keys, counts) of its occupied slots, and the sketch's multiplier."""

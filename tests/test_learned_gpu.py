@@ -96,25 +96,28 @@ def test_learned_split_beats_plain_at_equal_bytes(gpu):
     assert torch.equal(lk2.search(uniq), est_l)
 
 
-@pytest.mark.parametrize("max_batch", [1 << 18, 1 << 20])
-def test_split_is_exact_table_plus_sketch(gpu, max_batch):
-    # A table that training fills: every later key is looked up by pass 1 itself.  Then each
-    # table key's count is exactly its occurrences after the warm-up, and the sketch part is
-    # exactly a plain sketch (same size, multiplier and masks) fed the warm-up keys plus the
-    # later keys that are not in the table, in order.
+@pytest.mark.parametrize("max_batch,replay", [(1 << 18, 1), (1 << 20, 1), (1 << 20, 2)])
+def test_split_is_exact_table_plus_sketch(gpu, max_batch, replay):
+    # A table that training fills: every later key is looked up by pass 1 itself.  With the
+    # warm-up replayed through the router (replay 1, the default) each table key's count is
+    # exactly its occurrences in the whole stream, and the sketch part is exactly a plain
+    # sketch (same size, multiplier and masks) fed the keys that are not in the table, in
+    # order; keeping the warm-up counts in the sketch (replay 2) the table counts the keys
+    # after the warm-up and the sketch took every warm-up key.
     import qsketch_b200 as qs
     keys = data.class_keys(1 << 22, seed=17, perm_seed=19, n_class=1 << 12)
     warm = 1 << 20
     lk = LearnedSketch(budget_bytes=6 << 20, table_slots=1 << 12, warmup_keys=warm, hash_seed=2654435769,
-                       max_batch=max_batch, heavy_fraction=0.2, epochs=2)
+                       max_batch=max_batch, heavy_fraction=0.2, epochs=2, replay_warmup=replay)
     lk.insert(keys)
     info = lk.info()
     max_fill = int(0.75 * 4096)
     assert (max_fill - min(info["table_fill"], max_fill)) * 1024 < 4096, info  # (nearly) full at training
     tkeys, tcounts, seed = lk.table()
     assert tkeys.size == info["table_fill"] and seed == 2654435769
+    assert info["warmup_replayed"] == (1 if replay == 1 else 0)
     hk = keys.cpu().numpy()
-    rest = hk[warm:]
+    rest = hk[warm:] if replay == 2 else hk
     in_table = np.isin(rest, tkeys)
     u, c = np.unique(rest[in_table], return_counts=True)
     order = np.argsort(tkeys)
@@ -123,7 +126,8 @@ def test_split_is_exact_table_plus_sketch(gpu, max_batch):
     for k in tkeys.tolist():
         assert got_counts[k] == want_counts.get(k, 0), k
     plain = qs.Sketch_GPU_Sub_Warp_Level(info["n_low"], 8, info["n_high"], 32, hash_seed=seed)
-    plain.insert(keys[:warm])
+    if replay == 2:
+        plain.insert(keys[:warm])
     plain.insert(torch.from_numpy(rest[~in_table].astype(np.int32)).cuda().view(torch.uint32))
     q = torch.from_numpy(np.unique(hk).astype(np.int32)).cuda().view(torch.uint32)
     est = lk.search(q).cpu().numpy().astype(np.int64)
@@ -131,3 +135,23 @@ def test_split_is_exact_table_plus_sketch(gpu, max_batch):
     qk = q.cpu().numpy()
     tbl = np.array([got_counts.get(k, 0) for k in qk.tolist()], np.int64)
     assert np.array_equal(est, sk + tbl), f"{(est != sk + tbl).sum()} estimates differ"
+
+
+def test_oracle_admission_bounds_the_gain(gpu):
+    # Diagnostic: the stream's true heaviest keys admitted before the first insert (no
+    # training); every occurrence of them counts exactly in the table.
+    budget = 6 << 20
+    keys = data.class_keys(1 << 22, seed=11, perm_seed=13, n_class=1 << 12)
+    uniq, exact = data.exact_counts(keys)
+    top = uniq.view(torch.int32)[torch.argsort(exact.to(torch.int64), descending=True)[:3000]].cpu().numpy()
+    lk = LearnedSketch(budget_bytes=budget, table_slots=1 << 12, warmup_keys=1 << 20, hash_seed=2654435769)
+    lk.admit_keys(top)
+    lk.insert(keys)
+    tk, tc, _ = lk.table()
+    ex = dict(zip(uniq.cpu().numpy().tolist(), exact.cpu().numpy().tolist()))
+    top = top.view(np.uint32)
+    # (a key that finds no free slot within the probe limit stays out: a few at 73 % load)
+    assert 2950 <= tk.size <= 3000 and np.isin(tk, top).all()
+    assert all(ex[k] == c for k, c in zip(tk.tolist(), tc.tolist()))
+    est = lk.search(uniq)
+    assert bool((est.to(torch.int64) >= exact.to(torch.int64)).all())
