@@ -2,7 +2,7 @@
 """QSketch insert/query throughput on B200 — one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config zipf|uniform|mixed|cm|learned|batched|zipf_prof|batched_prof]
+                    [--config zipf|uniform|mixed|cm|ablation|learned|batched|zipf_prof|batched_prof]
 
 A step is one pass of the hot path over one batch of synthetic input: clear the sketch,
 insert the whole key stream, query the distinct keys.  The default workload is the
@@ -67,6 +67,12 @@ CONFIGS = {
     # the uniform configuration's 2^24 keys at (no more than) its 8 MB, queried for every key
     "cm": dict(workload="countmin_m3_n524287_uniform_2^24keys_query2^24", kind=5, n_keys=1 << 24, n_ranks=0,
                s=0.0, n_low=524287, rows=3, n_high=0, n_query=1 << 24),
+    # ablation: the two-level MSWS against the one-level sketches the reference also ships — the
+    # count-min (m = 3 rows), the warp sketch (32 counters per bucket) and the sub-warp sketches
+    # (8 and 16) — at no more than the uniform configuration's 8 MB of low table, on 2^24 uniform
+    # keys and 2^24 Zipf(1.1) keys over 2^22 ranks
+    "ablation": dict(workload="msws_vs_countmin_warp_subwarp_8MB_uniform_and_zipf1.1_2^24keys", kind=6,
+                     n_keys=1 << 24, n_ranks=1 << 22, s=1.1, n_low=262139, n_high=1 << 16, n_query=0),
     # a smaller skewed case for Nsight Compute captures (key stream still larger than L2)
     "zipf_prof": dict(workload="zipf1.1_2^25keys_2^22ranks_low16MB_high4MB_query2^22", kind=1, n_keys=1 << 25,
                       n_ranks=1 << 22, s=1.1, n_low=524287, n_high=1 << 15, n_query=1 << 22),
@@ -244,6 +250,8 @@ def run_ours(args, cfg):
         return run_batched(args, cfg)
     if cfg["kind"] == 5:
         return run_cm(args, cfg)
+    if cfg["kind"] == 6:
+        return run_ablation(args, cfg)
     if args.shard:
         return run_sharded(args, cfg)
     world, rank, local, barrier, max_over_ranks = init_ranks(args)
@@ -556,6 +564,84 @@ def run_sharded(args, cfg):
             "clocks": clk.summary(),
         }), flush=True)
     ss.local.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_ablation(args, cfg):
+    """The MSWS against the one-level sketches at equal bytes: insert and query Gkeys/s (CUDA
+    events, mean over the steps) and, on the Zipf stream, the average relative error against
+    exact counts of its distinct keys."""
+    import torch
+    import torch.distributed as dist
+
+    import qsketch_b200 as qs
+    from qsketch_b200 import data
+
+    world, rank, local, barrier, max_over_ranks = init_ranks(args)
+    stream = torch.cuda.current_stream()
+    n = cfg["n_keys"]
+    budget = cfg["n_low"] * 32  # the MSWS low table's bytes
+    streams = {"uniform": data.uniform_keys(n, seed=1000 + rank)}
+    zk, zr = data.zipf_keys(n, cfg["n_ranks"], cfg["s"], seed=1000 + rank, perm_seed=99 + rank, with_ranks=True)
+    streams["zipf"] = zk
+    zq = data.rank_keys(99 + rank, 0, cfg["n_ranks"])
+    zexact = data.rank_histogram(zr, cfg["n_ranks"])
+    del zr
+    keep = zexact.view(torch.int32) > 0  # (uint32 tensors index through an int32 view)
+    zq = zq.view(torch.int32)[keep].view(torch.uint32).contiguous()
+    zexact = zexact.view(torch.int32)[keep].view(torch.uint32).contiguous()
+    prime = qs.find_greatest_prime
+    makers = {
+        "msws": lambda: qs.Sketch_GPU_Sub_Warp_Level(cfg["n_low"], 8, cfg["n_high"], 32, hash_seed=SEED, mask_rng=1),
+        "countmin_m3": lambda: qs.Sketch_GPU_Thread(prime(budget // 12), 3, seed_rng=1),
+        "warp_m32": lambda: qs.Sketch_GPU_Warp(prime(budget // 128), 32, hash_seed=SEED, mask_rng=1),
+        "subwarp_m16": lambda: qs.Sketch_GPU_Sub_Warp(prime(budget // 64), 16, hash_seed=SEED, mask_rng=1),
+        "subwarp_m8": lambda: qs.Sketch_GPU_Sub_Warp(prime(budget // 32), 8, hash_seed=SEED, mask_rng=1),
+    }
+    rows = {}
+    with Clocks(local) as clk:
+        for name, make in makers.items():
+            sk = make()
+            row = {"table_bytes": int(sk.info()["n_low"]) * int(sk.info()["m_low"]) * 4}
+            for sname, keys in streams.items():
+                out = torch.empty(n, dtype=torch.uint32, device="cuda")
+                for _ in range(args.warmup):
+                    sk.clear()
+                    sk.insert(keys)
+                    sk.search(keys, counts=out)
+                ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+                barrier()
+                for e in ev:
+                    sk.clear()
+                    e[0].record(stream)
+                    sk.insert(keys)
+                    e[1].record(stream)
+                    sk.search(keys, counts=out)
+                    e[2].record(stream)
+                torch.cuda.synchronize()
+                ins = max_over_ranks(sum(e[0].elapsed_time(e[1]) for e in ev) / args.steps)
+                qry = max_over_ranks(sum(e[1].elapsed_time(e[2]) for e in ev) / args.steps)
+                row[sname] = {"insert_gkeys_per_s": round(n / (ins * 1e6), 3),
+                              "query_gkeys_per_s": round(n / (qry * 1e6), 3)}
+                if sname == "zipf":
+                    rel, _ = data.error_metrics(sk.search(zq), zexact)
+                    row[sname]["avg_rel_error"] = rel
+            rows[name] = row
+            sk.close()
+    if rank == 0:
+        m = rows["msws"]["uniform"]
+        print(json.dumps({
+            "metric": METRIC, "value": round(2 / (1 / m["insert_gkeys_per_s"] + 1 / m["query_gkeys_per_s"]), 4),
+            "unit": "Gkeys/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(2 * n / (2 / (1 / m["insert_gkeys_per_s"] + 1 / m["query_gkeys_per_s"])) / 1e6, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic: seeded uniform and Zipf(1.1) u32 keys",
+            "config": {"workload": cfg["workload"], "n_keys": n, "budget_bytes": budget,
+                       "note": "value: the MSWS on the uniform stream (insert + query of every key); the table "
+                               "compares every sketch on both streams"},
+            "ablation": rows, "gpu_launches": None, "clocks": clk.summary(),
+        }), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
@@ -1121,10 +1207,10 @@ def run_reference(args, cfg):
     world, rank, _ = dist_setup(args.gpus)
     if rank != 0:
         return
-    if cfg["kind"] in (3, 4):
-        print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned heavy-hitter split "
-                          "and no batched multi-sketch path; its plain path is timed under --config zipf, "
-                          "uniform, mixed and cm"}), flush=True)
+    if cfg["kind"] in (3, 4, 6):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned heavy-hitter split, "
+                          "no batched multi-sketch path and no CPU one-level bucket sketches; its plain path is "
+                          "timed under --config zipf, uniform, mixed and cm"}), flush=True)
         return
     threads = os.cpu_count() or 1
     keys, queries, same = reference_inputs(cfg)

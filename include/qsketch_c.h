@@ -49,8 +49,14 @@ typedef enum qs_status {
 typedef enum qs_kind {
     QS_KIND_MSWS = 0,     /* lock-free multi-level sub-warp sketch ("Level"),
                              reference Sketch_GPU_Sub_Warp_Level (device_sketch_v3.h:526) */
-    QS_KIND_PLAIN_CM = 1  /* plain count-min ("thread sketch"),
+    QS_KIND_PLAIN_CM = 1, /* plain count-min ("thread sketch"),
                              reference Sketch_GPU_Thread (device_sketch_v0.h:107) */
+    QS_KIND_BUCKET = 2    /* one-level bucket sketch: n_low buckets of m_low (8, 16 or 32) u32
+                             counters, a key's mask of m_low bits with hash_mask_ones set
+                             selecting its counters in bucket hv % n_low; the reference's warp
+                             sketch Sketch_GPU_Warp (device_sketch_v1.h:237, m = 32) and sub-warp
+                             sketch Sketch_GPU_Sub_Warp (device_sketch_v2.h:289, m < 32), kept for
+                             the ablation against the two-level MSWS */
 } qs_kind;
 
 /* Flags. */

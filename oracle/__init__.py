@@ -42,6 +42,9 @@ def _load():
         "or_msws_query": (None, [P, P, U64, P]),
         "or_msws_remove": (None, [P, P, U64]),
         "or_cm_remove": (None, [P, U64, U32, P, P, U64]),
+        "or_bucket_insert": (None, [P, U64, U32, U32, P, U32, P, U64]),
+        "or_bucket_query": (None, [P, U64, U32, U32, P, U32, P, U64, P]),
+        "or_bucket_remove": (None, [P, U64, U32, U32, P, U32, P, U64]),
         "or_cm_insert": (None, [P, U64, U32, P, P, U64]),
         "or_cm_insert_mt": (None, [P, U64, U32, P, P, U64, ctypes.c_int]),
         "or_cm_query": (None, [P, U64, U32, P, P, U64, P]),
@@ -152,6 +155,37 @@ class CountMin:
         out = np.zeros(k.size, np.uint32)
         lib.or_cm_query(self.table.ctypes.data, self.n, self.m, self.seeds.ctypes.data, k.ctypes.data, k.size,
                         out.ctypes.data)
+        return out
+
+
+class BucketSketch:
+    """One-level bucket sketch (the reference's warp / sub-warp sketches, device_sketch_v1.h /
+    device_sketch_v2.h): n buckets of m u32 counters, H masks of m bits (byte table)."""
+
+    def __init__(self, n, m, seed, mask_table):
+        self.n, self.m, self.seed = n, m, seed
+        mt = np.ascontiguousarray(np.asarray(mask_table, np.uint8)).reshape(-1, m // 8)
+        self.masks = np.zeros(mt.shape[0], np.uint32)
+        for k in range(m // 8):
+            self.masks |= mt[:, k].astype(np.uint32) << np.uint32(8 * k)
+        self.table = np.zeros(n * m, np.uint32)
+
+    def _args(self, k):
+        return (self.table.ctypes.data, self.n, self.m, self.seed, self.masks.ctypes.data, self.masks.size,
+                k.ctypes.data, k.size)
+
+    def insert(self, keys):
+        k = _u32(keys)
+        lib.or_bucket_insert(*self._args(k))
+
+    def remove(self, keys):
+        k = _u32(keys)
+        lib.or_bucket_remove(*self._args(k))
+
+    def query(self, keys):
+        k = _u32(keys)
+        out = np.zeros(k.size, np.uint32)
+        lib.or_bucket_query(*self._args(k), out.ctypes.data)
         return out
 
 

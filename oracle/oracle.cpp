@@ -312,6 +312,44 @@ void or_cm_query(const uint32_t* table, uint64_t n, uint32_t m, const uint32_t* 
 }
 
 // ---------------------------------------------------------------------------------------
+// One-level bucket sketch: the reference's warp sketch (device_sketch_v1.h:50-61 insert,
+// :135-158 query; m = 32) and sub-warp sketch (device_sketch_v2.h:54-64, :156-185; m < 32).
+// n buckets of m u32 counters; key -> hv = key * seed, bucket hv % n, mask word masks[hv % H]
+// (bit i selects counter i); insert adds 1 to every selected counter, query is their minimum,
+// remove takes 1 from every selected counter, floored at 0.
+void or_bucket_insert(uint32_t* table, uint64_t n, uint32_t m, uint32_t seed, const uint32_t* masks, uint32_t H,
+                      const uint32_t* keys, uint64_t nk) {
+    for (uint64_t i = 0; i < nk; ++i) {
+        const uint32_t hv = keys[i] * seed;
+        uint32_t* b = table + (hv % n) * m;
+        for (uint32_t mm = masks[hv % H]; mm; mm &= mm - 1) b[__builtin_ctz(mm)] += 1;
+    }
+}
+
+void or_bucket_query(const uint32_t* table, uint64_t n, uint32_t m, uint32_t seed, const uint32_t* masks, uint32_t H,
+                     const uint32_t* keys, uint64_t nk, uint32_t* out) {
+    for (uint64_t i = 0; i < nk; ++i) {
+        const uint32_t hv = keys[i] * seed;
+        const uint32_t* b = table + (hv % n) * m;
+        uint32_t c = 0xffffffffu;
+        for (uint32_t mm = masks[hv % H]; mm; mm &= mm - 1) c = std::min(c, b[__builtin_ctz(mm)]);
+        out[i] = c;
+    }
+}
+
+void or_bucket_remove(uint32_t* table, uint64_t n, uint32_t m, uint32_t seed, const uint32_t* masks, uint32_t H,
+                      const uint32_t* keys, uint64_t nk) {
+    for (uint64_t i = 0; i < nk; ++i) {
+        const uint32_t hv = keys[i] * seed;
+        uint32_t* b = table + (hv % n) * m;
+        for (uint32_t mm = masks[hv % H]; mm; mm &= mm - 1) {
+            uint32_t& c = b[__builtin_ctz(mm)];
+            if (c) --c;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // Exact counter (host_sketch.h:20-39): counts of `queries` among `keys`.
 void or_exact_counts(const uint32_t* keys, uint64_t n, const uint32_t* queries, uint64_t nq, uint32_t* out) {
     std::unordered_map<uint32_t, uint32_t> um;

@@ -20,6 +20,7 @@ QS_ERR_CAPACITY = 7
 
 QS_KIND_MSWS = 0
 QS_KIND_PLAIN_CM = 1
+QS_KIND_BUCKET = 2
 QS_FLAG_COMPAT_V3 = 0x1
 QS_FLAG_NO_CHUNK_RAMP = 0x2
 

@@ -348,7 +348,8 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
     if (!params || !out) return fail(QS_ERR_INVALID_ARG, "qs_create: null argument");
     *out = nullptr;
     const qs_params& p = *params;
-    if (p.kind != QS_KIND_MSWS && p.kind != QS_KIND_PLAIN_CM) return fail(QS_ERR_INVALID_ARG, "unknown kind %u", p.kind);
+    if (p.kind != QS_KIND_MSWS && p.kind != QS_KIND_PLAIN_CM && p.kind != QS_KIND_BUCKET)
+        return fail(QS_ERR_INVALID_ARG, "unknown kind %u", p.kind);
     if (p.seed_sz != 1) return fail(QS_ERR_INVALID_ARG, "seed_sz must be 1 (lib/default.cu:52)");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -481,6 +482,56 @@ qs_status qs_create(const qs_params* params, qs_sketch** out) {
         sk->L.lanes_per_key = (int)lpk;
         sk->L.tile_keys = (int)tile;
         sk->L.ctas_per_sm = tuned ? (int)tc.ctas_per_sm : (int)p.ctas_per_sm;
+    } else if (p.kind == QS_KIND_BUCKET) {
+        // the reference's warp (m = 32) and sub-warp (m = 8, 16) sketches: n buckets of m u32
+        // counters, masks of m bits with `ones` set (generate_hashmask(H, m), padding 0;
+        // device_sketch_v1.h:254-274)
+        const uint32_t m = p.m_low;
+        if (m != 8 && m != 16 && m != 32) return bail(fail(QS_ERR_INVALID_ARG, "bucket sketch: m_low must be 8, 16 or 32"));
+        const uint64_t n = p.n_low ? p.n_low : qs_find_greatest_prime(p.low_bytes / (4ull * m));
+        if (n == 0 || n > 0xffffffffull) return bail(fail(QS_ERR_INVALID_ARG, "bucket sketch: n out of range"));
+        const uint32_t H = p.hash_mask_table_sz;
+        if (H == 0 || H > 16384) return bail(fail(QS_ERR_INVALID_ARG, "hash_mask_table_sz out of [1, 16384]"));
+        const uint32_t mb = m / 8;  // bytes per mask
+        std::vector<uint8_t> bytes((size_t)H * mb);
+        if (p.mask_table) {
+            std::memcpy(bytes.data(), p.mask_table, bytes.size());
+        } else {
+            if (p.hash_mask_ones == 0 || p.hash_mask_ones > m)
+                return bail(fail(QS_ERR_INVALID_ARG, "hash_mask_ones out of [1, m_low]"));
+            gen_hashmask(p.mask_rng, H, m, p.hash_mask_ones, 0, bytes.data());
+        }
+        sk->masks.resize(H);
+        for (uint32_t i = 0; i < H; ++i) {
+            uint32_t w = 0;
+            for (uint32_t k = 0; k < mb; ++k) w |= (uint32_t)bytes[(size_t)mb * i + k] << (8 * k);
+            if (w == 0) return bail(fail(QS_ERR_INVALID_ARG, "mask %u selects no counter", i));
+            sk->masks[i] = w;
+        }
+        sk->seeds.resize(1);
+        if (p.seeds)
+            sk->seeds[0] = p.seeds[0];
+        else if (p.hash_seed)
+            sk->seeds[0] = p.hash_seed;
+        else
+            draw_seeds(p.seed_rng, 1, sk->seeds.data());  // ds.resize(1, _ss), device_sketch_v1.h:267
+        CmDev& C = sk->C;
+        C.n = n;
+        C.fm = make_fastmod((uint32_t)n);
+        C.rows = m;
+        C.seeds[0] = sk->seeds[0];
+        C.n_masks = H;
+        C.fm_mask = make_fastmod(H);
+        uint32_t* masks_d = nullptr;
+        CKB(sk->alloc(&C.table, n * m), "alloc bucket table");
+        CKB(sk->alloc(&masks_d, H), "alloc masks");
+        CKB(cudaMemcpy(masks_d, sk->masks.data(), (size_t)H * 4, cudaMemcpyHostToDevice), "upload masks");
+        C.masks = masks_d;
+        CKB(sk->alloc(&sk->D.ctl, 1), "alloc control");  // status word (bounded remove loops)
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        sk->cm_grid = sms * 8;
+        CKB(cudaDeviceSynchronize(), "create sync");
     } else {
         const uint32_t rows = p.m_low;
         if (rows == 0 || rows > (uint32_t)MAX_CM_ROWS) return bail(fail(QS_ERR_INVALID_ARG, "cm rows out of [1, 16]"));
@@ -712,6 +763,10 @@ qs_status qs_get_info(qs_sketch* sk, uint64_t* n_low, uint64_t* n_high, uint32_t
         if (n_low) *n_low = sk->C.n;
         if (n_high) *n_high = 0;
         if (m_low) *m_low = sk->C.rows;
+        if (mask_table_out && sk->kind == QS_KIND_BUCKET)  // H masks of m/8 bytes
+            for (size_t i = 0; i < sk->masks.size(); ++i)
+                for (uint32_t k = 0; k < sk->C.rows / 8; ++k)
+                    mask_table_out[i * (sk->C.rows / 8) + k] = (uint8_t)(sk->masks[i] >> (8 * k));
     }
     if (seeds_out) std::memcpy(seeds_out, sk->seeds.data(), sk->seeds.size() * 4);
     return QS_OK;
@@ -836,9 +891,10 @@ qs_status qs_snapshot_load(const void* h_buf, uint64_t bytes, int32_t device, qs
     std::memcpy(&h, in, sizeof h);
     if (std::memcmp(h.magic, SNAP_MAGIC, 8) != 0 || h.version != 1)
         return fail(QS_ERR_INVALID_ARG, "snapshot: not a version-1 QSketch snapshot");
-    const bool msws = h.kind == QS_KIND_MSWS;
-    if ((!msws && h.kind != QS_KIND_PLAIN_CM) || (msws && (h.m_low != LOW_WORDS || h.m_high != HIGH_WORDS)) ||
-        h.n_low == 0 || h.n_seeds == 0 || h.n_seeds > MAX_CM_ROWS || (msws && h.n_masks == 0))
+    const bool msws = h.kind == QS_KIND_MSWS, bucket = h.kind == QS_KIND_BUCKET;
+    if ((!msws && !bucket && h.kind != QS_KIND_PLAIN_CM) || (msws && (h.m_low != LOW_WORDS || h.m_high != HIGH_WORDS)) ||
+        (bucket && h.m_low != 8 && h.m_low != 16 && h.m_low != 32) || h.n_low == 0 || h.n_seeds == 0 ||
+        h.n_seeds > MAX_CM_ROWS || ((msws || bucket) && (h.n_masks == 0 || h.n_masks > 16384)))
         return fail(QS_ERR_INVALID_ARG, "snapshot: inconsistent header");
     const uint64_t lw = h.n_low * h.m_low, hw = msws ? h.n_high * h.m_high : 0;
     const uint64_t payload = 4 * ((uint64_t)h.n_seeds + h.n_masks + lw + hw);
@@ -861,10 +917,17 @@ qs_status qs_snapshot_load(const void* h_buf, uint64_t bytes, int32_t device, qs
     p.m_low = h.m_low;
     p.m_high = msws ? h.m_high : 32;
     p.n_high = msws ? h.n_high : 1024;
-    p.hash_mask_table_sz = msws ? h.n_masks : 1021;
+    p.hash_mask_table_sz = (msws || bucket) ? h.n_masks : 1021;
     p.hash_mask_ones = msws ? h.hash_mask_ones : 3;
     p.seeds = seeds.data();
-    p.mask_table = msws ? reinterpret_cast<const uint8_t*>(masks.data()) : nullptr;
+    std::vector<uint8_t> mbytes;
+    if (bucket) {  // H masks of m/8 bytes
+        const uint32_t mb = h.m_low / 8;
+        mbytes.resize((size_t)h.n_masks * mb);
+        for (size_t i = 0; i < masks.size(); ++i)
+            for (uint32_t k = 0; k < mb; ++k) mbytes[i * mb + k] = (uint8_t)(masks[i] >> (8 * k));
+    }
+    p.mask_table = msws ? reinterpret_cast<const uint8_t*>(masks.data()) : (bucket ? mbytes.data() : nullptr);
     p.device = device;
     qs_sketch* sk = nullptr;
     qs_status st = qs_create(&p, &sk);

@@ -151,13 +151,18 @@ struct BatchWindow {
     uint32_t pad;
 };
 
+// Plain count-min (rows x n counters, one seed per row) or, when `masks` is set, a one-level
+// bucket sketch: n buckets of `rows` u32 counters, a key's mask (of rows bits) selecting its
+// counters in its bucket hv % n (the reference's warp and sub-warp sketches, v1/v2).
 struct CmDev {
     uint32_t* table;  // rows * n
     uint64_t n;
     FastMod fm;
     uint32_t rows;
-    uint32_t pad;
+    uint32_t n_masks;       // bucket sketch: mask count H
     uint32_t seeds[16];
+    const uint32_t* masks;  // bucket sketch: H mask words (bit i selects counter i), else null
+    FastMod fm_mask;
 };
 
 constexpr int REPAIR_TILE = 4096;   // elements per tile in the ordered-replay passes

@@ -95,6 +95,13 @@ __global__ void __launch_bounds__(RM_THREADS) k_cm_remove(const uint32_t* __rest
         const uint32_t peers = __match_any_sync(0xffffffffu, key) & vmask;
         if (!valid || lane != __ffs(peers) - 1) continue;
         const uint32_t c = __popc(peers);
+        if (D.masks) {  // one-level bucket sketch: the selected counters of the key's bucket
+            const uint32_t hv = key * D.seeds[0];
+            uint32_t* bucket = D.table + (uint64_t)fast_mod(D.fm, hv) * D.rows;
+            for (uint32_t mm = __ldg(D.masks + fast_mod(D.fm_mask, hv)); mm; mm &= mm - 1)
+                ok &= sat_sub_u32(bucket + (__ffs(mm) - 1), c);
+            continue;
+        }
         for (uint32_t j = 0; j < D.rows; ++j)
             ok &= sat_sub_u32(D.table + (uint64_t)j * D.n + fast_mod(D.fm, key * D.seeds[j]), c);
     }

@@ -23,7 +23,8 @@ import os
 
 import numpy as np
 
-from ._lib import (QS_FLAG_COMPAT_V3, QS_FLAG_NO_CHUNK_RAMP, QS_KIND_MSWS, QS_KIND_PLAIN_CM, QsError, check, lib,
+from ._lib import (QS_FLAG_COMPAT_V3, QS_FLAG_NO_CHUNK_RAMP, QS_KIND_BUCKET, QS_KIND_MSWS, QS_KIND_PLAIN_CM, QsError,
+                   check, lib,
                    qs_params, qs_profile, qs_stats)
 
 try:  # torch only supplies device memory and the current stream
@@ -219,10 +220,11 @@ def _adopt(h):
     """A Python object over a qs_sketch handle made by qs_load / qs_snapshot_load."""
     p = qs_params()
     check(lib.qs_get_params(h, ctypes.byref(p)), "params")
-    obj = object.__new__(Sketch_GPU_Thread if p.kind == QS_KIND_PLAIN_CM else Sketch_GPU_Sub_Warp_Level)
+    cls = {QS_KIND_PLAIN_CM: Sketch_GPU_Thread, QS_KIND_BUCKET: Sketch_GPU_Warp}.get(p.kind, Sketch_GPU_Sub_Warp_Level)
+    obj = object.__new__(cls)
     obj._handle = h
     obj._keep = None
-    obj._n_masks = 0 if p.kind == QS_KIND_PLAIN_CM else p.hash_mask_table_sz
+    obj._n_masks = p.hash_mask_table_sz if p.kind == QS_KIND_MSWS else 0
     return obj
 
 
@@ -276,6 +278,49 @@ class Sketch_GPU_Sub_Warp_Level(Sketch):
             p.mask_table = mt.ctypes.data
         self._n_masks = n_hash_mask_table
         self._create(p)
+
+
+class Sketch_GPU_Warp(Sketch):
+    """One-level warp sketch (device_sketch_v1.h:237-334): n buckets of m (= 32) u32 counters,
+    each key's mask of m bits selecting hash_mask_ones of them.  Kept for the ablation against
+    the two-level MSWS."""
+
+    def __init__(self, n=0, m=32, seed_sz=1, n_hash_mask_table=1021, *, low_bytes=0, hash_mask_ones=3, hash_seed=0,
+                 seed_rng=1, mask_rng=1, mask_table=None, device=None, aggregate=0):
+        p = qs_params()
+        lib.qs_params_default(ctypes.byref(p))
+        p.kind = QS_KIND_BUCKET
+        p.n_low, p.low_bytes, p.m_low, p.seed_sz = n, low_bytes, m, seed_sz
+        p.hash_mask_table_sz, p.hash_mask_ones = n_hash_mask_table, hash_mask_ones
+        p.hash_seed, p.seed_rng, p.mask_rng, p.aggregate = hash_seed, seed_rng, mask_rng, aggregate
+        p.device = -1 if device is None else int(device)
+        self._keep = None
+        if mask_table is not None:
+            mt = np.ascontiguousarray(np.asarray(mask_table).view(np.uint8).ravel())
+            if mt.size != n_hash_mask_table * m // 8:
+                raise ValueError("mask_table must hold n_hash_mask_table * m / 8 bytes")
+            self._keep = mt
+            p.mask_table = mt.ctypes.data
+        self._n_masks = 0
+        self._create(p)
+
+    def info(self):
+        d = super().info()
+        nl, nh, m = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32()
+        check(lib.qs_get_info(self.handle, ctypes.byref(nl), ctypes.byref(nh), ctypes.byref(m), None, None), "info")
+        pp = qs_params()
+        check(lib.qs_get_params(self.handle, ctypes.byref(pp)), "params")
+        masks = np.zeros(pp.hash_mask_table_sz * m.value // 8, np.uint8)
+        check(lib.qs_get_info(self.handle, None, None, None, None, masks.ctypes.data), "info")
+        d["mask_table"] = masks
+        return d
+
+
+class Sketch_GPU_Sub_Warp(Sketch_GPU_Warp):
+    """One-level sub-warp sketch (device_sketch_v2.h:289-387): buckets of m = 8 or 16 counters."""
+
+    def __init__(self, n=0, m=8, seed_sz=1, n_hash_mask_table=1021, **kw):
+        super().__init__(n, m, seed_sz, n_hash_mask_table, **kw)
 
 
 class Sketch_GPU_Thread(Sketch):

@@ -206,3 +206,12 @@ def test_count_min_remove_floors_at_zero():
             c = j * n + (k * sd % (1 << 32)) % n
             want[c] = max(0, want[c] + d)
     assert np.array_equal(cm.table, want.astype(np.uint32)) and cm.query([1])[0] == 1
+
+
+def test_bucket_sketch_kat():
+    # one bucket of 8 counters, one mask {1, 4, 6}: three inserts of key 5, one removal
+    mt = np.array([(1 << 1) | (1 << 4) | (1 << 6)], np.uint8)
+    s = oracle.BucketSketch(1, 8, 1, mt)
+    s.insert(np.full(3, 5, np.uint32))
+    s.remove(np.array([5, 9], np.uint32))  # key 9 has the same bucket and mask
+    assert list(s.table) == [0, 1, 0, 0, 1, 0, 1, 0] and s.query([5])[0] == 1
