@@ -440,6 +440,11 @@ typedef struct qs_batch_params {
                                      most max_batch keys); 0 = 2^14; QS_FLAG_NO_CHUNK_RAMP in
                                      flags: flat windows of max_batch keys */
     int32_t device;
+    const uint32_t *class_lanes_per_key; /* optional host [64]: lanes per key of pass 1 for the
+                                     streams of size class c = floor(log2 n_low); 0 entries take
+                                     lanes_per_key (or its default).  Streams are grouped by size
+                                     class and each run of classes with one setting is one pass-1
+                                     launch.  qs_batch_autotune sets it from measurements. */
 } qs_batch_params;
 
 typedef struct qs_batch qs_batch;
@@ -464,6 +469,13 @@ qs_status qs_batch_insert_graph(qs_batch *b, const uint32_t *d_keys, const uint6
 qs_status qs_batch_query_graph(qs_batch *b, const uint32_t *d_keys, const uint64_t *d_offsets, uint64_t max_total,
                                uint32_t *d_counts, void *stream);
 qs_status qs_batch_clear(qs_batch *b, void *stream);
+/* The batch autotuner: times pass 1 of each size class's streams with every lanes-per-key
+ * setting (1, 2, 4, 8, 16, 32; at most 8 with fused routing) over `reps` inserts of the first
+ * window (at most max_batch keys) of the given batch into a cleared sketch, then keeps for each
+ * size class the fastest; no setting changes a result.  h_class_lpk (may be null) receives the
+ * 64 per-class choices (0 where no stream has that class).  Leaves the sketches cleared. */
+qs_status qs_batch_autotune(qs_batch *b, const uint32_t *d_keys, const uint64_t *d_offsets, uint64_t total,
+                            uint32_t reps, uint32_t *h_class_lpk);
 /* Waits for `stream`; returns the first latched error (any stream's pool running out is
  * QS_ERR_POOL_FULL; qs_batch_stream_status tells which). */
 qs_status qs_batch_sync(qs_batch *b, void *stream);

@@ -134,6 +134,7 @@ class qs_batch_params(ctypes.Structure):
         ("max_batch", ctypes.c_uint64),
         ("first_chunk", ctypes.c_uint64),
         ("device", ctypes.c_int32),
+        ("class_lanes_per_key", ctypes.c_void_p),
     ]
 
 
@@ -209,6 +210,7 @@ SIGNATURES = {
     "qs_batch_query": (_I, [_P, _P, _P, _U64, _P, _P]),
     "qs_batch_insert_graph": (_I, [_P, _P, _P, _U64, _P]),
     "qs_batch_query_graph": (_I, [_P, _P, _P, _U64, _P, _P]),
+    "qs_batch_autotune": (_I, [_P, _P, _P, _U64, _U32, _P]),
     "qs_batch_clear": (_I, [_P, _P]),
     "qs_batch_sync": (_I, [_P, _P]),
     "qs_batch_stream_status": (_I, [_P, _P]),

@@ -28,7 +28,7 @@ class BatchedSketches:
 
     def __init__(self, n_low, n_high, *, hash_seeds=None, seed_rng=1, mask_rng=1, hash_mask_table_sz=1021,
                  hash_mask_ones=3, compat_v3=False, aggregate=0, route=0, lanes_per_key=0, ctas_per_sm=0,
-                 max_batch=0, first_chunk=0, chunk_ramp=True, device=None):
+                 max_batch=0, first_chunk=0, chunk_ramp=True, device=None, class_lanes_per_key=None):
         nl = np.ascontiguousarray(n_low, dtype=np.uint64)
         nh = np.ascontiguousarray(n_high, dtype=np.uint64)
         if nl.shape != nh.shape or nl.ndim != 1:
@@ -55,6 +55,15 @@ class BatchedSketches:
         if device is None:
             device = torch.cuda.current_device() if torch.cuda.is_available() else -1
         p.device = device
+        self._cls = None
+        if class_lanes_per_key is not None:  # {size class: lanes per key} or a 64-entry sequence
+            arr = np.zeros(64, np.uint32)
+            items = class_lanes_per_key.items() if isinstance(class_lanes_per_key, dict) else \
+                enumerate(class_lanes_per_key)
+            for c, v in items:
+                arr[int(c)] = int(v)
+            self._cls = arr
+            p.class_lanes_per_key = arr.ctypes.data
         h = ctypes.c_void_p()
         check(lib.qs_batch_create(ctypes.byref(p), ctypes.byref(h)), "BatchedSketches")
         self._h = h
@@ -100,6 +109,15 @@ class BatchedSketches:
 
     def clear(self, stream=None):
         check(lib.qs_batch_clear(self.handle, _stream(stream)), "clear")
+
+    def autotune(self, keys, offsets, total=None, reps=3):
+        """qs_batch_autotune: the fastest lanes per key of each size class (floor(log2 n_low)),
+        timed on the first window of this batch; returns {size class: lanes per key}.  Leaves
+        the sketches cleared."""
+        out = np.zeros(64, np.uint32)
+        check(lib.qs_batch_autotune(self.handle, _ptr(keys, "keys"), _offsets_ptr(offsets),
+                                    self._total(offsets, total), reps, out.ctypes.data), "batch autotune")
+        return {c: int(v) for c, v in enumerate(out) if v}
 
     def sync(self, stream=None):
         check(lib.qs_batch_sync(self.handle, _stream(stream)), "sync")

@@ -1665,6 +1665,15 @@ struct qs_batch {
     int graph_ok = -1;  // -1 not tried, 1 works, 0 capture unsupported here
     uint64_t ramp_first = 0;  // per-stream chunk ramp of eager inserts: first slice, 0 = none
     qs_batch_info info{};
+    // Pass 1 runs one launch per run of size classes with the same lanes per key; streams are
+    // grouped by size class floor(log2 n_low) (the grouped order lives in B.cls_streams).
+    std::vector<uint32_t> grp_class;   // size class of each grouped position
+    uint32_t class_lpk[MAX_SIZE_CLASSES] = {};
+    struct Run {
+        uint32_t k_lo, k_hi;
+        int lpk;
+    };
+    std::vector<Run> runs;
 };
 
 namespace {
@@ -1678,6 +1687,18 @@ BatchWindow flat_window(uint64_t c0, uint64_t c1) {
     return W;
 }
 
+// Consecutive size classes with the same lanes per key share one pass-1 launch.
+void batch_rebuild_runs(qs_batch* b) {
+    b->runs.clear();
+    for (uint32_t k = 0; k < b->S; ++k) {
+        const int lpk = (int)b->class_lpk[b->grp_class[k]];
+        if (!b->runs.empty() && b->runs.back().lpk == lpk)
+            b->runs.back().k_hi = k + 1;
+        else
+            b->runs.push_back({k, k + 1, lpk});
+    }
+}
+
 qs_status batch_insert_seq(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets, const BatchWindow& W,
                            bool strict, cudaStream_t st, bool timed = true) {
     qs_sketch* sk = b->sk;
@@ -1685,7 +1706,10 @@ qs_status batch_insert_seq(qs_batch* b, const uint32_t* d_keys, const uint64_t* 
     B.key_off = d_offsets;
     CK(batch_plan(B, sk->D.ctl, W, strict, st), "batch plan");
     if (timed) CK(sk->prof_begin(0, st), "profile");
-    CK(batch_insert_pass(d_keys, sk->D, B, sk->L, sk->agg, st), "batch insert");
+    for (size_t r = 0; r < b->runs.size(); ++r)
+        CK(batch_insert_pass(d_keys, sk->D, B, sk->L, sk->agg, b->runs[r].lpk, b->runs[r].k_lo, b->runs[r].k_hi,
+                             (uint32_t)r, st),
+           "batch insert");
     if (timed) CK(sk->prof_end(0, st), "profile");
     if (timed) CK(sk->prof_begin(1, st), "profile");
     CK(batch_repair(d_keys, sk->D, B, sk->L, st), "batch repair");
@@ -1835,7 +1859,29 @@ qs_status qs_batch_create(const qs_batch_params* p, qs_batch** out) {
     CKB(sk->alloc(&B.item_off, (uint64_t)S + 1), "alloc work items");
     CKB(sk->alloc(&B.wpre, (uint64_t)S + 1), "alloc window prefix");
     CKB(sk->alloc(&B.win, 2), "alloc window");
-    CKB(sk->alloc(&B.work, 1), "alloc work queue");
+    CKB(sk->alloc(&B.work, MAX_SIZE_CLASSES), "alloc work queues");
+    {  // streams grouped by size class (stable), each class's lanes per key
+        std::vector<uint32_t> order(S);
+        for (uint32_t i = 0; i < S; ++i) order[i] = i;
+        auto cls = [&](uint32_t i) { return (uint32_t)size_class(p->n_low[i]); };
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) { return cls(a) < cls(c); });
+        b->grp_class.resize(S);
+        for (uint32_t k = 0; k < S; ++k) b->grp_class[k] = cls(order[k]);
+        uint32_t* d_order = nullptr;
+        CKB(sk->alloc(&d_order, S), "alloc grouped streams");
+        CKB(cudaMemcpy(d_order, order.data(), (size_t)S * 4, cudaMemcpyHostToDevice), "upload grouped streams");
+        B.cls_streams = d_order;
+        CKB(sk->alloc(&B.cls_item_off, (uint64_t)S + 1), "alloc grouped work items");
+        for (uint32_t c = 0; c < MAX_SIZE_CLASSES; ++c) {
+            const uint32_t v = p->class_lanes_per_key ? p->class_lanes_per_key[c] : 0u;
+            if (v && v != 1 && v != 2 && v != 4 && v != 8 && v != 16 && v != 32)
+                return bail(fail(QS_ERR_INVALID_ARG, "class_lanes_per_key[%u] must be 0, 1, 2, 4, 8, 16 or 32", c));
+            if (v > 8 && sk->D.route == 2)
+                return bail(fail(QS_ERR_INVALID_ARG, "class_lanes_per_key[%u]: fused routing takes at most 8", c));
+            b->class_lpk[c] = v ? v : (uint32_t)sk->L.lanes_per_key;
+        }
+        batch_rebuild_runs(b);
+    }
     CKB(sk->alloc(&B.next_id, S), "alloc allocators");
     CKB(sk->alloc(&B.status, S), "alloc stream status");
     CKB(sk->alloc(&B.first, S), "alloc link ranks");
@@ -1994,6 +2040,69 @@ qs_status qs_batch_query_graph(qs_batch* b, const uint32_t* d_keys, const uint64
     if (s == QS_OK && !ran) s = batch_query_seq(b, d_keys, d_offsets, max_total, d_counts, st);
     if (s == QS_OK) ++b->info.queries;
     return s;
+}
+
+qs_status qs_batch_autotune(qs_batch* b, const uint32_t* d_keys, const uint64_t* d_offsets, uint64_t total,
+                            uint32_t reps, uint32_t* h_class_lpk) {
+    if (!b || !d_keys || !d_offsets) return fail(QS_ERR_INVALID_ARG, "qs_batch_autotune: null argument");
+    qs_sketch* sk = b->sk;
+    DeviceGuard guard(sk->device);
+    reps = std::max(1u, reps);
+    // each size class's grouped range
+    std::vector<std::pair<uint32_t, uint32_t>> range(MAX_SIZE_CLASSES, {0u, 0u});
+    for (uint32_t k = 0; k < b->S; ++k) {
+        auto& r = range[b->grp_class[k]];
+        if (r.first == r.second) r.first = k;
+        r.second = k + 1;
+    }
+    std::vector<double> best(MAX_SIZE_CLASSES, 1e300);
+    uint32_t pick[MAX_SIZE_CLASSES] = {};
+    cudaEvent_t ev[2 * MAX_SIZE_CLASSES];
+    for (auto& e : ev) CK(cudaEventCreate(&e), "tuner events");
+    auto destroy = [&] {
+        for (auto& e : ev) cudaEventDestroy(e);
+    };
+    const BatchWindow W = flat_window(0, std::min<uint64_t>(total, sk->max_batch));
+    qs_status st = QS_OK;
+    for (int lpk : {4, 2, 8, 1, 16, 32}) {
+        if (lpk > 8 && sk->D.route == 2) continue;
+        std::vector<double> t(MAX_SIZE_CLASSES, 0.0);
+        for (uint32_t r = 0; r < reps && st == QS_OK; ++r) {
+            st = qs_batch_clear(b, nullptr);
+            if (st != QS_OK) break;
+            BatchDev B = b->B;
+            B.key_off = d_offsets;
+            cudaError_t e = batch_plan(B, sk->D.ctl, W, false, 0);
+            for (uint32_t c = 0; c < MAX_SIZE_CLASSES && e == cudaSuccess; ++c) {
+                if (range[c].first == range[c].second) continue;
+                cudaEventRecord(ev[2 * c], 0);
+                e = batch_insert_pass(d_keys, sk->D, B, sk->L, sk->agg, lpk, range[c].first, range[c].second, c, 0);
+                cudaEventRecord(ev[2 * c + 1], 0);
+            }
+            if (e == cudaSuccess) e = batch_repair(d_keys, sk->D, B, sk->L, 0);
+            if (e == cudaSuccess) e = cudaDeviceSynchronize();
+            for (uint32_t c = 0; c < MAX_SIZE_CLASSES && e == cudaSuccess; ++c) {
+                if (range[c].first == range[c].second) continue;
+                float ms = 0;
+                e = cudaEventElapsedTime(&ms, ev[2 * c], ev[2 * c + 1]);
+                t[c] += ms;
+            }
+            if (e != cudaSuccess) st = cuda_fail(e, "batch autotune");
+        }
+        if (st != QS_OK) break;
+        for (uint32_t c = 0; c < MAX_SIZE_CLASSES; ++c)
+            if (range[c].first != range[c].second && t[c] < best[c]) {
+                best[c] = t[c];
+                pick[c] = (uint32_t)lpk;
+            }
+    }
+    destroy();
+    if (st != QS_OK) return st;
+    for (uint32_t c = 0; c < MAX_SIZE_CLASSES; ++c)
+        if (pick[c]) b->class_lpk[c] = pick[c];
+    batch_rebuild_runs(b);
+    if (h_class_lpk) std::memcpy(h_class_lpk, pick, sizeof pick);
+    return qs_batch_clear(b, nullptr);
 }
 
 qs_status qs_batch_clear(qs_batch* b, void* stream) {

@@ -131,7 +131,9 @@ struct BatchDev {
     uint32_t* wpre;           // [n_streams + 1] prefix of the slices' key counts: window key i of
                               // stream s is flat key lo[s] + i - wpre[s]
     uint64_t* win;            // [2] 0 and the window's key count
-    uint32_t* work;           // work-queue head
+    uint32_t* work;           // work-queue heads, one per size-class launch of pass 1
+    const uint32_t* cls_streams; // [n_streams] the streams grouped by size class (pass-1 launches)
+    uint32_t* cls_item_off;   // [n_streams + 1] prefix of work items in the grouped order
     uint32_t* next_id;        // [n_streams] per-stream bump allocators (from FIRST_ID)
     uint32_t* status;         // [n_streams] latched ST_* bits per stream
     unsigned long long* first;// [n_streams] (repair generation << 32) | ~(lowest rank of the
@@ -168,6 +170,7 @@ struct CmDev {
 constexpr int REPAIR_TILE = 4096;   // elements per tile in the ordered-replay passes
 constexpr int REPAIR_THREADS = 512; // 16 warps x 256 elements
 constexpr int MAX_CM_ROWS = 16;
+constexpr uint32_t MAX_SIZE_CLASSES = 64;  // floor(log2 n_low) of a batched stream's sketch
 
 // Spread a 4-bit nibble to the low bit of each byte: b0->bit0, b1->bit8, b2->bit16, b3->bit24.
 __device__ __forceinline__ uint32_t expand_nibble(uint32_t nib) {

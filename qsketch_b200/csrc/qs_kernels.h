@@ -27,8 +27,9 @@ cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L);
 // most max_batch keys; the repair exits at once when nothing crossed.
 // Batched streams (StreamDesc / BatchDev in qs_common.cuh).
 cudaError_t batch_plan(const BatchDev& B, Ctl* ctl, const BatchWindow& W, bool strict, cudaStream_t st);
+// Pass 1 of the streams [k_lo, k_hi) of the size-class grouped order (work counter cls).
 cudaError_t batch_insert_pass(const uint32_t* d_keys, const MswsDev& D, const BatchDev& B, const MswsLaunch& L,
-                              int agg, cudaStream_t st);
+                              int agg, int lanes_per_key, uint32_t k_lo, uint32_t k_hi, uint32_t cls, cudaStream_t st);
 cudaError_t batch_repair(const uint32_t* d_window, const MswsDev& D, const BatchDev& B, const MswsLaunch& L,
                          cudaStream_t st);
 cudaError_t batch_query(const uint32_t* d_keys, uint32_t* d_out, const MswsDev& D, const BatchDev& B,

@@ -870,8 +870,9 @@ __device__ __forceinline__ ReplayOut replay_scan(const MswsDev& D, const uint2* 
 // records) for the link order; when its slot has a totals row (s < long_cap) the low words
 // are written now and the high increments wait in that row, otherwise the bucket is replayed
 // again once its high id is known.
-__device__ __forceinline__ void settle_bucket(const MswsDev& D, uint32_t s, uint32_t b, const ReplayOut& o,
-                                              uint32_t pos) {
+template <bool BATCH>
+__device__ __forceinline__ void settle_bucket(const MswsDev& D, const BatchDev& B, unsigned long long gen, uint32_t s,
+                                              uint32_t b, const ReplayOut& o, uint32_t pos) {
     const int lane = threadIdx.x & 31;
     if (o.found) {
         if (s < D.long_cap) {
@@ -883,6 +884,11 @@ __device__ __forceinline__ void settle_bucket(const MswsDev& D, uint32_t s, uint
             __stcg(D.sw + s, make_uint2(pos, o.n_after));
             atomicOr(D.sw_bits + (pos >> 5), 1u << (pos & 31));
             atomicAdd(D.sw_cnt + pos / SW_BLOCK, 1u);
+            if (BATCH) {  // the stream's first switch position of this repair, and its allocator
+                const uint32_t st = stream_of_bucket(B, b);  // (nothing writes it before the barrier)
+                atomicMax(B.first + st, (gen << 32) | (unsigned long long)(~pos));
+                __stcg(D.sw_base + s, __ldcg(B.next_id + st));
+            }
         }
     } else {
         if (lane == 0) __stcg(D.sw + s, make_uint2(NONE, 0u));
@@ -975,11 +981,11 @@ __device__ __forceinline__ void finish_link(const MswsDev& D, uint32_t s, uint32
 // chunk gets id next_id + r, as one-key-at-a-time insertion hands them out
 // (atomic_malloc, device_sketch_v3.h:69-85); once the pool is used up the remaining buckets
 // saturate.  Batched streams rank within their stream (each has its own allocator): the
-// stream's lowest rank in this repair is found with a generation-tagged atomicMax, then a
-// second pass links.  one_block: every slot lives in block 0 and only it runs this.
-// Returns false when a grid barrier timed out.
+// replay recorded the stream's first switch position (generation-tagged atomicMax) and its
+// allocator before the barrier, and a bucket's rank in its stream is its rank minus that
+// position's.  one_block: every slot lives in block 0 and only it runs this.
 template <bool BATCH, typename Rerun>
-__device__ __forceinline__ bool link_phase(const MswsDev& D, const BatchDev& B, uint32_t F, uint32_t K,
+__device__ __forceinline__ void link_phase(const MswsDev& D, const BatchDev& B, uint32_t F, uint32_t K,
                                            uint32_t base_id, unsigned long long gen, bool one_block, Rerun rerun,
                                            uint32_t* s_small, uint32_t* s_big) {
     Ctl* ctl = D.ctl;
@@ -999,35 +1005,18 @@ __device__ __forceinline__ bool link_phase(const MswsDev& D, const BatchDev& B, 
         if (!BATCH) {
             const uint32_t id = base_id + rank;
             finish_link(D, s, b, id, (uint64_t)(id - START) < D.n_high, w.y, rerun);
-        } else if (lane == 0) {
-            const uint32_t st = stream_of_bucket(B, b);
-            atomicMax(B.first + st, (gen << 32) | (unsigned long long)(~rank));
-            __stcg(D.sw_base + s, __ldcg(B.next_id + st));
-            __stcg(D.sw + s, make_uint2(rank, w.y));
+            continue;
         }
-    }
-    if (!BATCH) {
-        if (blockIdx.x == 0 && tid == 0) {  // the allocator stops at the pool's end, as the oracle's
-            const unsigned long long nid = min((unsigned long long)base_id + nfound, (unsigned long long)START + D.n_high);
-            if (nid > base_id) ctl->next_id = (uint32_t)nid;
-        }
-        return true;
-    }
-    if (one_block)
-        __syncthreads();
-    else if (!grid_barrier(ctl))
-        return false;
-    for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) {
-        const uint2 w = __ldcg(D.sw + s);
-        if (w.x == NONE) continue;
-        const uint32_t b = __ldcg(D.flag_list + s);
-        uint32_t st = 0, own = 0;
+        // batched streams: the rank among the stream's own switches (its positions are
+        // contiguous in the window) on top of the stream's allocator read before the barrier
+        uint32_t st = 0, fp = 0;
         if (lane == 0) {
             st = stream_of_bucket(B, b);
-            own = __ldcg(D.sw_base + s) + (w.x - ~(uint32_t)__ldcg(B.first + st));
+            fp = ~(uint32_t)__ldcg(B.first + st);
         }
         st = __shfl_sync(0xffffffffu, st, 0);
-        own = __shfl_sync(0xffffffffu, own, 0);
+        fp = __shfl_sync(0xffffffffu, fp, 0);
+        const uint32_t own = __ldcg(D.sw_base + s) + (rank - switch_rank(D, spre, fp));
         const uint32_t nh = __ldg(&B.desc[st].n_high);
         const bool ok = (uint64_t)(own - START) < nh;
         finish_link(D, s, b, own + __ldg(&B.desc[st].high_base), ok, w.y, rerun);
@@ -1036,7 +1025,10 @@ __device__ __forceinline__ bool link_phase(const MswsDev& D, const BatchDev& B, 
             if (!ok) atomicOr(B.status + st, ST_POOL_FULL);
         }
     }
-    return true;
+    if (!BATCH && blockIdx.x == 0 && tid == 0) {  // the allocator stops at the pool's end, as the oracle's
+        const unsigned long long nid = min((unsigned long long)base_id + nfound, (unsigned long long)START + D.n_high);
+        if (nid > base_id) ctl->next_id = (uint32_t)nid;
+    }
 }
 
 // BATCH: `keys` is the batch's flat key array and the chunk is the window the plan kernel
@@ -1233,7 +1225,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
             for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) {
                 const uint32_t b = __ldcg(D.flag_list + s);
                 const ReplayOut o = replay_scan(D, srec, s, K, b);
-                settle_bucket(D, s, b, o, o.L);
+                settle_bucket<BATCH>(D, B, gen, s, b, o, o.L);
             }
         }
         phase_mark(ctl, 5);
@@ -1247,7 +1239,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
             return;
         }
         auto rerun = [&](uint32_t s, uint32_t b) { return replay_scan(D, srec, s, K, b); };
-        if (!link_phase<BATCH>(D, B, F, K, base_id, gen, one_block, rerun, s_swpre, s_set)) return;
+        link_phase<BATCH>(D, B, F, K, base_id, gen, one_block, rerun, s_swpre, s_set);
         phase_mark(ctl, 9);
         finish_repair(ctl);
         return;
@@ -1519,7 +1511,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
     for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) {
         const uint32_t b = __ldcg(D.flag_list + s);
         const ReplayOut o = replay_sorted(D, sorted, s, F, K, b);
-        settle_bucket(D, s, b, o, o.found ? (fpos ? __ldcg(fpos + o.L) : o.L) : 0u);
+        settle_bucket<BATCH>(D, B, gen, s, b, o, o.found ? (fpos ? __ldcg(fpos + o.L) : o.L) : 0u);
     }
     phase_mark(ctl, 5);
     if (one_block) {
@@ -1532,7 +1524,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
         return;
     }
     auto rerun = [&](uint32_t s, uint32_t b) { return replay_sorted(D, sorted, s, F, K, b); };
-    if (!link_phase<BATCH>(D, B, F, K, base_id, gen, one_block, rerun, s_swpre, s_set)) return;
+    link_phase<BATCH>(D, B, F, K, base_id, gen, one_block, rerun, s_swpre, s_set);
     phase_mark(ctl, 9);
     finish_repair(ctl);
 }
@@ -1668,14 +1660,22 @@ __global__ void __launch_bounds__(1024) k_batch_plan(BatchDev B, BatchWindow W, 
         B.wpre[s] = (uint32_t)(hi - lo);
     }
     __syncthreads();
+    // the same work items in the grouped (size-class) order of the pass-1 launches
+    for (uint32_t k = threadIdx.x; k < S; k += blockDim.x) {
+        const uint32_t s = __ldg(B.cls_streams + k);
+        B.cls_item_off[k] = B.item_off[s];
+    }
+    __syncthreads();
     const uint32_t items = block_scan_array(B.item_off, S);
     const uint32_t keys = block_scan_array(B.wpre, S);
+    block_scan_array(B.cls_item_off, S);
+    for (uint32_t c = threadIdx.x; c < MAX_SIZE_CLASSES; c += blockDim.x) B.work[c] = 0;
     if (threadIdx.x == 0) {
         B.item_off[S] = items;
+        B.cls_item_off[S] = items;
         B.wpre[S] = keys;
         B.win[0] = 0;
         B.win[1] = keys;
-        *B.work = 0;
         if (bad) atomicOr(&ctl->status, ST_BAD_OFFSETS);
         if (strict && !bad && total > W.c1) atomicOr(&ctl->status, ST_CAPACITY);
     }
@@ -1699,12 +1699,32 @@ __device__ __forceinline__ uint32_t stream_of_item_warp(const BatchDev& B, uint3
     return lo;
 }
 
+// The grouped index k in [k_lo, k_hi) whose items hold work item `it` (cls_item_off[k] <=
+// it), by a whole warp as stream_of_item_warp.
+__device__ __forceinline__ uint32_t group_of_item_warp(const BatchDev& B, uint32_t it, uint32_t k_lo, uint32_t k_hi) {
+    const int lane = threadIdx.x & 31;
+    uint32_t lo = k_lo, hi = k_hi;
+    while (hi - lo > 1) {
+        const uint32_t step = (hi - lo + 31) / 32;
+        const uint32_t idx = lo + lane * step;
+        const bool le = idx < hi && __ldcg(B.cls_item_off + idx) <= it;
+        const uint32_t bal = __ballot_sync(0xffffffffu, le);  // lane 0 always holds
+        const uint32_t last = 31 - __clz(bal);
+        lo += last * step;
+        hi = min(hi, lo + step);
+    }
+    return lo;
+}
+
 // Pass 1 over a batch: a persistent grid pulls tiles from the work queue; a tile's keys
 // all belong to one stream, so they hash with its descriptor and the tile's shared-memory
 // merge table never mixes sketches.  Everything after hashing is the single-sketch pass 1.
+// One launch covers the streams [k_lo, k_hi) of the size-class grouped order (work counter
+// `cls`), so each size class runs with its own lanes per key.
 template <int AGG, int LPK>
 __global__ void __launch_bounds__(INS_THREADS, INS_MIN_CTAS) k_batch_insert(const uint32_t* __restrict__ keys, MswsDev D,
-                                                                 BatchDev B) {
+                                                                 BatchDev B, uint32_t k_lo, uint32_t k_hi,
+                                                                 uint32_t cls) {
     extern __shared__ __align__(128) uint8_t smem[];
     const InsShared S = ins_carve(smem, D.n_masks);
     __shared__ uint32_t s_item, s_stream;
@@ -1719,26 +1739,31 @@ __global__ void __launch_bounds__(INS_THREADS, INS_MIN_CTAS) k_batch_insert(cons
         S.misc[1] = 0;
         S.misc[2] = D.route == 2 ? ROUTE_FUSED : ROUTE_PRELOAD;
     }
-    const uint32_t n_items = __ldcg(B.item_off + B.n_streams);
+    const uint32_t item_lo = __ldcg(B.cls_item_off + k_lo), n_items = __ldcg(B.cls_item_off + k_hi);
     for (;;) {
         if (wid == 0) {  // warp 0 takes the next work item and finds its stream
             uint32_t it = 0;
-            if (lane == 0) it = atomicAdd(B.work, 1u);
+            if (lane == 0) it = item_lo + atomicAdd(B.work + cls, 1u);
             it = __shfl_sync(0xffffffffu, it, 0);
-            const uint32_t s = it < n_items ? stream_of_item_warp(B, it) : 0u;
+            uint32_t s = 0, first = 0;
+            if (it < n_items) {
+                const uint32_t k = group_of_item_warp(B, it, k_lo, k_hi);
+                s = __ldg(B.cls_streams + k);
+                first = __ldcg(B.cls_item_off + k);
+            }
             if (lane == 0) {
-                s_item = it;
-                s_stream = s;
+                s_item = it - first;  // the item's index within its stream
+                s_stream = it < n_items ? s : 0xffffffffu;
             }
         }
         __syncthreads();
-        const uint32_t it = s_item;
-        if (it >= n_items) break;
+        if (s_stream == 0xffffffffu) break;
         const uint32_t s = s_stream;
+        const uint32_t it_local = s_item;
         const StreamDesc* sd = B.desc + s;
         const uint32_t seed = __ldg(&sd->seed), base = __ldg(&sd->low_base);
         const FastMod fm{__ldg(&sd->fm_low.M), __ldg(&sd->fm_low.d), 0u};
-        const uint64_t t0 = __ldcg(B.lo + s) + (uint64_t)(it - __ldcg(B.item_off + s)) * INS_TILE;
+        const uint64_t t0 = __ldcg(B.lo + s) + (uint64_t)it_local * INS_TILE;
         const int cnt = (int)umin64(INS_TILE, __ldcg(B.hi + s) - t0);
         const int route = (int)S.misc[2];
         for (int b = wid * 32; b < cnt; b += INS_THREADS) {
@@ -1906,12 +1931,12 @@ cudaError_t batch_plan(const BatchDev& B, Ctl* ctl, const BatchWindow& W, bool s
 }
 
 cudaError_t batch_insert_pass(const uint32_t* d_keys, const MswsDev& D, const BatchDev& B, const MswsLaunch& L,
-                              int agg, cudaStream_t st) {
+                              int agg, int lanes_per_key, uint32_t k_lo, uint32_t k_hi, uint32_t cls, cudaStream_t st) {
     const size_t smem = msws_insert_smem(D.n_masks);
-    const int li = lpk_index(L.lanes_per_key);
+    const int li = lpk_index(lanes_per_key);
     MswsDev Dc = D;
     BatchDev Bc = B;
-    void* args[] = {(void*)&d_keys, (void*)&Dc, (void*)&Bc};
+    void* args[] = {(void*)&d_keys, (void*)&Dc, (void*)&Bc, (void*)&k_lo, (void*)&k_hi, (void*)&cls};
     return cudaLaunchKernel(ins_fn(agg, li, true), dim3(ins_grid(L, agg, li)), dim3(INS_THREADS), args, smem, st);
 }
 

@@ -220,3 +220,28 @@ def test_batch_uneven_streams_full_size(gpu):
     full = np.nonzero(b.stream_status() & 1)[0]
     assert full.size > 10, "the workload is meant to exhaust some pools"
     check_streams(b, w, got, tables=set(range(0, 512, 8)) | set(full.tolist()))
+
+
+def test_batch_per_size_class_lanes_per_key(gpu):
+    # every size class with its own lanes per key (one pass-1 launch per run of classes): each
+    # stream still equals the stream alone, tables included
+    w = workload(48, seed=13, max_len=1 << 16)
+    classes = sorted({int(np.floor(np.log2(float(n)))) for n in w["n_low"]})
+    lpk = {c: [1, 2, 4, 8, 16, 32][i % 6] for i, c in enumerate(classes)}
+    b = BatchedSketches(w["n_low"], w["n_high"], seed_rng=7, max_batch=1 << 18, class_lanes_per_key=lpk)
+    b.insert(w["keys"], w["offsets"])
+    got = b.search(w["keys"], w["offsets"])
+    b.sync()
+    check_streams(b, w, got)
+
+
+def test_batch_autotune_picks_per_class_and_keeps_results(gpu):
+    w = workload(32, seed=17, max_len=1 << 16)
+    b = BatchedSketches(w["n_low"], w["n_high"], seed_rng=3, max_batch=1 << 19)
+    picks = b.autotune(w["keys"], w["offsets"], reps=1)
+    classes = {int(np.floor(np.log2(float(n)))) for n in w["n_low"]}
+    assert set(picks) == classes and set(picks.values()) <= {1, 2, 4, 8, 16, 32}
+    b.insert(w["keys"], w["offsets"])
+    got = b.search(w["keys"], w["offsets"])
+    b.sync()
+    check_streams(b, w, got, tables=False)
