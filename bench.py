@@ -939,6 +939,14 @@ def run_batched(args, cfg):
     total = keys.numel()
     out = torch.empty(total, dtype=torch.uint32, device="cuda")
     b = BatchedSketches(w["n_low"], w["n_high"], seed_rng=1 + rank, max_batch=1 << 22)
+    # lanes per key per sketch-size class, timed on other keys of the same stream shapes
+    cls_lpk = {}
+    if args.autotune:
+        tw = data.uneven_streams(S, seed=1000 + rank, n_ranks=cfg["n_ranks"], max_len=cfg.get("max_len", 1 << 22),
+                                 key_seed=5000 + rank)
+        cls_lpk = b.autotune(tw["keys"], tw["offsets"], reps=2)
+        del tw
+        torch.cuda.empty_cache()
 
     def step(ev=None):
         b.clear()
@@ -1067,9 +1075,11 @@ def run_batched(args, cfg):
                        "table_bytes": int(info["table_bytes"]), "streams_pool_full": int(info["streams_pool_full"]),
                        "l2": "key stream of %d MB and tables of %d MB per step > 126 MB L2"
                              % (total * 4 >> 20, info["table_bytes"] >> 20),
-                       "parallelism": "independent batch per GPU" if world > 1 else "single GPU"},
+                       "parallelism": "independent batch per GPU" if world > 1 else "single GPU",
+                       "class_lanes_per_key": {str(k): v for k, v in cls_lpk.items()}},
             "insert_gkeys_per_s": round(world * total / (ins_ms * 1e6), 4),
             "query_gkeys_per_s": round(world * total / (q_ms * 1e6), 4),
+            "repair_phase_ms": [round(x, 3) for x in prof["repair_phase_ms"]],
             "alone": {"ms": round(alone_ms, 3), "gkeys_per_s": round(2 * total / (alone_ms * 1e6), 4),
                       "note": "the same streams through %d separate sketches, one insert + one query call each" % S},
             "serving_batch": {"keys": int(sv_keys.numel()), "eager_ms": round(lat["eager"], 4),

@@ -471,9 +471,12 @@ qs_status qs_batch_query_graph(qs_batch *b, const uint32_t *d_keys, const uint64
 qs_status qs_batch_clear(qs_batch *b, void *stream);
 /* The batch autotuner: times pass 1 of each size class's streams with every lanes-per-key
  * setting (1, 2, 4, 8, 16, 32; at most 8 with fused routing) over `reps` inserts of the first
- * window (at most max_batch keys) of the given batch into a cleared sketch, then keeps for each
- * size class the fastest; no setting changes a result.  h_class_lpk (may be null) receives the
- * 64 per-class choices (0 where no stream has that class).  Leaves the sketches cleared. */
+ * window (at most max_batch keys) of the given batch into a cleared sketch and picks each
+ * class's fastest; then, because per-class settings split pass 1 into one launch per run of
+ * classes, it times the whole qs_batch_insert of the batch with each width for every class and
+ * with the per-class picks, and keeps the fastest of those.  No setting changes a result.
+ * h_class_lpk (may be null) receives the 64 per-class settings in effect (0 where no stream
+ * has that class).  Leaves the sketches cleared. */
 qs_status qs_batch_autotune(qs_batch *b, const uint32_t *d_keys, const uint64_t *d_offsets, uint64_t total,
                             uint32_t reps, uint32_t *h_class_lpk);
 /* Waits for `stream`; returns the first latched error (any stream's pool running out is

@@ -2096,12 +2096,60 @@ qs_status qs_batch_autotune(qs_batch* b, const uint32_t* d_keys, const uint64_t*
                 pick[c] = (uint32_t)lpk;
             }
     }
+    if (st != QS_OK) {
+        destroy();
+        return st;
+    }
+    // Per-class picks split pass 1 into several launches per window; a launch has a fixed cost.
+    // So the whole insert call decides: each width for every class, and the per-class picks,
+    // timed over the full batch (clear + qs_batch_insert), the fastest kept.
+    auto time_insert = [&](double* ms) -> qs_status {
+        double tot = 0;
+        for (uint32_t r = 0; r < reps; ++r) {
+            qs_status q = qs_batch_clear(b, nullptr);
+            if (q != QS_OK) return q;
+            CK(cudaEventRecord(ev[0], 0), "tuner event");
+            q = qs_batch_insert(b, d_keys, d_offsets, total, nullptr);
+            if (q != QS_OK) return q;
+            CK(cudaEventRecord(ev[1], 0), "tuner event");
+            CK(cudaEventSynchronize(ev[1]), "tuner sync");
+            float m = 0;
+            CK(cudaEventElapsedTime(&m, ev[0], ev[1]), "tuner time");
+            tot += m;
+        }
+        *ms = tot / reps;
+        return QS_OK;
+    };
+    uint32_t best_set[MAX_SIZE_CLASSES];
+    double best_ms = 1e300;
+    auto try_set = [&](const uint32_t* set) -> qs_status {
+        std::memcpy(b->class_lpk, set, sizeof b->class_lpk);
+        batch_rebuild_runs(b);
+        double ms = 0;
+        qs_status q = time_insert(&ms);
+        if (q == QS_OK && ms < best_ms) {
+            best_ms = ms;
+            std::memcpy(best_set, set, sizeof best_set);
+        }
+        return q;
+    };
+    for (int lpk : {4, 2, 8, 1, 16, 32}) {
+        if ((lpk > 8 && sk->D.route == 2) || st != QS_OK) continue;
+        uint32_t set[MAX_SIZE_CLASSES];
+        for (auto& x : set) x = (uint32_t)lpk;
+        st = try_set(set);
+    }
+    if (st == QS_OK) {
+        uint32_t set[MAX_SIZE_CLASSES];
+        for (uint32_t c = 0; c < MAX_SIZE_CLASSES; ++c) set[c] = pick[c] ? pick[c] : best_set[0];
+        st = try_set(set);
+    }
     destroy();
     if (st != QS_OK) return st;
-    for (uint32_t c = 0; c < MAX_SIZE_CLASSES; ++c)
-        if (pick[c]) b->class_lpk[c] = pick[c];
+    std::memcpy(b->class_lpk, best_set, sizeof b->class_lpk);
     batch_rebuild_runs(b);
-    if (h_class_lpk) std::memcpy(h_class_lpk, pick, sizeof pick);
+    if (h_class_lpk)
+        for (uint32_t c = 0; c < MAX_SIZE_CLASSES; ++c) h_class_lpk[c] = pick[c] ? best_set[c] : 0u;
     return qs_batch_clear(b, nullptr);
 }
 

@@ -74,12 +74,13 @@ def probe(kind, nbytes, ops=1 << 26):
 
 
 def uneven_streams(n_streams, seed, min_len=1 << 10, max_len=1 << 22, n_ranks=1 << 20, s_range=(0.6, 1.4),
-                   min_bytes=32 << 10, max_bytes=16 << 20, pool_div=4, device="cuda", stream=None):
+                   min_bytes=32 << 10, max_bytes=16 << 20, pool_div=4, device="cuda", stream=None, key_seed=None):
     """The batched-streams workload: per stream a length and a sketch size drawn log-uniformly,
     a Zipf exponent drawn uniformly, and a Zipf key stream over n_ranks ranks under the
     stream's own seeded bijection.  Sketch of stream s: n_low = find_greatest_prime(bytes/32),
     high pool bytes/pool_div.  Returns a dict: keys (flat uint32), offsets (int64, n+1),
-    lengths, s, n_low, n_high (numpy)."""
+    lengths, s, n_low, n_high (numpy).  key_seed (default: seed) draws other keys for the same
+    shapes (lengths, exponents, sketch sizes)."""
     import numpy as np
 
     from .sketch import find_greatest_prime
@@ -92,8 +93,9 @@ def uneven_streams(n_streams, seed, min_len=1 << 10, max_len=1 << 22, n_ranks=1 
     offsets = np.zeros(n_streams + 1, np.int64)
     offsets[1:] = np.cumsum(lengths)
     keys = torch.empty(int(offsets[-1]), dtype=torch.uint32, device=device)
+    ks = seed if key_seed is None else key_seed
     for i in range(n_streams):
-        check(lib.qs_gen_keys(1, seed * 1000003 + i, n_ranks, float(expo[i]), seed * 7919 + i,
+        check(lib.qs_gen_keys(1, ks * 1000003 + i, n_ranks, float(expo[i]), ks * 7919 + i,
                               keys.data_ptr() + int(offsets[i]) * 4, None, int(lengths[i]), _s(stream)),
               "uneven_streams")
     return {"keys": keys, "offsets": torch.from_numpy(offsets).to(device), "lengths": lengths, "s": expo,
