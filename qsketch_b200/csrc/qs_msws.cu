@@ -26,8 +26,11 @@ namespace qsb {
 constexpr int INS_THREADS = 256;
 constexpr int INS_WARPS = INS_THREADS / 32;
 constexpr int INS_TILE = 2048;  // keys per TMA stage (8 KiB)
-constexpr int INS_STAGES = 3;
-constexpr int INS_MIN_CTAS = 4;  // resident pass-1 CTAs per SM the register budget is cut for (6 measured slower)
+constexpr int INS_STAGES = 2;      // one tile in flight while one is inserted (a tile takes ~30 us; two
+                                   // stages leave the shared memory of five CTAs per SM)
+constexpr int INS_MIN_CTAS = 5;  // resident pass-1 CTAs per SM the register budget is cut for: the
+                                 // returning atomics are latency bound, so warps in flight pay (4: 17 % slower
+                                 // on Zipf 1.1; 6 forces 40 registers and is slower again)
 constexpr int AGG_SLOTS = 1024; // per-CTA table merging the linked keys of a tile
 // mbarriers of the stages (+ one spare word), padded so the uint4 staging area that follows
 // the 4-byte tables stays 16-byte aligned for any stage count
@@ -141,10 +144,58 @@ __device__ __forceinline__ bool agg_insert(const InsShared& S, uint32_t key, uin
 
 // Does a selected byte (nibble bit k selects byte k) of the pre-add word `old` reach CROSS
 // once c is added: byte + c >= CROSS, i.e. byte >= CROSS - c, four bytes at a time.
+// Selected bytes all below 64 with c below 64 cannot reach CROSS: a two-operation test
+// settles the common case before the four-byte comparison.
 __device__ __forceinline__ bool crosses(uint32_t old, uint32_t nib, uint32_t c) {
     if (!nib) return false;
     if (c >= CROSS) return true;
-    return (__vcmpgeu4(old, (CROSS - c) * 0x01010101u) & (expand_nibble(nib) * 0xffu)) != 0u;
+    const uint32_t sel = expand_nibble(nib) * 0xffu;
+    if (c < 64u && !(old & sel & 0xC0C0C0C0u)) return false;
+    return (__vcmpgeu4(old, (CROSS - c) * 0x01010101u) & sel) != 0u;
+}
+
+// One lane, one key (or merged count c of one key) of an unlinked bucket: the selected 8-bit
+// counters get c with one returning atomic per word they touch (a mask touches at most
+// four words in the unrolled part; more go through the loop), all atomics in flight before
+// any result is used.  Returns whether the bucket crosses (flag it).
+__device__ __forceinline__ bool low_add(const MswsDev& D, uint32_t b, uint32_t m, uint32_t c) {
+    uint32_t* bw = D.low + (uint64_t)b * LOW_WORDS;
+    uint32_t mm = m;  // bits 0..27 (checked at creation): words 0..6, never the index word
+    uint32_t wv[4], nv[4], old[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const uint32_t f = __ffs(mm);
+        const uint32_t w = f ? (f - 1u) >> 2 : 0u;
+        nv[i] = f ? (mm >> (4u * w)) & 0xfu : 0u;
+        wv[i] = w;
+        mm &= ~(nv[i] << (4u * w));
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) old[i] = nv[i] ? atomicAdd(bw + wv[i], expand_nibble(nv[i]) * c) : 0u;
+    bool cross = false;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) cross |= crosses(old[i], nv[i], c);
+    while (mm) {
+        const uint32_t w = (uint32_t)(__ffs(mm) - 1) >> 2, nib = (mm >> (4u * w)) & 0xfu;
+        mm &= ~(nib << (4u * w));
+        cross |= crosses(atomicAdd(bw + w, expand_nibble(nib) * c), nib, c);
+    }
+    return cross;
+}
+
+// One lane: c to the selected high counters of linked bucket `id` (insert_high,
+// device_sketch_v3.h:54-65).
+__device__ __forceinline__ void high_add(const MswsDev& D, uint32_t id, uint32_t m, uint32_t c) {
+    uint32_t* hb = D.high + (uint64_t)(id - START) * HIGH_WORDS;
+    uint32_t mm = m;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if (mm) {
+            atomicAdd(hb + (__ffs(mm) - 1), c);
+            mm &= mm - 1;
+        }
+    }
+    for (; mm; mm &= mm - 1) atomicAdd(hb + (__ffs(mm) - 1), c);
 }
 
 // Sub-warp rounds over the staged entries of this warp: entry j = (target, mask, count,
@@ -344,6 +395,14 @@ __device__ __forceinline__ void insert_group(const MswsDev& D, const InsShared& 
             tabled = agg_insert(S, key, c, 0u);
     }
     const bool act = (c && !linked && !sat && !tabled) || direct_high;
+    if constexpr (LPK == 1) {  // one lane per key: its own atomics, no staging
+        if (direct_high) {
+            high_add(D, w7, m, c);
+        } else if (act && low_add(D, b, m, c)) {
+            flag_bucket(D, b);
+        }
+        return;
+    }
     const uint32_t am = __ballot_sync(0xffffffffu, act);
     if (act) st[__popc(am & lanemask_lt())] = make_uint4(direct_high ? w7 : b, m, c, direct_high ? 1u : 0u);
     __syncwarp();
@@ -379,6 +438,13 @@ __device__ __forceinline__ void drain_table(const MswsDev& D, const InsShared& S
                 atomicAdd(D.tbl_counts + (id & ~AGG_TBL), c);
                 has = false;
             }
+        }
+        if constexpr (LPK == 1) {  // one lane per slot
+            if (has) {
+                if (id) high_add(D, id, m, c);
+                else if (low_add(D, b, m, c)) flag_bucket(D, b);
+            }
+            continue;
         }
         const uint32_t am = __ballot_sync(0xffffffffu, has);
         if (!am) continue;
@@ -503,7 +569,6 @@ constexpr uint32_t SEMI_TILES = 4;  // radix tiles per block kept as offsets and
 static_assert(SEMI_TILES * (REPAIR_THREADS / 32) * 256 * 2 + SEMI_TILES * REPAIR_TILE <= SET_SLOTS * 4,
               "the offsets and ranks of SEMI_TILES tiles fit the shared space");
 constexpr uint32_t SCAN_CAP = SET_SLOTS / 2;  // records replayed without a sort (64 KiB of uint2)
-static_assert(BLOOM_WORDS <= SET_SLOTS, "filter fits the shared space");
 constexpr uint32_t NONE = 0xffffffffu;
 
 __device__ __forceinline__ int radix_passes(uint32_t F) {
@@ -512,15 +577,18 @@ __device__ __forceinline__ int radix_passes(uint32_t F) {
     return (bits + 7) / 8;
 }
 
-// Slot of bucket b if it was flagged in this chunk, else NONE.  A per-block filter in shared
-// memory (one bit per hash of each flagged bucket) answers "no" for almost every key with one
-// shared load; a filter hit reads the bucket's index word, which pass 1 left at FLAG | slot.
+// Is bucket b flagged in this chunk?  A per-block filter in shared memory (one bit per hash
+// of each flagged bucket) answers "no" for almost every key with one shared load; a filter
+// hit reads the bucket's index word, which pass 1 left at FLAG | slot (flag_bucket).
 __device__ __forceinline__ uint32_t bloom_bit(uint32_t b) { return (b * 0x9E3779B1u) >> (32 - BLOOM_BITS); }
 
-__device__ __forceinline__ uint32_t flagged_slot(const MswsDev& D, const uint32_t* sbloom, uint32_t b, uint32_t F) {
+__device__ __forceinline__ bool bloom_hit(const uint32_t* sbloom, uint32_t b) {
     const uint32_t h = bloom_bit(b);
-    if (!((sbloom[h >> 5] >> (h & 31)) & 1u)) return NONE;
-    const uint32_t w7 = __ldcg(D.low + (uint64_t)b * LOW_WORDS + 7);
+    return (sbloom[h >> 5] >> (h & 31)) & 1u;
+}
+
+// The slot an index word names, or NONE if its bucket was not flagged in this chunk.
+__device__ __forceinline__ uint32_t flag_slot(uint32_t w7, uint32_t F) {
     return ((w7 & FLAG) && (w7 & ~FLAG) < F) ? (w7 & ~FLAG) : NONE;
 }
 
@@ -597,9 +665,12 @@ struct KeyMap {
         if (BATCH) s = stream_of_window_key(B, i);
     }
     __device__ __forceinline__ uint64_t flat(const BatchDev& B, uint32_t i) {
-        if (!BATCH) return i;
-        while (i >= __ldg(B.wpre + s + 1)) ++s;
-        return __ldg(B.lo + s) + (i - __ldg(B.wpre + s));
+        if constexpr (!BATCH) {
+            return i;
+        } else {
+            while (i >= __ldg(B.wpre + s + 1)) ++s;
+            return __ldg(B.lo + s) + (i - __ldg(B.wpre + s));
+        }
     }
     // window keys of the current stream end here (exclusive)
     __device__ __forceinline__ uint32_t end(const BatchDev& B) const {
@@ -1095,28 +1166,33 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
     // consecutive keys of a tile (8 per lane) and stages their records at its own place, so
     // no block-wide synchronisation happens per tile: the warp's record count goes to wcnt
     // (the histogram buffer, unused until the radix passes) and into the tile's count in
-    // shared memory.  The next tile's keys are loaded before the current tile is tested.
+    // shared memory.
     uint32_t* wcnt = D.hist;  // [ntk][NW]
-    uint32_t k[PER], skip8 = 0;
-    KeyMap<BATCH> km;
-    if (blockIdx.x < ntk) repair_tile_keys<BATCH>(keys, n, D, B, (uint64_t)blockIdx.x * REPAIR_TILE + tid * PER, k, skip8, km);
-    for (uint32_t t = blockIdx.x, rk = 0; t < ntk; t += gridDim.x, ++rk) {
+    auto test_tile = [&](uint32_t t, uint32_t rk, const uint32_t (&k)[PER], uint32_t skip8, KeyMap<BATCH> km) {
         const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
-        uint32_t kn[PER] = {}, skipn = 0;
-        KeyMap<BATCH> kmn;
-        if (t + gridDim.x < ntk)
-            repair_tile_keys<BATCH>(keys, n, D, B, base + (uint64_t)gridDim.x * REPAIR_TILE, kn, skipn, kmn);
-        uint32_t hit = 0, slot[PER];
+        // the filter first for all eight keys, then their index words (filter hits only) as
+        // eight independent loads in flight together, then the slots
+        uint32_t hit = 0, cand = 0, slot[PER];
         KeyMap<BATCH> km0 = km;
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
-            slot[j] = NONE;
+            slot[j] = 0u;
             if (base + j < n && !((skip8 >> j) & 1u)) {
                 if (BATCH) km.flat(B, (uint32_t)(base + j));  // moves the cursor to key j's stream
                 uint32_t hv;
                 const uint32_t b = km.bucket(D, B, k[j], hv);
-                slot[j] = flagged_slot(D, sbloom, b, F);
+                if (bloom_hit(sbloom, b)) {
+                    cand |= 1u << j;
+                    slot[j] = b;
+                }
             }
+        }
+#pragma unroll
+        for (int j = 0; j < PER; ++j)
+            slot[j] = ((cand >> j) & 1u) ? __ldcg(D.low + (uint64_t)slot[j] * LOW_WORDS + 7) : 0u;
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            slot[j] = ((cand >> j) & 1u) ? flag_slot(slot[j], F) : NONE;
             if (slot[j] != NONE) hit |= 1u << j;
         }
         const uint32_t hc = __popc(hit);
@@ -1148,10 +1224,26 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
                 }
             }
         }
+    };
+    const uint32_t my_tiles = blockIdx.x < ntk ? (ntk - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
+    {
+        // the next tile's keys are loaded before the current tile is tested
+        uint32_t k[PER], skip8 = 0;
+        KeyMap<BATCH> km;
+        if (my_tiles) repair_tile_keys<BATCH>(keys, n, D, B, (uint64_t)blockIdx.x * REPAIR_TILE + tid * PER, k, skip8, km);
+        for (uint32_t i = 0; i < my_tiles; ++i) {
+            const uint32_t t = blockIdx.x + i * gridDim.x;
+            uint32_t kn[PER] = {}, skipn = 0;
+            KeyMap<BATCH> kmn;
+            if (i + 1 < my_tiles)
+                repair_tile_keys<BATCH>(keys, n, D, B, (uint64_t)(t + gridDim.x) * REPAIR_TILE + tid * PER, kn, skipn,
+                                        kmn);
+            test_tile(t, i, k, skip8, km);
 #pragma unroll
-        for (int j = 0; j < PER; ++j) k[j] = kn[j];
-        skip8 = skipn;
-        km = kmn;
+            for (int j = 0; j < PER; ++j) k[j] = kn[j];
+            skip8 = skipn;
+            km = kmn;
+        }
     }
     __syncthreads();
     for (uint32_t r = tid; blockIdx.x + r * gridDim.x < ntk; r += REPAIR_THREADS)

@@ -93,6 +93,9 @@ class ShardedSketch:
 
     def insert(self, keys):
         """Collective: every rank inserts its batch (uint32 keys on this rank's device)."""
+        if self.world == 1:  # one shard owns every bucket: no routing
+            self.local.insert(keys)
+            return 0
         parts, counts, _ = self._partition(keys, False)
         recv, _ = self._exchange(parts, counts)
         self.local.insert(recv)
@@ -100,6 +103,8 @@ class ShardedSketch:
 
     def search(self, keys):
         """Collective: estimates of this rank's `keys`, in their order."""
+        if self.world == 1:
+            return self.local.search(keys)
         parts, counts, perm = self._partition(keys, True)
         recv, rcounts = self._exchange(parts, counts)
         est = self.local.search(recv)
