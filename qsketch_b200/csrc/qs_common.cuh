@@ -41,8 +41,14 @@ inline FastMod make_fastmod(uint32_t d) {
 
 __host__ __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 
+// a % d as Lemire's direct remainder: low = M * a mod 2^64, a % d = (low * d) >> 64.  With d
+// below 2^32 the 128-bit product's high word is (hi * d + mulhi(lo, d)) >> 32 for the 32-bit
+// halves hi, lo of low (the fractional part lo * d mod 2^32 cannot carry into it): two
+// 32-bit wide multiplies and one high multiply instead of a 64 x 64 product.
 __device__ __forceinline__ uint32_t fast_mod(const FastMod& f, uint32_t a) {
-    return (uint32_t)__umul64hi(f.M * (uint64_t)a, (uint64_t)f.d);
+    const uint64_t low = f.M * (uint64_t)a;
+    const uint32_t lo = (uint32_t)low, hi = (uint32_t)(low >> 32);
+    return (uint32_t)(((uint64_t)hi * f.d + __umulhi(lo, f.d)) >> 32);
 }
 
 // Per-sketch device control block.

@@ -1626,6 +1626,31 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
 constexpr int QRY_THREADS = 256;
 constexpr int QRY_KPT = 4;
 
+// The estimate from a key's low bucket words u (word 7 the index) and mask m, h4 holding its
+// first four selected high counters when the bucket is linked (calculation_s2_search,
+// device_sketch_v3.h:340-357, 397-402; search_high :293-307, 364-395): min over the selected
+// 8-bit counters, plus the min over the selected high counters if linked.
+__device__ __forceinline__ uint32_t msws_estimate(const MswsDev& D, const uint32_t (&u)[8], uint32_t m,
+                                                  const uint32_t (&h4)[4]) {
+    uint32_t acc = 0xffffffffu;
+#pragma unroll
+    for (int w = 0; w < 7; ++w) {
+        const uint32_t sel = expand_nibble((m >> (4 * w)) & 0xfu) * 0xffu;
+        acc = __vminu4(acc, u[w] | ~sel);
+    }
+    acc = __vminu4(acc, acc >> 16);
+    const uint32_t lo = min(acc & 0xffu, (acc >> 8) & 0xffu);
+    const uint32_t ptr = u[7];
+    if (!(ptr > START && (uint64_t)(ptr - START) < D.n_high)) return lo;
+    uint32_t hi = min(min(h4[0], h4[1]), min(h4[2], h4[3]));
+    uint32_t mm = m;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) mm &= mm - 1;
+    const uint32_t* hb = D.high + (uint64_t)(ptr - START) * HIGH_WORDS;
+    for (; mm; mm &= mm - 1) hi = min(hi, __ldg(hb + (__ffs(mm) - 1)));  // masks of more than four counters
+    return lo + hi;
+}
+
 __device__ __forceinline__ uint32_t msws_lookup(const MswsDev& D, const uint32_t* s_masks, uint32_t key,
                                                 uint32_t seed, const FastMod& fm_low, uint32_t base) {
     const uint32_t hv = key * seed;
@@ -1646,9 +1671,17 @@ __device__ __forceinline__ uint32_t msws_lookup(const MswsDev& D, const uint32_t
     const uint32_t ptr = u[7];
     uint32_t hi = 0;
     if (ptr > START && (uint64_t)(ptr - START) < D.n_high) {  // search_high, device_sketch_v3.h:293-307, 364-395
+        // the first four selected counters as independent loads (no loop: the lookups of a
+        // thread's keys interleave), the rest of a wider mask after them
         const uint32_t* hb = D.high + (uint64_t)(ptr - START) * HIGH_WORDS;
-        hi = 0xffffffffu;
-        for (uint32_t mm = m; mm; mm &= mm - 1) hi = min(hi, __ldg(hb + (__ffs(mm) - 1)));
+        uint32_t mm = m, h4[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            h4[i] = mm ? __ldg(hb + (__ffs(mm) - 1)) : 0xffffffffu;
+            mm &= mm - 1;
+        }
+        hi = min(min(h4[0], h4[1]), min(h4[2], h4[3]));
+        for (; mm; mm &= mm - 1) hi = min(hi, __ldg(hb + (__ffs(mm) - 1)));
     }
     return lo + hi;
 }
@@ -1675,8 +1708,36 @@ __global__ void __launch_bounds__(QRY_THREADS) k_msws_query(const uint32_t* __re
                 k[j] = i < n ? __ldcs(keys + i) : 0u;
             }
         }
+        // the low buckets of all QRY_KPT keys first, then the high counters of the linked ones,
+        // so the loads of the thread's keys are in flight together at each level
+        uint4 la[QRY_KPT], lc[QRY_KPT];
+        uint32_t m[QRY_KPT];
 #pragma unroll
-        for (int j = 0; j < QRY_KPT; ++j) r[j] = msws_lookup(D, s_masks, k[j], D.seed, D.fm_low, 0u);
+        for (int j = 0; j < QRY_KPT; ++j) {
+            const uint32_t hv = k[j] * D.seed;
+            const uint4* bp = reinterpret_cast<const uint4*>(D.low + (uint64_t)fast_mod(D.fm_low, hv) * LOW_WORDS);
+            m[j] = s_masks[fast_mod(D.fm_mask, hv)];
+            la[j] = __ldg(bp);
+            lc[j] = __ldg(bp + 1);
+        }
+        uint32_t h4[QRY_KPT][4];
+#pragma unroll
+        for (int j = 0; j < QRY_KPT; ++j) {
+            const uint32_t ptr = lc[j].w;
+            const bool linked = ptr > START && (uint64_t)(ptr - START) < D.n_high;
+            const uint32_t* hb = D.high + (uint64_t)(linked ? ptr - START : 0u) * HIGH_WORDS;
+            uint32_t mm = m[j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                h4[j][i] = (linked && mm) ? __ldg(hb + (__ffs(mm) - 1)) : 0xffffffffu;
+                mm &= mm - 1;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < QRY_KPT; ++j) {
+            const uint32_t u[8] = {la[j].x, la[j].y, la[j].z, la[j].w, lc[j].x, lc[j].y, lc[j].z, lc[j].w};
+            r[j] = msws_estimate(D, u, m[j], h4[j]);
+        }
 #pragma unroll
         for (int j = 0; j < QRY_KPT; ++j) {
             const uint64_t i = base + j * stride;
