@@ -1121,6 +1121,14 @@ qs_status mlp_init_params(qs_learned* lk) {
 }
 
 // One pass of Adam over the examples in order; returns the mean loss of the last batch.
+// The classifier kernels latch ST_TIMEOUT in M.status if a tensor-core wait gave up.
+qs_status mlp_status(qs_learned* lk) {
+    uint32_t v = 0;
+    CK(cudaMemcpy(&v, lk->M.status, 4, cudaMemcpyDeviceToHost), "mlp status");
+    if (v & ST_TIMEOUT) return fail(QS_ERR_TIMEOUT, "a tensor-core wait of the classifier timed out");
+    return QS_OK;
+}
+
 qs_status mlp_train_pass(qs_learned* lk, const uint32_t* d_keys, const uint8_t* d_labels, uint64_t n, uint32_t batch,
                          float lr, float pos_weight, double* last_loss, cudaStream_t st) {
     float h_loss = 0.0f;
@@ -1137,7 +1145,7 @@ qs_status mlp_train_pass(qs_learned* lk, const uint32_t* d_keys, const uint8_t* 
         }
     }
     *last_loss = h_loss;
-    return QS_OK;
+    return mlp_status(lk);
 }
 
 qs_status learned_train(qs_learned* lk, cudaStream_t st) {
@@ -1254,6 +1262,11 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     std::vector<float> z(D);
     CKT(cudaMemcpyAsync(z.data(), d_logit, D * 4, cudaMemcpyDeviceToHost, st), "logit copy");
     CKT(cudaStreamSynchronize(st), "logit sync");
+    s = mlp_status(lk);
+    if (s != QS_OK) {
+        cleanup();
+        return s;
+    }
     // eligibility cut: the largest logit threshold that keeps `eligible_recall` of the
     // labelled-heavy warm-up keys (the network filters, the sketch's counts rank)
     std::vector<float> zpos;
@@ -1443,8 +1456,9 @@ qs_status qs_learned_create(const qs_learned_params* p, qs_learned** out) {
     CKB(lk->alloc(&M.adam_m, MLP_PARAMS), "adam m");
     CKB(lk->alloc(&M.adam_v, MLP_PARAMS), "adam v");
     CKB(lk->alloc(&M.W1, MLP_BF16_PARAMS), "mlp bf16");
-    CKB(lk->alloc(&M.partials, (uint64_t)MLP_MAX_TILES * MLP_PARAMS), "mlp partial gradients");
+    CKB(lk->alloc(&M.partials, (uint64_t)MLP_MAX_TILES * MLP_PARTIAL_STRIDE), "mlp partial gradients");
     CKB(lk->alloc(&M.ploss, MLP_MAX_TILES), "mlp partial losses");
+    CKB(lk->alloc(&M.status, 1, 0), "mlp status");
     M.W2 = M.W1 + MLP_W1_N;
     M.b1 = M.params + MLP_BF16_PARAMS;
     M.b2 = M.b1 + 128;
@@ -1630,7 +1644,7 @@ qs_status qs_mlp_grads(qs_learned* lk, const uint32_t* d_keys, const uint8_t* d_
     CK(cudaMemcpy(h_grads, lk->M.grads, MLP_PARAMS * 4, cudaMemcpyDeviceToHost), "grads copy");
     CK(cudaMemset(lk->M.grads, 0, MLP_PARAMS * 4), "grads reset");
     *loss = (double)l / (double)n;
-    return QS_OK;
+    return mlp_status(lk);
 }
 
 qs_status qs_mlp_train(qs_learned* lk, const uint32_t* d_keys, const uint8_t* d_labels, size_t n, uint32_t epochs,

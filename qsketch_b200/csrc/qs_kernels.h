@@ -73,12 +73,16 @@ struct MlpDev {
     float* grads;       // same layout
     float *gW1, *gW2, *gb1, *gb2, *g3, *gb3;
     float *adam_m, *adam_v;
-    float* partials;    // MLP_MAX_TILES * MLP_PARAMS per-tile gradients (fixed-order reduction)
+    float* partials;    // MLP_MAX_TILES * MLP_PARTIAL_STRIDE per-tile gradients (fixed-order reduction)
     float* ploss;       // MLP_MAX_TILES tile losses
+    uint32_t* status;   // ST_TIMEOUT once a tensor-core wait gave up
 };
-constexpr uint32_t MLP_MAX_TILES = 256;  // 64-example tiles per backward launch
+constexpr uint32_t MLP_TILE_EXAMPLES = 128;  // examples per CTA tile (the MMAs' M)
+constexpr uint32_t MLP_PARTIAL_STRIDE = (MLP_PARAMS + 3u) & ~3u;  // floats per tile partial: 16-byte rows
+constexpr uint32_t MLP_MAX_TILES = 256;      // tiles per backward launch
 
 size_t mlp_smem_bytes();
+size_t mlp_fwd_smem_bytes();
 cudaError_t mlp_configure();
 cudaError_t mlp_forward(const uint32_t* d_keys, uint64_t n, const MlpDev& M, float* d_logits, cudaStream_t st);
 cudaError_t mlp_backward(const uint32_t* d_keys, const uint8_t* d_labels, uint64_t n, float pos_weight,
