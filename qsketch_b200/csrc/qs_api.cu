@@ -1153,13 +1153,18 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     const uint64_t W = lk->warm_seen;
     uint32_t set_slots = 1;
     while (set_slots < 2 * W) set_slots <<= 1;
-    uint32_t *d_set = nullptr, *d_distinct = nullptr, *d_cnt = nullptr, *d_est = nullptr;
-    float* d_logit = nullptr;
-    uint8_t* d_lab = nullptr;
-    uint32_t* d_perm_keys = nullptr;
+    // device buffers, freed on every exit (D distinct warm-up keys; the sort scratch is S's)
+    uint32_t *d_set = nullptr, *d_distinct = nullptr, *d_cnt = nullptr, *d_est = nullptr, *d_tmp = nullptr;
+    uint32_t *d_train = nullptr, *d_perm_keys = nullptr, *d_hkeys = nullptr, *d_hest = nullptr, *d_okeys = nullptr,
+             *d_oest = nullptr;
+    float *d_logit = nullptr, *d_z1 = nullptr, *d_z2 = nullptr;
+    uint8_t *d_labels = nullptr, *d_take = nullptr, *d_tlab = nullptr, *d_plab = nullptr;
+    TrainScratch S;
     auto cleanup = [&] {
-        for (void* v : {(void*)d_set, (void*)d_distinct, (void*)d_cnt, (void*)d_est, (void*)d_logit, (void*)d_lab,
-                        (void*)d_perm_keys})
+        for (void* v : {(void*)d_set, (void*)d_distinct, (void*)d_cnt, (void*)d_est, (void*)d_tmp, (void*)d_train,
+                        (void*)d_perm_keys, (void*)d_hkeys, (void*)d_hest, (void*)d_okeys, (void*)d_oest,
+                        (void*)d_logit, (void*)d_z1, (void*)d_z2, (void*)d_labels, (void*)d_take, (void*)d_tlab,
+                        (void*)d_plab})
             if (v) cudaFree(v);
     };
 #define CKT(expr, what)                                 \
@@ -1172,132 +1177,99 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     } while (0)
     CKT(cudaMalloc(&d_set, (size_t)set_slots * 4), "train set");
     CKT(cudaMalloc(&d_distinct, W * 4 + 4), "train distinct");
-    CKT(cudaMalloc(&d_cnt, 8), "train count");
+    CKT(cudaMalloc(&d_cnt, 16), "train count");
     // the warm-up window's distinct keys in ascending order (a fixed order for training)
     CKT(distinct_sorted(lk->warm, (uint32_t)W, d_set, d_distinct, d_cnt, st), "distinct");
     uint32_t hc = 0;
     CKT(cudaMemcpyAsync(&hc, d_cnt, 4, cudaMemcpyDeviceToHost, st), "distinct count");
     CKT(cudaStreamSynchronize(st), "distinct sync");
-    const uint64_t D = hc;
+    const uint32_t D = hc;
     const auto t_distinct = std::chrono::steady_clock::now();
-    std::vector<uint32_t> keys(D);
-    CKT(cudaMemcpy(keys.data(), d_distinct, D * 4, cudaMemcpyDeviceToHost), "distinct copy");
-    // labels from the sketch's own estimates
-    CKT(cudaMalloc(&d_est, D * 4 + 4), "train est");
+    // labels from the sketch's own estimates: heavy = among the top heavy_fraction (ties in)
+    const size_t DW = (size_t)D * 4 + 16;
+    CKT(cudaMalloc(&d_est, DW), "train est");
+    CKT(cudaMalloc(&d_tmp, DW), "train scratch");
+    CKT(cudaMalloc(&d_labels, D + 16), "train labels");
+    CKT(cudaMalloc(&d_take, D + 16), "train sample");
+    CKT(cudaMalloc(&d_train, DW), "train set");
+    CKT(cudaMalloc(&d_tlab, D + 16), "train set labels");
     qs_status s = query_device(lk->sk, d_distinct, D, d_est, st);
     if (s != QS_OK) {
         cleanup();
         return s;
     }
-    std::vector<uint32_t> est(D);
-    CKT(cudaMemcpyAsync(est.data(), d_est, D * 4, cudaMemcpyDeviceToHost, st), "est copy");
-    CKT(cudaStreamSynchronize(st), "est sync");
-    const uint64_t k = std::max<uint64_t>(1, (uint64_t)std::ceil(lk->p.heavy_fraction * (double)D));
-    std::vector<uint32_t> tmp(est);
-    std::nth_element(tmp.begin(), tmp.begin() + (k - 1), tmp.end(), std::greater<uint32_t>());
-    const uint32_t thr = tmp[k - 1];
-    std::vector<uint8_t> lab(D);
-    uint64_t npos = 0;
-    for (uint64_t i = 0; i < D; ++i) npos += (lab[i] = est[i] >= thr ? 1 : 0);
+    const uint32_t k = (uint32_t)std::max<uint64_t>(1, (uint64_t)std::ceil(lk->p.heavy_fraction * (double)D));
+    uint32_t thr = 0, npos32 = 0, tn32 = 0;
+    if (D) CKT(kth_largest(d_est, D, k, d_tmp, S, &thr, st), "heavy threshold");
+    CKT(label_keys(d_est, D, thr, d_labels, d_cnt, st), "labels");
+    CKT(cudaMemcpyAsync(&npos32, d_cnt, 4, cudaMemcpyDeviceToHost, st), "positives");
+    CKT(cudaStreamSynchronize(st), "labels sync");
+    const uint64_t npos = npos32;
     // the training set: every labelled-heavy key and a seeded sample of neg_per_pos light keys
     // per heavy one (a key is in the sample when its hash falls below the sampling rate), in
     // ascending key order
     const uint32_t npp = lk->p.neg_per_pos ? lk->p.neg_per_pos : 16u;
     const double rate = std::min(1.0, (double)npp * (double)npos / (double)std::max<uint64_t>(1, D - npos));
     const uint64_t cut = (uint64_t)(rate * 4294967296.0);
-    std::vector<uint32_t> tkeys;
-    std::vector<uint8_t> tlab;
-    tkeys.reserve(npos + (uint64_t)(rate * (double)(D - npos)) + 16);
-    uint64_t nneg = 0;
-    for (uint64_t i = 0; i < D; ++i) {
-        uint32_t h = keys[i] ^ lk->p.init_seed;  // murmur3 finaliser: a seeded, key-only sample
-        h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
-        if (lab[i] || (uint64_t)h < cut) {
-            tkeys.push_back(keys[i]);
-            tlab.push_back(lab[i]);
-            nneg += !lab[i];
-        }
-    }
-    const uint64_t TN = tkeys.size();
+    CKT(training_set(d_distinct, d_labels, D, lk->p.init_seed, cut, d_take, d_train, d_tlab, d_cnt, S, st),
+        "training set");
+    CKT(cudaMemcpyAsync(&tn32, d_cnt, 4, cudaMemcpyDeviceToHost, st), "training set size");
+    CKT(cudaStreamSynchronize(st), "training set sync");
+    const uint64_t TN = tn32, nneg = TN - npos;
     const auto t_labels = std::chrono::steady_clock::now();
     const float pw = std::min(lk->p.max_pos_weight, (float)nneg / (float)std::max<uint64_t>(1, npos));
     // epochs over a seeded order of the examples, drawn on the device per epoch
-    uint8_t* d_lab_sorted = nullptr;
-    uint32_t* d_train = nullptr;
-    CKT(cudaMalloc(&d_lab, TN + 4), "train labels");
-    CKT(cudaMalloc(&d_perm_keys, TN * 4 + 4), "train keys");
-    CKT(cudaMalloc(&d_lab_sorted, TN + 4), "train labels");
-    CKT(cudaMalloc(&d_train, TN * 4 + 4), "train set");
-    {
-        cudaError_t e = cudaMemcpy(d_lab_sorted, tlab.data(), TN, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(d_train, tkeys.data(), TN * 4, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) {
-            cudaFree(d_lab_sorted);
-            cudaFree(d_train);
-            CKT(e, "train set upload");
-        }
-    }
+    CKT(cudaMalloc(&d_plab, TN + 16), "train labels");
+    CKT(cudaMalloc(&d_perm_keys, TN * 4 + 16), "train keys");
     double loss = 0.0, first = -1.0;
     for (uint32_t ep = 0; ep < lk->p.epochs && s == QS_OK; ++ep) {
         const uint64_t seed = ((uint64_t)lk->p.init_seed << 32) ^ (0x5bd1e995ull * (ep + 1));
-        const cudaError_t e = permute_examples(d_train, d_lab_sorted, (uint32_t)TN, seed, d_perm_keys, d_lab, st);
-        if (e != cudaSuccess) {
-            cudaFree(d_lab_sorted);
-            cudaFree(d_train);
-            CKT(e, "permute examples");
-        }
-        s = mlp_train_pass(lk, d_perm_keys, d_lab, TN, lk->p.batch, lk->p.lr, pw, &loss, st);
+        CKT(permute_examples(d_train, d_tlab, (uint32_t)TN, seed, d_perm_keys, d_plab, st), "permute examples");
+        s = mlp_train_pass(lk, d_perm_keys, d_plab, TN, lk->p.batch, lk->p.lr, pw, &loss, st);
         if (first < 0) first = loss;
     }
-    cudaFree(d_lab_sorted);
-    cudaFree(d_train);
     if (s != QS_OK) {
         cleanup();
         return s;
     }
     const auto t_epochs = std::chrono::steady_clock::now();
     // predictions on the warm-up keys: admit the predicted heavy, most confident first
-    CKT(cudaMalloc(&d_logit, D * 4 + 4), "train logits");
+    CKT(cudaMalloc(&d_logit, DW), "train logits");
     CKT(mlp_forward(d_distinct, D, lk->M, d_logit, st), "train forward");
-    std::vector<float> z(D);
-    CKT(cudaMemcpyAsync(z.data(), d_logit, D * 4, cudaMemcpyDeviceToHost, st), "logit copy");
-    CKT(cudaStreamSynchronize(st), "logit sync");
+    // eligibility cut: the largest logit threshold that keeps `eligible_recall` of the
+    // labelled-heavy warm-up keys (the network filters, the sketch's counts rank)
+    float zthr = 0.0f;
+    if (npos) {
+        CKT(cudaMalloc(&d_z1, DW), "train logits");
+        CKT(cudaMalloc(&d_z2, DW), "train logits");
+        const double miss = std::min(1.0, std::max(0.0, 1.0 - (double)lk->p.eligible_recall));
+        float zq = 0.0f;
+        CKT(positive_logit_quantile(d_logit, d_labels, D, (uint32_t)npos, miss, d_z1, d_z2, d_cnt, S, &zq, st),
+            "logit quantile");
+        zthr = std::min(0.0f, zq);
+    }
     s = mlp_status(lk);
     if (s != QS_OK) {
         cleanup();
         return s;
     }
-    // eligibility cut: the largest logit threshold that keeps `eligible_recall` of the
-    // labelled-heavy warm-up keys (the network filters, the sketch's counts rank)
-    std::vector<float> zpos;
-    for (uint64_t i = 0; i < D; ++i)
-        if (lab[i]) zpos.push_back(z[i]);
-    float zthr = 0.0f;
-    if (!zpos.empty()) {
-        std::sort(zpos.begin(), zpos.end());
-        const double miss = std::min(1.0, std::max(0.0, 1.0 - (double)lk->p.eligible_recall));
-        zthr = std::min(0.0f, zpos[(size_t)std::floor(miss * (double)(zpos.size() - 1))]);
-    }
     lk->R.z_threshold = zthr;
-    uint64_t tp = 0, fp = 0, fn = 0;
-    std::vector<std::pair<int64_t, uint32_t>> heavy;
-    heavy.reserve(D / 8);
-    for (uint64_t i = 0; i < D; ++i) {
-        const bool pred = z[i] >= zthr;
-        tp += pred && lab[i];
-        fp += pred && !lab[i];
-        fn += !pred && lab[i];
-        if (pred) heavy.push_back({-(int64_t)est[i], keys[i]});
-    }
+    uint32_t conf[3] = {0, 0, 0}, H = 0;
+    CKT(predict_keys(d_logit, d_labels, D, zthr, d_take, d_cnt, st), "predict");
+    CKT(cudaMemcpyAsync(conf, d_cnt, 12, cudaMemcpyDeviceToHost, st), "confusion counts");
     // the network decides who may enter the table; the sketch's own counts rank them (only the
-    // first max_fill of the order can enter, so only they are sorted; keys are distinct, so the
-    // order is total)
-    const uint32_t take = (uint32_t)std::min<uint64_t>(heavy.size(), lk->T.max_fill);
-    if (take < heavy.size()) std::nth_element(heavy.begin(), heavy.begin() + take, heavy.end());
-    std::sort(heavy.begin(), heavy.begin() + take);
+    // first max_fill of the order can enter); keys are distinct, so the order is total
+    CKT(cudaMalloc(&d_hkeys, DW), "heavy keys");
+    CKT(cudaMalloc(&d_hest, DW), "heavy estimates");
+    CKT(cudaMalloc(&d_okeys, DW), "heavy order");
+    CKT(cudaMalloc(&d_oest, DW), "heavy order");
+    CKT(rank_predicted(d_distinct, d_est, d_take, D, d_hkeys, d_hest, d_okeys, d_oest, d_cnt, S, &H, st), "rank");
+    const uint64_t tp = conf[0], fp = conf[1], fn = conf[2];
+    const uint32_t take = (uint32_t)std::min<uint64_t>(H, lk->T.max_fill);
     std::vector<uint32_t> order(take);
-    for (uint32_t i = 0; i < take; ++i) order[i] = heavy[i].second;
     if (take) {
+        CKT(cudaMemcpyAsync(order.data(), d_okeys, (size_t)take * 4, cudaMemcpyDeviceToHost, st), "order copy");
+        CKT(cudaStreamSynchronize(st), "order sync");
         s = learned_admit(lk, order.data(), take, st);
         if (s != QS_OK) {
             cleanup();

@@ -125,5 +125,27 @@ cudaError_t distinct_sorted(const uint32_t* d_keys, uint32_t n, uint32_t* d_tmp,
 // Training examples in a seeded order (a Feistel-network bijection of [0, n)).
 cudaError_t permute_examples(const uint32_t* d_keys, const uint8_t* d_labels, uint32_t n, uint64_t seed,
                              uint32_t* d_okeys, uint8_t* d_olabels, cudaStream_t st);
+// Device scratch of the training-set and admission sorts (grown on demand, freed with it).
+struct TrainScratch {
+    void* p = nullptr;
+    size_t size = 0;
+    cudaError_t ensure(size_t bytes);
+    ~TrainScratch();
+};
+cudaError_t kth_largest(const uint32_t* d_in, uint32_t n, uint32_t k, uint32_t* d_tmp, TrainScratch& S,
+                        uint32_t* h_out, cudaStream_t st);
+cudaError_t label_keys(const uint32_t* d_est, uint32_t n, uint32_t thr, uint8_t* d_lab, uint32_t* d_npos,
+                       cudaStream_t st);
+cudaError_t training_set(const uint32_t* d_keys, const uint8_t* d_lab, uint32_t n, uint32_t seed, uint64_t cut,
+                         uint8_t* d_take, uint32_t* d_tkeys, uint8_t* d_tlab, uint32_t* d_count, TrainScratch& S,
+                         cudaStream_t st);
+cudaError_t positive_logit_quantile(const float* d_z, const uint8_t* d_lab, uint32_t n, uint32_t npos,
+                                    double quantile, float* d_tmp, float* d_tmp2, uint32_t* d_count,
+                                    TrainScratch& S, float* h_out, cudaStream_t st);
+cudaError_t predict_keys(const float* d_z, const uint8_t* d_lab, uint32_t n, float zthr, uint8_t* d_pred,
+                         uint32_t* d_counts, cudaStream_t st);
+cudaError_t rank_predicted(const uint32_t* d_keys, const uint32_t* d_est, const uint8_t* d_pred, uint32_t n,
+                           uint32_t* d_hkeys, uint32_t* d_hest, uint32_t* d_okeys, uint32_t* d_oest,
+                           uint32_t* d_count, TrainScratch& S, uint32_t* h_count, cudaStream_t st);
 
 }  // namespace qsb

@@ -189,4 +189,154 @@ cudaError_t distinct_sorted(const uint32_t* d_keys, uint32_t n, uint32_t* d_tmp,
 }
 
 
+// ---- training set and admission on the device ------------------------------------------------
+// Scratch for the device-wide sorts and selections, grown on demand.
+cudaError_t TrainScratch::ensure(size_t bytes) {
+    if (bytes <= size) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    size = 0;
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) size = bytes;
+    return e;
+}
+TrainScratch::~TrainScratch() {
+    if (p) cudaFree(p);
+}
+
+// The k-th largest (k >= 1) of n values: a descending device radix sort into d_tmp (n words),
+// then element k-1 read back.
+cudaError_t kth_largest(const uint32_t* d_in, uint32_t n, uint32_t k, uint32_t* d_tmp, TrainScratch& S,
+                        uint32_t* h_out, cudaStream_t st) {
+    size_t b = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortKeysDescending(nullptr, b, d_in, d_tmp, n, 0, 32, st);
+    if (e == cudaSuccess) e = S.ensure(b);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeysDescending(S.p, b, d_in, d_tmp, n, 0, 32, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_out, d_tmp + (k - 1), 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e;
+}
+
+// Labels of the distinct warm-up keys (heavy: estimate >= thr) and their count.
+__global__ void k_label(const uint32_t* __restrict__ est, uint32_t n, uint32_t thr, uint8_t* __restrict__ lab,
+                        uint32_t* __restrict__ npos) {
+    uint32_t c = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint8_t l = __ldg(est + i) >= thr ? 1 : 0;
+        lab[i] = l;
+        c += l;
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(npos, c);
+}
+
+// The training sample: every labelled-heavy key and the light keys whose seeded hash (murmur3
+// finaliser of key ^ seed) falls below `cut` (a rate in 2^-32 units).
+__global__ void k_sample(const uint32_t* __restrict__ keys, const uint8_t* __restrict__ lab, uint32_t n,
+                         uint32_t seed, uint64_t cut, uint8_t* __restrict__ take) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t h = __ldg(keys + i) ^ seed;
+        h ^= h >> 16;
+        h *= 0x85EBCA6Bu;
+        h ^= h >> 13;
+        h *= 0xC2B2AE35u;
+        h ^= h >> 16;
+        take[i] = (lab[i] || (uint64_t)h < cut) ? 1 : 0;
+    }
+}
+
+cudaError_t label_keys(const uint32_t* d_est, uint32_t n, uint32_t thr, uint8_t* d_lab, uint32_t* d_npos,
+                       cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(d_npos, 0, 4, st);
+    if (e != cudaSuccess || n == 0) return e;
+    k_label<<<148 * 4, 256, 0, st>>>(d_est, n, thr, d_lab, d_npos);
+    return cudaGetLastError();
+}
+
+// The training set in ascending key order: keys and labels of the sample (stable selection);
+// *d_count receives its size.
+cudaError_t training_set(const uint32_t* d_keys, const uint8_t* d_lab, uint32_t n, uint32_t seed, uint64_t cut,
+                         uint8_t* d_take, uint32_t* d_tkeys, uint8_t* d_tlab, uint32_t* d_count, TrainScratch& S,
+                         cudaStream_t st) {
+    if (n) k_sample<<<148 * 4, 256, 0, st>>>(d_keys, d_lab, n, seed, cut, d_take);
+    cudaError_t e = cudaGetLastError();
+    size_t b1 = 0, b2 = 0;
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(nullptr, b1, d_keys, d_take, d_tkeys, d_count, n, st);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(nullptr, b2, d_lab, d_take, d_tlab, d_count, n, st);
+    if (e == cudaSuccess) e = S.ensure(std::max(b1, b2));
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(S.p, b2, d_lab, d_take, d_tlab, d_count, n, st);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(S.p, b1, d_keys, d_take, d_tkeys, d_count, n, st);
+    return e;
+}
+
+// Eligibility and confusion counts of the trained network on the labelled keys: pred = z >=
+// zthr; counts[0..2] += true positives, false positives, false negatives.
+__global__ void k_predict(const float* __restrict__ z, const uint8_t* __restrict__ lab, uint32_t n, float zthr,
+                          uint8_t* __restrict__ pred, uint32_t* __restrict__ counts) {
+    uint32_t tp = 0, fp = 0, fn = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const bool p = z[i] >= zthr, l = lab[i] != 0;
+        pred[i] = p ? 1 : 0;
+        tp += p && l;
+        fp += p && !l;
+        fn += !p && l;
+    }
+    tp = __reduce_add_sync(0xffffffffu, tp);
+    fp = __reduce_add_sync(0xffffffffu, fp);
+    fn = __reduce_add_sync(0xffffffffu, fn);
+    if ((threadIdx.x & 31) == 0) {
+        if (tp) atomicAdd(counts + 0, tp);
+        if (fp) atomicAdd(counts + 1, fp);
+        if (fn) atomicAdd(counts + 2, fn);
+    }
+}
+
+// The logit below which `quantile` (0..1) of the labelled-heavy keys fall: their logits
+// selected and sorted ascending, element floor(quantile * (npos - 1)) read back.
+cudaError_t positive_logit_quantile(const float* d_z, const uint8_t* d_lab, uint32_t n, uint32_t npos,
+                                    double quantile, float* d_tmp, float* d_tmp2, uint32_t* d_count,
+                                    TrainScratch& S, float* h_out, cudaStream_t st) {
+    size_t b1 = 0, b2 = 0;
+    cudaError_t e = cub::DeviceSelect::Flagged(nullptr, b1, d_z, d_lab, d_tmp, d_count, n, st);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(nullptr, b2, d_tmp, d_tmp2, npos, 0, 32, st);
+    if (e == cudaSuccess) e = S.ensure(std::max(b1, b2));
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(S.p, b1, d_z, d_lab, d_tmp, d_count, n, st);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(S.p, b2, d_tmp, d_tmp2, npos, 0, 32, st);
+    const uint32_t at = (uint32_t)std::floor(quantile * (double)(npos - 1));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_out, d_tmp2 + at, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e;
+}
+
+cudaError_t predict_keys(const float* d_z, const uint8_t* d_lab, uint32_t n, float zthr, uint8_t* d_pred,
+                         uint32_t* d_counts, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(d_counts, 0, 12, st);
+    if (e != cudaSuccess || n == 0) return e;
+    k_predict<<<148 * 4, 256, 0, st>>>(d_z, d_lab, n, zthr, d_pred, d_counts);
+    return cudaGetLastError();
+}
+
+// The predicted-heavy keys ranked by the sketch's estimate, highest first, ties in ascending
+// key order (the keys come in ascending order and the descending radix sort is stable):
+// d_okeys receives them, *d_count how many.
+cudaError_t rank_predicted(const uint32_t* d_keys, const uint32_t* d_est, const uint8_t* d_pred, uint32_t n,
+                           uint32_t* d_hkeys, uint32_t* d_hest, uint32_t* d_okeys, uint32_t* d_oest,
+                           uint32_t* d_count, TrainScratch& S, uint32_t* h_count, cudaStream_t st) {
+    size_t b1 = 0, b2 = 0, b3 = 0;
+    cudaError_t e = cub::DeviceSelect::Flagged(nullptr, b1, d_keys, d_pred, d_hkeys, d_count, n, st);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(nullptr, b2, d_est, d_pred, d_hest, d_count, n, st);
+    if (e == cudaSuccess) e = S.ensure(std::max(b1, b2));
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(S.p, b2, d_est, d_pred, d_hest, d_count, n, st);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(S.p, b1, d_keys, d_pred, d_hkeys, d_count, n, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_count, d_count, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess || *h_count == 0) return e;
+    const uint32_t H = *h_count;
+    e = cub::DeviceRadixSort::SortPairsDescending(nullptr, b3, d_hest, d_oest, d_hkeys, d_okeys, H, 0, 32, st);
+    if (e == cudaSuccess) e = S.ensure(b3);
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairsDescending(S.p, b3, d_hest, d_oest, d_hkeys, d_okeys, H, 0, 32, st);
+    return e;
+}
+
 }  // namespace qsb
