@@ -1062,6 +1062,14 @@ struct qs_learned {
     uint32_t admit_cap = 0;
     float* d_loss = nullptr;
     uint8_t* d_labels_tmp = nullptr;
+    // training buffers, allocated with the sketch (training runs once, inside an insert):
+    // word buffers of the warm-up length W (the distinct-key set 2W) and byte buffers of W
+    struct {
+        uint32_t *set, *distinct, *cnt, *est, *tmp, *train, *perm, *z2;
+        uint8_t *labels, *take, *tlab, *plab;
+        uint32_t set_slots;
+    } tb{};
+    TrainScratch tscratch;
     qs_learned_info info{};
     uint32_t adam_step = 0;
     bool table_full = false;  // (almost) no admission possible: routing skips the classifier
@@ -1151,22 +1159,18 @@ qs_status mlp_train_pass(qs_learned* lk, const uint32_t* d_keys, const uint8_t* 
 qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     const auto t0 = std::chrono::steady_clock::now();
     const uint64_t W = lk->warm_seen;
-    uint32_t set_slots = 1;
-    while (set_slots < 2 * W) set_slots <<= 1;
-    // device buffers, freed on every exit (D distinct warm-up keys; the sort scratch is S's)
-    uint32_t *d_set = nullptr, *d_distinct = nullptr, *d_cnt = nullptr, *d_est = nullptr, *d_tmp = nullptr;
-    uint32_t *d_train = nullptr, *d_perm_keys = nullptr, *d_hkeys = nullptr, *d_hest = nullptr, *d_okeys = nullptr,
-             *d_oest = nullptr;
-    float *d_logit = nullptr, *d_z1 = nullptr, *d_z2 = nullptr;
-    uint8_t *d_labels = nullptr, *d_take = nullptr, *d_tlab = nullptr, *d_plab = nullptr;
-    TrainScratch S;
-    auto cleanup = [&] {
-        for (void* v : {(void*)d_set, (void*)d_distinct, (void*)d_cnt, (void*)d_est, (void*)d_tmp, (void*)d_train,
-                        (void*)d_perm_keys, (void*)d_hkeys, (void*)d_hest, (void*)d_okeys, (void*)d_oest,
-                        (void*)d_logit, (void*)d_z1, (void*)d_z2, (void*)d_labels, (void*)d_take, (void*)d_tlab,
-                        (void*)d_plab})
-            if (v) cudaFree(v);
-    };
+    // the sketch's training buffers (every one holds W elements; the distinct-key set 2W):
+    // after the distinct keys the set holds the ranked keys, after the labels tmp the logits,
+    // after the epochs perm the positives' logits and then the admission order
+    auto& tb = lk->tb;
+    uint32_t *d_set = tb.set, *d_distinct = tb.distinct, *d_cnt = tb.cnt, *d_est = tb.est, *d_tmp = tb.tmp;
+    uint32_t *d_train = tb.train, *d_perm_keys = tb.perm;
+    uint32_t *d_hkeys = tb.set, *d_hest = tb.set + (W + 16), *d_okeys = tb.perm, *d_oest = tb.z2;
+    float *d_logit = reinterpret_cast<float*>(tb.tmp), *d_z1 = reinterpret_cast<float*>(tb.perm),
+          *d_z2 = reinterpret_cast<float*>(tb.z2);
+    uint8_t *d_labels = tb.labels, *d_take = tb.take, *d_tlab = tb.tlab, *d_plab = tb.plab;
+    TrainScratch& S = lk->tscratch;
+    auto cleanup = [] {};
 #define CKT(expr, what)                                 \
     do {                                                \
         cudaError_t _e = (expr);                        \
@@ -1175,24 +1179,13 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
             return cuda_fail(_e, what);                 \
         }                                               \
     } while (0)
-    CKT(cudaMalloc(&d_set, (size_t)set_slots * 4), "train set");
-    CKT(cudaMalloc(&d_distinct, W * 4 + 4), "train distinct");
-    CKT(cudaMalloc(&d_cnt, 16), "train count");
-    // the warm-up window's distinct keys in ascending order (a fixed order for training)
-    CKT(distinct_sorted(lk->warm, (uint32_t)W, d_set, d_distinct, d_cnt, st), "distinct");
+    CKT(distinct_sorted(lk->warm, (uint32_t)W, d_set, d_distinct, d_cnt, S, st), "distinct");
     uint32_t hc = 0;
     CKT(cudaMemcpyAsync(&hc, d_cnt, 4, cudaMemcpyDeviceToHost, st), "distinct count");
     CKT(cudaStreamSynchronize(st), "distinct sync");
     const uint32_t D = hc;
     const auto t_distinct = std::chrono::steady_clock::now();
     // labels from the sketch's own estimates: heavy = among the top heavy_fraction (ties in)
-    const size_t DW = (size_t)D * 4 + 16;
-    CKT(cudaMalloc(&d_est, DW), "train est");
-    CKT(cudaMalloc(&d_tmp, DW), "train scratch");
-    CKT(cudaMalloc(&d_labels, D + 16), "train labels");
-    CKT(cudaMalloc(&d_take, D + 16), "train sample");
-    CKT(cudaMalloc(&d_train, DW), "train set");
-    CKT(cudaMalloc(&d_tlab, D + 16), "train set labels");
     qs_status s = query_device(lk->sk, d_distinct, D, d_est, st);
     if (s != QS_OK) {
         cleanup();
@@ -1219,8 +1212,6 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     const auto t_labels = std::chrono::steady_clock::now();
     const float pw = std::min(lk->p.max_pos_weight, (float)nneg / (float)std::max<uint64_t>(1, npos));
     // epochs over a seeded order of the examples, drawn on the device per epoch
-    CKT(cudaMalloc(&d_plab, TN + 16), "train labels");
-    CKT(cudaMalloc(&d_perm_keys, TN * 4 + 16), "train keys");
     double loss = 0.0, first = -1.0;
     for (uint32_t ep = 0; ep < lk->p.epochs && s == QS_OK; ++ep) {
         const uint64_t seed = ((uint64_t)lk->p.init_seed << 32) ^ (0x5bd1e995ull * (ep + 1));
@@ -1234,14 +1225,11 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     }
     const auto t_epochs = std::chrono::steady_clock::now();
     // predictions on the warm-up keys: admit the predicted heavy, most confident first
-    CKT(cudaMalloc(&d_logit, DW), "train logits");
     CKT(mlp_forward(d_distinct, D, lk->M, d_logit, st), "train forward");
     // eligibility cut: the largest logit threshold that keeps `eligible_recall` of the
     // labelled-heavy warm-up keys (the network filters, the sketch's counts rank)
     float zthr = 0.0f;
     if (npos) {
-        CKT(cudaMalloc(&d_z1, DW), "train logits");
-        CKT(cudaMalloc(&d_z2, DW), "train logits");
         const double miss = std::min(1.0, std::max(0.0, 1.0 - (double)lk->p.eligible_recall));
         float zq = 0.0f;
         CKT(positive_logit_quantile(d_logit, d_labels, D, (uint32_t)npos, miss, d_z1, d_z2, d_cnt, S, &zq, st),
@@ -1259,10 +1247,6 @@ qs_status learned_train(qs_learned* lk, cudaStream_t st) {
     CKT(cudaMemcpyAsync(conf, d_cnt, 12, cudaMemcpyDeviceToHost, st), "confusion counts");
     // the network decides who may enter the table; the sketch's own counts rank them (only the
     // first max_fill of the order can enter); keys are distinct, so the order is total
-    CKT(cudaMalloc(&d_hkeys, DW), "heavy keys");
-    CKT(cudaMalloc(&d_hest, DW), "heavy estimates");
-    CKT(cudaMalloc(&d_okeys, DW), "heavy order");
-    CKT(cudaMalloc(&d_oest, DW), "heavy order");
     CKT(rank_predicted(d_distinct, d_est, d_take, D, d_hkeys, d_hest, d_okeys, d_oest, d_cnt, S, &H, st), "rank");
     const uint64_t tp = conf[0], fp = conf[1], fn = conf[2];
     const uint32_t take = (uint32_t)std::min<uint64_t>(H, lk->T.max_fill);
@@ -1444,6 +1428,19 @@ qs_status qs_learned_create(const qs_learned_params* p, qs_learned** out) {
     M.gb3 = M.g3 + 128;
     CKB(lk->alloc(&lk->d_loss, 4), "loss");
     CKB(lk->alloc(&lk->warm, p->warmup_keys), "warm-up keys");
+    {
+        auto& tb = lk->tb;
+        const uint64_t Wk = p->warmup_keys + 16;
+        tb.set_slots = 1;
+        while (tb.set_slots < 2 * p->warmup_keys) tb.set_slots <<= 1;
+        CKB(lk->alloc(&tb.set, std::max<uint64_t>(tb.set_slots, 2 * Wk)), "train set");
+        CKB(lk->alloc(&tb.distinct, Wk), "train distinct");
+        CKB(lk->alloc(&tb.cnt, 16), "train counts");
+        for (uint32_t** b : {&tb.est, &tb.tmp, &tb.train, &tb.perm, &tb.z2}) CKB(lk->alloc(b, Wk), "train buffer");
+        for (uint8_t** b : {&tb.labels, &tb.take, &tb.tlab, &tb.plab}) CKB(lk->alloc(b, Wk), "train buffer");
+        cudaError_t e = train_scratch_reserve(lk->tscratch, (uint32_t)p->warmup_keys, tb.set_slots);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "train scratch"));
+    }
     cudaError_t e = mlp_configure();
     if (e != cudaSuccess) return bail(cuda_fail(e, "mlp configure"));
     s = mlp_init_params(lk);
@@ -1467,6 +1464,8 @@ qs_status qs_learned_destroy(qs_learned* lk) {
         DeviceGuard guard(lk->device);
         cudaDeviceSynchronize();
         for (void* v : lk->allocs) cudaFree(v);
+        if (lk->tscratch.p) cudaFree(lk->tscratch.p);
+        lk->tscratch.p = nullptr;
         if (lk->sk) qs_destroy(lk->sk);
     }
     delete lk;

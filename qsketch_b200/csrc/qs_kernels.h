@@ -120,11 +120,6 @@ uint32_t table_admit_host(uint32_t* keys, uint32_t slots, const uint32_t* order,
                           uint32_t max_fill);
 cudaError_t learned_query(const uint32_t* d_keys, uint64_t n, const TableDev& T, const MswsDev& D, const MswsLaunch& L,
                           uint32_t* d_out, cudaStream_t st);
-cudaError_t distinct_sorted(const uint32_t* d_keys, uint32_t n, uint32_t* d_tmp, uint32_t* d_out, uint32_t* d_count,
-                            cudaStream_t st);
-// Training examples in a seeded order (a Feistel-network bijection of [0, n)).
-cudaError_t permute_examples(const uint32_t* d_keys, const uint8_t* d_labels, uint32_t n, uint64_t seed,
-                             uint32_t* d_okeys, uint8_t* d_olabels, cudaStream_t st);
 // Device scratch of the training-set and admission sorts (grown on demand, freed with it).
 struct TrainScratch {
     void* p = nullptr;
@@ -132,6 +127,13 @@ struct TrainScratch {
     cudaError_t ensure(size_t bytes);
     ~TrainScratch();
 };
+cudaError_t distinct_sorted(const uint32_t* d_keys, uint32_t n, uint32_t* d_tmp, uint32_t* d_out, uint32_t* d_count,
+                            TrainScratch& S, cudaStream_t st);
+// Training examples in a seeded order (a Feistel-network bijection of [0, n)).
+cudaError_t permute_examples(const uint32_t* d_keys, const uint8_t* d_labels, uint32_t n, uint64_t seed,
+                             uint32_t* d_okeys, uint8_t* d_olabels, cudaStream_t st);
+
+cudaError_t train_scratch_reserve(TrainScratch& S, uint32_t n, uint32_t set_slots);
 cudaError_t kth_largest(const uint32_t* d_in, uint32_t n, uint32_t k, uint32_t* d_tmp, TrainScratch& S,
                         uint32_t* h_out, cudaStream_t st);
 cudaError_t label_keys(const uint32_t* d_est, uint32_t n, uint32_t thr, uint8_t* d_lab, uint32_t* d_npos,

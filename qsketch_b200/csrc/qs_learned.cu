@@ -171,23 +171,17 @@ cudaError_t permute_examples(const uint32_t* d_keys, const uint8_t* d_labels, ui
 }
 
 // Distinct keys in ascending order: a device radix sort into d_tmp (n words), then unique into
-// d_out; *d_count (device) receives how many.  The scratch of the two passes is allocated here.
+// d_out; *d_count (device) receives how many.
 cudaError_t distinct_sorted(const uint32_t* d_keys, uint32_t n, uint32_t* d_tmp, uint32_t* d_out, uint32_t* d_count,
-                            cudaStream_t st) {
+                            TrainScratch& S, cudaStream_t st) {
     size_t b1 = 0, b2 = 0;
     cudaError_t e = cub::DeviceRadixSort::SortKeys(nullptr, b1, d_keys, d_tmp, n, 0, 32, st);
     if (e == cudaSuccess) e = cub::DeviceSelect::Unique(nullptr, b2, d_tmp, d_out, d_count, n, st);
-    if (e != cudaSuccess) return e;
-    void* scratch = nullptr;
-    e = cudaMalloc(&scratch, std::max<size_t>(std::max(b1, b2), 16));
-    if (e != cudaSuccess) return e;
-    e = cub::DeviceRadixSort::SortKeys(scratch, b1, d_keys, d_tmp, n, 0, 32, st);
-    if (e == cudaSuccess) e = cub::DeviceSelect::Unique(scratch, b2, d_tmp, d_out, d_count, n, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(scratch);
+    if (e == cudaSuccess) e = S.ensure(std::max(b1, b2));
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(S.p, b1, d_keys, d_tmp, n, 0, 32, st);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Unique(S.p, b2, d_tmp, d_out, d_count, n, st);
     return e;
 }
-
 
 // ---- training set and admission on the device ------------------------------------------------
 // Scratch for the device-wide sorts and selections, grown on demand.
@@ -202,6 +196,36 @@ cudaError_t TrainScratch::ensure(size_t bytes) {
 }
 TrainScratch::~TrainScratch() {
     if (p) cudaFree(p);
+}
+
+// Reserve the scratch of every sort and selection of a training on n keys, so training
+// allocates nothing.
+cudaError_t train_scratch_reserve(TrainScratch& S, uint32_t n, uint32_t set_slots) {
+    (void)set_slots;
+    size_t b = 0, m = 0;
+    const uint32_t* u = nullptr;
+    uint32_t* o = nullptr;
+    const uint8_t* f = nullptr;
+    uint8_t* o8 = nullptr;
+    const float* fz = nullptr;
+    float* oz = nullptr;
+    cudaError_t e = cub::DeviceRadixSort::SortKeys(nullptr, b, u, o, n, 0, 32);
+    m = std::max(m, b);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Unique(nullptr, b, u, o, o, n);
+    m = std::max(m, b);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeysDescending(nullptr, b, u, o, n, 0, 32);
+    m = std::max(m, b);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(nullptr, b, u, f, o, o, n);
+    m = std::max(m, b);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(nullptr, b, f, f, o8, o, n);
+    m = std::max(m, b);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(nullptr, b, fz, f, oz, o, n);
+    m = std::max(m, b);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(nullptr, b, fz, oz, n, 0, 32);
+    m = std::max(m, b);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairsDescending(nullptr, b, u, o, u, o, n, 0, 32);
+    m = std::max(m, b);
+    return e == cudaSuccess ? S.ensure(m) : e;
 }
 
 // The k-th largest (k >= 1) of n values: a descending device radix sort into d_tmp (n words),
