@@ -217,7 +217,8 @@ typedef struct qs_profile {
     uint64_t insert_timed, repair_timed, query_timed;
     uint64_t insert_launches, repair_launches, query_launches;
     /* MSWS ordered repair, measured on the device (globaltimer) since the previous
-     * qs_get_profile: invocations that found crossed buckets, and time per phase —
+     * qs_get_profile: invocations that found crossed buckets, and, while profiling is on,
+     * time per phase —
      * 8 filter build, 0 flag test (and staging of the records), 1 tile scan, 2 record
      * move, radix passes split into 6 tile digit counts, 7 digit scans and 3 scatters,
      * 4 segments and totals, 5 replay, 9 link order (ranks, high buckets written);

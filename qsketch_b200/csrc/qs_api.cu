@@ -706,6 +706,7 @@ qs_status qs_set_profiling(qs_sketch* sk, int enable) {
     DeviceGuard guard(sk->device);
     CK(cudaDeviceSynchronize(), "profiling sync");
     sk->prof = enable != 0;
+    sk->D.prof = enable != 0 ? 1u : 0u;  // the repair's device phase timers
     for (int k = 0; k < 3; ++k) sk->ev_used[k] = 0;
     return QS_OK;
 }

@@ -103,6 +103,7 @@ struct MswsDev {
     uint32_t* skip_out;
     uint32_t tbl_slots;
     uint32_t ins_tile;       // pass-1 keys per tile (0: the stage size)
+    uint32_t prof;           // repair phase timers on (qs_set_profiling); off they cost nothing
     // Link order.  One-key-at-a-time insertion hands out high ids in the array order of the
     // keys that switch buckets to the high level; the ordered replay does the same:
     uint32_t* rpos[2];       // per record: its position in array order, carried through the

@@ -598,9 +598,11 @@ __device__ __forceinline__ uint64_t globaltimer() {
     return t;
 }
 
-// Accumulate the time since the previous mark into phase k (block 0, thread 0).
-__device__ __forceinline__ void phase_mark(Ctl* ctl, int k) {
+// Accumulate the time since the previous mark into phase k (block 0, thread 0), when profiling.
+__device__ __forceinline__ void phase_mark(const MswsDev& D, int k) {
+    if (!D.prof) return;  // the timers' global reads and writes would delay block 0 at every barrier
     if (blockIdx.x == 0 && threadIdx.x == 0) {
+        Ctl* ctl = D.ctl;
         const uint64_t now = globaltimer();
         if (k >= 0) ctl->phase_ns[k] += now - ctl->phase_t;
         ctl->phase_t = now;
@@ -1121,7 +1123,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
     // Read before the first grid barrier; only the link phase, after it, writes them.
     const uint32_t base_id = __ldcg(&ctl->next_id);
     const unsigned long long gen = (unsigned long long)__ldcg(&ctl->link_gen) + 1ull;
-    phase_mark(ctl, -1);
+    phase_mark(D, -1);
     if (BATCH) n = __ldcg(B.win + 1);
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -1160,7 +1162,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
     const uint32_t ntot = min(F, D.long_cap);
     for (uint32_t i = gtid; i < ntot * LOW_COUNTERS; i += nthreads) __stcg(D.totals + i, 0u);
     for (uint32_t i = gtid; i < ntot; i += nthreads) __stcg(D.seg_beg + i, 0u);  // record counts (scan mode)
-    phase_mark(ctl, 8);
+    phase_mark(D, 8);
 
     // Phase 1: the keys of flagged buckets, per tile of the chunk.  Each warp owns 256
     // consecutive keys of a tile (8 per lane) and stages their records at its own place, so
@@ -1168,8 +1170,12 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
     // (the histogram buffer, unused until the radix passes) and into the tile's count in
     // shared memory.
     uint32_t* wcnt = D.hist;  // [ntk][NW]
+    const uint32_t seed = D.seed;      // one sketch (not batched): its hash and bucket count
+    const FastMod fm_low = D.fm_low;
     auto test_tile = [&](uint32_t t, uint32_t rk, const uint32_t (&k)[PER], uint32_t skip8, KeyMap<BATCH> km) {
         const uint64_t base = (uint64_t)t * REPAIR_TILE + (uint64_t)tid * PER;
+        const uint32_t nv = base >= n ? 0u : (uint32_t)umin64(PER, n - base);
+        const uint32_t live = ((1u << nv) - 1u) & ~skip8;  // keys of the chunk, not skipped
         // the filter first for all eight keys, then their index words (filter hits only) as
         // eight independent loads in flight together, then the slots
         uint32_t hit = 0, cand = 0, slot[PER];
@@ -1177,10 +1183,15 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
             slot[j] = 0u;
-            if (base + j < n && !((skip8 >> j) & 1u)) {
-                if (BATCH) km.flat(B, (uint32_t)(base + j));  // moves the cursor to key j's stream
-                uint32_t hv;
-                const uint32_t b = km.bucket(D, B, k[j], hv);
+            if ((live >> j) & 1u) {
+                uint32_t b;
+                if constexpr (BATCH) {
+                    km.flat(B, (uint32_t)(base + j));  // moves the cursor to key j's stream
+                    uint32_t hv;
+                    b = km.bucket(D, B, k[j], hv);
+                } else {
+                    b = fast_mod(fm_low, k[j] * seed);
+                }
                 if (bloom_hit(sbloom, b)) {
                     cand |= 1u << j;
                     slot[j] = b;
@@ -1216,9 +1227,13 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
 #pragma unroll
             for (int j = 0; j < PER; ++j) {
                 if ((hit >> j) & 1u) {
-                    if (BATCH) km0.flat(B, (uint32_t)(base + j));
                     uint32_t hv;
-                    km0.bucket(D, B, k[j], hv);
+                    if constexpr (BATCH) {
+                        km0.flat(B, (uint32_t)(base + j));
+                        km0.bucket(D, B, k[j], hv);
+                    } else {
+                        hv = k[j] * seed;
+                    }
                     __stcg(stage + pos, make_uint2(slot[j], __ldg(D.masks + fast_mod(D.fm_mask, hv))));
                     ++pos;
                 }
@@ -1249,16 +1264,23 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
     for (uint32_t r = tid; blockIdx.x + r * gridDim.x < ntk; r += REPAIR_THREADS)
         __stcg(D.tile_counts + blockIdx.x + r * gridDim.x, s_tc[r]);
     if (!grid_barrier(ctl)) return;
-    phase_mark(ctl, 0);
+    phase_mark(D, 0);
     // Phase 2: every block scans the tile counts itself (exclusive, in shared memory — the
     // flag filter is not needed after phase 1), which gives its tiles' record offsets
     // and the record total K without another grid barrier.
     uint32_t* spre = s_set;
-    for (uint32_t i = tid; i < ntk; i += REPAIR_THREADS) spre[i] = __ldcg(D.tile_counts + i);
+    for (uint32_t i0 = tid; i0 < ntk; i0 += 4 * REPAIR_THREADS) {  // four loads in flight
+        uint32_t v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = i0 + u * REPAIR_THREADS < ntk ? __ldcg(D.tile_counts + i0 + u * REPAIR_THREADS) : 0u;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (i0 + u * REPAIR_THREADS < ntk) spre[i0 + u * REPAIR_THREADS] = v[u];
+    }
     __syncthreads();
     const uint32_t K = block_scan_smem(spre, ntk);
     if (blockIdx.x == 0 && tid == 0) __stcg(&ctl->n_records, K);
-    phase_mark(ctl, 1);
+    phase_mark(D, 1);
     // Few records (K <= SCAN_CAP): the replay scans them unsorted, and the per-slot counter
     // totals and record counts it needs are accumulated here with global atomics.
     const bool scan_mode = K <= SCAN_CAP;
@@ -1302,7 +1324,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
         }
     }
     if (!grid_barrier(ctl)) return;
-    phase_mark(ctl, 2);
+    phase_mark(D, 2);
 
     // Few records: no sort.  Every block that replays a slot stages all K records in shared
     // memory (the flag filter is no longer needed; the 64 KiB hold SCAN_CAP records)
@@ -1320,7 +1342,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
                 settle_bucket<BATCH>(D, B, gen, s, b, o, o.L);
             }
         }
-        phase_mark(ctl, 5);
+        phase_mark(D, 5);
         if (one_block) {
             if (blockIdx.x != 0) {
                 finish_repair(ctl);
@@ -1332,7 +1354,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
         }
         auto rerun = [&](uint32_t s, uint32_t b) { return replay_scan(D, srec, s, K, b); };
         link_phase<BATCH>(D, B, F, K, base_id, gen, one_block, rerun, s_swpre, s_set);
-        phase_mark(ctl, 9);
+        phase_mark(D, 9);
         finish_repair(ctl);
         return;
     }
@@ -1443,29 +1465,37 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
             }
         }
         if (!grid_barrier(ctl)) return;
-        phase_mark(ctl, 6);
+        phase_mark(D, 6);
         // one warp per digit scans its row of tile counts (exclusive, in place) and stores the
         // digit's total; then every block forms the 256 digit bases itself
         uint32_t* dtot = D.hist + 256ull * D.max_tiles;
         for (uint32_t d = blockIdx.x * NW + wid; d < 256; d += gridDim.x * NW) {
             uint32_t* row = D.hist + (uint64_t)d * ntr;
             uint32_t run = 0;
-            for (uint32_t t0 = 0; t0 < ntr; t0 += 32) {
-                const uint32_t t = t0 + lane;
-                const uint32_t v = t < ntr ? __ldcg(row + t) : 0u;
-                uint32_t x = v;
+            for (uint32_t t0 = 0; t0 < ntr; t0 += 128) {  // four rows of 32 counts in flight
+                uint32_t v4[4];
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-                    if (lane >= o) x += y;
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t t = t0 + u * 32 + lane;
+                    v4[u] = t < ntr ? __ldcg(row + t) : 0u;
                 }
-                if (t < ntr) __stcg(row + t, run + x - v);
-                run += __shfl_sync(0xffffffffu, x, 31);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t t = t0 + u * 32 + lane, v = v4[u];
+                    uint32_t x = v;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                        if (lane >= o) x += y;
+                    }
+                    if (t < ntr) __stcg(row + t, run + x - v);
+                    run += __shfl_sync(0xffffffffu, x, 31);
+                }
             }
             if (lane == 0) __stcg(dtot + d, run);
         }
         if (!grid_barrier(ctl)) return;
-        phase_mark(ctl, 7);
+        phase_mark(D, 7);
         {
             uint32_t total;
             const uint32_t ex = block_exclusive_scan(tid < 256 ? __ldcg(dtot + tid) : 0u, &total);
@@ -1547,7 +1577,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
             __syncthreads();
         }
         if (!grid_barrier(ctl)) return;
-        phase_mark(ctl, 3);
+        phase_mark(D, 3);
     }
 
     // Phase 5: segment starts, and per-counter totals of slots < long_cap; each block a
@@ -1594,7 +1624,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
         }
     }
     if (!grid_barrier(ctl)) return;
-    phase_mark(ctl, 4);
+    phase_mark(D, 4);
 
     // Phase 6: replay each flagged bucket in array order, one warp per slot; then link the
     // switched buckets in the array order of their switching keys (the records' positions
@@ -1605,7 +1635,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
         const ReplayOut o = replay_sorted(D, sorted, s, F, K, b);
         settle_bucket<BATCH>(D, B, gen, s, b, o, o.found ? (fpos ? __ldcg(fpos + o.L) : o.L) : 0u);
     }
-    phase_mark(ctl, 5);
+    phase_mark(D, 5);
     if (one_block) {
         if (blockIdx.x != 0) {
             finish_repair(ctl);
@@ -1617,7 +1647,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
     }
     auto rerun = [&](uint32_t s, uint32_t b) { return replay_sorted(D, sorted, s, F, K, b); };
     link_phase<BATCH>(D, B, F, K, base_id, gen, one_block, rerun, s_swpre, s_set);
-    phase_mark(ctl, 9);
+    phase_mark(D, 9);
     finish_repair(ctl);
 }
 
