@@ -2291,9 +2291,11 @@ qs_status qs_autotune(const qs_params* base, const uint32_t* d_keys, size_t n, u
                        2048u, 0u, 0.0};
     s = run(cur);
     if (s != QS_OK) return cleanup(s);
+    // a setting replaces the incumbent only when it is at least 1 % faster: differences below
+    // that are run-to-run noise, and the search order (smaller chunks first) then decides
     auto consider = [&](qs_tune_config c) -> qs_status {
         qs_status q = run(c);
-        if (q == QS_OK && c.insert_ms < cur.insert_ms) cur = c;
+        if (q == QS_OK && c.insert_ms < 0.99 * cur.insert_ms) cur = c;
         return q;
     };
     for (uint32_t lpk : {4u, 2u, 1u, 16u, 32u}) {

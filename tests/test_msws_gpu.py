@@ -306,7 +306,10 @@ def test_autotune_picks_a_timed_setting_and_create_uses_it(gpu):
     best, allc = autotune.autotune(524287, 1 << 15, keys, reps=2)
     print("autotune best:", best, "of", len(allc))
     assert len(allc) >= 10
-    assert best["insert_ms"] == min(c["insert_ms"] for c in allc)
+    # the pick is within 1 % of the fastest setting timed: a setting replaces the incumbent only
+    # when 1 % faster, and incumbents only get faster, so every rejected one was >= 0.99 x the pick
+    assert best["insert_ms"] <= min(c["insert_ms"] for c in allc) / 0.99 * (1 + 1e-6)
+    assert best in allc
     assert autotune.lookup(524287) == best
     assert autotune.lookup(300000) == best  # same size class (2^18 <= n < 2^19)
     # a sketch of that class with knobs left at 0 uses the tuned setting: same results
