@@ -1340,7 +1340,7 @@ void qs_learned_params_default(qs_learned_params* p) {
     p->warmup_keys = 1ull << 24;
     p->heavy_fraction = 0.005;
     p->epochs = 4;
-    p->batch = 16384;  // 256 tiles of 64 examples: one backward launch fills the GPU
+    p->batch = 16384;  // 128 tiles of 128 examples: one backward launch, one tile per SM
     p->lr = 4e-3f;
     p->max_pos_weight = 64.0f;
     p->eligible_recall = 0.95f;
