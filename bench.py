@@ -477,6 +477,9 @@ def run_ours(args, cfg):
                                                "of 8"},
             "kernel_ms_per_step": {"insert": round(prof["insert_ms"], 4), "repair": round(prof["repair_ms"], 4),
                                    "query": round(prof["query_ms"], 4)},
+            # the instrumented step's repair by phase (indices as qs_profile documents them)
+            "repair_phase_ms": [round(x, 3) for x in prof["repair_phase_ms"]],
+            "repairs_active": int(prof["repairs_active"]),
             "clocks": clk.summary(),
         }
         if args.cpu_baseline:
