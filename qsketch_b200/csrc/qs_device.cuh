@@ -58,6 +58,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return false;
 }
 
+// ---- programmatic dependent launch ---------------------------------------------------
+// A kernel launched with programmatic stream serialization may start while the previous
+// kernel of its stream is still running; griddep_wait() returns once that kernel has
+// completed and its writes are visible (at once for a kernel launched without it), so every
+// such kernel calls it before it reads anything a kernel writes, and before it can return.
+// griddep_launch_dependents() lets the next such kernel be scheduled before this one ends.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---- grid barrier for cooperative launches (bounded) ---------------------------------
 // All blocks of the grid are co-resident (cudaLaunchCooperativeKernel).  Thread 0 of each
 // block reads the generation before the block arrives (it cannot advance earlier), fences

@@ -464,11 +464,14 @@ __global__ void __launch_bounds__(INS_THREADS, INS_MIN_CTAS) k_msws_insert(const
     __shared__ int s_ok;
 
     const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
+    griddep_launch_dependents();  // the replay may be scheduled now: it waits for this pass
+    // the mask table (written by the host only) is staged while the previous kernel drains
     for (uint32_t i = tid; i < D.n_masks; i += blockDim.x) S.masks[i] = __ldg(D.masks + i);
     for (int i = tid; i < AGG_SLOTS; i += blockDim.x) {
         S.akey[i] = AGG_EMPTY;
         S.acnt[i] = 0;
     }
+    griddep_wait();
     if (tid == 0) {
         S.misc[0] = 0;
         S.misc[1] = 0;
@@ -1117,6 +1120,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
     __shared__ uint32_t s_tc[TC_MAX];       // phase 1: counts of this block's tiles, by round
     __shared__ uint32_t s_swpre[64];        // link order: prefix of the switch counts (small chunks)
     extern __shared__ __align__(16) uint32_t s_set[];
+    griddep_wait();  // pass 1 has ended (its flags, tables and counters are final)
     Ctl* ctl = D.ctl;
     const uint32_t F = min(__ldcg(&ctl->n_flagged), D.flag_cap);
     if (F == 0) return;
@@ -1719,6 +1723,8 @@ __device__ __forceinline__ uint32_t msws_lookup(const MswsDev& D, const uint32_t
 __global__ void __launch_bounds__(QRY_THREADS) k_msws_query(const uint32_t* __restrict__ keys, uint64_t n,
                                                             uint32_t* __restrict__ out, MswsDev D) {
     extern __shared__ __align__(16) uint32_t s_masks[];
+    griddep_wait();  // the previous kernel (an insert or its replay) has ended
+    griddep_launch_dependents();
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     uint64_t base = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t k[QRY_KPT], r[QRY_KPT];
@@ -2078,6 +2084,33 @@ cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
     return cudaSuccess;
 }
 
+// Launch with programmatic stream serialization: the kernel may be scheduled while the
+// previous kernel of the stream drains (hiding the launch gap between the dependent passes);
+// each kernel launched this way calls griddep_wait() before it reads what a kernel writes.
+// A driver that refuses the attribute next to a cooperative launch gets the plain one.
+static cudaError_t launch_pdl(const void* fn, dim3 grid, dim3 block, size_t smem, cudaStream_t st, void** args,
+                              bool cooperative) {
+    static bool coop_pdl_refused = false;
+    if (cooperative && coop_pdl_refused) return cudaLaunchCooperativeKernel(fn, grid, block, args, smem, st);
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    at[1].id = cudaLaunchAttributeCooperative;
+    at[1].val.cooperative = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = cooperative ? 2 : 1;
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
+    if (e == cudaSuccess || !cooperative) return e;
+    (void)cudaGetLastError();  // a refused configuration is not sticky
+    coop_pdl_refused = true;
+    return cudaLaunchCooperativeKernel(fn, grid, block, args, smem, st);
+}
+
 cudaError_t msws_insert_pass(const uint32_t* d_keys, uint64_t n, const MswsDev& D, const MswsLaunch& L, int agg,
                              cudaStream_t st) {
     if (n == 0) return cudaSuccess;
@@ -2096,7 +2129,7 @@ cudaError_t msws_insert_pass(const uint32_t* d_keys, uint64_t n, const MswsDev& 
     const uint64_t tiles = (n + Dc.ins_tile - 1) / Dc.ins_tile;
     const int grid = (int)std::min<uint64_t>(G, std::max<uint64_t>(1ull, tiles));
     void* args[] = {(void*)&d_keys, (void*)&n, (void*)&Dc};
-    return cudaLaunchKernel(ins_fn(agg, li, false), dim3(grid), dim3(INS_THREADS), args, smem, st);
+    return launch_pdl(ins_fn(agg, li, false), dim3(grid), dim3(INS_THREADS), smem, st, args, false);
 }
 
 cudaError_t msws_repair(const uint32_t* d_keys, uint64_t n, const MswsDev& D, const MswsLaunch& L, cudaStream_t st) {
@@ -2104,8 +2137,8 @@ cudaError_t msws_repair(const uint32_t* d_keys, uint64_t n, const MswsDev& D, co
     MswsDev Dc = D;
     BatchDev Bn{};
     void* args[] = {(void*)&d_keys, (void*)&n, (void*)&Dc, (void*)&Bn};
-    return cudaLaunchCooperativeKernel((const void*)k_msws_repair<false>, dim3(L.repair_grid), dim3(REPAIR_THREADS),
-                                       args, msws_repair_smem(), st);
+    return launch_pdl((const void*)k_msws_repair<false>, dim3(L.repair_grid), dim3(REPAIR_THREADS), msws_repair_smem(),
+                      st, args, true);
 }
 
 cudaError_t batch_plan(const BatchDev& B, Ctl* ctl, const BatchWindow& W, bool strict, cudaStream_t st) {
@@ -2145,8 +2178,9 @@ cudaError_t msws_query(const uint32_t* d_keys, uint64_t n, uint32_t* d_out, cons
     if (n == 0) return cudaSuccess;
     const uint64_t want = (n + QRY_THREADS * QRY_KPT - 1) / (QRY_THREADS * QRY_KPT);
     const int grid = (int)umin64((uint64_t)L.query_grid, std::max<uint64_t>(1ull, want));
-    k_msws_query<<<grid, QRY_THREADS, (size_t)D.n_masks * 4, st>>>(d_keys, n, d_out, D);
-    return cudaGetLastError();
+    MswsDev Dc = D;
+    void* args[] = {(void*)&d_keys, (void*)&n, (void*)&d_out, (void*)&Dc};
+    return launch_pdl((const void*)k_msws_query, dim3(grid), dim3(QRY_THREADS), (size_t)D.n_masks * 4, st, args, false);
 }
 
 }  // namespace qsb
