@@ -1006,6 +1006,43 @@ __device__ __forceinline__ uint32_t switch_rank(const MswsDev& D, const uint32_t
     return spre[q] + __reduce_add_sync(0xffffffffu, c);
 }
 
+// The same rank in a chunk of at most SCAN_CAP records: the set bits of all switch words
+// before p, eight loads per lane in flight, with no prefix of the per-block counts.
+__device__ __forceinline__ uint32_t switch_rank_small(const MswsDev& D, uint32_t p) {
+    static_assert(SCAN_CAP / 32 == 8 * 32, "eight switch words per lane");
+    const int lane = threadIdx.x & 31;
+    const uint32_t w = p >> 5;
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t wi = k * 32 + lane;
+        v[k] = wi < w ? __ldcg(D.sw_bits + wi) : (wi == w ? __ldcg(D.sw_bits + w) & ((1u << (p & 31)) - 1u) : 0u);
+    }
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) c += __popc(v[k]);
+    return __reduce_add_sync(0xffffffffu, c);
+}
+
+// What the replay of a warp's first slot leaves in registers for the link phase, which
+// would otherwise read it back: the bucket, the switch (position, keys from it on) and
+// the high increments of lane c.
+struct SlotCache {
+    uint32_t s = NONE;  // the slot (NONE: nothing cached)
+    uint32_t b = 0, pos = NONE, n_after = 0, H = 0;
+};
+
+__device__ __forceinline__ SlotCache slot_cache(const MswsDev& D, uint32_t s, uint32_t b, const ReplayOut& o,
+                                                uint32_t pos) {
+    SlotCache c;
+    c.s = s;
+    c.b = b;
+    c.pos = o.found ? pos : NONE;
+    c.n_after = o.found ? o.n_after : 0u;
+    c.H = o.found ? high_increments(D, o) : 0u;
+    return c;
+}
+
 // The 8 keys of the chunk from position `base` (a multiple of 8) and their skip bits; km is
 // left at base's stream.  Two 16-byte loads when the keys are whole, contiguous (one
 // stream) and aligned; keys past n read as 0 (the caller skips them).
@@ -1038,10 +1075,12 @@ __device__ __forceinline__ void repair_tile_keys(const uint32_t* __restrict__ ke
 // bucket is replayed again by `rerun` now that its id is known.
 template <typename Rerun>
 __device__ __forceinline__ void finish_link(const MswsDev& D, uint32_t s, uint32_t b, uint32_t id, bool ok,
-                                            uint32_t n_after, Rerun& rerun) {
+                                            uint32_t n_after, Rerun& rerun, const SlotCache& sc) {
     const int lane = threadIdx.x & 31;
     uint32_t H;
-    if (s < D.long_cap) {
+    if (s < D.long_cap && s == sc.s) {
+        H = sc.H;
+    } else if (s < D.long_cap) {
         H = lane < LOW_COUNTERS ? __ldcg(D.totals + (uint64_t)s * LOW_COUNTERS + lane) : 0u;
     } else {
         const ReplayOut o = rerun(s, b);
@@ -1063,24 +1102,32 @@ __device__ __forceinline__ void finish_link(const MswsDev& D, uint32_t s, uint32
 template <bool BATCH, typename Rerun>
 __device__ __forceinline__ void link_phase(const MswsDev& D, const BatchDev& B, uint32_t F, uint32_t K,
                                            uint32_t base_id, unsigned long long gen, bool one_block, Rerun rerun,
-                                           uint32_t* s_small, uint32_t* s_big) {
+                                           uint32_t* s_small, uint32_t* s_big, const SlotCache& sc) {
     Ctl* ctl = D.ctl;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     constexpr int NW = REPAIR_THREADS / 32;
     const uint32_t nq = (K + SW_BLOCK - 1) / SW_BLOCK;  // K <= 2^26: at most 16384 counts
     uint32_t* spre = nq <= 64 ? s_small : s_big;        // the sort-free replay (K <= SCAN_CAP) keeps
                                                         // its records in s_big
-    for (uint32_t i = tid; i < nq; i += REPAIR_THREADS) spre[i] = __ldcg(D.sw_cnt + i);
-    __syncthreads();
-    const uint32_t nfound = block_scan_smem(spre, nq);
+    // one sketch, few records: ranks straight from the switch bits, no prefix of the counts
+    const bool small = !BATCH && K <= SCAN_CAP;
+    uint32_t nfound = 0;
+    if (!small) {
+        for (uint32_t i = tid; i < nq; i += REPAIR_THREADS) spre[i] = __ldcg(D.sw_cnt + i);
+        __syncthreads();
+        nfound = block_scan_smem(spre, nq);
+    } else if (blockIdx.x == 0 && tid == 0) {
+        for (uint32_t i = 0; i < nq; ++i) nfound += __ldcg(D.sw_cnt + i);
+    }
     for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) {
-        const uint2 w = __ldcg(D.sw + s);
+        const bool cached = s == sc.s;
+        const uint2 w = cached ? make_uint2(sc.pos, sc.n_after) : __ldcg(D.sw + s);
         if (w.x == NONE) continue;  // warp-uniform
-        const uint32_t b = __ldcg(D.flag_list + s);
-        const uint32_t rank = switch_rank(D, spre, w.x);
+        const uint32_t b = cached ? sc.b : __ldcg(D.flag_list + s);
+        const uint32_t rank = small ? switch_rank_small(D, w.x) : switch_rank(D, spre, w.x);
         if (!BATCH) {
             const uint32_t id = base_id + rank;
-            finish_link(D, s, b, id, (uint64_t)(id - START) < D.n_high, w.y, rerun);
+            finish_link(D, s, b, id, (uint64_t)(id - START) < D.n_high, w.y, rerun, sc);
             continue;
         }
         // batched streams: the rank among the stream's own switches (its positions are
@@ -1095,7 +1142,7 @@ __device__ __forceinline__ void link_phase(const MswsDev& D, const BatchDev& B, 
         const uint32_t own = __ldcg(D.sw_base + s) + (rank - switch_rank(D, spre, fp));
         const uint32_t nh = __ldg(&B.desc[st].n_high);
         const bool ok = (uint64_t)(own - START) < nh;
-        finish_link(D, s, b, own + __ldg(&B.desc[st].high_base), ok, w.y, rerun);
+        finish_link(D, s, b, own + __ldg(&B.desc[st].high_base), ok, w.y, rerun, sc);
         if (lane == 0) {
             atomicMax(B.next_id + st, (uint32_t)min((unsigned long long)own + 1ull, (unsigned long long)START + nh));
             if (!ok) atomicOr(B.status + st, ST_POOL_FULL);
@@ -1335,6 +1382,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
     // and each warp scans them for its slot in array order.
     // The switch position of a record is its index here (array order).
     const bool one_block = F <= (uint32_t)NW;  // every slot in block 0: no grid barrier to link
+    SlotCache sc;  // the replay of the warp's first slot, kept for the link phase (one sketch)
     if (scan_mode) {
         uint2* srec = reinterpret_cast<uint2*>(s_set);
         if (blockIdx.x * NW < F) {
@@ -1344,6 +1392,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
                 const uint32_t b = __ldcg(D.flag_list + s);
                 const ReplayOut o = replay_scan(D, srec, s, K, b);
                 settle_bucket<BATCH>(D, B, gen, s, b, o, o.L);
+                if (!BATCH && s == blockIdx.x * NW + wid) sc = slot_cache(D, s, b, o, o.L);
             }
         }
         phase_mark(D, 5);
@@ -1357,7 +1406,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
             return;
         }
         auto rerun = [&](uint32_t s, uint32_t b) { return replay_scan(D, srec, s, K, b); };
-        link_phase<BATCH>(D, B, F, K, base_id, gen, one_block, rerun, s_swpre, s_set);
+        link_phase<BATCH>(D, B, F, K, base_id, gen, one_block, rerun, s_swpre, s_set, sc);
         phase_mark(D, 9);
         finish_repair(ctl);
         return;
@@ -1637,7 +1686,9 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
     for (uint32_t s = blockIdx.x * NW + wid; s < F; s += gridDim.x * NW) {
         const uint32_t b = __ldcg(D.flag_list + s);
         const ReplayOut o = replay_sorted(D, sorted, s, F, K, b);
-        settle_bucket<BATCH>(D, B, gen, s, b, o, o.found ? (fpos ? __ldcg(fpos + o.L) : o.L) : 0u);
+        const uint32_t pos = o.found ? (fpos ? __ldcg(fpos + o.L) : o.L) : 0u;
+        settle_bucket<BATCH>(D, B, gen, s, b, o, pos);
+        if (!BATCH && s == blockIdx.x * NW + wid) sc = slot_cache(D, s, b, o, pos);
     }
     phase_mark(D, 5);
     if (one_block) {
@@ -1650,7 +1701,7 @@ __global__ void __launch_bounds__(REPAIR_THREADS, 2) k_msws_repair(const uint32_
         return;
     }
     auto rerun = [&](uint32_t s, uint32_t b) { return replay_sorted(D, sorted, s, F, K, b); };
-    link_phase<BATCH>(D, B, F, K, base_id, gen, one_block, rerun, s_swpre, s_set);
+    link_phase<BATCH>(D, B, F, K, base_id, gen, one_block, rerun, s_swpre, s_set, sc);
     phase_mark(D, 9);
     finish_repair(ctl);
 }
