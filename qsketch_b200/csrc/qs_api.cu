@@ -1143,10 +1143,9 @@ qs_status mlp_train_pass(qs_learned* lk, const uint32_t* d_keys, const uint8_t* 
     float h_loss = 0.0f;
     for (uint64_t off = 0; off < n; off += batch) {
         const uint64_t b = std::min<uint64_t>(batch, n - off);
-        CK(cudaMemsetAsync(lk->d_loss, 0, 4, st), "loss reset");
-        CK(mlp_backward(d_keys + off, d_labels + off, b, pos_weight, 1.0f / (float)b, lk->M, lk->d_loss, st),
-           "mlp backward");
-        CK(mlp_adam(lk->M, ++lk->adam_step, lr, st), "adam");
+        CK(mlp_train_step(d_keys + off, d_labels + off, b, pos_weight, 1.0f / (float)b, lk->M, lk->d_loss,
+                          ++lk->adam_step, lr, st),
+           "mlp train step");
         if (off + batch >= n) {
             CK(cudaMemcpyAsync(&h_loss, lk->d_loss, 4, cudaMemcpyDeviceToHost, st), "loss");
             CK(cudaStreamSynchronize(st), "train sync");

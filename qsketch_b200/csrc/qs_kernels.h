@@ -81,6 +81,11 @@ constexpr uint32_t MLP_TILE_EXAMPLES = 128;  // examples per CTA tile (the MMAs'
 constexpr uint32_t MLP_PARTIAL_STRIDE = (MLP_PARAMS + 3u) & ~3u;  // floats per tile partial: 16-byte rows
 constexpr uint32_t MLP_MAX_TILES = 256;      // tiles per backward launch
 
+// Launch with programmatic stream serialization (the kernel waits with griddep_wait before
+// it reads what the previous kernel of the stream wrote); cooperative launches keep that
+// property.
+cudaError_t launch_pdl(const void* fn, dim3 grid, dim3 block, size_t smem, cudaStream_t st, void** args,
+                       bool cooperative);
 size_t mlp_smem_bytes();
 size_t mlp_fwd_smem_bytes();
 cudaError_t mlp_configure();
@@ -88,6 +93,11 @@ cudaError_t mlp_forward(const uint32_t* d_keys, uint64_t n, const MlpDev& M, flo
 cudaError_t mlp_backward(const uint32_t* d_keys, const uint8_t* d_labels, uint64_t n, float pos_weight,
                          float inv_batch, const MlpDev& M, float* d_loss, cudaStream_t st);
 cudaError_t mlp_adam(const MlpDev& M, uint32_t step, float lr, cudaStream_t st);
+// One Adam step on a batch of n examples: the backward pass, then the tile reduction fused
+// with the update, *d_loss set to the batch's loss sum (same arithmetic, in the same order,
+// as mlp_backward into a zeroed loss followed by mlp_adam).
+cudaError_t mlp_train_step(const uint32_t* d_keys, const uint8_t* d_labels, uint64_t n, float pos_weight,
+                           float inv_batch, const MlpDev& M, float* d_loss, uint32_t step, float lr, cudaStream_t st);
 cudaError_t mlp_refresh_bf16(const MlpDev& M, cudaStream_t st);
 
 // ---- learned split: exact table of heavy keys and routing -----------------------------------

@@ -326,6 +326,7 @@ __global__ void __launch_bounds__(MLP_THREADS) k_mlp_backward(const uint32_t* __
     float* G = partials + (uint64_t)blockIdx.x * MLP_PARTIAL_STRIDE;
     const uint64_t base = (tile0 + blockIdx.x) * MLP_T;
     const uint64_t i = base + t;
+    griddep_wait();  // the previous step's update of the weights has ended
     tc_setup(S, M, 512);
     const uint32_t lane_base = S.tmem + ((uint32_t)(warp * 32) << 16);
     tc_load_features(S, i < n ? __ldg(keys + i) : 0u);
@@ -466,6 +467,35 @@ __global__ void k_mlp_reduce(const float* __restrict__ partials, const float* __
     }
 }
 
+// One training step's reduction and update: grads[i] plus the tiles' partials of parameter
+// i (in tile order), then Adam as k_adam does, gradients left cleared; *loss = the tiles'
+// loss sum.  The next step's backward may be scheduled at once (it waits for this kernel).
+__global__ void k_mlp_reduce_adam(const float* __restrict__ partials, const float* __restrict__ ploss,
+                                  uint32_t tiles, float* __restrict__ loss, float* __restrict__ p,
+                                  float* __restrict__ g, float* __restrict__ m, float* __restrict__ v, uint32_t count,
+                                  float lr, float b1, float b2, float eps, float c1, float c2,
+                                  __nv_bfloat16* __restrict__ w_bf16, uint32_t n_bf16) {
+    griddep_wait();
+    griddep_launch_dependents();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        float gi = g[i];
+        for (uint32_t t = 0; t < tiles; ++t) gi += partials[(uint64_t)t * MLP_PARTIAL_STRIDE + i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        p[i] = pi;
+        g[i] = 0.0f;
+        if (i < n_bf16) w_bf16[i] = __float2bfloat16(pi);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        float s = 0.0f;
+        for (uint32_t t = 0; t < tiles; ++t) s += ploss[t];
+        *loss = s;
+    }
+}
+
 // Adam (Kingma & Ba 2015) on the fp32 master parameters; refreshes the bf16 copies and
 // clears the gradients.  Parameters are one flat fp32 array: W1 | W2 | b1 | b2 | w3 | b3.
 __global__ void k_adam(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
@@ -535,6 +565,39 @@ cudaError_t mlp_adam(const MlpDev& M, uint32_t step, float lr, cudaStream_t st) 
     k_adam<<<64, 256, 0, st>>>(M.params, M.grads, M.adam_m, M.adam_v, MLP_PARAMS, lr, b1, b2, eps, c1, c2, M.W1,
                                MLP_BF16_PARAMS);
     return cudaGetLastError();
+}
+
+cudaError_t mlp_train_step(const uint32_t* d_keys, const uint8_t* d_labels, uint64_t n, float pos_weight,
+                           float inv_batch, const MlpDev& M, float* d_loss, uint32_t step, float lr, cudaStream_t st) {
+    const uint64_t tiles = (n + MLP_T - 1) / MLP_T;
+    if (tiles > MLP_MAX_TILES) {  // several backward launches accumulate into the gradients
+        cudaError_t e = cudaMemsetAsync(d_loss, 0, 4, st);
+        if (e == cudaSuccess) e = mlp_backward(d_keys, d_labels, n, pos_weight, inv_batch, M, d_loss, st);
+        if (e == cudaSuccess) e = mlp_adam(M, step, lr, st);
+        return e;
+    }
+    uint32_t nt = (uint32_t)std::max<uint64_t>(1ull, tiles);
+    uint64_t tile0 = 0;
+    MlpDev Mc = M;
+    float* partials = M.partials;
+    float* ploss = M.ploss;
+    void* bargs[] = {(void*)&d_keys, (void*)&d_labels, (void*)&n, (void*)&tile0, (void*)&pos_weight, (void*)&inv_batch,
+                     (void*)&Mc, (void*)&partials, (void*)&ploss};
+    cudaError_t e = launch_pdl((const void*)k_mlp_backward, dim3(nt), dim3(MLP_THREADS), mlp_smem_bytes(), st, bargs,
+                               false);
+    if (e != cudaSuccess) return e;
+    float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    float* params = M.params;
+    float* grads = M.grads;
+    float* am = M.adam_m;
+    float* av = M.adam_v;
+    uint32_t count = MLP_PARAMS, n_bf16 = MLP_BF16_PARAMS;
+    __nv_bfloat16* w = M.W1;
+    void* rargs[] = {(void*)&partials, (void*)&ploss, (void*)&nt, (void*)&d_loss, (void*)&params, (void*)&grads,
+                     (void*)&am, (void*)&av, (void*)&count, (void*)&lr, (void*)&b1, (void*)&b2, (void*)&eps,
+                     (void*)&c1, (void*)&c2, (void*)&w, (void*)&n_bf16};
+    return launch_pdl((const void*)k_mlp_reduce_adam, dim3(82), dim3(256), 0, st, rargs, false);
 }
 
 cudaError_t mlp_refresh_bf16(const MlpDev& M, cudaStream_t st) {

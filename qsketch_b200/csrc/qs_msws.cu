@@ -2139,8 +2139,8 @@ cudaError_t msws_configure(int device, uint32_t n_masks, MswsLaunch* L) {
 // previous kernel of the stream drains (hiding the launch gap between the dependent passes);
 // each kernel launched this way calls griddep_wait() before it reads what a kernel writes.
 // A driver that refuses the attribute next to a cooperative launch gets the plain one.
-static cudaError_t launch_pdl(const void* fn, dim3 grid, dim3 block, size_t smem, cudaStream_t st, void** args,
-                              bool cooperative) {
+cudaError_t launch_pdl(const void* fn, dim3 grid, dim3 block, size_t smem, cudaStream_t st, void** args,
+                       bool cooperative) {
     static bool coop_pdl_refused = false;
     if (cooperative && coop_pdl_refused) return cudaLaunchCooperativeKernel(fn, grid, block, args, smem, st);
     cudaLaunchAttribute at[2];
