@@ -527,15 +527,23 @@ def run_sharded(args, cfg):
         step()
     torch.cuda.synchronize()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    def local_launches():
+        p = ss.local.profile()
+        return p["insert_launches"] + p["repair_launches"] + p["query_launches"]
+
     with Clocks(local) as clk:
         barrier()
         torch.cuda.synchronize()
+        launches0 = local_launches()
         t0.record(stream)
         for _ in range(args.steps):
             out = step()
         t1.record(stream)
         torch.cuda.synchronize()
         barrier()
+    # the local sketch's kernels, plus per step with several ranks the routing kernels: count,
+    # scan and scatter per partition (insert and query) and the query's unpartition
+    launches = local_launches() - launches0 + (7 * args.steps if world > 1 else 0)
     ms_per_step = max_over_ranks(t0.elapsed_time(t1)) / args.steps
     hk, hq = keys.cpu().pin_memory(), queries.cpu().pin_memory()
     ho = torch.empty(queries.numel(), dtype=torch.uint32).pin_memory()
@@ -563,7 +571,7 @@ def run_sharded(args, cfg):
             "e2e": {"value": round((n + nq) / (e2e_ms * 1e6), 4), "unit": "Gkeys/s",
                     "h2d_bytes_per_step": (n + nq) * 4, "d2h_bytes_per_step": nq * 4, "ms_per_step": round(e2e_ms, 3),
                     "api": "ShardedSketch.insert + search"},
-            "gpu_launches": None,
+            "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }), flush=True)
     ss.local.close()
@@ -603,6 +611,7 @@ def run_ablation(args, cfg):
         "subwarp_m8": lambda: qs.Sketch_GPU_Sub_Warp(prime(budget // 32), 8, hash_seed=SEED, mask_rng=1),
     }
     rows = {}
+    launches = 0  # every sketch's kernels inside the timed loops
     with Clocks(local) as clk:
         for name, make in makers.items():
             sk = make()
@@ -615,6 +624,7 @@ def run_ablation(args, cfg):
                     sk.search(keys, counts=out)
                 ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
                 barrier()
+                p0 = sk.profile()
                 for e in ev:
                     sk.clear()
                     e[0].record(stream)
@@ -623,6 +633,8 @@ def run_ablation(args, cfg):
                     sk.search(keys, counts=out)
                     e[2].record(stream)
                 torch.cuda.synchronize()
+                p1 = sk.profile()
+                launches += sum(p1[k] - p0[k] for k in ("insert_launches", "repair_launches", "query_launches"))
                 ins = max_over_ranks(sum(e[0].elapsed_time(e[1]) for e in ev) / args.steps)
                 qry = max_over_ranks(sum(e[1].elapsed_time(e[2]) for e in ev) / args.steps)
                 row[sname] = {"insert_gkeys_per_s": round(n / (ins * 1e6), 3),
@@ -643,7 +655,7 @@ def run_ablation(args, cfg):
             "config": {"workload": cfg["workload"], "n_keys": n, "budget_bytes": budget,
                        "note": "value: the MSWS on the uniform stream (insert + query of every key); the table "
                                "compares every sketch on both streams"},
-            "ablation": rows, "gpu_launches": None, "clocks": clk.summary(),
+            "ablation": rows, "gpu_launches": int(launches), "clocks": clk.summary(),
         }), flush=True)
     if world > 1:
         dist.destroy_process_group()
