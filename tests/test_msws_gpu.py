@@ -265,6 +265,32 @@ def test_mixed_interleaved_small(gpu):
     assert_same_tables(sk, orc)
 
 
+def test_calls_that_reuse_each_others_buffers(gpu):
+    # Back-to-back calls on one stream, where each kernel may be scheduled while the previous
+    # one drains: a query's output is the next insert's keys, and a key buffer is overwritten
+    # by a torch kernel between an insert and the next insert and query.
+    sk, orc = make_pair(65521, 1 << 13)
+    keys = data.zipf_keys(1 << 20, 1 << 16, 1.1, seed=51, perm_seed=52)
+    out = torch.empty_like(keys)
+    sk.insert(keys)
+    orc.insert(keys.cpu().numpy())
+    sk.search(keys, counts=out)
+    sk.insert(out)  # the estimates, read as keys
+    orc.insert(orc.query(keys.cpu().numpy()))
+    buf = keys.clone()
+    sk.insert(buf)
+    buf.copy_(data.zipf_keys(1 << 20, 1 << 16, 1.1, seed=53, perm_seed=54))
+    sk.insert(buf)
+    got = sk.search(buf).cpu().numpy()
+    sk.sync()
+    orc.insert(keys.cpu().numpy())
+    hb = buf.cpu().numpy()
+    orc.insert(hb)
+    want = orc.query(hb)
+    assert np.array_equal(got, want), f"{(got != want).sum()} estimates differ"
+    assert_same_tables(sk, orc)
+
+
 def test_mixed_config3_full_size(gpu):
     # 2^28 operations in 2^20 batches (90 % inserts then 10 % queries), Zipf 0.8 over 2^26,
     # 256 MB low table (n_low = 8388593), 64 MB high pool
