@@ -58,10 +58,11 @@ struct Ctl {
     uint32_t n_flagged;    // buckets flagged in the current chunk
     uint32_t n_records;    // records gathered for the ordered replay
     uint32_t n_long;       // slots whose segment needed a grid-wide count
-    uint32_t bar_count;    // grid barrier
-    uint32_t bar_gen;
+    uint32_t bar_count;    // blocks that finished the current repair (its last block resets)
     uint32_t link_gen;     // repairs that linked buckets since the create/clear (never reset
                            // otherwise): tags the per-stream link ranks of batched streams
+    unsigned long long bar_arrive;  // grid barrier arrivals (a barrier ends at the next multiple
+                                    // of the grid size)
     unsigned long long dropped;
     unsigned long long repaired_buckets;
     unsigned long long repaired_keys;

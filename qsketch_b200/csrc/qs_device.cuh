@@ -68,40 +68,40 @@ __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wa
 __device__ __forceinline__ void griddep_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // ---- grid barrier for cooperative launches (bounded) ---------------------------------
-// All blocks of the grid are co-resident (cudaLaunchCooperativeKernel).  Thread 0 of each
-// block reads the generation before the block arrives (it cannot advance earlier), fences
-// the block's writes and arrives with atomicInc, which wraps the counter to 0 on the last
-// arrival; the last block fences again and advances the generation, the others poll it
-// with acquire loads.  Returns false (and latches ST_TIMEOUT) if the other blocks do not
-// arrive within the spin limit.
+// All blocks of the grid are co-resident (cudaLaunchCooperativeKernel).  Arrivals count up in
+// one 64-bit word that is never reset: thread 0 of each block fences the block's writes and
+// adds 1, and the count before its add gives the barrier's end, the next multiple of the
+// grid size; it then polls the count with acquire loads until it gets there (the last block
+// to arrive at once).  One returning atomic per block and no second hop through a generation
+// word.  Returns false (and latches ST_TIMEOUT) if the other blocks do not arrive within the
+// spin limit.
 __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
     uint32_t v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+__device__ __forceinline__ unsigned long long ld_acquire_gpu_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
 
 __device__ __forceinline__ bool grid_barrier(Ctl* ctl, uint32_t limit = SPIN_LIMIT) {
     __shared__ int s_ok;
-    uint32_t gen = 0;
-    if (threadIdx.x == 0) gen = ld_acquire_gpu(&ctl->bar_gen);
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        const uint32_t arrived = atomicInc(&ctl->bar_count, gridDim.x - 1);
+        const unsigned long long g = gridDim.x;
+        const unsigned long long end = (atomicAdd(&ctl->bar_arrive, 1ull) / g + 1ull) * g;
         int ok = 1;
-        if (arrived == gridDim.x - 1) {
-            __threadfence();
-            atomicAdd(&ctl->bar_gen, 1u);
-        } else {
-            uint32_t it = 0;
-            while (ld_acquire_gpu(&ctl->bar_gen) == gen) {
-                if (++it > limit) {
-                    ok = 0;
-                    atomicOr(&ctl->status, ST_TIMEOUT);
-                    break;
-                }
-                if (it > 256) __nanosleep(64);
+        uint32_t it = 0;
+        while (ld_acquire_gpu_u64(&ctl->bar_arrive) < end) {
+            if (++it > limit) {
+                ok = 0;
+                atomicOr(&ctl->status, ST_TIMEOUT);
+                break;
             }
+            if (it > 256) __nanosleep(64);
         }
         s_ok = ok;
     }

@@ -612,8 +612,8 @@ __device__ __forceinline__ void phase_mark(const MswsDev& D, int k) {
     }
 }
 
-// End of a repair: the last block to finish (counted on the grid barrier's counter, which
-// wraps back to 0) resets the chunk's counters; no block waits for the others.
+// End of a repair: the last block to finish (counted on bar_count, which wraps back to 0)
+// resets the chunk's counters and the barrier arrivals; no block waits for the others.
 __device__ __forceinline__ void finish_repair(Ctl* ctl) {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -626,6 +626,7 @@ __device__ __forceinline__ void finish_repair(Ctl* ctl) {
             ctl->n_flagged = 0;
             ctl->n_records = 0;
             ctl->n_long = 0;
+            ctl->bar_arrive = 0;  // every block is past its last grid barrier
             ctl->repairs += 1;
             ctl->link_gen += 1;
             __threadfence();

@@ -59,6 +59,7 @@ __global__ void k_noalloc_begin(Ctl* st) {
     st->n_records = 0;
     st->n_long = 0;
     st->bar_count = 0;
+    st->bar_arrive = 0;
 }
 
 struct NaDevice {
